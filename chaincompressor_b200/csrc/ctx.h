@@ -1,0 +1,124 @@
+// Host-side context, device arena and error plumbing of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "../../include/chain_b200.h"
+
+namespace chain {
+
+// Bump allocator over one device allocation.  reserve() grows the allocation between
+// calls (never while kernels of the current call are queued on it).
+struct Arena {
+    uint8_t* base = nullptr;
+    size_t cap = 0;
+    size_t used = 0;
+    cudaError_t reserve(size_t bytes) {
+        used = 0;
+        if (bytes <= cap) return cudaSuccess;
+        if (base) cudaFree(base);
+        base = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 8 + (1u << 20);
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&base), want);
+        if (e != cudaSuccess) { base = nullptr; return e; }
+        cap = want;
+        return cudaSuccess;
+    }
+    template <typename T>
+    T* take(size_t count) {
+        const size_t off = (used + 255) & ~size_t(255);
+        const size_t bytes = count * sizeof(T);
+        if (off + bytes > cap) return nullptr;
+        used = off + bytes;
+        return reinterpret_cast<T*>(base + off);
+    }
+    static size_t need(size_t count, size_t elem) { return ((count * elem + 255) & ~size_t(255)); }
+    void release() {
+        if (base) cudaFree(base);
+        base = nullptr;
+        cap = used = 0;
+    }
+};
+
+struct PinnedBuf {
+    uint8_t* ptr = nullptr;
+    size_t cap = 0;
+    cudaError_t reserve(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        cap = 0;
+        cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&ptr), bytes);
+        if (e != cudaSuccess) { ptr = nullptr; return e; }
+        cap = bytes;
+        return cudaSuccess;
+    }
+    void release() {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        cap = 0;
+    }
+};
+
+struct EncodeDebug {
+    const uint32_t* idrel = nullptr;
+    const uint32_t* diff = nullptr;
+    const uint32_t* keep = nullptr;
+    const uint32_t* choice2 = nullptr;
+    const uint32_t* rel = nullptr;
+    uint64_t n = 0, ndiff = 0, nkeep = 0, nblocks = 0;
+    uint32_t dims = 0;
+};
+
+}  // namespace chain
+
+struct chain_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    chain::Arena frame;    // per-frame working buffers (encoder)
+    chain::Arena coded;    // encoder entropy/output buffers
+    chain::Arena dec;      // decoder buffers
+    chain::PinnedBuf pinned;
+    void* state_dev = nullptr;    // device scratch scalars (EncState / DecState)
+    void* state_host = nullptr;   // pinned mirror
+    size_t state_bytes = 0;
+    const uint8_t* result = nullptr;  // device container of the last compress
+    size_t result_len = 0;
+    chain::EncodeDebug dbg;
+};
+
+namespace chain {
+
+chain_status set_err(chain_status st, const std::string& msg);
+chain_status cuda_err(cudaError_t e, const char* what);
+bool is_device_ptr(const void* p);
+
+#define CHAIN_CUDA(expr)                                        \
+    do {                                                        \
+        cudaError_t _e = (expr);                                \
+        if (_e != cudaSuccess) return ::chain::cuda_err(_e, #expr); \
+    } while (0)
+
+#define CHAIN_LAUNCH_CHECK(what)                                \
+    do {                                                        \
+        cudaError_t _e = cudaGetLastError();                    \
+        if (_e != cudaSuccess) return ::chain::cuda_err(_e, what); \
+    } while (0)
+
+chain_status ensure_state(chain_ctx* ctx, size_t bytes);
+
+chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype, chain_layout layout,
+                          uint64_t n, uint32_t dims, double eb, int64_t p, int64_t threshold,
+                          int bl, int l1, int l2, uint32_t bytes_per_lane, size_t* out_len);
+
+chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, chain_dtype out_dtype,
+                          chain_layout out_layout, void* out, size_t out_capacity, uint64_t* n,
+                          uint32_t* dims);
+
+}  // namespace chain

@@ -1,0 +1,580 @@
+// Chain decoder on sm_100a: interleaved-rANS decode, bit unpacking, the level-2
+// inverse as a modular reset-scan, the level-1 inverse by pointer jumping to each
+// chain's explicit block, FP64 reconstruction and exact corrections.
+//
+// Semantics follow the reference CPU decoder (cpp/chain/lcps_cpp.cpp:1833-1995, also
+// cpp/decompress/lcps_cpu_decompress_serial.cpp:1182-1326), including its validation:
+// every malformed value sets an error bit instead of being trusted.
+//   level-2 inverse      lcps_cpp.cpp:1890-1934
+//   level-1 inverse      lcps_cpp.cpp:1936-1961 (backward pass; here: roots by jumping)
+//   reconstruction       lcps_cpp.cpp:1963-1993 (fma(q + 0.5, 2 eb, min), corrections)
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <vector>
+
+#include "chain_common.cuh"
+#include "chain_format.h"
+#include "ctx.h"
+#include "rans.cuh"
+#include "scan.cuh"
+
+namespace chain {
+
+struct DecState {
+    uint32_t err;
+    uint32_t jump_active;   // pointer jumping: 1 while some parent moved in the last round
+    uint32_t zeros;         // idrel == 0 count
+    uint32_t ndiff_seen;
+    uint64_t tag_bits[kStreams];
+    uint32_t maxtag[kStreams];
+    DecodePlan plan;
+};
+
+__global__ void k_dec_init(DecState* st) {
+    if (threadIdx.x || blockIdx.x) return;
+    st->err = 0;
+    st->jump_active = 1;
+    st->zeros = 0;
+    st->ndiff_seen = 0;
+    for (int s = 0; s < kStreams; ++s) { st->tag_bits[s] = 0; st->maxtag[s] = 0; }
+}
+
+__global__ void k_parse(const uint8_t* data, uint64_t len, DecState* st) {
+    if (threadIdx.x || blockIdx.x) return;
+    parse_container(data, len, &st->plan);
+}
+
+// Per rANS section: token table -> prob/cum, and chunk byte offsets.  One CTA each.
+struct SectionRef {
+    const SectionPlan* sec;   // device pointer into the plan
+    uint32_t* prob;
+    uint32_t* cum;
+    uint32_t* lookup;
+    uint64_t* chunk_off;
+};
+struct SectionRefs {
+    SectionRef r[kStreams];
+    int count;
+};
+
+__global__ void __launch_bounds__(1024) k_section_setup(SectionRefs refs, const uint8_t* data, DecState* st) {
+    const SectionRef R = refs.r[blockIdx.x];
+    const SectionPlan& s = *R.sec;
+    __shared__ uint64_t red[33];
+    if (threadIdx.x == 0) {
+        if (!parse_table(data + s.table_off, s.table_len, s.alphabet, s.prec, R.prob, R.cum))
+            set_error(&st->err, kErrCorrupt);
+    }
+    // chunk offsets: exclusive prefix of the u32 chunk lengths
+    uint64_t carry = s.payload_off;
+    for (uint32_t base = 0; base < s.chunks; base += blockDim.x) {
+        const uint32_t c = base + threadIdx.x;
+        uint64_t len = 0;
+        if (c < s.chunks) {
+            const uint8_t* q = data + s.chunk_tab_off + 4ull * c;
+            len = static_cast<uint64_t>(q[0]) | (static_cast<uint64_t>(q[1]) << 8) | (static_cast<uint64_t>(q[2]) << 16) |
+                  (static_cast<uint64_t>(q[3]) << 24);
+        }
+        uint64_t tot;
+        const uint64_t ex = block_exclusive_sum(len, red, &tot);
+        if (c < s.chunks) R.chunk_off[c] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) R.chunk_off[s.chunks] = carry;
+}
+
+// slot -> symbol: binary search of the cumulative table (any grid; blockIdx.y = section).
+__global__ void __launch_bounds__(256) k_lookup(SectionRefs refs, const DecState* st) {
+    if (st->err) return;
+    const SectionRef R = refs.r[blockIdx.y];
+    const SectionPlan& s = *R.sec;
+    const uint32_t M = 1u << s.prec;
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < M; slot += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = s.alphabet - 1;   // last symbol with cum <= slot and prob > 0
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (R.cum[mid] <= slot) lo = mid; else hi = mid - 1;
+        }
+        // zero-probability symbols share their successor's cum; step back to the owner
+        while (R.prob[lo] == 0 && lo > 0) --lo;
+        R.lookup[slot] = lo;
+    }
+}
+
+// Copies the u32 little-endian state words of every chunk (unaligned in the container).
+__global__ void __launch_bounds__(256) k_states(SectionRefs refs, const uint8_t* data, uint32_t* states_base,
+                                                 const uint64_t* states_first) {
+    const SectionRef R = refs.r[blockIdx.y];
+    const SectionPlan& s = *R.sec;
+    uint32_t* out = states_base + states_first[blockIdx.y];
+    const uint64_t words = 32ull * s.chunks;
+    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < words;
+         w += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint8_t* q = data + s.states_off + 4 * w;
+        out[w] = static_cast<uint32_t>(q[0]) | (static_cast<uint32_t>(q[1]) << 8) | (static_cast<uint32_t>(q[2]) << 16) |
+                 (static_cast<uint32_t>(q[3]) << 24);
+    }
+}
+
+__device__ __forceinline__ uint64_t read_bits_msb(const uint8_t* bytes, uint64_t bit, int width) {
+    // width <= 32; reads up to 5 bytes
+    const uint64_t b0 = bit >> 3;
+    const int off = static_cast<int>(bit & 7);
+    const int nbytes = (off + width + 7) >> 3;
+    uint64_t acc = 0;
+    for (int i = 0; i < nbytes; ++i) acc = (acc << 8) | bytes[b0 + i];
+    const int total = nbytes * 8;
+    acc >>= (total - off - width);
+    return width == 64 ? acc : (acc & ((1ull << width) - 1));
+}
+
+// Fixed: one thread per value.
+__global__ void __launch_bounds__(256) k_unpack_fixed(const uint8_t* data, const CompPlan* cp, uint32_t* out,
+                                                       DecState* st) {
+    const CompPlan& c = *cp;
+    const uint64_t n = c.records * c.dims;
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t k = j / c.dims;
+        const uint32_t d = static_cast<uint32_t>(j - k * c.dims);
+        const int w = c.width[d];
+        const uint64_t off = read_bits_msb(data + c.packed_off[d], k * w, w);
+        const uint64_t v = c.minv[d] + off;
+        if (v > 0xffffffffull) { set_error(&st->err, kErrCorrupt); continue; }
+        out[j] = static_cast<uint32_t>(v);
+    }
+}
+
+struct TagIn {
+    const uint32_t* tags;
+    uint32_t D;
+    __device__ uint64_t operator()(uint64_t j) const { return static_cast<uint64_t>(tags[j]) * D; }
+};
+struct TagUnpackOut {
+    const uint8_t* payload;
+    const uint32_t* tags;
+    const CompPlan* cp;
+    uint32_t* out;
+    DecState* st;
+    int s;
+    __device__ void operator()(uint64_t j, uint64_t bit, uint64_t nbits) const {
+        const uint32_t D = cp->dims;
+        const uint32_t t = tags[j];
+        if (t < 1 || t > 32) { set_error(&st->err, kErrCorrupt); return; }
+        atomicMax(&st->maxtag[s], t);
+        if (j + 1 == cp->records) st->tag_bits[s] = bit + nbits;
+        if (bit + nbits > cp->packed_bits) { set_error(&st->err, kErrCorrupt); return; }
+        for (uint32_t d = 0; d < D; ++d, bit += t) out[j * D + d] = static_cast<uint32_t>(read_bits_msb(payload, bit, t));
+    }
+};
+
+__global__ void k_check_tagged(const DecState* st_c, DecState* st) {
+    if (threadIdx.x || blockIdx.x) return;
+    for (int s = 0; s < kStreams; ++s) {
+        const CompPlan& c = st_c->plan.comp[s];
+        if (c.enc != kEncTagged) continue;
+        if (st->tag_bits[s] != c.packed_bits || st->maxtag[s] != c.max_width) set_error(&st->err, kErrCorrupt);
+    }
+}
+
+// ------------------------------------------------------------------- level 2
+// Reset-scan element: bit 63 = "this record is kept" (restart), low 32 bits = offset
+// from wrap_min (kept record) or the modular step -correction (difference record).
+struct ResetAddOp {
+    uint64_t range;
+    __device__ __forceinline__ uint64_t operator()(uint64_t a, uint64_t b) const {
+        if (b >> 63) return b;
+        const uint64_t v = ((a & 0xffffffffull) + (b & 0xffffffffull)) % range;
+        return (a & (1ull << 63)) | v;
+    }
+    __device__ __forceinline__ static uint64_t identity() { return 0; }
+};
+
+// Choice values are clamped to {0, 1} for the ranks (so every derived index stays in
+// bounds) and validated separately (lcps_cpp.cpp:1899-1900, 1911-1912).
+struct ChoiceIn {
+    const uint32_t* choice2;
+    __device__ uint32_t operator()(uint64_t j) const { return choice2[j] ? 1u : 0u; }
+};
+struct ChoiceRankOut {
+    const uint32_t* choice2;
+    uint32_t* drank;
+    DecState* st;
+    __device__ void operator()(uint64_t j, uint32_t pre, uint32_t) const {
+        const uint32_t c = choice2[j];
+        if (c > 1 || (j == 0 && c != 0)) set_error(&st->err, kErrCorrupt);
+        drank[j] = pre;
+    }
+};
+
+struct Level2TermIn {
+    const uint32_t* choice2;
+    const uint32_t* drank;
+    const uint32_t* keep;
+    const uint32_t* diff;
+    const DecState* st;
+    uint32_t d;
+    __device__ uint64_t operator()(uint64_t j) const {
+        const DecodePlan& P = st->plan;
+        const uint32_t D = P.D;
+        const uint64_t range = static_cast<uint64_t>(P.wrap_max - P.wrap_min) + 1;
+        const uint32_t dr = drank[j];
+        if (choice2[j] == 0) {
+            const int64_t v = keep[static_cast<uint64_t>(j - dr) * D + d];
+            const uint64_t off = static_cast<uint64_t>(v - P.wrap_min);  // validated in Level2TermOut
+            return (1ull << 63) | (off & 0xffffffffull);
+        }
+        const uint64_t sym = diff[static_cast<uint64_t>(dr) * D + d];
+        const int64_t corr = (sym & 1u) ? -static_cast<int64_t>(sym >> 1) - 1 : static_cast<int64_t>(sym >> 1);
+        // offset_j = offset_{j-1} - corr (mod range)
+        const int64_t r = static_cast<int64_t>(range);
+        int64_t step = (-corr) % r;
+        if (step < 0) step += r;
+        return static_cast<uint64_t>(step);
+    }
+};
+struct Level2TermOut {
+    const uint32_t* choice2;
+    const uint32_t* drank;
+    const uint32_t* keep;
+    const uint32_t* diff;
+    const DecState* stc;
+    DecState* st;
+    uint32_t d;
+    uint32_t* compact;   // [B * D]
+    __device__ void operator()(uint64_t j, uint64_t prefix, uint64_t term) const {
+        const DecodePlan& P = stc->plan;
+        const uint32_t D = P.D;
+        const uint64_t range = static_cast<uint64_t>(P.wrap_max - P.wrap_min) + 1;
+        // validate the record's raw value (lcps_cpp.cpp:1905-1922)
+        if (choice2[j] == 0) {
+            const int64_t v = keep[static_cast<uint64_t>(j - drank[j]) * D + d];
+            if (v < P.wrap_min || v > P.wrap_max) set_error(&st->err, kErrCorrupt);
+        } else {
+            const uint64_t sym = diff[static_cast<uint64_t>(drank[j]) * D + d];
+            const int64_t corr = (sym & 1u) ? -static_cast<int64_t>(sym >> 1) - 1 : static_cast<int64_t>(sym >> 1);
+            const int64_t r = static_cast<int64_t>(range);
+            const int64_t maxc = r / 2 - ((r & 1) == 0 ? 1 : 0), minc = -(r / 2);
+            if (corr < minc || corr > maxc) set_error(&st->err, kErrCorrupt);
+        }
+        const uint64_t inc = ResetAddOp{range}(prefix, term);
+        compact[j * D + d] = static_cast<uint32_t>(P.wrap_min + static_cast<int64_t>(inc & 0xffffffffull));
+    }
+};
+
+// ------------------------------------------------------------------- level 1
+struct ZeroIn {
+    const uint32_t* idrel;
+    __device__ uint32_t operator()(uint64_t i) const { return idrel[i] == 0 ? 1u : 0u; }
+};
+struct ZeroRankOut {
+    const uint32_t* idrel;
+    uint32_t* parent;
+    uint32_t* zrank;
+    DecState* st;
+    uint64_t n;
+    __device__ void operator()(uint64_t i, uint32_t pre, uint32_t z) const {
+        zrank[i] = pre;
+        const uint32_t j = idrel[i];
+        if (z) { parent[i] = static_cast<uint32_t>(i); return; }
+        if (static_cast<uint64_t>(j) >= n - i) { set_error(&st->err, kErrCorrupt); parent[i] = static_cast<uint32_t>(i); return; }
+        parent[i] = static_cast<uint32_t>(i + j);
+    }
+};
+
+// One pointer-jumping round.  A round that moves no pointer clears jump_active, and every
+// later round returns at once.  Jumps only point forward, so rounds <= ceil(log2 N).
+__global__ void __launch_bounds__(256) k_jump(uint32_t* parent, const uint32_t* idrel, uint64_t n, DecState* st,
+                                               uint32_t* moved) {
+    if (!st->jump_active) return;
+    bool any = false;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t p = parent[i];
+        if (idrel[p] == 0) continue;
+        const uint32_t pp = parent[p];
+        if (pp != p) { parent[i] = pp; any = true; }
+    }
+    if (__syncthreads_or(any) && threadIdx.x == 0) atomicOr(moved, 1u);
+}
+__global__ void k_jump_flag(DecState* st, uint32_t* moved) {
+    if (threadIdx.x || blockIdx.x) return;
+    if (st->jump_active && *moved == 0) st->jump_active = 0;
+    *moved = 0;
+}
+
+// q = block(root) * p + offset, then x = fma(q + 0.5, 2 eb, min) (lcps_cpp.cpp:1496-1500).
+template <typename OT, bool SOA>
+__global__ void __launch_bounds__(256)
+k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ zrank,
+              const uint32_t* __restrict__ compact, const uint32_t* __restrict__ rel, const DecState* stc,
+              DecState* st, OT* __restrict__ out, int64_t* __restrict__ q_out) {
+    const DecodePlan& P = stc->plan;
+    const uint32_t D = P.D;
+    const uint64_t n = P.N;
+    const int64_t p = P.p;
+    const double two_eb = 2.0 * P.eb;
+    const uint32_t B = static_cast<uint32_t>(P.comp[3].records);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t root = parent[i];
+        const uint32_t cr = zrank[root];
+        bool bad = cr >= B;
+        for (uint32_t d = 0; d < D; ++d) {
+            const int64_t off = rel[i * D + d];
+            if (off >= p) bad = true;
+            const int64_t blk = bad ? 0 : compact[static_cast<uint64_t>(cr) * D + d];
+            if (blk > (INT64_MAX - off) / p) bad = true;
+            const int64_t q = bad ? 0 : blk * p + off;
+            if (q_out) q_out[static_cast<uint64_t>(d) * n + i] = q;
+            const double x = fma(__dadd_rn(static_cast<double>(q), 0.5), two_eb, P.minima[d]);
+            out[SOA ? static_cast<uint64_t>(d) * n + i : i * D + d] = static_cast<OT>(x);
+        }
+        if (bad) set_error(&st->err, kErrCorrupt);
+    }
+}
+
+template <typename OT, bool SOA>
+__global__ void k_corrections(const uint8_t* data, const DecState* stc, DecState* st, OT* out) {
+    const DecodePlan& P = stc->plan;
+    const uint64_t cnt = P.exc_count;
+    const uint64_t nd = P.N * P.D;
+    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < cnt;
+         k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t idx = 0, prev = 0, vb = 0;
+        for (int b = 0; b < 8; ++b) idx |= static_cast<uint64_t>(data[P.exc_idx_off + 8 * k + b]) << (8 * b);
+        if (k) for (int b = 0; b < 8; ++b) prev |= static_cast<uint64_t>(data[P.exc_idx_off + 8 * (k - 1) + b]) << (8 * b);
+        for (int b = 0; b < 8; ++b) vb |= static_cast<uint64_t>(data[P.exc_val_off + 8 * k + b]) << (8 * b);
+        double v;
+        memcpy(&v, &vb, 8);
+        if (idx >= nd || (k && idx <= prev) || !chain_isfinite(v)) { set_error(&st->err, kErrCorrupt); continue; }
+        const uint64_t i = idx / P.D, d = idx - i * P.D;
+        out[SOA ? d * P.N + i : idx] = static_cast<OT>(v);
+    }
+}
+
+// --------------------------------------------------------------------- host
+static unsigned dgrid(uint64_t n, int threads = 256, unsigned cap = 148u * 16u) {
+    uint64_t g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return static_cast<unsigned>(g);
+}
+
+chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, chain_dtype out_dtype,
+                          chain_layout out_layout, void* out, size_t out_capacity, uint64_t* n_out,
+                          uint32_t* dims_out) {
+    cudaStream_t stream = ctx->stream;
+    chain_status s0 = ensure_state(ctx, sizeof(DecState));
+    if (s0 != CHAIN_OK) return s0;
+    DecState* st = static_cast<DecState*>(ctx->state_dev);
+    DecState* hs = static_cast<DecState*>(ctx->state_host);
+    const bool host_in = !is_device_ptr(container);
+    DecodePlan plan;
+    if (host_in) {
+        if (!parse_container(static_cast<const uint8_t*>(container), len, &plan))
+            return set_err(CHAIN_ERR_CORRUPT_STREAM, "LCG2: container failed validation (check at chain_format.h:" +
+                                                         std::to_string(plan.why) + ")");
+    }
+    // sizes for the arena: parse on the device when the container lives there
+    const uint8_t* dcont = static_cast<const uint8_t*>(container);
+    size_t base_need = host_in ? Arena::need(len + 16, 1) : 0;
+    if (!host_in) {
+        k_dec_init<<<1, 1, 0, stream>>>(st);
+        k_parse<<<1, 1, 0, stream>>>(dcont, len, st);
+        CHAIN_LAUNCH_CHECK("parse");
+        CHAIN_CUDA(cudaMemcpyAsync(&hs->plan, &st->plan, sizeof(DecodePlan), cudaMemcpyDeviceToHost, stream));
+        CHAIN_CUDA(cudaStreamSynchronize(stream));
+        plan = hs->plan;
+        if (!plan.ok)
+            return set_err(CHAIN_ERR_CORRUPT_STREAM, "LCG2: container failed validation (check at chain_format.h:" +
+                                                         std::to_string(plan.why) + ")");
+    }
+    const uint64_t N = plan.N;
+    const uint32_t D = plan.D;
+    const uint64_t nd = N * D;
+    const size_t osz = out_dtype == CHAIN_F64 ? 8 : 4;
+    if (n_out) *n_out = N;
+    if (dims_out) *dims_out = D;
+    if (out_capacity < nd * osz)
+        return set_err(CHAIN_ERR_BUFFER_TOO_SMALL, "output buffer holds " + std::to_string(out_capacity) +
+                                                       " bytes, need " + std::to_string(nd * osz));
+    const uint64_t B = plan.comp[3].records;
+    uint64_t max_prec_slots = 0, total_chunks = 0, max_alpha = 0, tags_total = 0;
+    uint64_t tag_off[kStreams] = {0};
+    for (int s = 0; s < kStreams; ++s) {
+        const CompPlan& c = plan.comp[s];
+        if (c.enc == kEncRaw || c.enc == kEncTagged) {
+            max_prec_slots += 1ull << c.sec.prec;
+            total_chunks += c.sec.chunks;
+            max_alpha += c.sec.alphabet;
+        }
+        if (c.enc == kEncTagged) {
+            tag_off[s] = tags_total;
+            tags_total += c.records;
+        }
+    }
+    const bool host_out = !is_device_ptr(out);
+    size_t need = base_need;
+    need += Arena::need(N, 4) * 4;           // idrel, choice2, zrank, parent
+    need += Arena::need(nd, 4) * 4;          // diff, keep, rel, compact
+    need += Arena::need(N, 4);               // drank
+    need += Arena::need(tags_total + 1, 4);
+    need += Arena::need(max_prec_slots + 1, 4) + Arena::need(max_alpha + 1, 4) * 2;
+    need += Arena::need(total_chunks + kStreams + 1, 8) + Arena::need(total_chunks * 32 + 1, 4);
+    need += Arena::need(scan_tiles(std::max<uint64_t>(nd, N)) + 16, 8);
+    need += Arena::need(16, 8);
+    if (host_out) need += Arena::need(nd, osz);
+    need += 24 * 256;
+    CHAIN_CUDA(ctx->dec.reserve(need));
+    Arena& A = ctx->dec;
+    if (host_in) {
+        uint8_t* d = A.take<uint8_t>(len + 16);
+        CHAIN_CUDA(cudaMemcpyAsync(d, container, len, cudaMemcpyHostToDevice, stream));
+        dcont = d;
+        hs->plan = plan;
+        k_dec_init<<<1, 1, 0, stream>>>(st);
+        CHAIN_CUDA(cudaMemcpyAsync(&st->plan, &hs->plan, sizeof(DecodePlan), cudaMemcpyHostToDevice, stream));
+    }
+    uint32_t* streams[kStreams];
+    streams[0] = A.take<uint32_t>(N);
+    streams[1] = A.take<uint32_t>(nd);
+    streams[2] = A.take<uint32_t>(nd);
+    streams[3] = A.take<uint32_t>(N);
+    streams[4] = A.take<uint32_t>(nd);
+    uint32_t* compact = A.take<uint32_t>(nd);
+    uint32_t* zrank = A.take<uint32_t>(N);
+    uint32_t* parent = A.take<uint32_t>(N);
+    uint32_t* drank = A.take<uint32_t>(N);
+    uint32_t* tags = A.take<uint32_t>(tags_total + 1);
+    uint32_t* lookup = A.take<uint32_t>(max_prec_slots + 1);
+    uint32_t* prob = A.take<uint32_t>(max_alpha + 1);
+    uint32_t* cum = A.take<uint32_t>(max_alpha + 1);
+    uint64_t* chunk_off = A.take<uint64_t>(total_chunks + kStreams + 1);
+    uint32_t* states = A.take<uint32_t>(total_chunks * 32 + 1);
+    uint64_t* scanbuf = A.take<uint64_t>(scan_tiles(std::max<uint64_t>(nd, N)) + 16);
+    uint64_t* misc = A.take<uint64_t>(16);
+    void* dout = host_out ? A.take<uint8_t>(nd * osz) : out;
+    if (!misc || !dout) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "decoder arena too small");
+    uint32_t* moved = reinterpret_cast<uint32_t*>(misc);
+    CHAIN_CUDA(cudaMemsetAsync(misc, 0, 16 * sizeof(uint64_t), stream));
+
+    // ---- entropy sections
+    SectionRefs refs{};
+    RansJobs jobs{};
+    uint64_t states_first[kStreams] = {0};
+    uint64_t slot_base = 0, alpha_base = 0, chunk_base = 0, off_base = 0;
+    uint32_t first = 0;
+    int nsec = 0;
+    for (int s = 0; s < kStreams; ++s) {
+        const CompPlan& c = plan.comp[s];
+        if (c.enc != kEncRaw && c.enc != kEncTagged) continue;
+        SectionRef& R = refs.r[nsec];
+        R.sec = &st->plan.comp[s].sec;
+        R.prob = prob + alpha_base;
+        R.cum = cum + alpha_base;
+        R.lookup = lookup + slot_base;
+        R.chunk_off = chunk_off + off_base;
+        states_first[nsec] = chunk_base * 32;
+        RansJob& jb = jobs.job[jobs.njobs++];
+        jb.count = c.sec.count;
+        jb.prob = R.prob;
+        jb.cum = R.cum;
+        jb.lookup = R.lookup;
+        jb.prec = c.sec.prec;
+        jb.chunks = c.sec.chunks;
+        jb.S = c.sec.S;
+        jb.bytes = const_cast<uint8_t*>(dcont);
+        jb.chunk_off = R.chunk_off;
+        jb.states = states + chunk_base * 32;
+        jb.out = c.enc == kEncRaw ? streams[s] : tags + tag_off[s];
+        jb.first_chunk = first;
+        first += c.sec.chunks;
+        slot_base += 1ull << c.sec.prec;
+        alpha_base += c.sec.alphabet;
+        chunk_base += c.sec.chunks;
+        off_base += c.sec.chunks + 1;
+        ++nsec;
+    }
+    refs.count = nsec;
+    jobs.total_chunks = first;
+    uint64_t* d_states_first = misc + 8;   // nsec <= 5 entries -> misc[8..12]
+    CHAIN_CUDA(cudaMemcpyAsync(d_states_first, states_first, sizeof(uint64_t) * kStreams, cudaMemcpyHostToDevice, stream));
+    if (nsec) {
+        k_section_setup<<<nsec, 1024, 0, stream>>>(refs, dcont, st);
+        k_lookup<<<dim3(256, nsec), 256, 0, stream>>>(refs, st);
+        k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states, d_states_first);
+        const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((jobs.total_chunks + 3) / 4, 148u * 64u));
+        rans_decode_kernel<<<blocks, 128, 0, stream>>>(jobs, &st->err);
+    }
+    CHAIN_LAUNCH_CHECK("entropy decode");
+    // ---- tagged and fixed components
+    for (int s = 0; s < kStreams; ++s) {
+        const CompPlan& c = plan.comp[s];
+        const CompPlan* dc = &st->plan.comp[s];
+        if (c.enc == kEncFixed) {
+            k_unpack_fixed<<<dgrid(c.records * c.dims), 256, 0, stream>>>(dcont, dc, streams[s], st);
+        } else if (c.enc == kEncTagged) {
+            uint32_t* tg = tags + tag_off[s];
+            device_exclusive_scan<uint64_t>(TagIn{tg, c.dims},
+                                            TagUnpackOut{dcont + c.tagged_off, tg, dc, streams[s], st, s}, c.records,
+                                            scanbuf, static_cast<uint64_t*>(nullptr), stream);
+        }
+    }
+    if (tags_total) k_check_tagged<<<1, 1, 0, stream>>>(st, st);
+    CHAIN_LAUNCH_CHECK("unpack");
+
+    // ---- level 2 inverse: choice ranks, then one reset-scan per dimension
+    const uint64_t range = static_cast<uint64_t>(plan.wrap_max - plan.wrap_min) + 1;
+    uint32_t* ndiff_dev = reinterpret_cast<uint32_t*>(misc + 1);
+    device_exclusive_scan<uint32_t>(ChoiceIn{streams[3]}, ChoiceRankOut{streams[3], drank, st}, B,
+                                    reinterpret_cast<uint32_t*>(scanbuf), ndiff_dev, stream);
+    for (uint32_t d = 0; d < D; ++d) {
+        device_exclusive_scan<uint64_t>(
+            Level2TermIn{streams[3], drank, streams[2], streams[1], st, d},
+            Level2TermOut{streams[3], drank, streams[2], streams[1], st, st, d, compact}, B, scanbuf,
+            static_cast<uint64_t*>(nullptr), stream, ResetAddOp{range});
+    }
+    // ---- level 1 inverse
+    uint32_t* zeros_dev = reinterpret_cast<uint32_t*>(misc + 2);
+    device_exclusive_scan<uint32_t>(ZeroIn{streams[0]}, ZeroRankOut{streams[0], parent, zrank, st, N}, N,
+                                    reinterpret_cast<uint32_t*>(scanbuf), zeros_dev, stream);
+    int rounds = 1;
+    while ((1ull << rounds) < N) ++rounds;
+    for (int r = 0; r < rounds + 1; ++r) {
+        k_jump<<<dgrid(N), 256, 0, stream>>>(parent, streams[0], N, st, moved);
+        k_jump_flag<<<1, 1, 0, stream>>>(st, moved);
+    }
+    CHAIN_LAUNCH_CHECK("levels");
+    // ---- reconstruction
+    const bool soa = out_layout == CHAIN_SOA;
+    const unsigned g = dgrid(N);
+    const unsigned gc = dgrid(plan.exc_count);
+    if (out_dtype == CHAIN_F64) {
+        double* o = static_cast<double*>(dout);
+        if (soa) { k_reconstruct<double, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+                   if (plan.exc_count) k_corrections<double, true><<<gc, 256, 0, stream>>>(dcont, st, st, o); }
+        else { k_reconstruct<double, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+               if (plan.exc_count) k_corrections<double, false><<<gc, 256, 0, stream>>>(dcont, st, st, o); }
+    } else {
+        float* o = static_cast<float*>(dout);
+        if (soa) { k_reconstruct<float, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+                   if (plan.exc_count) k_corrections<float, true><<<gc, 256, 0, stream>>>(dcont, st, st, o); }
+        else { k_reconstruct<float, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+               if (plan.exc_count) k_corrections<float, false><<<gc, 256, 0, stream>>>(dcont, st, st, o); }
+    }
+    CHAIN_LAUNCH_CHECK("reconstruct");
+    if (host_out) CHAIN_CUDA(cudaMemcpyAsync(out, dout, nd * osz, cudaMemcpyDeviceToHost, stream));
+    CHAIN_CUDA(cudaMemcpyAsync(hs, st, offsetof(DecState, plan), cudaMemcpyDeviceToHost, stream));
+    uint32_t counts[4] = {0, 0, 0, 0};
+    CHAIN_CUDA(cudaMemcpyAsync(counts, misc + 1, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+    CHAIN_CUDA(cudaStreamSynchronize(stream));
+    const uint32_t ndiff_seen = counts[0], zeros_seen = counts[2];
+    if (hs->err || ndiff_seen != plan.comp[1].records || zeros_seen != B || hs->jump_active)
+        return set_err(CHAIN_ERR_CORRUPT_STREAM, "LCG2: invalid integer payload (flags " + std::to_string(hs->err) +
+                                                     ")");
+    return CHAIN_OK;
+}
+
+}  // namespace chain

@@ -1,0 +1,1110 @@
+// Chain encoder on sm_100a: FP64 quantization, Z-order block keys + stable radix sort,
+// level-1 chaining, level-2 block differencing, candidate selection and the
+// interleaved-rANS / bit-packing entropy stage, assembled into an LCG2 v2 container.
+//
+// Integer semantics follow the reference CPU encoder bit for bit:
+//   quantization + exact corrections   cpp/chain/lcps_cpp.cpp:2069-2110 (:1496-1523)
+//   next point in the same block       lcps_cpp.cpp:2116-2138
+//   level-1 choice                     lcps_cpp.cpp:2155-2200
+//   level-2 keep/difference split      lcps_cpp.cpp:1305-1454 (:1221-1262, :1456-1478)
+//   candidate codings                  lcps_cpp.cpp:1140-1174 (fixed :856-933,
+//                                      tagged :1005-1058, raw value rANS :935-995)
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "chain_common.cuh"
+#include "chain_format.h"
+#include "ctx.h"
+#include "radix_sort.cuh"
+#include "rans.cuh"
+#include "scan.cuh"
+
+namespace chain {
+
+// ------------------------------------------------------------------------ state
+struct StreamStats {
+    uint32_t minv[kMaxDims];
+    uint32_t maxv[kMaxDims];
+    uint32_t maxall;
+    uint32_t maxtag;
+    uint64_t tag_bits;        // sum over records of dims * tag
+    uint32_t tag_hist[34];    // tag_hist[t], t in 1..32
+};
+
+struct StreamChoice {
+    uint8_t enc;
+    uint8_t max_width;
+    uint8_t width[kMaxDims];
+    uint32_t dims;
+    uint64_t records;
+    uint64_t est[4];          // estimated body bytes by encoding (index = Encoding)
+    uint32_t sec_prec, sec_alphabet, sec_chunks, table_len;
+    uint64_t sec_S, sec_count;
+    uint64_t packed_bits;
+    uint64_t body_bytes;      // exact, after coding
+};
+
+struct EncState {
+    uint32_t err;
+    uint32_t dims;
+    uint64_t n;
+    double eb;
+    uint64_t p;
+    int64_t threshold;
+    uint64_t minbits[kMaxDims], maxbits[kMaxDims];
+    uint64_t zero_first[kMaxDims][2];   // first index of -0.0 / +0.0
+    double mins[kMaxDims];
+    uint32_t qmax[kMaxDims];
+    uint32_t bmax_all;
+    int32_t kb;
+    int32_t key_bits;
+    int32_t maxb_bits;
+    uint64_t ncorr;
+    uint32_t B, nkeep, ndiff, pad0;
+    uint32_t rec_min, rec_max, rec_maxdiff, pad1;
+    int64_t wrap_min, wrap_max, wrap_range, wrap_min_corr, wrap_max_corr;
+    StreamStats st[kStreams];
+    RansTableDev raw_tab[kStreams];
+    RansTableDev tag_tab[kStreams];
+    StreamChoice ch[kStreams];
+    uint64_t total_bytes;
+    uint32_t npieces;
+    uint32_t pad2;
+};
+
+struct Piece {
+    const uint8_t* src;
+    uint64_t dst;
+    uint64_t len;
+};
+
+// --------------------------------------------------------------- quantization
+template <typename FT, bool SOA>
+__device__ __forceinline__ double load_coord(const FT* p, uint64_t n, uint32_t D, uint64_t i, uint32_t d) {
+    return static_cast<double>(SOA ? p[static_cast<uint64_t>(d) * n + i] : p[i * D + d]);
+}
+
+template <typename FT, bool SOA>
+__global__ void __launch_bounds__(256) k_minmax(const FT* __restrict__ p, uint64_t n, uint32_t D, EncState* st) {
+    const uint32_t d = blockIdx.y;
+    uint64_t mn = ~0ull, mx = 0, zneg = ~0ull, zpos = ~0ull;
+    bool bad = false;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const double x = load_coord<FT, SOA>(p, n, D, i, d);
+        if (!chain_isfinite(x)) { bad = true; continue; }
+        const uint64_t o = ordered_bits(x);
+        mn = o < mn ? o : mn;
+        mx = o > mx ? o : mx;
+        if (x == 0.0) {
+            if (signbit(x)) zneg = i < zneg ? i : zneg;
+            else zpos = i < zpos ? i : zpos;
+        }
+    }
+    mn = warp_min(mn); mx = warp_max(mx); zneg = warp_min(zneg); zpos = warp_min(zpos);
+    __shared__ uint64_t s[4][8];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { s[0][w] = mn; s[1][w] = mx; s[2][w] = zneg; s[3][w] = zpos; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < static_cast<int>(blockDim.x >> 5); ++k) {
+            mn = s[0][k] < mn ? s[0][k] : mn; mx = s[1][k] > mx ? s[1][k] : mx;
+            zneg = s[2][k] < zneg ? s[2][k] : zneg; zpos = s[3][k] < zpos ? s[3][k] : zpos;
+        }
+        atomicMin(reinterpret_cast<unsigned long long*>(&st->minbits[d]), mn);
+        atomicMax(reinterpret_cast<unsigned long long*>(&st->maxbits[d]), mx);
+        if (zneg != ~0ull) atomicMin(reinterpret_cast<unsigned long long*>(&st->zero_first[d][0]), zneg);
+        if (zpos != ~0ull) atomicMin(reinterpret_cast<unsigned long long*>(&st->zero_first[d][1]), zpos);
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) set_error(&st->err, kErrNonFinite);
+}
+
+// Per-axis minimum exactly as std::min keeps it (first of equal values, which only
+// matters for +0.0 vs -0.0), the largest quantized value and the block-key width.
+__global__ void k_qparams(EncState* st) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (st->err & kErrNonFinite) return;
+    const double denom = 2.0 * st->eb;
+    uint32_t bmax = 0;
+    int kb = 0;
+    for (uint32_t d = 0; d < st->dims; ++d) {
+        double mn = from_ordered_bits(st->minbits[d]);
+        if (mn == 0.0) mn = st->zero_first[d][0] < st->zero_first[d][1] ? -0.0 : 0.0;
+        st->mins[d] = mn;
+        const double mx = from_ordered_bits(st->maxbits[d]);
+        const double qv = floor((mx - mn) / denom);
+        if (!(qv >= 0.0 && qv < 0x1p63)) { set_error(&st->err, kErrQuantOverflow); return; }
+        if (qv >= 2147483648.0) { set_error(&st->err, kErrUnsupported); return; }
+        st->qmax[d] = static_cast<uint32_t>(qv);
+        const uint32_t b = static_cast<uint32_t>(static_cast<uint64_t>(st->qmax[d]) / st->p);
+        bmax = b > bmax ? b : bmax;
+        kb = bitlen32(b) > kb ? bitlen32(b) : kb;
+    }
+    st->bmax_all = bmax;
+    st->kb = kb;
+    st->key_bits = kb * static_cast<int>(st->dims);
+    st->maxb_bits = bitlen32(bmax);
+    if (st->key_bits > 64) set_error(&st->err, kErrUnsupported);
+}
+
+// lcps_cpp.cpp:1502-1523
+__device__ __forceinline__ bool within_error_bound(double restored, double original, double eb) {
+    if (!chain_isfinite(restored)) return false;
+    const double difference = __dsub_rn(restored, original);
+    const double magnitude = fabs(difference);
+    if (magnitude < eb) return true;
+    if (!(magnitude == eb)) return false;
+    const double virtual_original = __dsub_rn(difference, restored);
+    const double remainder = __dadd_rn(__dsub_rn(restored, __dsub_rn(difference, virtual_original)),
+                                       __dsub_rn(-original, virtual_original));
+    return difference >= 0.0 ? remainder <= 0.0 : remainder >= 0.0;
+}
+
+template <typename FT, bool SOA, typename KT>
+__global__ void __launch_bounds__(256)
+k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D, EncState* st, KT* __restrict__ key_out,
+           uint32_t* __restrict__ rel_out, uint64_t* __restrict__ corr_idx, double* __restrict__ corr_val,
+           uint64_t corr_cap) {
+    __shared__ double s_min[kMaxDims];
+    __shared__ double s_eb, s_denom;
+    __shared__ uint64_t s_p;
+    __shared__ int s_kb;
+    if (threadIdx.x < D) s_min[threadIdx.x] = st->mins[threadIdx.x];
+    if (threadIdx.x == 0) { s_eb = st->eb; s_denom = 2.0 * st->eb; s_p = st->p; s_kb = st->kb; }
+    __syncthreads();
+    const double eb = s_eb, denom = s_denom, two_eb = 2.0 * s_eb;
+    const uint64_t pp = s_p;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint32_t b[kMaxDims];
+        for (uint32_t d = 0; d < D; ++d) {
+            const double x = load_coord<FT, SOA>(p, n, D, i, d);
+            const double qv = floor(__ddiv_rn(__dsub_rn(x, s_min[d]), denom));
+            const uint32_t q = static_cast<uint32_t>(qv);
+            const double restored = fma(__dadd_rn(static_cast<double>(q), 0.5), two_eb, s_min[d]);
+            if (!within_error_bound(restored, x, eb)) {
+                const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(&st->ncorr), 1ull);
+                if (slot < corr_cap) {
+                    corr_idx[slot] = i * D + d;
+                    corr_val[slot] = x;
+                }
+            }
+            const uint32_t bb = static_cast<uint32_t>(static_cast<uint64_t>(q) / pp);
+            b[d] = bb;
+            rel_out[i * D + d] = static_cast<uint32_t>(q - static_cast<uint64_t>(bb) * pp);
+        }
+        key_out[i] = static_cast<KT>(block_key(b, static_cast<int>(D), s_kb));
+    }
+}
+
+// ------------------------------------------------------------------- level 1
+// One thread per sorted position: the sorted neighbour with an equal key is the next
+// point of the same block (stable sort keeps indices increasing within a block).
+template <typename KT>
+__global__ void __launch_bounds__(256)
+k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_t n, const EncState* st,
+         uint32_t* __restrict__ idrel) {
+    const int D = static_cast<int>(st->dims);
+    const int kb = st->kb;
+    const int64_t maxb_bits = st->maxb_bits;
+    const int64_t thr = st->threshold;
+    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const KT key = skey[k];
+        const uint32_t i = sidx[k];
+        uint32_t out = 0;
+        if (k + 1 < n && skey[k + 1] == key) {
+            const uint32_t dist = sidx[k + 1] - i;
+            uint32_t b[kMaxDims];
+            block_unkey(static_cast<uint64_t>(key), D, kb, b);
+            uint32_t mx = b[0];
+            for (int d = 1; d < D; ++d) mx = b[d] > mx ? b[d] : mx;
+            const int local_bits = bitlen32(mx);
+            const int tag_bits = bitlen32(static_cast<uint32_t>(local_bits));
+            const int64_t a = static_cast<int64_t>(local_bits) * D + tag_bits;
+            const int64_t c = static_cast<int64_t>(D) * maxb_bits;
+            const int64_t smaller = a < c ? a : c;
+            const int dl = bitlen32(dist);
+            if (static_cast<int64_t>(dl + bitlen32(static_cast<uint32_t>(dl))) < smaller - thr) out = dist;
+        }
+        idrel[i] = out;
+    }
+}
+
+// Explicit block records, in index order (lcps_cpp.cpp:2196-2199).
+template <typename KT>
+struct ExplicitIn {
+    const uint32_t* idrel;
+    __device__ uint32_t operator()(uint64_t i) const { return idrel[i] == 0 ? 1u : 0u; }
+};
+template <typename KT>
+struct ExplicitOut {
+    const KT* key;
+    const EncState* st;
+    uint32_t* rec;
+    __device__ void operator()(uint64_t i, uint32_t pos, uint32_t flag) const {
+        if (!flag) return;
+        const int D = static_cast<int>(st->dims);
+        uint32_t b[kMaxDims];
+        block_unkey(static_cast<uint64_t>(key[i]), D, st->kb, b);
+        for (int d = 0; d < D; ++d) rec[static_cast<uint64_t>(pos) * D + d] = b[d];
+    }
+};
+
+// ------------------------------------------------------------------- level 2
+__global__ void __launch_bounds__(256) k_l2_stats(const uint32_t* __restrict__ rec, EncState* st) {
+    const uint32_t B = st->B;
+    const uint32_t D = st->dims;
+    uint32_t mn = 0xffffffffu, mx = 0, md = 0;
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < B;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        for (uint32_t d = 0; d < D; ++d) {
+            const uint32_t v = rec[j * D + d];
+            mn = v < mn ? v : mn;
+            mx = v > mx ? v : mx;
+            if (j) {
+                const uint32_t u = rec[(j - 1) * D + d];
+                const uint32_t a = v >= u ? v - u : u - v;
+                md = a > md ? a : md;
+            }
+        }
+    }
+    mn = warp_min(mn); mx = warp_max(mx); md = warp_max(md);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&st->rec_min, mn);
+        atomicMax(&st->rec_max, mx);
+        atomicMax(&st->rec_maxdiff, md);
+    }
+}
+
+// lcps_cpp.cpp:1221-1253 wrap parameters; also the !l2 keep-all variant (:1456-1478).
+__global__ void k_l2_params(EncState* st) {
+    if (threadIdx.x || blockIdx.x) return;
+    const int64_t mn = st->B ? st->rec_min : 0;
+    const int64_t mx = st->rec_max;
+    const int64_t range = mx - mn + 1;
+    st->wrap_min = mn;
+    st->wrap_max = mx;
+    st->wrap_range = range;
+    st->wrap_max_corr = range / 2 - ((range & 1) == 0 ? 1 : 0);
+    st->wrap_min_corr = -(range / 2);
+}
+
+struct Level2In {
+    const uint32_t* rec;
+    const EncState* st;
+    int l2;
+    __device__ uint32_t operator()(uint64_t j) const {
+        if (!l2 || j == 0 || j >= st->B) return 0u;
+        const uint32_t D = st->dims;
+        const uint64_t fvb = static_cast<uint64_t>(D) * bitlen32(st->rec_max);
+        const uint64_t fdb = static_cast<uint64_t>(D) * bitlen32(st->rec_maxdiff);
+        uint32_t mv = 0, md = 0;
+        for (uint32_t d = 0; d < D; ++d) {
+            const uint32_t v = rec[j * D + d], u = rec[(j - 1) * D + d];
+            mv = v > mv ? v : mv;
+            const uint32_t a = v >= u ? v - u : u - v;
+            md = a > md ? a : md;
+        }
+        const int tvw = bitlen32(mv), tdw = bitlen32(md);
+        const uint64_t tvb = static_cast<uint64_t>(D) * tvw + bitlen32(static_cast<uint32_t>(tvw));
+        const uint64_t tdb = static_cast<uint64_t>(D) * tdw + bitlen32(static_cast<uint32_t>(tdw));
+        const uint64_t value_bits = tvb < fvb ? tvb : fvb;
+        const uint64_t diff_bits = tdb > fdb ? tdb : fdb;
+        return value_bits >= diff_bits ? 1u : 0u;
+    }
+};
+struct Level2Out {
+    const uint32_t* rec;
+    const EncState* st;
+    uint32_t* choice2;
+    uint32_t* keep;
+    uint32_t* diff;
+    __device__ void operator()(uint64_t j, uint32_t drank, uint32_t use_diff) const {
+        if (j >= st->B) return;
+        const uint32_t D = st->dims;
+        choice2[j] = use_diff;
+        if (!use_diff) {
+            const uint64_t k = j - drank;
+            for (uint32_t d = 0; d < D; ++d) keep[k * D + d] = rec[j * D + d];
+            return;
+        }
+        for (uint32_t d = 0; d < D; ++d) {
+            // prediction = previous record (already inside [wrap_min, wrap_max])
+            int64_t corr = static_cast<int64_t>(rec[(j - 1) * D + d]) - static_cast<int64_t>(rec[j * D + d]);
+            if (corr < st->wrap_min_corr) corr += st->wrap_range;
+            else if (corr > st->wrap_max_corr) corr -= st->wrap_range;
+            const uint64_t zz = corr >= 0 ? static_cast<uint64_t>(corr) << 1
+                                          : (static_cast<uint64_t>(-(corr + 1)) << 1) | 1u;
+            diff[static_cast<uint64_t>(drank) * D + d] = static_cast<uint32_t>(zz);
+        }
+    }
+};
+
+__global__ void k_l2_counts(EncState* st) {
+    if (threadIdx.x || blockIdx.x) return;
+    st->nkeep = st->B - st->ndiff;
+}
+
+// ------------------------------------------------------------- stream stats
+struct StreamRef {
+    const uint32_t* data;   // record-major
+    uint32_t dims;
+    const uint32_t* count_dev;  // records (device) or null -> count_const
+    uint64_t count_const;
+};
+struct StreamRefs {
+    StreamRef s[kStreams];
+};
+
+__device__ __forceinline__ uint64_t stream_records(const StreamRef& r) {
+    return r.count_dev ? static_cast<uint64_t>(*r.count_dev) : r.count_const;
+}
+
+__global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState* st) {
+    const int s = blockIdx.y;
+    const StreamRef r = refs.s[s];
+    const uint64_t nrec = stream_records(r);
+    __shared__ uint32_t smin[kMaxDims], smax[kMaxDims], stag[34];
+    __shared__ unsigned long long sbits;
+    if (threadIdx.x < kMaxDims) { smin[threadIdx.x] = 0xffffffffu; smax[threadIdx.x] = 0; }
+    if (threadIdx.x < 34) stag[threadIdx.x] = 0;
+    if (threadIdx.x == 0) sbits = 0;
+    __syncthreads();
+    const uint32_t D = r.dims;
+    uint64_t bits = 0;
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nrec;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint32_t tag = 1;
+        for (uint32_t d = 0; d < D; ++d) {
+            const uint32_t v = r.data[j * D + d];
+            atomicMin(&smin[d], v);
+            atomicMax(&smax[d], v);
+            const uint32_t w = bitlen32(v);
+            tag = w > tag ? w : tag;
+        }
+        atomicAdd(&stag[tag], 1u);
+        bits += static_cast<uint64_t>(D) * tag;
+    }
+    bits = warp_sum(bits);
+    if ((threadIdx.x & 31) == 0 && bits) atomicAdd(&sbits, static_cast<unsigned long long>(bits));
+    __syncthreads();
+    StreamStats& g = st->st[s];
+    if (threadIdx.x < D) {
+        atomicMin(&g.minv[threadIdx.x], smin[threadIdx.x]);
+        atomicMax(&g.maxv[threadIdx.x], smax[threadIdx.x]);
+        atomicMax(&g.maxall, smax[threadIdx.x]);
+    }
+    if (threadIdx.x < 34 && stag[threadIdx.x]) {
+        atomicAdd(&g.tag_hist[threadIdx.x], stag[threadIdx.x]);
+        atomicMax(&g.maxtag, threadIdx.x);
+    }
+    if (threadIdx.x == 0 && sbits) atomicAdd(reinterpret_cast<unsigned long long*>(&g.tag_bits), sbits);
+}
+
+// Value histograms for the raw candidate (alphabet = max + 1 < 2^18).
+constexpr int kSmemHistBins = 8192;
+__global__ void __launch_bounds__(256) k_value_hist(StreamRefs refs, const EncState* st, uint32_t* hist,
+                                                     uint64_t hist_stride) {
+    const int s = blockIdx.y;
+    const StreamRef r = refs.s[s];
+    const uint32_t maxall = st->st[s].maxall;
+    const uint64_t nrec = stream_records(r);
+    if (nrec == 0 || maxall >= kRansMaxAlphabet) return;
+    const uint32_t A = maxall + 1;
+    uint32_t* h = hist + hist_stride * s;
+    const uint64_t nval = nrec * r.dims;
+    __shared__ uint32_t sh[kSmemHistBins];
+    const bool use_smem = A <= kSmemHistBins;
+    if (use_smem) {
+        for (uint32_t t = threadIdx.x; t < A; t += blockDim.x) sh[t] = 0;
+        __syncthreads();
+    }
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nval;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t v = r.data[j];
+        if (use_smem) atomicAdd(&sh[v], 1u);
+        else atomicAdd(&h[v], 1u);
+    }
+    if (use_smem) {
+        __syncthreads();
+        for (uint32_t t = threadIdx.x; t < A; t += blockDim.x)
+            if (sh[t]) atomicAdd(&h[t], sh[t]);
+    }
+}
+
+// One CTA per (stream, kind): kind 0 = raw value table, kind 1 = tag table.
+__global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncState* st, const uint32_t* hist,
+                                                           uint64_t hist_stride, uint32_t* prob, uint32_t* cum,
+                                                           uint32_t* tag_prob, uint32_t* tag_cum) {
+    const int s = blockIdx.x, kind = blockIdx.y;
+    const StreamRef r = refs.s[s];
+    const uint64_t nrec = stream_records(r);
+    if (kind == 0) {
+        const uint32_t maxall = st->st[s].maxall;
+        const bool ok = nrec > 0 && maxall < kRansMaxAlphabet;
+        build_rans_table(hist + hist_stride * s, ok ? maxall + 1 : 0, ok ? nrec * r.dims : 0,
+                         prob + hist_stride * s, cum + hist_stride * s, &st->raw_tab[s]);
+    } else {
+        const uint32_t A = nrec ? st->st[s].maxtag + 1 : 0;
+        build_rans_table(st->st[s].tag_hist, A, nrec, tag_prob + 64 * s, tag_cum + 64 * s, &st->tag_tab[s]);
+    }
+}
+
+__device__ inline uint64_t section_overhead(uint32_t table_bytes, uint32_t chunks) {
+    return 1 + 4 + 4 + static_cast<uint64_t>(table_bytes) + 8 + 4 + static_cast<uint64_t>(chunks) * (4 + 128);
+}
+
+__device__ inline void plan_chunks(uint64_t count, double est_payload, uint32_t bytes_per_lane, uint32_t* chunks,
+                                   uint64_t* S) {
+    uint64_t lanes = static_cast<uint64_t>(est_payload / bytes_per_lane) + 1;
+    uint64_t ch = (lanes + 31) / 32;
+    const uint64_t max_ch = (count + 31) / 32;
+    if (ch > max_ch) ch = max_ch;
+    if (ch < 1) ch = 1;
+    uint64_t s = (count + ch - 1) / ch;
+    s = (s + 31) & ~31ull;
+    if (s < 32) s = 32;
+    *S = s;
+    *chunks = static_cast<uint32_t>((count + s - 1) / s);
+}
+
+// Chooses each component's encoding: the smallest estimated size among tagged, fixed
+// and raw (ties in that order, as lcps_cpp.cpp:1150-1170), empty when no records.
+__global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane) {
+    const int s = threadIdx.x;
+    if (s >= kStreams || blockIdx.x) return;
+    const StreamRef r = refs.s[s];
+    const uint64_t nrec = stream_records(r);
+    StreamChoice& c = st->ch[s];
+    const StreamStats& g = st->st[s];
+    c.dims = r.dims;
+    c.records = nrec;
+    c.enc = kEncEmpty;
+    c.sec_chunks = 0;
+    c.sec_S = 0;
+    c.sec_count = 0;
+    c.packed_bits = 0;
+    c.max_width = 0;
+    c.est[0] = c.est[1] = c.est[2] = c.est[3] = ~0ull;
+    if (nrec == 0) {
+        c.est[kEncEmpty] = 13;
+        return;
+    }
+    if (st->tag_tab[s].alphabet == 0xFFFFFFFFu || st->raw_tab[s].alphabet == 0xFFFFFFFFu)
+        set_error(&st->err, kErrInternal);
+    // fixed
+    uint64_t fixed = 13 + 9ull * r.dims;
+    for (uint32_t d = 0; d < r.dims; ++d) {
+        const uint32_t span = g.maxv[d] - g.minv[d];
+        const int w = span ? bitlen32(span) : 1;
+        c.width[d] = static_cast<uint8_t>(w);
+        fixed += (nrec * w + 7) / 8;
+    }
+    c.est[kEncFixed] = fixed;
+    // tagged
+    {
+        const RansTableDev& t = st->tag_tab[s];
+        const double payload = t.cost_bits / 8.0;
+        uint32_t ch;
+        uint64_t S;
+        plan_chunks(nrec, payload, bytes_per_lane, &ch, &S);
+        c.est[kEncTagged] = 13 + 1 + section_overhead(t.table_bytes, ch) + static_cast<uint64_t>(payload) + 1 + 8 +
+                            (g.tag_bits + 7) / 8;
+    }
+    // raw
+    if (g.maxall < kRansMaxAlphabet && st->raw_tab[s].alphabet != 0) {
+        const RansTableDev& t = st->raw_tab[s];
+        const double payload = t.cost_bits / 8.0;
+        uint32_t ch;
+        uint64_t S;
+        plan_chunks(nrec * r.dims, payload, bytes_per_lane, &ch, &S);
+        c.est[kEncRaw] = 13 + section_overhead(t.table_bytes, ch) + static_cast<uint64_t>(payload) + 1;
+    }
+    uint8_t best = kEncTagged;
+    if (c.est[kEncFixed] < c.est[best]) best = kEncFixed;
+    if (c.est[kEncRaw] < c.est[best]) best = kEncRaw;
+    c.enc = best;
+    if (best == kEncTagged) {
+        const RansTableDev& t = st->tag_tab[s];
+        plan_chunks(nrec, t.cost_bits / 8.0, bytes_per_lane, &c.sec_chunks, &c.sec_S);
+        c.sec_count = nrec;
+        c.sec_prec = t.prec;
+        c.sec_alphabet = t.alphabet;
+        c.packed_bits = g.tag_bits;
+        c.max_width = static_cast<uint8_t>(g.maxtag);
+    } else if (best == kEncRaw) {
+        const RansTableDev& t = st->raw_tab[s];
+        plan_chunks(nrec * r.dims, t.cost_bits / 8.0, bytes_per_lane, &c.sec_chunks, &c.sec_S);
+        c.sec_count = nrec * r.dims;
+        c.sec_prec = t.prec;
+        c.sec_alphabet = t.alphabet;
+    }
+}
+
+// ------------------------------------------------------------------ packing
+// Tags of a tagged component: max(1, max_d bitlen(v)) per record (lcps_cpp.cpp:1032-1046).
+__global__ void __launch_bounds__(256) k_tags(const uint32_t* __restrict__ data, uint32_t D, uint64_t nrec,
+                                               uint32_t* __restrict__ tags) {
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nrec;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint32_t t = 1;
+        for (uint32_t d = 0; d < D; ++d) {
+            const uint32_t w = bitlen32(data[j * D + d]);
+            t = w > t ? w : t;
+        }
+        tags[j] = t;
+    }
+}
+
+// Writes `width` bits of v (MSB first) at bit offset `bit` of a big-endian bitstream
+// held as 32-bit words in big-endian byte order (converted when copied out).
+__device__ __forceinline__ void put_bits(uint32_t* words, uint64_t bit, uint32_t v, int width) {
+    const uint64_t w0 = bit >> 5;
+    const int off = static_cast<int>(bit & 31);
+    const uint64_t vv = static_cast<uint64_t>(v) << (64 - width);   // left-aligned
+    const uint64_t sh = vv >> off;                                  // bits for words w0, w0+1
+    const uint32_t hi = static_cast<uint32_t>(sh >> 32), lo = static_cast<uint32_t>(sh);
+    if (hi) atomicOr(&words[w0], hi);
+    if (lo) atomicOr(&words[w0 + 1], lo);
+}
+
+struct TagBitsIn {
+    const uint32_t* tags;
+    uint32_t D;
+    __device__ uint64_t operator()(uint64_t j) const { return static_cast<uint64_t>(tags[j]) * D; }
+};
+struct TagPackOut {
+    const uint32_t* data;
+    const uint32_t* tags;
+    uint32_t D;
+    uint32_t* words;
+    __device__ void operator()(uint64_t j, uint64_t bit, uint64_t) const {
+        const int t = static_cast<int>(tags[j]);
+        for (uint32_t d = 0; d < D; ++d, bit += t) put_bits(words, bit, data[j * D + d], t);
+    }
+};
+
+// Fixed-width packing of one dimension: one thread per output 32-bit word.
+__global__ void __launch_bounds__(256) k_pack_fixed(const uint32_t* __restrict__ data, uint32_t D, uint32_t d,
+                                                     uint64_t nrec, uint32_t minv, int width,
+                                                     uint32_t* __restrict__ words, uint64_t nwords) {
+    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < nwords;
+         w += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t b0 = w * 32, b1 = b0 + 32;
+        uint64_t first = b0 / width;
+        uint64_t last = (b1 - 1) / width;
+        if (last >= nrec) last = nrec - 1;
+        uint32_t acc = 0;
+        for (uint64_t k = first; k <= last; ++k) {
+            const uint64_t v = static_cast<uint64_t>(data[k * D + d] - minv);
+            const int64_t start = static_cast<int64_t>(k * width) - static_cast<int64_t>(b0);  // bit pos in word
+            // value occupies [start, start + width) relative to word start (MSB = bit 0)
+            const int64_t shift = 32 - (start + width);
+            if (shift >= 0) acc |= static_cast<uint32_t>(v << shift);
+            else acc |= static_cast<uint32_t>(v >> (-shift));
+        }
+        words[w] = acc;
+    }
+}
+
+// Big-endian words -> bytes in place (so that byte 0 holds the first 8 bits).
+__global__ void k_words_to_bytes(uint32_t* words, uint64_t nwords) {
+    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < nwords;
+         w += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        words[w] = __byte_perm(words[w], 0, 0x0123);
+}
+
+// Serialises every chosen table (one thread per stream).
+__global__ void k_serialize_tables(EncState* st, const uint32_t* prob, const uint32_t* tag_prob,
+                                   uint64_t hist_stride, uint8_t* out, uint64_t out_stride) {
+    const int s = threadIdx.x;
+    if (s >= kStreams) return;
+    StreamChoice& c = st->ch[s];
+    c.table_len = 0;
+    if (c.enc == kEncRaw) c.table_len = serialize_table(prob + hist_stride * s, c.sec_alphabet, out + out_stride * s);
+    else if (c.enc == kEncTagged) c.table_len = serialize_table(tag_prob + 64 * s, c.sec_alphabet, out + out_stride * s);
+}
+
+// --------------------------------------------------------------- assembly
+struct AssemblyIn {
+    const uint8_t* table_bytes;   // [kStreams] x table_stride
+    uint64_t table_stride;
+    const uint32_t* chunk_len[kStreams];
+    const uint32_t* states[kStreams];
+    const uint8_t* slots[kStreams];
+    uint64_t slot_cap[kStreams];
+    const uint8_t* packed[kStreams];         // fixed/tagged payload (bytes)
+    uint64_t packed_dim_stride[kStreams];    // fixed: bytes between dimension payloads
+    const uint64_t* corr_idx;
+    const double* corr_val;
+    uint8_t input_dtype;
+};
+
+struct Writer {
+    uint8_t* p;
+    uint64_t pos;
+    __device__ void u8(uint8_t v) { p[pos++] = v; }
+    __device__ void uint(uint64_t v, int bytes) {
+        for (int i = 0; i < bytes; ++i) p[pos++] = static_cast<uint8_t>(v >> (8 * i));
+    }
+    __device__ void f64(double d) {
+        uint64_t u;
+        memcpy(&u, &d, 8);
+        uint(u, 8);
+    }
+    __device__ void raw(const char* s, int n) {
+        for (int i = 0; i < n; ++i) p[pos++] = static_cast<uint8_t>(s[i]);
+    }
+};
+
+// Single thread: writes every header field and emits the list of payload pieces.
+__global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* pieces, uint32_t max_pieces) {
+    if (threadIdx.x || blockIdx.x) return;
+    Writer w{out, 0};
+    uint32_t np = 0;
+    auto piece = [&](const uint8_t* src, uint64_t len) {
+        if (len == 0) return;
+        if (np < max_pieces) pieces[np] = Piece{src, w.pos, len};
+        ++np;
+        w.pos += len;
+    };
+    const uint32_t D = st->dims;
+    w.raw("LCG2", 4);
+    w.uint(kFormatVersion, 4);
+    w.uint(D, 4);
+    w.uint(st->n, 8);
+    w.uint(st->p, 8);
+    w.f64(st->eb);
+    w.uint(static_cast<uint64_t>(st->wrap_min), 8);
+    w.uint(static_cast<uint64_t>(st->wrap_max), 8);
+    for (uint32_t d = 0; d < D; ++d) w.f64(st->mins[d]);
+    w.u8(in.input_dtype);
+    w.uint(kStreams, 4);
+    for (int s = 0; s < kStreams; ++s) {
+        StreamChoice& c = st->ch[s];
+        char name[4];
+        stream_name(s, name);
+        w.raw(name, 4);
+        const uint64_t len_pos = w.pos;
+        w.pos += 8;
+        const uint64_t body0 = w.pos;
+        w.u8(c.enc);
+        w.uint(c.dims, 4);
+        w.uint(c.records, 8);
+        if (c.enc == kEncFixed) {
+            for (uint32_t d = 0; d < c.dims; ++d) {
+                w.uint(st->st[s].minv[d], 8);
+                w.u8(c.width[d]);
+            }
+            for (uint32_t d = 0; d < c.dims; ++d)
+                piece(in.packed[s] + in.packed_dim_stride[s] * d, (c.records * c.width[d] + 7) / 8);
+        } else if (c.enc == kEncTagged || c.enc == kEncRaw) {
+            if (c.enc == kEncTagged) w.u8(c.max_width);
+            w.u8(static_cast<uint8_t>(c.sec_prec));
+            w.uint(c.sec_alphabet, 4);
+            w.uint(c.table_len, 4);
+            piece(in.table_bytes + in.table_stride * s, c.table_len);
+            w.uint(c.sec_S, 8);
+            w.uint(c.sec_chunks, 4);
+            piece(reinterpret_cast<const uint8_t*>(in.chunk_len[s]), 4ull * c.sec_chunks);
+            piece(reinterpret_cast<const uint8_t*>(in.states[s]), 128ull * c.sec_chunks);
+            for (uint32_t k = 0; k < c.sec_chunks; ++k) {
+                const uint32_t len = in.chunk_len[s][k];
+                piece(in.slots[s] + in.slot_cap[s] * k + (in.slot_cap[s] - len), len);
+            }
+            if (c.enc == kEncTagged) {
+                w.uint(c.packed_bits, 8);
+                piece(in.packed[s], (c.packed_bits + 7) / 8);
+            }
+        }
+        c.body_bytes = w.pos - body0;
+        const uint64_t save = w.pos;
+        w.pos = len_pos;
+        w.uint(c.body_bytes, 8);
+        w.pos = save;
+    }
+    w.raw("EXC0", 4);
+    w.uint(8 + 16 * st->ncorr, 8);
+    w.uint(st->ncorr, 8);
+    piece(reinterpret_cast<const uint8_t*>(in.corr_idx), 8 * st->ncorr);
+    piece(reinterpret_cast<const uint8_t*>(in.corr_val), 8 * st->ncorr);
+    st->total_bytes = w.pos;
+    st->npieces = np;
+    if (np > max_pieces) set_error(&st->err, kErrInternal);
+}
+
+__global__ void __launch_bounds__(256) k_copy_pieces(const Piece* pieces, const EncState* st, uint8_t* out) {
+    const uint32_t np = st->npieces;
+    for (uint32_t k = blockIdx.x; k < np; k += gridDim.x) {
+        const Piece pc = pieces[k];
+        uint8_t* dst = out + pc.dst;
+        for (uint64_t b = threadIdx.x; b < pc.len; b += blockDim.x) dst[b] = pc.src[b];
+    }
+}
+
+__global__ void k_gather_corrections(const uint32_t* perm, const uint64_t* idx_sorted_in, const double* val_in,
+                                     uint64_t* idx_out, double* val_out, uint64_t count) {
+    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < count;
+         k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        idx_out[k] = idx_sorted_in[k];
+        val_out[k] = val_in[perm[k]];
+    }
+}
+
+__global__ void k_init_state(EncState* st, uint32_t dims, uint64_t n, double eb, uint64_t p, int64_t threshold) {
+    if (threadIdx.x || blockIdx.x) return;
+    st->err = 0;
+    st->dims = dims;
+    st->n = n;
+    st->eb = eb;
+    st->p = p;
+    st->threshold = threshold;
+    for (int d = 0; d < kMaxDims; ++d) {
+        st->minbits[d] = ~0ull;
+        st->maxbits[d] = 0;
+        st->zero_first[d][0] = st->zero_first[d][1] = ~0ull;
+    }
+    st->ncorr = 0;
+    st->B = st->nkeep = st->ndiff = 0;
+    st->rec_min = 0xffffffffu;
+    st->rec_max = 0;
+    st->rec_maxdiff = 0;
+    for (int s = 0; s < kStreams; ++s) {
+        StreamStats& g = st->st[s];
+        for (int d = 0; d < kMaxDims; ++d) { g.minv[d] = 0xffffffffu; g.maxv[d] = 0; }
+        g.maxall = 0;
+        g.maxtag = 0;
+        g.tag_bits = 0;
+        for (int t = 0; t < 34; ++t) g.tag_hist[t] = 0;
+    }
+    st->total_bytes = 0;
+    st->npieces = 0;
+}
+
+// ------------------------------------------------------------------- host
+static unsigned grid_for(uint64_t n, int threads = 256, unsigned cap = 148u * 16u) {
+    uint64_t g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return static_cast<unsigned>(g);
+}
+
+static chain_status status_from_err(uint32_t err) {
+    if (err & kErrNonFinite) return set_err(CHAIN_ERR_NONFINITE_INPUT, "LCPS coordinates must be finite");
+    if (err & kErrQuantOverflow) return set_err(CHAIN_ERR_QUANT_OVERFLOW, "quantized coordinate does not fit int64");
+    if (err & kErrUnsupported)
+        return set_err(CHAIN_ERR_UNSUPPORTED,
+                       "quantized coordinates need more than 31 bits or block keys more than 64 bits "
+                       "(eb too small relative to the coordinate range for this build)");
+    if (err & kErrCapacity) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "device buffer capacity exceeded");
+    return set_err(CHAIN_ERR_DEVICE, "internal encoder error (flags " + std::to_string(err) + ")");
+}
+
+template <typename FT, bool SOA, typename KT>
+static void launch_quantize(const void* pts, uint64_t n, uint32_t D, EncState* st, void* key, uint32_t* rel,
+                            uint64_t* cidx, double* cval, uint64_t cap, cudaStream_t s) {
+    k_quantize<FT, SOA, KT><<<grid_for(n), 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st,
+                                                         static_cast<KT*>(key), rel, cidx, cval, cap);
+}
+
+template <typename FT, bool SOA>
+static void launch_minmax(const void* pts, uint64_t n, uint32_t D, EncState* st, cudaStream_t s) {
+    dim3 g(grid_for(n, 256, 148u * 8u), D);
+    k_minmax<FT, SOA><<<g, 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st);
+}
+
+chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype, chain_layout layout, uint64_t n,
+                          uint32_t dims, double eb, int64_t p, int64_t threshold, int bl, int l1, int l2,
+                          uint32_t bytes_per_lane, size_t* out_len) {
+    cudaStream_t stream = ctx->stream;
+    const size_t esz = dtype == CHAIN_F64 ? 8 : 4;
+    const uint64_t nd = n * dims;
+    const int64_t p_eff = bl ? p : 1;
+    if (bytes_per_lane == 0) bytes_per_lane = 1024;
+
+    chain_status st_ = ensure_state(ctx, sizeof(EncState));
+    if (st_ != CHAIN_OK) return st_;
+    EncState* st = static_cast<EncState*>(ctx->state_dev);
+    EncState* hs = static_cast<EncState*>(ctx->state_host);
+
+    // ---- frame arena (sizes known from n and dims)
+    const uint64_t corr_cap = std::min<uint64_t>(nd, 1ull << 20);
+    const uint64_t sort_counts = radix_counts_elems(std::max<uint64_t>(n, corr_cap));
+    const uint64_t hist_stride = kRansMaxAlphabet;
+    size_t need = 0;
+    const bool host_input = !is_device_ptr(points);
+    if (host_input) need += Arena::need(nd, esz);
+    const uint64_t nsort = std::max<uint64_t>(n, corr_cap);
+    need += Arena::need(n, 8) + Arena::need(nsort, 8) * 2;  // keys (index order), sort ping-pong
+    need += Arena::need(nsort, 4) * 2;                      // sort values ping-pong
+    need += Arena::need(sort_counts, 4);
+    need += Arena::need(scan_tiles(std::max<uint64_t>(sort_counts, nd)) + 16, 8);
+    need += Arena::need(nd, 4) * 4;           // rel, rec, keep, diff
+    need += Arena::need(n, 4) * 2;            // idrel, choice2
+    need += Arena::need(corr_cap, 8) * 4;     // corrections idx/val + sorted copies
+    need += Arena::need(hist_stride * kStreams, 4) * 3;  // hist, prob, cum
+    need += Arena::need(64 * kStreams, 4) * 2;
+    need += 64 * 256;
+    CHAIN_CUDA(ctx->frame.reserve(need));
+    Arena& A = ctx->frame;
+    const void* pts = points;
+    if (host_input) {
+        void* d = A.take<uint8_t>(nd * esz);
+        CHAIN_CUDA(cudaMemcpyAsync(d, points, nd * esz, cudaMemcpyHostToDevice, stream));
+        pts = d;
+    }
+    uint64_t* key_idx = A.take<uint64_t>(n);
+    uint64_t* key_a = A.take<uint64_t>(nsort);
+    uint64_t* key_b = A.take<uint64_t>(nsort);
+    uint32_t* val_a = A.take<uint32_t>(nsort);
+    uint32_t* val_b = A.take<uint32_t>(nsort);
+    uint32_t* counts = A.take<uint32_t>(sort_counts);
+    uint64_t* scanbuf = A.take<uint64_t>(scan_tiles(std::max<uint64_t>(sort_counts, nd)) + 16);
+    uint32_t* rel = A.take<uint32_t>(nd);
+    uint32_t* rec = A.take<uint32_t>(nd);
+    uint32_t* keep = A.take<uint32_t>(nd);
+    uint32_t* diff = A.take<uint32_t>(nd);
+    uint32_t* idrel = A.take<uint32_t>(n);
+    uint32_t* choice2 = A.take<uint32_t>(n);
+    uint64_t* corr_idx = A.take<uint64_t>(corr_cap);
+    double* corr_val = A.take<double>(corr_cap);
+    uint64_t* corr_idx_s = A.take<uint64_t>(corr_cap);
+    double* corr_val_s = A.take<double>(corr_cap);
+    uint32_t* hist = A.take<uint32_t>(hist_stride * kStreams);
+    uint32_t* prob = A.take<uint32_t>(hist_stride * kStreams);
+    uint32_t* cum = A.take<uint32_t>(hist_stride * kStreams);
+    uint32_t* tag_prob = A.take<uint32_t>(64 * kStreams);
+    uint32_t* tag_cum = A.take<uint32_t>(64 * kStreams);
+    if (!tag_cum) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder frame arena too small");
+
+    k_init_state<<<1, 1, 0, stream>>>(st, dims, n, eb, static_cast<uint64_t>(p_eff), threshold);
+    CHAIN_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * hist_stride * kStreams, stream));
+
+    // ---- phase 1: extrema and quantization parameters
+    const bool soa = layout == CHAIN_SOA;
+    if (dtype == CHAIN_F32) soa ? launch_minmax<float, true>(pts, n, dims, st, stream)
+                            : launch_minmax<float, false>(pts, n, dims, st, stream);
+    else soa ? launch_minmax<double, true>(pts, n, dims, st, stream)
+             : launch_minmax<double, false>(pts, n, dims, st, stream);
+    k_qparams<<<1, 1, 0, stream>>>(st);
+    CHAIN_LAUNCH_CHECK("encoder phase 1");
+    CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
+    CHAIN_CUDA(cudaStreamSynchronize(stream));
+    if (hs->err) return status_from_err(hs->err);
+    const int key_bits = hs->key_bits;
+    const bool wide = key_bits > 32;
+
+    // ---- phase 2: quantize, sort, level 1, level 2, statistics, plan
+#define CHAIN_Q(FT, SOA_, KT) launch_quantize<FT, SOA_, KT>(pts, n, dims, st, key_idx, rel, corr_idx, corr_val, corr_cap, stream)
+    if (dtype == CHAIN_F32) {
+        if (soa) { if (wide) CHAIN_Q(float, true, uint64_t); else CHAIN_Q(float, true, uint32_t); }
+        else { if (wide) CHAIN_Q(float, false, uint64_t); else CHAIN_Q(float, false, uint32_t); }
+    } else {
+        if (soa) { if (wide) CHAIN_Q(double, true, uint64_t); else CHAIN_Q(double, true, uint32_t); }
+        else { if (wide) CHAIN_Q(double, false, uint64_t); else CHAIN_Q(double, false, uint32_t); }
+    }
+#undef CHAIN_Q
+    CHAIN_LAUNCH_CHECK("quantize");
+
+    if (l1) {
+        if (wide) {
+            const bool in_b = radix_sort_pairs<uint64_t>(key_idx, key_a, val_a, key_b, val_b, n, key_bits, counts,
+                                                         reinterpret_cast<uint32_t*>(scanbuf), stream);
+            k_level1<uint64_t><<<grid_for(n), 256, 0, stream>>>(in_b ? key_b : key_a, in_b ? val_b : val_a, n, st, idrel);
+        } else {
+            uint32_t* k32 = reinterpret_cast<uint32_t*>(key_idx);
+            uint32_t* ka = reinterpret_cast<uint32_t*>(key_a);
+            uint32_t* kb = reinterpret_cast<uint32_t*>(key_b);
+            const bool in_b = radix_sort_pairs<uint32_t>(k32, ka, val_a, kb, val_b, n, key_bits, counts,
+                                                         reinterpret_cast<uint32_t*>(scanbuf), stream);
+            k_level1<uint32_t><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel);
+        }
+    } else {
+        CHAIN_CUDA(cudaMemsetAsync(idrel, 0, sizeof(uint32_t) * n, stream));
+    }
+    CHAIN_LAUNCH_CHECK("level 1");
+    uint32_t* scan32 = reinterpret_cast<uint32_t*>(scanbuf);
+    if (wide)
+        device_exclusive_scan<uint32_t>(ExplicitIn<uint64_t>{idrel}, ExplicitOut<uint64_t>{key_idx, st, rec}, n,
+                                        scan32, &st->B, stream);
+    else
+        device_exclusive_scan<uint32_t>(ExplicitIn<uint32_t>{idrel},
+                                        ExplicitOut<uint32_t>{reinterpret_cast<uint32_t*>(key_idx), st, rec}, n,
+                                        scan32, &st->B, stream);
+    k_l2_stats<<<grid_for(n), 256, 0, stream>>>(rec, st);
+    k_l2_params<<<1, 1, 0, stream>>>(st);
+    device_exclusive_scan<uint32_t>(Level2In{rec, st, l2}, Level2Out{rec, st, choice2, keep, diff}, n, scan32,
+                                    &st->ndiff, stream);
+    k_l2_counts<<<1, 1, 0, stream>>>(st);
+    CHAIN_LAUNCH_CHECK("level 2");
+    // The level-2 scan covers n >= B entries; its functors ignore entries j >= B (read
+    // from the device), so no host round trip is needed for B.
+
+    StreamRefs refs;
+    refs.s[0] = StreamRef{idrel, 1, nullptr, n};
+    refs.s[1] = StreamRef{diff, dims, &st->ndiff, 0};
+    refs.s[2] = StreamRef{keep, dims, &st->nkeep, 0};
+    refs.s[3] = StreamRef{choice2, 1, &st->B, 0};
+    refs.s[4] = StreamRef{rel, dims, nullptr, n};
+    k_stream_stats<<<dim3(grid_for(n, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st);
+    k_value_hist<<<dim3(grid_for(nd, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, hist, hist_stride);
+    k_tables<<<dim3(kStreams, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob,
+                                                               tag_cum);
+    k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane);
+    CHAIN_LAUNCH_CHECK("plan");
+    CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
+    CHAIN_CUDA(cudaStreamSynchronize(stream));
+    if (hs->err) return status_from_err(hs->err);
+    if (hs->ncorr > corr_cap)
+        return set_err(CHAIN_ERR_UNSUPPORTED, "more exact corrections than this build buffers (" +
+                                                  std::to_string(hs->ncorr) + ")");
+
+    // ---- phase 3: coding buffers
+    uint64_t slots_total = 0, packed_total = 0, tags_total = 0, total_chunks = 0;
+    uint64_t slot_cap[kStreams] = {0}, slot_off[kStreams] = {0}, packed_off[kStreams] = {0},
+             packed_stride[kStreams] = {0}, tags_off[kStreams] = {0};
+    for (int s = 0; s < kStreams; ++s) {
+        const StreamChoice& c = hs->ch[s];
+        if (c.enc == kEncRaw || c.enc == kEncTagged) {
+            slot_cap[s] = ((3 * c.sec_S + 64) + 15) & ~15ull;
+            slot_off[s] = slots_total;
+            slots_total += slot_cap[s] * c.sec_chunks;
+            total_chunks += c.sec_chunks;
+        }
+        if (c.enc == kEncFixed) {
+            uint64_t maxw = 0;
+            for (uint32_t d = 0; d < c.dims; ++d) maxw = std::max<uint64_t>(maxw, c.width[d]);
+            packed_stride[s] = ((c.records * maxw + 31) / 32 + 1) * 4;
+            packed_off[s] = packed_total;
+            packed_total += packed_stride[s] * c.dims;
+        }
+        if (c.enc == kEncTagged) {
+            packed_off[s] = packed_total;
+            packed_total += ((c.packed_bits + 31) / 32 + 2) * 4;
+            tags_off[s] = tags_total;
+            tags_total += c.records;
+        }
+    }
+    const uint64_t table_stride = 4 * kRansMaxAlphabet + 64;
+    const uint64_t max_pieces = total_chunks + 64;
+    uint64_t bound = header_bytes(dims) + 20 + 16 * hs->ncorr;
+    for (int s = 0; s < kStreams; ++s) {
+        const StreamChoice& c = hs->ch[s];
+        bound += 12 + 13 + 1 + 9ull * c.dims;
+        if (c.enc == kEncFixed) bound += packed_stride[s] * c.dims;
+        if (c.enc == kEncRaw || c.enc == kEncTagged)
+            bound += 64 + 3ull * kRansMaxAlphabet + 132ull * c.sec_chunks + slot_cap[s] * c.sec_chunks;
+        if (c.enc == kEncTagged) bound += 8 + (c.packed_bits + 7) / 8;
+    }
+    size_t need2 = Arena::need(slots_total, 1) + Arena::need(packed_total, 1) + Arena::need(tags_total + 1, 4) +
+                   Arena::need(total_chunks + 1, 4) + Arena::need(total_chunks * 32 + 1, 4) +
+                   Arena::need(table_stride * kStreams, 1) + Arena::need(max_pieces, sizeof(Piece)) +
+                   Arena::need(bound, 1) + 8 * 256;
+    CHAIN_CUDA(ctx->coded.reserve(need2));
+    Arena& C = ctx->coded;
+    uint8_t* slots = C.take<uint8_t>(slots_total + 1);
+    uint8_t* packed = C.take<uint8_t>(packed_total + 1);
+    uint32_t* tags = C.take<uint32_t>(tags_total + 1);
+    uint32_t* chunk_len = C.take<uint32_t>(total_chunks + 1);
+    uint32_t* states = C.take<uint32_t>(total_chunks * 32 + 1);
+    uint8_t* tables = C.take<uint8_t>(table_stride * kStreams);
+    Piece* pieces = C.take<Piece>(max_pieces);
+    uint8_t* container = C.take<uint8_t>(bound);
+    if (!container) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder coding arena too small");
+    if (packed_total) CHAIN_CUDA(cudaMemsetAsync(packed, 0, packed_total, stream));
+
+    // exact corrections in increasing index order
+    if (hs->ncorr) {
+        const uint64_t nc = hs->ncorr;
+        const int bits = std::max(1, bitlen64(nd - 1));
+        uint64_t* ka = reinterpret_cast<uint64_t*>(key_a);
+        uint64_t* kb2 = reinterpret_cast<uint64_t*>(key_b);
+        const bool in_b = radix_sort_pairs<uint64_t>(corr_idx, ka, val_a, kb2, val_b, nc, bits, counts,
+                                                     reinterpret_cast<uint32_t*>(scanbuf), stream);
+        k_gather_corrections<<<grid_for(nc), 256, 0, stream>>>(in_b ? val_b : val_a, in_b ? kb2 : ka, corr_val,
+                                                               corr_idx_s, corr_val_s, nc);
+    }
+
+    RansJobs jobs{};
+    jobs.njobs = 0;
+    uint32_t first = 0;
+    AssemblyIn ain{};
+    ain.table_bytes = tables;
+    ain.table_stride = table_stride;
+    ain.corr_idx = corr_idx_s;
+    ain.corr_val = corr_val_s;
+    ain.input_dtype = static_cast<uint8_t>(esz);
+    uint64_t chunk_base = 0;
+    for (int s = 0; s < kStreams; ++s) {
+        const StreamChoice& c = hs->ch[s];
+        const StreamRef& r = refs.s[s];
+        if (c.enc == kEncFixed) {
+            for (uint32_t d = 0; d < c.dims; ++d) {
+                const uint64_t nwords = (c.records * c.width[d] + 31) / 32;
+                uint32_t* words = reinterpret_cast<uint32_t*>(packed + packed_off[s] + packed_stride[s] * d);
+                k_pack_fixed<<<grid_for(nwords), 256, 0, stream>>>(r.data, c.dims, d, c.records,
+                                                                     hs->st[s].minv[d], c.width[d], words, nwords);
+                k_words_to_bytes<<<grid_for(nwords), 256, 0, stream>>>(words, nwords);
+            }
+            ain.packed[s] = packed + packed_off[s];
+            ain.packed_dim_stride[s] = packed_stride[s];
+        }
+        const uint32_t* symbols = r.data;
+        if (c.enc == kEncTagged) {
+            uint32_t* tg = tags + tags_off[s];
+            k_tags<<<grid_for(c.records), 256, 0, stream>>>(r.data, c.dims, c.records, tg);
+            uint32_t* words = reinterpret_cast<uint32_t*>(packed + packed_off[s]);
+            device_exclusive_scan<uint64_t>(TagBitsIn{tg, c.dims}, TagPackOut{r.data, tg, c.dims, words}, c.records,
+                                            scanbuf, static_cast<uint64_t*>(nullptr), stream);
+            const uint64_t nwords = (c.packed_bits + 31) / 32;
+            k_words_to_bytes<<<grid_for(nwords), 256, 0, stream>>>(words, nwords);
+            ain.packed[s] = packed + packed_off[s];
+            symbols = tg;
+        }
+        if (c.enc == kEncRaw || c.enc == kEncTagged) {
+            RansJob& jb = jobs.job[jobs.njobs++];
+            jb.sym = symbols;
+            jb.count = c.sec_count;
+            jb.prob = c.enc == kEncRaw ? prob + hist_stride * s : tag_prob + 64 * s;
+            jb.cum = c.enc == kEncRaw ? cum + hist_stride * s : tag_cum + 64 * s;
+            jb.prec = c.sec_prec;
+            jb.chunks = c.sec_chunks;
+            jb.S = c.sec_S;
+            jb.bytes = slots + slot_off[s];
+            jb.slot_cap = slot_cap[s];
+            jb.chunk_len = chunk_len + chunk_base;
+            jb.states = states + chunk_base * 32;
+            jb.first_chunk = first;
+            first += c.sec_chunks;
+            ain.chunk_len[s] = jb.chunk_len;
+            ain.states[s] = jb.states;
+            ain.slots[s] = jb.bytes;
+            ain.slot_cap[s] = slot_cap[s];
+            chunk_base += c.sec_chunks;
+        }
+    }
+    jobs.total_chunks = first;
+    k_serialize_tables<<<1, 32, 0, stream>>>(st, prob, tag_prob, hist_stride, tables, table_stride);
+    if (jobs.total_chunks) {
+        const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((jobs.total_chunks + 3) / 4, 148u * 64u));
+        rans_encode_kernel<<<blocks, 128, 0, stream>>>(jobs, &st->err);
+    }
+    CHAIN_LAUNCH_CHECK("entropy coding");
+    k_layout<<<1, 1, 0, stream>>>(st, ain, container, pieces, static_cast<uint32_t>(max_pieces));
+    k_copy_pieces<<<148u * 8u, 256, 0, stream>>>(pieces, st, container);
+    CHAIN_LAUNCH_CHECK("assembly");
+    CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
+    CHAIN_CUDA(cudaStreamSynchronize(stream));
+    if (hs->err) return status_from_err(hs->err);
+    if (hs->total_bytes > bound) return set_err(CHAIN_ERR_DEVICE, "container exceeds its bound");
+    ctx->result = container;
+    ctx->result_len = hs->total_bytes;
+    ctx->dbg = EncodeDebug{idrel, diff, keep, choice2, rel, n, hs->ndiff, hs->nkeep, hs->B, dims};
+    *out_len = hs->total_bytes;
+    return CHAIN_OK;
+}
+
+}  // namespace chain

@@ -1,0 +1,127 @@
+/*
+ * chain_b200 -- C ABI of the B200-native Chain compressor (order-preserving,
+ * error-bounded lossy compression of particle coordinates).
+ *
+ * This is the drop-in boundary for the reference's GPU compress/decompress path.
+ * Every entry point takes plain pointers and sizes.  Host or device buffers are
+ * both accepted wherever a buffer is passed (the library asks the CUDA runtime
+ * which one it got).  Errors never abort the process: each call returns a status
+ * and leaves a message for chain_last_error_message().
+ *
+ * Reference interfaces replaced (paths within the reference project):
+ *   chain_compress      <- lcps_gpu_cpp.lcps_compress2_gpu
+ *                          (cu/chain/lcps_gpu_cpp.cu:718-1091, module :1095-1102),
+ *                          wrapped by chain_caller.chain_gpu (chain_caller.py:38-40)
+ *   chain_decompress    <- lcps_gpu_decompress_ans.lcps_decompress_gpu
+ *                          (cu/decompress/lcps_gpu_decompress_ans.cu:2701-2896,
+ *                          module :2898-2921), wrapped by chain_caller.gpu_decompress
+ *                          (chain_caller.py:33-35)
+ * Integer semantics follow the reference CPU encoder cpp/chain/lcps_cpp.cpp:2017-2338
+ * bit for bit (FP64 quantization, level-1 chaining, level-2 block differencing).
+ */
+#ifndef CHAIN_B200_H
+#define CHAIN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHAIN_B200_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define CHAIN_API __attribute__((visibility("default")))
+#else
+#define CHAIN_API
+#endif
+
+/* Status codes.  They mirror the reference's validation classes: std::invalid_argument
+ * (CHAIN_ERR_INVALID_ARGUMENT) and std::runtime_error for everything else. */
+typedef enum chain_status {
+    CHAIN_OK = 0,
+    CHAIN_ERR_INVALID_ARGUMENT = 1, /* eb <= 0, p <= 0, bad shape, bad options        */
+    CHAIN_ERR_NONFINITE_INPUT = 2,  /* lcps_cpp.cpp:2075 "coordinates must be finite" */
+    CHAIN_ERR_QUANT_OVERFLOW = 3,   /* quantized value outside the supported range    */
+    CHAIN_ERR_CORRUPT_STREAM = 4,   /* decoder: container failed validation           */
+    CHAIN_ERR_DEVICE = 5,           /* CUDA runtime error                             */
+    CHAIN_ERR_OUT_OF_MEMORY = 6,    /* device arena or host allocation failed         */
+    CHAIN_ERR_UNSUPPORTED = 7,      /* valid input outside this build's limits        */
+    CHAIN_ERR_BUFFER_TOO_SMALL = 8  /* caller buffer smaller than the result          */
+} chain_status;
+
+typedef enum chain_dtype { CHAIN_F32 = 4, CHAIN_F64 = 8 } chain_dtype;
+
+/* CHAIN_SOA: coordinates as (D, N), C-contiguous -- the layout lcps_compress2_gpu takes.
+ * CHAIN_AOS: coordinates as (N, D), C-contiguous -- the layout lcps_compress2 takes. */
+typedef enum chain_layout { CHAIN_SOA = 0, CHAIN_AOS = 1 } chain_layout;
+
+typedef struct chain_ctx chain_ctx;
+
+/* Options.  Zero-initialise, set struct_size = sizeof(chain_opts), then override.
+ * bl/l1/l2 are the reference CPU encoder's ablation switches (lcps_cpp.cpp:2340-2355):
+ * a negative value means "default" (enabled). */
+typedef struct chain_opts {
+    uint32_t struct_size;
+    int32_t bl;                     /* block partitioning (p used as given; else p = 1)   */
+    int32_t l1;                     /* level-1 chaining                                   */
+    int32_t l2;                     /* level-2 block differencing                         */
+    uint32_t rans_bytes_per_lane;   /* entropy-stage lane sizing; 0 = library default     */
+    uint32_t reserved[11];
+} chain_opts;
+
+/* Creates a context bound to CUDA device `device`.  `cuda_stream` is a cudaStream_t
+ * (NULL = a stream owned by the context).  The context owns a device arena that
+ * grows on demand and is reused across calls; calls on one context are serialised
+ * by the caller. */
+CHAIN_API chain_status chain_ctx_create(int device, void* cuda_stream, chain_ctx** out);
+CHAIN_API void chain_ctx_destroy(chain_ctx* ctx);
+
+/* Message of the last failed call on this thread ("" if none). */
+CHAIN_API const char* chain_last_error_message(void);
+
+/* Upper bound of the container size for n points of `dims` coordinates. */
+CHAIN_API size_t chain_compress_bound(uint64_t n, uint32_t dims);
+
+/* Compresses n points of `dims` coordinates (float32 or float64) with absolute error
+ * bound eb, block size p and level-1 threshold `threshold`.  `points` may be host or
+ * device memory.  On success the container stays in the context and *out_len is its
+ * size; fetch it with chain_result_copy or read it in place at chain_result_device_ptr.
+ * Synchronous: returns after the device work is complete. */
+CHAIN_API chain_status chain_compress(chain_ctx* ctx, const void* points, chain_dtype dtype,
+                            chain_layout layout, uint64_t n, uint32_t dims, double eb,
+                            int64_t p, int64_t threshold, const chain_opts* opts,
+                            size_t* out_len);
+
+/* Copies the last container of this context to dst (host or device). */
+CHAIN_API chain_status chain_result_copy(chain_ctx* ctx, void* dst, size_t capacity);
+
+/* Device address of the last container of this context (valid until the next call). */
+CHAIN_API const void* chain_result_device_ptr(const chain_ctx* ctx);
+
+/* Reads N, D and the stored input dtype of a container held in HOST memory. */
+CHAIN_API chain_status chain_peek(const void* container, size_t len, uint64_t* n, uint32_t* dims,
+                        chain_dtype* input_dtype);
+
+/* Decompresses a container (host or device memory) into `out` (host or device),
+ * which must hold n*dims values of out_dtype in out_layout.  CHAIN_F64 output
+ * reproduces the reference CPU decoder bit for bit (lcps_cpp.cpp:1963-1993);
+ * CHAIN_F32 output is that value rounded to float32. */
+CHAIN_API chain_status chain_decompress(chain_ctx* ctx, const void* container, size_t len,
+                              chain_dtype out_dtype, chain_layout out_layout, void* out,
+                              size_t out_capacity_bytes, uint64_t* n, uint32_t* dims);
+
+/* Debug/parity entry: after chain_compress on this context, copies the encoder's
+ * integer streams to host buffers (each may be NULL).  Layout is record-major
+ * (point-major) int64, matching the order the reference feeds its entropy stage
+ * (lcps_cpp.cpp:970-986):  idrel[n], diff[ndiff*dims], keep[nkeep*dims],
+ * choice2[nblocks], rel[n*dims]; counts are returned through the pointers. */
+CHAIN_API chain_status chain_debug_streams(chain_ctx* ctx, int64_t* idrel, int64_t* diff,
+                                 uint64_t* ndiff, int64_t* keep, uint64_t* nkeep,
+                                 int64_t* choice2, uint64_t* nblocks, int64_t* rel);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHAIN_B200_H */

@@ -1,0 +1,125 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle, bit for bit.
+
+For every case: the five integer streams the GPU encoder produced equal the oracle's
+(the restatement of cpp/chain/lcps_cpp.cpp:2017-2250), the GPU decoder's float64
+output equals the oracle decoder's bit for bit, max |err| <= eb, and the container is
+within 1% of the reference CPU Chain's LCP2 size when the reference modules are built.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from cases import GPU_CASES, case
+from chaincompressor_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+
+
+def _soa(pts):
+    return np.ascontiguousarray(pts.T)
+
+
+@pytest.mark.parametrize("name", GPU_CASES)
+def test_streams_and_decode_bit_exact(codec, name):
+    pts, eb, p, t, kw = case(name)
+    n, d = pts.shape
+    data = codec.compress(_soa(pts), eb, p, t, layout=N.CHAIN_SOA, **kw)
+    got = codec.debug_streams(n, d)
+    want = oracle.streams(pts, eb, p, t, **kw)
+    for k in ("idrel", "diff", "keep", "choice2", "rel"):
+        assert got[k].shape == want[k].shape, (k, got[k].shape, want[k].shape)
+        assert np.array_equal(got[k], want[k]), k
+    dec = codec.decompress(data)
+    ref_dec = oracle.decode(want)
+    assert np.array_equal(dec.view(np.uint64), ref_dec.view(np.uint64))
+    err = np.abs(dec - pts.astype(np.float64)).max()
+    assert err <= eb
+    # SoA float32 output is the float64 result rounded
+    dec32 = codec.decompress(data, dtype=np.float32, layout=N.CHAIN_SOA)
+    assert np.array_equal(dec32, ref_dec.T.astype(np.float32))
+
+
+@pytest.mark.parametrize("name", ["column", "blobs200k", "traj_f64_e4_p1", "blobs_clipped", "uniform_p64_t25"])
+def test_size_within_one_percent_of_reference(codec, name):
+    if not oracle.ref_available():
+        pytest.skip("reference CPU modules not built")
+    pts, eb, p, t, kw = case(name)
+    ours = codec.compress(_soa(pts), eb, p, t, layout=N.CHAIN_SOA, **kw)
+    ref = oracle.ref_compress(pts, eb, p, t, **kw)
+    assert len(ours) <= 1.01 * len(ref), (len(ours), len(ref))
+
+
+def test_aos_and_host_device_inputs_agree(codec):
+    import torch
+    pts, eb, p, t, _ = case("blobs200k")
+    a = codec.compress(pts, eb, p, t, layout=N.CHAIN_AOS)
+    b = codec.compress(_soa(pts), eb, p, t, layout=N.CHAIN_SOA)
+    dev = torch.from_numpy(_soa(pts)).cuda()
+    c = codec.compress(dev, eb, p, t, layout=N.CHAIN_SOA)
+    assert a == b == c
+
+
+def test_deterministic(codec):
+    pts, eb, p, t, _ = case("column")
+    outs = {codec.compress(_soa(pts), eb, p, t, layout=N.CHAIN_SOA) for _ in range(3)}
+    assert len(outs) == 1
+
+
+def test_errors(codec):
+    pts, eb, p, t, _ = case("column")
+    with pytest.raises(N.ChainError) as e:
+        codec.compress(_soa(pts), -1.0, p, t, layout=N.CHAIN_SOA)
+    assert e.value.status == N.CHAIN_ERR_INVALID_ARGUMENT
+    with pytest.raises(N.ChainError) as e:
+        codec.compress(_soa(pts), eb, 0, t, layout=N.CHAIN_SOA)
+    assert e.value.status == N.CHAIN_ERR_INVALID_ARGUMENT
+    bad = pts.copy()
+    bad[17, 1] = np.nan
+    with pytest.raises(N.ChainError) as e:
+        codec.compress(_soa(bad), eb, p, t, layout=N.CHAIN_SOA)
+    assert e.value.status == N.CHAIN_ERR_NONFINITE_INPUT
+    # the context stays usable after errors
+    data = codec.compress(_soa(pts), eb, p, t, layout=N.CHAIN_SOA)
+    assert codec.decompress(data).shape == pts.shape
+
+
+def test_corrupt_containers_are_rejected(codec):
+    pts, eb, p, t, _ = case("column")
+    data = bytearray(codec.compress(_soa(pts), eb, p, t, layout=N.CHAIN_SOA))
+    rng = np.random.default_rng(0)
+    rejected = 0
+    for trial in range(40):
+        bad = bytearray(data)
+        if trial % 4 == 0:
+            bad = bad[: rng.integers(1, len(bad))]
+        else:
+            for _ in range(int(rng.integers(1, 6))):
+                k = int(rng.integers(0, len(bad)))
+                bad[k] ^= int(rng.integers(1, 256))
+        try:
+            out = codec.decompress(bytes(bad))
+        except N.ChainError as e:
+            assert e.status in (N.CHAIN_ERR_CORRUPT_STREAM, N.CHAIN_ERR_UNSUPPORTED, N.CHAIN_ERR_OUT_OF_MEMORY)
+            rejected += 1
+            continue
+        assert out.shape[1] == pts.shape[1]
+    assert rejected >= 20
+    # still healthy
+    assert np.array_equal(codec.decompress(bytes(data)), codec.decompress(bytes(data)))
+
+
+def test_pybind_surface_matches_reference_api():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from chaincompressor_b200 import chain_caller
+    pts, eb, p, t, _ = case("column")
+    data = chain_caller.chain_gpu(_soa(pts), eb, p, t, 0)
+    assert isinstance(data, bytes) and data[:4] == b"LCG2"
+    out = chain_caller.gpu_decompress(data)
+    assert out.shape == pts.shape and out.dtype == np.float64
+    assert np.abs(out - pts).max() <= eb
+    soa = chain_caller.lcps_gpu_decompress_ans.lcps_decompress_gpu(data, output_soa=True)
+    assert np.array_equal(soa, out.T)
+    with pytest.raises(ValueError):
+        chain_caller.chain_gpu(_soa(pts), 0.0, p, t, 0)
