@@ -30,7 +30,7 @@ CHAIN_SOA, CHAIN_AOS = 0, 1
 # Every entry point declared in include/chain_b200.h.
 EXPORTS = ("chain_ctx_create", "chain_ctx_destroy", "chain_last_error_message", "chain_compress_bound",
            "chain_compress", "chain_result_copy", "chain_result_device_ptr", "chain_peek", "chain_decompress",
-           "chain_debug_streams")
+           "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times")
 
 
 class ChainError(RuntimeError):
@@ -72,7 +72,7 @@ def load() -> ctypes.CDLL:
         L.chain_debug_streams.argtypes = [P, P, P, ctypes.POINTER(u64), P, ctypes.POINTER(u64), P,
                                           ctypes.POINTER(u64), P]
         for f in ("chain_ctx_create", "chain_compress", "chain_result_copy", "chain_peek", "chain_decompress",
-                  "chain_debug_streams"):
+                  "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times"):
             getattr(L, f).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -166,6 +166,16 @@ class Codec:
             "choice2": choice2[: nb_.value].reshape(1, nb_.value),
             "rel": rel.reshape(n, dims).T.copy(),
         }
+
+    def set_stage_timing(self, enabled: bool):
+        _check(self.L.chain_set_stage_timing(self.h, int(bool(enabled))))
+
+    def stage_times(self) -> list:
+        """[(stage, ms)] of the last call (stage timing must be enabled)."""
+        names = (ctypes.c_char_p * 64)()
+        ms = (ctypes.c_float * 64)()
+        k = self.L.chain_stage_times(self.h, names, ms, 64)
+        return [(names[i].decode(), float(ms[i])) for i in range(k)]
 
     # ------------------------------------------------------------ decompress
     def decompress_ptr(self, src_ptr: int, length: int, out_ptr: int, capacity: int, dtype: int = CHAIN_F64,

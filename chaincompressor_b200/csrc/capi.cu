@@ -106,6 +106,7 @@ void chain_ctx_destroy(chain_ctx* ctx) {
     ctx->coded.release();
     ctx->dec.release();
     ctx->pinned.release();
+    ctx->timer.release();
     if (ctx->state_dev) cudaFree(ctx->state_dev);
     if (ctx->state_host) cudaFreeHost(ctx->state_host);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -214,6 +215,22 @@ chain_status chain_debug_streams(chain_ctx* ctx, int64_t* idrel, int64_t* diff, 
     if ((s = fetch(d.choice2, d.nblocks, choice2)) != CHAIN_OK) return s;
     if ((s = fetch(d.rel, d.n * d.dims, rel)) != CHAIN_OK) return s;
     return CHAIN_OK;
+}
+
+chain_status chain_set_stage_timing(chain_ctx* ctx, int enabled) {
+    if (!ctx) return set_err(CHAIN_ERR_INVALID_ARGUMENT, "null context");
+    ctx->timer.enabled = enabled != 0;
+    return CHAIN_OK;
+}
+
+int chain_stage_times(const chain_ctx* ctx, const char** names, float* ms, int max) {
+    if (!ctx) return 0;
+    const int n = ctx->timer.ready > 0 ? ctx->timer.ready - 1 : 0;
+    for (int i = 0; i < n && i < max; ++i) {
+        if (names) names[i] = ctx->timer.names[i + 1];
+        if (ms) ms[i] = ctx->timer.ms[i + 1];
+    }
+    return n;
 }
 
 }  // extern "C"

@@ -65,6 +65,45 @@ struct PinnedBuf {
     }
 };
 
+// Optional per-stage timing with CUDA events on the library stream (enabled per
+// context; used by bench.py for the per-kernel roofline and by tracing).
+struct StageTimer {
+    static constexpr int kMax = 48;
+    bool enabled = false;
+    int count = 0;
+    const char* names[kMax];
+    cudaEvent_t ev[kMax];
+    bool created = false;
+    float ms[kMax];
+    int ready = 0;
+    void begin(cudaStream_t s) {
+        count = 0;
+        ready = 0;
+        if (!enabled) return;
+        if (!created) {
+            for (int i = 0; i < kMax; ++i) cudaEventCreate(&ev[i]);
+            created = true;
+        }
+        mark("start", s);
+    }
+    void mark(const char* name, cudaStream_t s) {
+        if (!enabled || count >= kMax) return;
+        names[count] = name;
+        cudaEventRecord(ev[count], s);
+        ++count;
+    }
+    // Call after the stream was synchronised.
+    void finish() {
+        if (!enabled) return;
+        for (int i = 1; i < count; ++i) cudaEventElapsedTime(&ms[i], ev[i - 1], ev[i]);
+        ready = count;
+    }
+    void release() {
+        if (created) for (int i = 0; i < kMax; ++i) cudaEventDestroy(ev[i]);
+        created = false;
+    }
+};
+
 struct EncodeDebug {
     const uint32_t* idrel = nullptr;
     const uint32_t* diff = nullptr;
@@ -91,6 +130,7 @@ struct chain_ctx {
     const uint8_t* result = nullptr;  // device container of the last compress
     size_t result_len = 0;
     chain::EncodeDebug dbg;
+    chain::StageTimer timer;
 };
 
 namespace chain {

@@ -371,6 +371,8 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     DecState* st = static_cast<DecState*>(ctx->state_dev);
     DecState* hs = static_cast<DecState*>(ctx->state_host);
     const bool host_in = !is_device_ptr(container);
+    StageTimer& T = ctx->timer;
+    T.begin(stream);
     DecodePlan plan;
     if (host_in) {
         if (!parse_container(static_cast<const uint8_t*>(container), len, &plan))
@@ -386,6 +388,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         CHAIN_LAUNCH_CHECK("parse");
         CHAIN_CUDA(cudaMemcpyAsync(&hs->plan, &st->plan, sizeof(DecodePlan), cudaMemcpyDeviceToHost, stream));
         CHAIN_CUDA(cudaStreamSynchronize(stream));
+        T.mark("parse+sync", stream);
         plan = hs->plan;
         if (!plan.ok)
             return set_err(CHAIN_ERR_CORRUPT_STREAM, "LCG2: container failed validation (check at chain_format.h:" +
@@ -436,6 +439,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         hs->plan = plan;
         k_dec_init<<<1, 1, 0, stream>>>(st);
         CHAIN_CUDA(cudaMemcpyAsync(&st->plan, &hs->plan, sizeof(DecodePlan), cudaMemcpyHostToDevice, stream));
+        T.mark("h2d_container", stream);
     }
     uint32_t* streams[kStreams];
     streams[0] = A.take<uint32_t>(N);
@@ -505,10 +509,12 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         k_section_setup<<<nsec, 1024, 0, stream>>>(refs, dcont, st);
         k_lookup<<<dim3(256, nsec), 256, 0, stream>>>(refs, st);
         k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states, d_states_first);
+        T.mark("tables", stream);
         const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((jobs.total_chunks + 3) / 4, 148u * 64u));
         rans_decode_kernel<<<blocks, 128, 0, stream>>>(jobs, &st->err);
     }
     CHAIN_LAUNCH_CHECK("entropy decode");
+    T.mark("rans_decode", stream);
     // ---- tagged and fixed components
     for (int s = 0; s < kStreams; ++s) {
         const CompPlan& c = plan.comp[s];
@@ -524,6 +530,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     }
     if (tags_total) k_check_tagged<<<1, 1, 0, stream>>>(st, st);
     CHAIN_LAUNCH_CHECK("unpack");
+    T.mark("unpack", stream);
 
     // ---- level 2 inverse: choice ranks, then one reset-scan per dimension
     const uint64_t range = static_cast<uint64_t>(plan.wrap_max - plan.wrap_min) + 1;
@@ -536,10 +543,12 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
             Level2TermOut{streams[3], drank, streams[2], streams[1], st, st, d, compact}, B, scanbuf,
             static_cast<uint64_t*>(nullptr), stream, ResetAddOp{range});
     }
+    T.mark("level2_inverse", stream);
     // ---- level 1 inverse
     uint32_t* zeros_dev = reinterpret_cast<uint32_t*>(misc + 2);
     device_exclusive_scan<uint32_t>(ZeroIn{streams[0]}, ZeroRankOut{streams[0], parent, zrank, st, N}, N,
                                     reinterpret_cast<uint32_t*>(scanbuf), zeros_dev, stream);
+    T.mark("zero_ranks", stream);
     int rounds = 1;
     while ((1ull << rounds) < N) ++rounds;
     for (int r = 0; r < rounds + 1; ++r) {
@@ -547,6 +556,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         k_jump_flag<<<1, 1, 0, stream>>>(st, moved);
     }
     CHAIN_LAUNCH_CHECK("levels");
+    T.mark("pointer_jump", stream);
     // ---- reconstruction
     const bool soa = out_layout == CHAIN_SOA;
     const unsigned g = dgrid(N);
@@ -565,11 +575,16 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
                if (plan.exc_count) k_corrections<float, false><<<gc, 256, 0, stream>>>(dcont, st, st, o); }
     }
     CHAIN_LAUNCH_CHECK("reconstruct");
-    if (host_out) CHAIN_CUDA(cudaMemcpyAsync(out, dout, nd * osz, cudaMemcpyDeviceToHost, stream));
+    T.mark("reconstruct", stream);
+    if (host_out) {
+        CHAIN_CUDA(cudaMemcpyAsync(out, dout, nd * osz, cudaMemcpyDeviceToHost, stream));
+        T.mark("d2h_points", stream);
+    }
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, offsetof(DecState, plan), cudaMemcpyDeviceToHost, stream));
     uint32_t counts[4] = {0, 0, 0, 0};
     CHAIN_CUDA(cudaMemcpyAsync(counts, misc + 1, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
     CHAIN_CUDA(cudaStreamSynchronize(stream));
+    T.finish();
     const uint32_t ndiff_seen = counts[0], zeros_seen = counts[2];
     if (hs->err || ndiff_seen != plan.comp[1].records || zeros_seen != B || hs->jump_active)
         return set_err(CHAIN_ERR_CORRUPT_STREAM, "LCG2: invalid integer payload (flags " + std::to_string(hs->err) +

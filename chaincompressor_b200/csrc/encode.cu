@@ -851,10 +851,13 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     CHAIN_CUDA(ctx->frame.reserve(need));
     Arena& A = ctx->frame;
     const void* pts = points;
+    StageTimer& T = ctx->timer;
+    T.begin(stream);
     if (host_input) {
         void* d = A.take<uint8_t>(nd * esz);
         CHAIN_CUDA(cudaMemcpyAsync(d, points, nd * esz, cudaMemcpyHostToDevice, stream));
         pts = d;
+        T.mark("h2d_points", stream);
     }
     uint64_t* key_idx = A.take<uint64_t>(n);
     uint64_t* key_a = A.take<uint64_t>(nsort);
@@ -891,8 +894,10 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
              : launch_minmax<double, false>(pts, n, dims, st, stream);
     k_qparams<<<1, 1, 0, stream>>>(st);
     CHAIN_LAUNCH_CHECK("encoder phase 1");
+    T.mark("extrema", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
     CHAIN_CUDA(cudaStreamSynchronize(stream));
+    T.mark("sync1", stream);
     if (hs->err) return status_from_err(hs->err);
     const int key_bits = hs->key_bits;
     const bool wide = key_bits > 32;
@@ -908,6 +913,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     }
 #undef CHAIN_Q
     CHAIN_LAUNCH_CHECK("quantize");
+    T.mark("quantize", stream);
 
     if (l1) {
         if (wide) {
@@ -926,6 +932,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         CHAIN_CUDA(cudaMemsetAsync(idrel, 0, sizeof(uint32_t) * n, stream));
     }
     CHAIN_LAUNCH_CHECK("level 1");
+    T.mark("sort+level1", stream);
     uint32_t* scan32 = reinterpret_cast<uint32_t*>(scanbuf);
     if (wide)
         device_exclusive_scan<uint32_t>(ExplicitIn<uint64_t>{idrel}, ExplicitOut<uint64_t>{key_idx, st, rec}, n,
@@ -934,12 +941,14 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         device_exclusive_scan<uint32_t>(ExplicitIn<uint32_t>{idrel},
                                         ExplicitOut<uint32_t>{reinterpret_cast<uint32_t*>(key_idx), st, rec}, n,
                                         scan32, &st->B, stream);
+    T.mark("explicit_records", stream);
     k_l2_stats<<<grid_for(n), 256, 0, stream>>>(rec, st);
     k_l2_params<<<1, 1, 0, stream>>>(st);
     device_exclusive_scan<uint32_t>(Level2In{rec, st, l2}, Level2Out{rec, st, choice2, keep, diff}, n, scan32,
                                     &st->ndiff, stream);
     k_l2_counts<<<1, 1, 0, stream>>>(st);
     CHAIN_LAUNCH_CHECK("level 2");
+    T.mark("level2", stream);
     // The level-2 scan covers n >= B entries; its functors ignore entries j >= B (read
     // from the device), so no host round trip is needed for B.
 
@@ -955,8 +964,10 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
                                                                tag_cum);
     k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane);
     CHAIN_LAUNCH_CHECK("plan");
+    T.mark("stats+tables+plan", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
     CHAIN_CUDA(cudaStreamSynchronize(stream));
+    T.mark("sync2", stream);
     if (hs->err) return status_from_err(hs->err);
     if (hs->ncorr > corr_cap)
         return set_err(CHAIN_ERR_UNSUPPORTED, "more exact corrections than this build buffers (" +
@@ -1087,17 +1098,24 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         }
     }
     jobs.total_chunks = first;
+    T.mark("corrections+packing", stream);
     k_serialize_tables<<<1, 32, 0, stream>>>(st, prob, tag_prob, hist_stride, tables, table_stride);
+    T.mark("serialize_tables", stream);
     if (jobs.total_chunks) {
         const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((jobs.total_chunks + 3) / 4, 148u * 64u));
         rans_encode_kernel<<<blocks, 128, 0, stream>>>(jobs, &st->err);
     }
     CHAIN_LAUNCH_CHECK("entropy coding");
+    T.mark("rans_encode", stream);
     k_layout<<<1, 1, 0, stream>>>(st, ain, container, pieces, static_cast<uint32_t>(max_pieces));
     k_copy_pieces<<<148u * 8u, 256, 0, stream>>>(pieces, st, container);
     CHAIN_LAUNCH_CHECK("assembly");
+    T.mark("assemble", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
     CHAIN_CUDA(cudaStreamSynchronize(stream));
+    T.mark("sync3", stream);
+    CHAIN_CUDA(cudaStreamSynchronize(stream));
+    T.finish();
     if (hs->err) return status_from_err(hs->err);
     if (hs->total_bytes > bound) return set_err(CHAIN_ERR_DEVICE, "container exceeds its bound");
     ctx->result = container;

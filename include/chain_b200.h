@@ -121,6 +121,13 @@ CHAIN_API chain_status chain_debug_streams(chain_ctx* ctx, int64_t* idrel, int64
                                  uint64_t* ndiff, int64_t* keep, uint64_t* nkeep,
                                  int64_t* choice2, uint64_t* nblocks, int64_t* rel);
 
+/* Stage timing: when enabled, each call records CUDA events between its stages on the
+ * context's stream.  chain_stage_times returns the stages of the last call (name and
+ * milliseconds since the previous stage) and their count.  Tracing aid only: timing
+ * adds one event record per stage. */
+CHAIN_API chain_status chain_set_stage_timing(chain_ctx* ctx, int enabled);
+CHAIN_API int chain_stage_times(const chain_ctx* ctx, const char** names, float* ms, int max);
+
 #ifdef __cplusplus
 }
 #endif
