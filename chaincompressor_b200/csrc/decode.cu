@@ -48,6 +48,7 @@ __global__ void k_parse(const uint8_t* data, uint64_t len, DecState* st) {
 // Per rANS section: token table -> prob/cum, and chunk byte offsets.  One CTA each.
 struct SectionRef {
     const SectionPlan* sec;   // device pointer into the plan
+    uint32_t* scratch;        // table-parse scratch: 8 * (table_len / 64 + 2) u32
     uint32_t* prob;
     uint32_t* cum;
     uint32_t* lookup;
@@ -62,10 +63,9 @@ __global__ void __launch_bounds__(1024) k_section_setup(SectionRefs refs, const 
     const SectionRef R = refs.r[blockIdx.x];
     const SectionPlan& s = *R.sec;
     __shared__ uint64_t red[33];
-    if (threadIdx.x == 0) {
-        if (!parse_table(data + s.table_off, s.table_len, s.alphabet, s.prec, R.prob, R.cum))
-            set_error(&st->err, kErrCorrupt);
-    }
+    if (!parse_table_block(data + s.table_off, s.table_len, s.alphabet, s.prec, R.prob, R.cum, R.scratch) &&
+        threadIdx.x == 0)
+        set_error(&st->err, kErrCorrupt);
     // chunk offsets: exclusive prefix of the u32 chunk lengths
     uint64_t carry = s.payload_off;
     for (uint32_t base = 0; base < s.chunks; base += blockDim.x) {
@@ -404,7 +404,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         return set_err(CHAIN_ERR_BUFFER_TOO_SMALL, "output buffer holds " + std::to_string(out_capacity) +
                                                        " bytes, need " + std::to_string(nd * osz));
     const uint64_t B = plan.comp[3].records;
-    uint64_t max_prec_slots = 0, total_chunks = 0, max_alpha = 0, tags_total = 0;
+    uint64_t max_prec_slots = 0, total_chunks = 0, max_alpha = 0, tags_total = 0, parse_scratch = 0;
     uint64_t tag_off[kStreams] = {0};
     for (int s = 0; s < kStreams; ++s) {
         const CompPlan& c = plan.comp[s];
@@ -412,6 +412,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
             max_prec_slots += 1ull << c.sec.prec;
             total_chunks += c.sec.chunks;
             max_alpha += c.sec.alphabet;
+            parse_scratch += 8ull * (c.sec.table_len / kParseSeg + 2);
         }
         if (c.enc == kEncTagged) {
             tag_off[s] = tags_total;
@@ -428,6 +429,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     need += Arena::need(total_chunks + kStreams + 1, 8) + Arena::need(total_chunks * 32 + 1, 4);
     need += Arena::need(scan_tiles(std::max<uint64_t>(nd, N)) + 16, 8);
     need += Arena::need(16, 8);
+    need += Arena::need(parse_scratch + 1, 4);
     if (host_out) need += Arena::need(nd, osz);
     need += 24 * 256;
     CHAIN_CUDA(ctx->dec.reserve(need));
@@ -459,6 +461,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     uint32_t* states = A.take<uint32_t>(total_chunks * 32 + 1);
     uint64_t* scanbuf = A.take<uint64_t>(scan_tiles(std::max<uint64_t>(nd, N)) + 16);
     uint64_t* misc = A.take<uint64_t>(16);
+    uint32_t* pscratch = A.take<uint32_t>(parse_scratch + 1);
     void* dout = host_out ? A.take<uint8_t>(nd * osz) : out;
     if (!misc || !dout) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "decoder arena too small");
     uint32_t* moved = reinterpret_cast<uint32_t*>(misc);
@@ -468,7 +471,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     SectionRefs refs{};
     RansJobs jobs{};
     uint64_t states_first[kStreams] = {0};
-    uint64_t slot_base = 0, alpha_base = 0, chunk_base = 0, off_base = 0;
+    uint64_t slot_base = 0, alpha_base = 0, chunk_base = 0, off_base = 0, pscr_base = 0;
     uint32_t first = 0;
     int nsec = 0;
     for (int s = 0; s < kStreams; ++s) {
@@ -476,6 +479,8 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         if (c.enc != kEncRaw && c.enc != kEncTagged) continue;
         SectionRef& R = refs.r[nsec];
         R.sec = &st->plan.comp[s].sec;
+        R.scratch = pscratch + pscr_base;
+        pscr_base += 8ull * (c.sec.table_len / kParseSeg + 2);
         R.prob = prob + alpha_base;
         R.cum = cum + alpha_base;
         R.lookup = lookup + slot_base;
@@ -487,14 +492,16 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         jb.cum = R.cum;
         jb.lookup = R.lookup;
         jb.prec = c.sec.prec;
+        jb.alphabet = c.sec.alphabet;
         jb.chunks = c.sec.chunks;
         jb.S = c.sec.S;
         jb.bytes = const_cast<uint8_t*>(dcont);
+        jb.bytes_len = len;
         jb.chunk_off = R.chunk_off;
         jb.states = states + chunk_base * 32;
         jb.out = c.enc == kEncRaw ? streams[s] : tags + tag_off[s];
-        jb.first_chunk = first;
-        first += c.sec.chunks;
+        jb.first_block = first;
+        first += (c.sec.chunks + kRansWarps - 1) / kRansWarps;
         slot_base += 1ull << c.sec.prec;
         alpha_base += c.sec.alphabet;
         chunk_base += c.sec.chunks;
@@ -502,7 +509,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         ++nsec;
     }
     refs.count = nsec;
-    jobs.total_chunks = first;
+    jobs.total_blocks = first;
     uint64_t* d_states_first = misc + 8;   // nsec <= 5 entries -> misc[8..12]
     CHAIN_CUDA(cudaMemcpyAsync(d_states_first, states_first, sizeof(uint64_t) * kStreams, cudaMemcpyHostToDevice, stream));
     if (nsec) {
@@ -510,8 +517,11 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         k_lookup<<<dim3(256, nsec), 256, 0, stream>>>(refs, st);
         k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states, d_states_first);
         T.mark("tables", stream);
-        const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((jobs.total_chunks + 3) / 4, 148u * 64u));
-        rans_decode_kernel<<<blocks, 128, 0, stream>>>(jobs, &st->err);
+        {  // per device, cheap; set on every call
+            CHAIN_CUDA(cudaFuncSetAttribute(rans_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(kRansDecSmem)));
+        }
+        rans_decode_kernel<<<jobs.total_blocks, 32 * kRansWarps, kRansDecSmem, stream>>>(jobs, &st->err);
     }
     CHAIN_LAUNCH_CHECK("entropy decode");
     T.mark("rans_decode", stream);

@@ -72,13 +72,18 @@ struct EncState {
     uint64_t total_bytes;
     uint32_t npieces;
     uint32_t pad2;
+    uint64_t nsegs;
 };
 
+// A byte range copied into the container.  Pieces are cut into kCopySeg-byte
+// segments so that large payloads spread over many CTAs.
 struct Piece {
     const uint8_t* src;
     uint64_t dst;
     uint64_t len;
+    uint64_t seg_begin;   // index of this piece's first segment
 };
+constexpr uint64_t kCopySeg = 4096;
 
 // --------------------------------------------------------------- quantization
 template <typename FT, bool SOA>
@@ -363,6 +368,17 @@ __device__ __forceinline__ uint64_t stream_records(const StreamRef& r) {
     return r.count_dev ? static_cast<uint64_t>(*r.count_dev) : r.count_const;
 }
 
+// Warp-aggregated histogram increment: lanes holding equal values add once.
+__device__ __forceinline__ void warp_hist_add(uint32_t* bins, uint32_t v, bool valid) {
+    const uint32_t active = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    const uint32_t peers = __match_any_sync(active, v);
+    if ((peers & lanemask_lt()) == 0) atomicAdd(&bins[v], static_cast<uint32_t>(__popc(peers)));
+}
+
+// Per-stream statistics: per-dimension min/max, overall max, record tags
+// (max(1, max_d bitlen v)) histogram and their bit total.  Registers hold the
+// extrema; the tag histogram is warp-aggregated in shared memory.
 __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState* st) {
     const int s = blockIdx.y;
     const StreamRef r = refs.s[s];
@@ -374,25 +390,43 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
     if (threadIdx.x == 0) sbits = 0;
     __syncthreads();
     const uint32_t D = r.dims;
+    uint32_t mn[kMaxDims], mx[kMaxDims];
+#pragma unroll
+    for (int d = 0; d < kMaxDims; ++d) { mn[d] = 0xffffffffu; mx[d] = 0; }
     uint64_t bits = 0;
-    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nrec;
-         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t rounds = (nrec + stride - 1) / stride;
+    for (uint64_t rr = 0; rr < rounds; ++rr) {
+        const uint64_t j = rr * stride + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+        const bool valid = j < nrec;
         uint32_t tag = 1;
-        for (uint32_t d = 0; d < D; ++d) {
-            const uint32_t v = r.data[j * D + d];
-            atomicMin(&smin[d], v);
-            atomicMax(&smax[d], v);
-            const uint32_t w = bitlen32(v);
-            tag = w > tag ? w : tag;
+        if (valid) {
+#pragma unroll
+            for (int d = 0; d < kMaxDims; ++d) {
+                if (d < static_cast<int>(D)) {
+                    const uint32_t v = r.data[j * D + d];
+                    mn[d] = v < mn[d] ? v : mn[d];
+                    mx[d] = v > mx[d] ? v : mx[d];
+                    const uint32_t w = bitlen32(v);
+                    tag = w > tag ? w : tag;
+                }
+            }
+            bits += static_cast<uint64_t>(D) * tag;
         }
-        atomicAdd(&stag[tag], 1u);
-        bits += static_cast<uint64_t>(D) * tag;
+        warp_hist_add(stag, tag, valid);
+    }
+#pragma unroll
+    for (int d = 0; d < kMaxDims; ++d) {
+        if (d < static_cast<int>(D)) {
+            const uint32_t a = warp_min(mn[d]), b = warp_max(mx[d]);
+            if ((threadIdx.x & 31) == 0) { atomicMin(&smin[d], a); atomicMax(&smax[d], b); }
+        }
     }
     bits = warp_sum(bits);
     if ((threadIdx.x & 31) == 0 && bits) atomicAdd(&sbits, static_cast<unsigned long long>(bits));
     __syncthreads();
     StreamStats& g = st->st[s];
-    if (threadIdx.x < D) {
+    if (threadIdx.x < D && smax[threadIdx.x] >= smin[threadIdx.x]) {
         atomicMin(&g.minv[threadIdx.x], smin[threadIdx.x]);
         atomicMax(&g.maxv[threadIdx.x], smax[threadIdx.x]);
         atomicMax(&g.maxall, smax[threadIdx.x]);
@@ -404,7 +438,9 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
     if (threadIdx.x == 0 && sbits) atomicAdd(reinterpret_cast<unsigned long long*>(&g.tag_bits), sbits);
 }
 
-// Value histograms for the raw candidate (alphabet = max + 1 < 2^18).
+// Value histograms for the raw candidate (alphabet = max + 1 < 2^18).  Values below
+// kSmemHistBins count in shared memory, larger ones in global memory; both paths are
+// warp-aggregated, so a hot value costs one atomic per warp instead of one per lane.
 constexpr int kSmemHistBins = 8192;
 __global__ void __launch_bounds__(256) k_value_hist(StreamRefs refs, const EncState* st, uint32_t* hist,
                                                      uint64_t hist_stride) {
@@ -417,22 +453,22 @@ __global__ void __launch_bounds__(256) k_value_hist(StreamRefs refs, const EncSt
     uint32_t* h = hist + hist_stride * s;
     const uint64_t nval = nrec * r.dims;
     __shared__ uint32_t sh[kSmemHistBins];
-    const bool use_smem = A <= kSmemHistBins;
-    if (use_smem) {
-        for (uint32_t t = threadIdx.x; t < A; t += blockDim.x) sh[t] = 0;
-        __syncthreads();
+    const uint32_t ns = A < kSmemHistBins ? A : kSmemHistBins;
+    for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) sh[t] = 0;
+    __syncthreads();
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t rounds = (nval + stride - 1) / stride;
+    for (uint64_t rr = 0; rr < rounds; ++rr) {
+        const uint64_t j = rr * stride + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+        const bool valid = j < nval;
+        const uint32_t v = valid ? r.data[j] : 0u;
+        const bool small = v < kSmemHistBins;
+        warp_hist_add(sh, v, valid && small);
+        warp_hist_add(h, v, valid && !small);
     }
-    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nval;
-         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint32_t v = r.data[j];
-        if (use_smem) atomicAdd(&sh[v], 1u);
-        else atomicAdd(&h[v], 1u);
-    }
-    if (use_smem) {
-        __syncthreads();
-        for (uint32_t t = threadIdx.x; t < A; t += blockDim.x)
-            if (sh[t]) atomicAdd(&h[t], sh[t]);
-    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x)
+        if (sh[t]) atomicAdd(&h[t], sh[t]);
 }
 
 // One CTA per (stream, kind): kind 0 = raw value table, kind 1 = tag table.
@@ -617,15 +653,15 @@ __global__ void k_words_to_bytes(uint32_t* words, uint64_t nwords) {
         words[w] = __byte_perm(words[w], 0, 0x0123);
 }
 
-// Serialises every chosen table (one thread per stream).
-__global__ void k_serialize_tables(EncState* st, const uint32_t* prob, const uint32_t* tag_prob,
-                                   uint64_t hist_stride, uint8_t* out, uint64_t out_stride) {
-    const int s = threadIdx.x;
-    if (s >= kStreams) return;
+// Serialises every chosen table (one CTA per stream).
+__global__ void __launch_bounds__(1024) k_serialize_tables(EncState* st, const uint32_t* prob, const uint32_t* tag_prob,
+                                                            uint64_t hist_stride, uint8_t* out, uint64_t out_stride) {
+    const int s = blockIdx.x;
     StreamChoice& c = st->ch[s];
-    c.table_len = 0;
-    if (c.enc == kEncRaw) c.table_len = serialize_table(prob + hist_stride * s, c.sec_alphabet, out + out_stride * s);
-    else if (c.enc == kEncTagged) c.table_len = serialize_table(tag_prob + 64 * s, c.sec_alphabet, out + out_stride * s);
+    uint32_t len = 0;
+    if (c.enc == kEncRaw) len = serialize_table_block(prob + hist_stride * s, c.sec_alphabet, out + out_stride * s);
+    else if (c.enc == kEncTagged) len = serialize_table_block(tag_prob + 64 * s, c.sec_alphabet, out + out_stride * s);
+    if (threadIdx.x == 0) c.table_len = len;
 }
 
 // --------------------------------------------------------------- assembly
@@ -665,10 +701,12 @@ __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* piece
     if (threadIdx.x || blockIdx.x) return;
     Writer w{out, 0};
     uint32_t np = 0;
+    uint64_t segs = 0;
     auto piece = [&](const uint8_t* src, uint64_t len) {
         if (len == 0) return;
-        if (np < max_pieces) pieces[np] = Piece{src, w.pos, len};
+        if (np < max_pieces) pieces[np] = Piece{src, w.pos, len, segs};
         ++np;
+        segs += (len + kCopySeg - 1) / kCopySeg;
         w.pos += len;
     };
     const uint32_t D = st->dims;
@@ -733,15 +771,25 @@ __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* piece
     piece(reinterpret_cast<const uint8_t*>(in.corr_val), 8 * st->ncorr);
     st->total_bytes = w.pos;
     st->npieces = np;
+    st->nsegs = segs;
     if (np > max_pieces) set_error(&st->err, kErrInternal);
 }
 
+// One CTA per 4 KB segment; the piece of a segment is found by binary search.
 __global__ void __launch_bounds__(256) k_copy_pieces(const Piece* pieces, const EncState* st, uint8_t* out) {
     const uint32_t np = st->npieces;
-    for (uint32_t k = blockIdx.x; k < np; k += gridDim.x) {
-        const Piece pc = pieces[k];
+    const uint64_t nsegs = st->nsegs;
+    for (uint64_t g = blockIdx.x; g < nsegs; g += gridDim.x) {
+        uint32_t lo = 0, hi = np - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (pieces[mid].seg_begin <= g) lo = mid; else hi = mid - 1;
+        }
+        const Piece pc = pieces[lo];
+        const uint64_t off = (g - pc.seg_begin) * kCopySeg;
+        const uint64_t end = min(off + kCopySeg, pc.len);
         uint8_t* dst = out + pc.dst;
-        for (uint64_t b = threadIdx.x; b < pc.len; b += blockDim.x) dst[b] = pc.src[b];
+        for (uint64_t b = off + threadIdx.x; b < end; b += blockDim.x) dst[b] = pc.src[b];
     }
 }
 
@@ -1082,14 +1130,15 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
             jb.prob = c.enc == kEncRaw ? prob + hist_stride * s : tag_prob + 64 * s;
             jb.cum = c.enc == kEncRaw ? cum + hist_stride * s : tag_cum + 64 * s;
             jb.prec = c.sec_prec;
+            jb.alphabet = c.sec_alphabet;
             jb.chunks = c.sec_chunks;
             jb.S = c.sec_S;
             jb.bytes = slots + slot_off[s];
             jb.slot_cap = slot_cap[s];
             jb.chunk_len = chunk_len + chunk_base;
             jb.states = states + chunk_base * 32;
-            jb.first_chunk = first;
-            first += c.sec_chunks;
+            jb.first_block = first;
+            first += (c.sec_chunks + kRansWarps - 1) / kRansWarps;
             ain.chunk_len[s] = jb.chunk_len;
             ain.states[s] = jb.states;
             ain.slots[s] = jb.bytes;
@@ -1097,13 +1146,16 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
             chunk_base += c.sec_chunks;
         }
     }
-    jobs.total_chunks = first;
+    jobs.total_blocks = first;
     T.mark("corrections+packing", stream);
-    k_serialize_tables<<<1, 32, 0, stream>>>(st, prob, tag_prob, hist_stride, tables, table_stride);
+    k_serialize_tables<<<kStreams, 1024, 0, stream>>>(st, prob, tag_prob, hist_stride, tables, table_stride);
     T.mark("serialize_tables", stream);
-    if (jobs.total_chunks) {
-        const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((jobs.total_chunks + 3) / 4, 148u * 64u));
-        rans_encode_kernel<<<blocks, 128, 0, stream>>>(jobs, &st->err);
+    if (jobs.total_blocks) {
+        {  // per device, cheap; set on every call
+            CHAIN_CUDA(cudaFuncSetAttribute(rans_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(kRansEncSmem)));
+        }
+        rans_encode_kernel<<<jobs.total_blocks, 32 * kRansWarps, kRansEncSmem, stream>>>(jobs, &st->err);
     }
     CHAIN_LAUNCH_CHECK("entropy coding");
     T.mark("rans_encode", stream);

@@ -188,128 +188,331 @@ __device__ inline void build_rans_table(const uint32_t* __restrict__ hist, uint3
     __syncthreads();
 }
 
-// Serialises a probability table into tokens (single thread).  Token forms:
-//   p in [1, 2^6):  1 byte  p<<2
-//   p in [2^6,2^14):2 bytes (p<<2)|1, p>>6
-//   p in [2^14,..): 3 bytes (p<<2)|2, p>>6, p>>14
-//   zero run of k in [1,64]: 1 byte ((k-1)<<2)|3
-// Returns the number of bytes written.
-__device__ inline uint32_t serialize_table(const uint32_t* prob, uint32_t A, uint8_t* out) {
-    uint32_t o = 0;
-    for (uint32_t s = 0; s < A; ++s) {
-        const uint32_t p = prob[s];
-        if (p == 0) {
-            uint32_t extra = 0;
-            while (extra < 63 && s + extra + 1 < A && prob[s + extra + 1] == 0) ++extra;
-            out[o++] = static_cast<uint8_t>((extra << 2) | 3u);
-            s += extra;
-            continue;
-        }
-        const uint32_t eb = (p >= (1u << 6)) + (p >= (1u << 14));
-        out[o++] = static_cast<uint8_t>((p << 2) | eb);
-        for (uint32_t b = 0; b < eb; ++b) out[o++] = static_cast<uint8_t>(p >> (8 * (b + 1) - 2));
+// Probability-table tokens (the scheme of lcps_cpp.cpp:686-729 without the leading
+// alphabet varint, which the section header carries):
+//   p in [1, 2^6):   1 byte  p<<2
+//   p in [2^6,2^14): 2 bytes (p<<2)|1, p>>6
+//   p in [2^14, ..): 3 bytes (p<<2)|2, p>>6, p>>14
+//   zero run of k in [1, 64]: 1 byte ((k-1)<<2)|3
+// Both directions run with a whole CTA.
+
+// ------------------------------------------------------------ parallel tables
+
+// Block-wide inclusive max-scan for blockDim.x <= 1024 (values >= 0).
+__device__ inline uint32_t block_inclusive_max(uint32_t v, uint32_t* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v = t > v ? t : v;
     }
-    return o;
+    if (lane == 31) scratch[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nwarps ? scratch[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w = t > w ? t : w;
+        }
+        if (lane < nwarps) scratch[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = warp ? scratch[warp - 1] : 0u;
+    __syncthreads();
+    return before > v ? before : v;
 }
 
-// Parses tokens back (single thread).  Returns false on malformed input.
-__host__ __device__ inline bool parse_table(const uint8_t* in, uint32_t len, uint32_t A, uint32_t prec,
-                                            uint32_t* prob, uint32_t* cum) {
-    uint32_t o = 0, s = 0;
-    uint64_t sum = 0;
-    const uint64_t M = 1ull << prec;
-    while (s < A) {
-        if (o >= len) return false;
-        const uint8_t first = in[o++];
-        const uint32_t tok = first & 3u;
-        if (tok == 3u) {
-            const uint32_t k = (first >> 2) + 1;
-            if (k > A - s) return false;
-            for (uint32_t j = 0; j < k; ++j) { prob[s] = 0; cum[s] = static_cast<uint32_t>(sum); ++s; }
-            continue;
+// Serialises prob[0..A) into tokens with the whole CTA.  Returns the byte count (in
+// every thread).  A zero at s starts a token when (s - run_start) % 64 == 0; the
+// token covers up to 64 zeros of its run.
+__device__ inline uint32_t serialize_table_block(const uint32_t* prob, uint32_t A, uint8_t* out) {
+    __shared__ uint32_t mscratch[33];
+    __shared__ uint64_t sscratch[33];
+    uint32_t carry_last = 0;   // (index of the last nonzero so far) + 1
+    uint64_t carry_off = 0;
+    for (uint32_t base = 0; base < A; base += blockDim.x) {
+        const uint32_t s = base + threadIdx.x;
+        const uint32_t p = s < A ? prob[s] : 1u;
+        // run start of a zero = 1 + index of the last nonzero before it
+        uint32_t key = (s < A && p != 0) ? s + 1 : 0u;
+        uint32_t incl = block_inclusive_max(key, mscratch);
+        incl = incl > carry_last ? incl : carry_last;
+        uint32_t size = 0, extra = 0;
+        if (s < A) {
+            if (p) {
+                extra = (p >= (1u << 6)) + (p >= (1u << 14));
+                size = 1 + extra;
+            } else {
+                const uint32_t run_start = incl;   // no nonzero at s, so incl excludes s
+                if (((s - run_start) & 63u) == 0) {
+                    uint32_t k = 0;
+                    while (k < 63 && s + k + 1 < A && prob[s + k + 1] == 0) ++k;
+                    extra = k;
+                    size = 1;
+                }
+            }
         }
-        uint32_t p = first >> 2;
-        for (uint32_t b = 0; b < tok; ++b) {
-            if (o >= len) return false;
-            p |= static_cast<uint32_t>(in[o++]) << (6 + 8 * b);
+        uint64_t tot;
+        const uint64_t off = carry_off + block_exclusive_sum(static_cast<uint64_t>(size), sscratch, &tot);
+        if (size) {
+            if (p) {
+                out[off] = static_cast<uint8_t>((p << 2) | extra);
+                for (uint32_t b = 0; b < extra; ++b) out[off + 1 + b] = static_cast<uint8_t>(p >> (8 * (b + 1) - 2));
+            } else {
+                out[off] = static_cast<uint8_t>((extra << 2) | 3u);
+            }
         }
-        if (p == 0 || p > M - sum) return false;
-        prob[s] = p;
-        cum[s] = static_cast<uint32_t>(sum);
-        sum += p;
-        ++s;
+        carry_off += tot;
+        // carry for the next chunk: the max over this chunk's keys
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) mscratch[32] = incl;
+        __syncthreads();
+        carry_last = mscratch[32];
+        __syncthreads();
     }
-    return o == len && sum == M;
+    return static_cast<uint32_t>(carry_off);
+}
+
+// Token length and symbol count from a token's first byte.
+__device__ __forceinline__ void token_shape(uint8_t first, uint32_t* bytes, uint32_t* syms) {
+    const uint32_t t = first & 3u;
+    if (t == 3u) { *bytes = 1; *syms = (first >> 2) + 1; }
+    else { *bytes = 1 + t; *syms = 1; }
+}
+
+constexpr uint32_t kParseSeg = 64;
+
+// Parses tokens with the whole CTA.  Every 64-byte segment is parsed speculatively
+// from each of its 3 possible entry offsets (a token is at most 3 bytes); one thread
+// then chains the true entries, a scan gives each segment's first symbol, and the
+// segments are parsed again for real.  scratch: 8 * (len / 64 + 2) u32.
+// Returns false (in every thread) on malformed input.
+__device__ inline bool parse_table_block(const uint8_t* in, uint32_t len, uint32_t A, uint32_t prec,
+                                         uint32_t* prob, uint32_t* cum, uint32_t* scratch) {
+    __shared__ int s_ok;
+    __shared__ uint64_t sscratch[33];
+    const uint32_t nseg = (len + kParseSeg - 1) / kParseSeg;
+    uint32_t* ex = scratch;              // [nseg][3] exit offset into the next segment
+    uint32_t* cnt = scratch + 3 * nseg;  // [nseg][3] symbols
+    uint32_t* entry = scratch + 6 * nseg;
+    uint32_t* first_sym = scratch + 7 * nseg;
+    if (threadIdx.x == 0) s_ok = (len > 0 && A > 0) ? 1 : 0;
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < nseg; k += blockDim.x) {
+        const uint32_t beg = k * kParseSeg, end = min(beg + kParseSeg, len);
+        for (uint32_t e = 0; e < 3; ++e) {
+            uint32_t pos = beg + e, c = 0;
+            while (pos < end) {
+                uint32_t b, sy;
+                token_shape(in[pos], &b, &sy);
+                pos += b;
+                c += sy;
+            }
+            ex[3 * k + e] = pos - end;   // 0..2 (may point past len; checked below)
+            cnt[3 * k + e] = c;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t e = 0;
+        for (uint32_t k = 0; k < nseg; ++k) {
+            entry[k] = e;
+            if (k * kParseSeg + e > len) { s_ok = 0; break; }
+            e = ex[3 * k + e];
+        }
+        // the last segment must end exactly at len
+        if (s_ok && nseg) {
+            const uint32_t k = nseg - 1;
+            if (ex[3 * k + entry[k]] != 0) s_ok = 0;
+        }
+    }
+    __syncthreads();
+    if (!s_ok) return false;
+    // first symbol of each segment
+    uint64_t carry = 0;
+    for (uint32_t base = 0; base < nseg; base += blockDim.x) {
+        const uint32_t k = base + threadIdx.x;
+        const uint64_t c = k < nseg ? cnt[3 * k + entry[k]] : 0;
+        uint64_t tot;
+        const uint64_t ex_sum = block_exclusive_sum(c, sscratch, &tot);
+        if (k < nseg) first_sym[k] = static_cast<uint32_t>(carry + ex_sum > 0xffffffffull ? 0xffffffffu : carry + ex_sum);
+        carry += tot;
+    }
+    if (carry != A) return false;   // uniform: every thread computed the same total
+    const uint64_t M = 1ull << prec;
+    for (uint32_t k = threadIdx.x; k < nseg; k += blockDim.x) {
+        const uint32_t end = min((k + 1) * kParseSeg, len);
+        uint32_t pos = k * kParseSeg + entry[k], s = first_sym[k];
+        bool ok = true;
+        while (pos < end && ok) {
+            const uint8_t first = in[pos];
+            uint32_t b, sy;
+            token_shape(first, &b, &sy);
+            if (pos + b > len || s + sy > A) { ok = false; break; }
+            if ((first & 3u) == 3u) {
+                for (uint32_t j = 0; j < sy; ++j) prob[s + j] = 0;
+            } else {
+                uint32_t p = first >> 2;
+                for (uint32_t j = 1; j < b; ++j) p |= static_cast<uint32_t>(in[pos + j]) << (6 + 8 * (j - 1));
+                if (p == 0 || p > M) ok = false;
+                prob[s] = p;
+            }
+            pos += b;
+            s += sy;
+        }
+        if (!ok) atomicExch(&s_ok, 0);
+    }
+    __syncthreads();
+    if (!s_ok) return false;
+    // cumulative table and total
+    carry = 0;
+    for (uint32_t base = 0; base < A; base += blockDim.x) {
+        const uint32_t s = base + threadIdx.x;
+        const uint64_t p = s < A ? prob[s] : 0;
+        uint64_t tot;
+        const uint64_t e = block_exclusive_sum(p, sscratch, &tot);
+        if (s < A) cum[s] = static_cast<uint32_t>(carry + e > 0xffffffffull ? 0xffffffffu : carry + e);
+        carry += tot;
+    }
+    return carry == M;
 }
 
 // ----------------------------------------------------------------------------- coding
 // A rANS section is coded as `chunks` chunks of S symbols (S a multiple of 32; the last
 // chunk may be shorter).  Per chunk: 32 final states and one byte stream.
 struct RansJob {
-    const uint32_t* sym;      // symbols (encode input / decode output)
+    const uint32_t* sym;      // encode: symbols
+    uint32_t* out;            // decode: symbol output
     uint64_t count;           // symbols
     const uint32_t* prob;     // [A]
     const uint32_t* cum;      // [A]
     const uint32_t* lookup;   // decode: slot -> symbol [M]
     uint32_t prec;
+    uint32_t alphabet;
     uint32_t chunks;
-    uint64_t S;               // symbols per chunk
-    uint8_t* bytes;           // encode: chunk slots (slot_cap each); decode: section payload
+    uint32_t first_block;     // first CTA of this job (kRansWarps chunks per CTA)
+    uint64_t S;               // symbols per chunk (multiple of 32)
+    uint8_t* bytes;           // encode: chunk slots (slot_cap each); decode: container
+    uint64_t bytes_len;       // decode: container length (staged loads stay inside it)
     uint64_t slot_cap;        // encode only
-    const uint64_t* chunk_off;  // decode: byte offset of each chunk in `bytes` (chunks+1)
+    const uint64_t* chunk_off;  // decode: absolute byte offset of each chunk (chunks + 1)
     uint32_t* chunk_len;      // encode: bytes per chunk
-    uint32_t* states;         // encode: out [chunks*32]; decode: in
-    uint32_t* out;            // decode: symbol output
-    uint32_t first_chunk;     // global chunk index of this job's chunk 0
-    uint32_t pad;
+    uint32_t* states;         // encode: out [chunks * 32]; decode: in
 };
 
 constexpr int kMaxRansJobs = 16;
+constexpr int kRansWarps = 4;                 // chunks (warps) per CTA
+constexpr int kRansTile = 32;                 // steps per staged tile
+constexpr uint32_t kSmemTableSyms = 4096;     // prob/cum in shared memory up to this alphabet
+constexpr uint32_t kSmemLookupSlots = 16384;  // u16 decode lookup in shared memory up to this M
+constexpr uint32_t kWindow = 4096;            // decoder byte window per warp
+constexpr size_t kRansEncSmem = kSmemTableSyms * 8 + kRansWarps * 2 * kRansTile * 32 * 4;
+constexpr size_t kRansDecSmem = kSmemTableSyms * 8 + kSmemLookupSlots * 2 + kRansWarps * kWindow;
+
 struct RansJobs {
     RansJob job[kMaxRansJobs];
     uint32_t njobs;
-    uint32_t total_chunks;
+    uint32_t total_blocks;
 };
 
-__device__ inline int find_job(const RansJobs& J, uint32_t g) {
+__device__ __forceinline__ int job_of_block(const RansJobs& J) {
     int j = 0;
-    while (j + 1 < static_cast<int>(J.njobs) && g >= J.job[j + 1].first_chunk) ++j;
+    while (j + 1 < static_cast<int>(J.njobs) && blockIdx.x >= J.job[j + 1].first_block) ++j;
     return j;
 }
 
-// One warp per chunk; any grid (warps stride over the global chunk list).
-static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uint32_t* err) {
+// Loads symbols [tb, te) (a tile of up to 1024) into regs; full tiles use 16-byte loads.
+__device__ __forceinline__ void tile_load(const uint32_t* sym, uint64_t tb, uint64_t te, uint32_t (&r)[32],
+                                          bool& vec) {
     const int lane = threadIdx.x & 31;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t g = gw; g < J.total_chunks; g += nw) {
-        const RansJob& jb = J.job[find_job(J, g)];
-        const uint32_t c = g - jb.first_chunk;
-        const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
-        const uint64_t cend = min(cbeg + jb.S, jb.count);
-        const uint32_t steps = static_cast<uint32_t>((cend - cbeg + 31) / 32);
-        const uint32_t prec = jb.prec;
-        const uint32_t L = 4u << prec;
-        uint32_t x = L;
-        uint8_t* out = jb.bytes + static_cast<uint64_t>(c) * jb.slot_cap;
-        uint64_t pos = jb.slot_cap;
-        bool overflow = false;
-        for (int t = static_cast<int>(steps) - 1; t >= 0; --t) {
-            const uint64_t k = cbeg + static_cast<uint64_t>(t) * 32 + lane;
-            const bool act = k < cend;
+    vec = (te - tb == 1024) && ((reinterpret_cast<uintptr_t>(sym + tb) & 15) == 0);
+    if (vec) {
+        const uint4* p = reinterpret_cast<const uint4*>(sym + tb);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const uint4 v = __ldg(p + lane + 32 * i);
+            r[4 * i] = v.x; r[4 * i + 1] = v.y; r[4 * i + 2] = v.z; r[4 * i + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            const uint64_t k = tb + lane + 32 * i;
+            r[i] = k < te ? __ldg(sym + k) : 0u;
+        }
+    }
+}
+__device__ __forceinline__ void tile_store(uint32_t* buf, const uint32_t (&r)[32], bool vec) {
+    const int lane = threadIdx.x & 31;
+    if (vec) {
+        uint4* p = reinterpret_cast<uint4*>(buf);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) p[lane + 32 * i] = make_uint4(r[4 * i], r[4 * i + 1], r[4 * i + 2], r[4 * i + 3]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) buf[lane + 32 * i] = r[i];
+    }
+}
+
+// Encoder: one warp per chunk, kRansWarps chunks of one job per CTA.  The job's table
+// sits in shared memory when small; symbols are prefetched one 32-step tile ahead
+// into shared memory; the warp's byte counts are prefix-summed with two ballots
+// (0..3 bytes per lane).
+static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uint32_t* err) {
+    extern __shared__ __align__(16) uint8_t rsm[];
+    const RansJob& jb = J.job[job_of_block(J)];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint2* tab = reinterpret_cast<uint2*>(rsm);
+    const bool smem_tab = jb.alphabet <= kSmemTableSyms;
+    if (smem_tab)
+        for (uint32_t s = threadIdx.x; s < jb.alphabet; s += blockDim.x) tab[s] = make_uint2(jb.prob[s], jb.cum[s]);
+    __syncthreads();
+    const uint32_t c = (blockIdx.x - jb.first_block) * kRansWarps + warp;
+    if (c >= jb.chunks) return;
+    uint32_t* buf = reinterpret_cast<uint32_t*>(rsm + kSmemTableSyms * 8) + warp * 2 * 1024;
+    const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
+    const uint64_t cend = min(cbeg + jb.S, jb.count);
+    const uint32_t steps = static_cast<uint32_t>((cend - cbeg + 31) / 32);
+    const uint32_t ntiles = (steps + kRansTile - 1) / kRansTile;
+    const uint32_t prec = jb.prec;
+    const uint32_t L = 4u << prec;
+    const uint32_t lt = lanemask_lt();
+    uint32_t x = L;
+    uint8_t* out = jb.bytes + static_cast<uint64_t>(c) * jb.slot_cap;
+    uint64_t pos = jb.slot_cap;
+    bool overflow = false;
+    uint32_t r[32];
+    bool vec;
+    {
+        const uint64_t tb = cbeg + 1024ull * (ntiles - 1);
+        tile_load(jb.sym, tb, min(tb + 1024, cend), r, vec);
+        tile_store(buf + ((ntiles - 1) & 1) * 1024, r, vec);
+        __syncwarp();
+    }
+    for (int k = static_cast<int>(ntiles) - 1; k >= 0 && !overflow; --k) {
+        if (k > 0) {
+            const uint64_t tb = cbeg + 1024ull * (k - 1);
+            tile_load(jb.sym, tb, min(tb + 1024, cend), r, vec);
+        }
+        const uint32_t* cur = buf + (k & 1) * 1024;
+        const int t_hi = min(static_cast<int>(steps) - 1, 32 * k + 31);
+        for (int t = t_hi; t >= 32 * k; --t) {
+            const uint64_t kk = cbeg + static_cast<uint64_t>(t) * 32 + lane;
+            const bool act = kk < cend;
             uint32_t nb = 0, f = 1, cm = 0;
             if (act) {
-                const uint32_t s = __ldg(jb.sym + k);
-                f = __ldg(jb.prob + s);
-                cm = __ldg(jb.cum + s);
+                const uint32_t s = cur[(t - 32 * k) * 32 + lane];
+                if (smem_tab) { const uint2 e = tab[s]; f = e.x; cm = e.y; }
+                else { f = __ldg(jb.prob + s); cm = __ldg(jb.cum + s); }
                 const uint32_t xmax = f << 10;  // ((L >> prec) << 8) * f
-                uint32_t y = x;
-                while (y >= xmax) { y >>= 8; ++nb; }
+                if (x >= xmax) { nb = 1; if ((x >> 8) >= xmax) { nb = 2; if ((x >> 16) >= xmax) nb = 3; } }
             }
-            const uint32_t inc = warp_inclusive_sum(nb);
-            const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+            const uint32_t b0 = __ballot_sync(0xffffffffu, nb & 1u), b1 = __ballot_sync(0xffffffffu, nb & 2u);
+            const uint32_t pre = __popc(b0 & lt) + 2 * __popc(b1 & lt);
+            const uint32_t total = __popc(b0) + 2 * __popc(b1);
             if (total > pos) { overflow = true; break; }
-            const uint64_t base = pos - total + (inc - nb);
+            const uint64_t base = pos - total + pre;
             for (uint32_t j = 0; j < nb; ++j) out[base + j] = static_cast<uint8_t>(x >> (8 * (nb - 1 - j)));
             pos -= total;
             if (act) {
@@ -317,64 +520,111 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
                 x = (x / f) * (1u << prec) + (x % f) + cm;
             }
         }
-        if (__any_sync(0xffffffffu, overflow)) {
-            if (lane == 0) set_error(err, kErrInternal);
-            continue;
+        if (k > 0) {
+            __syncwarp();
+            tile_store(buf + ((k - 1) & 1) * 1024, r, vec);
+            __syncwarp();
         }
-        jb.states[static_cast<uint64_t>(c) * 32 + lane] = x;
-        if (lane == 0) jb.chunk_len[c] = static_cast<uint32_t>(jb.slot_cap - pos);
     }
+    if (__any_sync(0xffffffffu, overflow)) {
+        if (lane == 0) set_error(err, kErrInternal);
+        return;
+    }
+    jb.states[static_cast<uint64_t>(c) * 32 + lane] = x;
+    if (lane == 0) jb.chunk_len[c] = static_cast<uint32_t>(jb.slot_cap - pos);
 }
 
-// One warp per chunk.  Every read is bounds-checked against the chunk's byte range;
-// a malformed stream sets kErrCorrupt and the warp stops.
-static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uint32_t* err) {
-    if (*err) return;  // a failed table parse leaves no valid lookup table
+// Refills a warp's byte window so that it starts at `pos` rounded down to 16 bytes.
+__device__ __forceinline__ void window_fill(uint8_t* win, const uint8_t* bytes, uint64_t len, uint64_t wbase) {
     const int lane = threadIdx.x & 31;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t g = gw; g < J.total_chunks; g += nw) {
-        const RansJob& jb = J.job[find_job(J, g)];
-        const uint32_t c = g - jb.first_chunk;
-        const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
-        const uint64_t cend = min(cbeg + jb.S, jb.count);
-        const uint32_t steps = static_cast<uint32_t>((cend - cbeg + 31) / 32);
-        const uint32_t prec = jb.prec;
-        const uint32_t M = 1u << prec, L = 4u << prec;
-        const uint8_t* in = jb.bytes;
-        uint64_t pos = jb.chunk_off[c];
-        const uint64_t end = jb.chunk_off[c + 1];
-        uint32_t x = jb.states[static_cast<uint64_t>(c) * 32 + lane];
-        bool bad = (x < L) || (static_cast<uint64_t>(x) >= (static_cast<uint64_t>(L) << 8));
-        if (__any_sync(0xffffffffu, bad)) {
-            if (lane == 0) set_error(err, kErrCorrupt);
-            continue;
+    const bool vec = wbase + kWindow <= len && ((reinterpret_cast<uintptr_t>(bytes + wbase) & 15) == 0);
+    if (vec) {
+        const uint4* p = reinterpret_cast<const uint4*>(bytes + wbase);
+        uint4* w = reinterpret_cast<uint4*>(win);
+#pragma unroll
+        for (int i = 0; i < static_cast<int>(kWindow / 16 / 32); ++i) w[lane + 32 * i] = __ldg(p + lane + 32 * i);
+    } else {
+        for (uint32_t i = lane; i < kWindow; i += 32) {
+            const uint64_t a = wbase + i;
+            win[i] = a < len ? bytes[a] : 0;
         }
-        for (uint32_t t = 0; t < steps; ++t) {
-            const uint64_t k = cbeg + static_cast<uint64_t>(t) * 32 + lane;
-            const bool act = k < cend;
-            uint32_t nb = 0;
-            if (act) {
-                const uint32_t slot = x & (M - 1);
-                const uint32_t s = __ldg(jb.lookup + slot);
-                x = __ldg(jb.prob + s) * (x >> prec) + slot - __ldg(jb.cum + s);
-                jb.out[k] = s;
-                // a valid step leaves x >= 4, so at most 3 bytes are needed; more means
-                // a corrupt stream (and a zero state would never terminate)
-                uint32_t y = x;
-                while (y < L && nb < 4) { y <<= 8; ++nb; }
-                if (nb == 4) { bad = true; nb = 0; }
-            }
-            const uint32_t inc = warp_inclusive_sum(nb);
-            const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
-            if (__any_sync(0xffffffffu, bad) || pos + total > end) { bad = true; break; }
-            const uint64_t base = pos + (inc - nb);
-            for (uint32_t j = 0; j < nb; ++j) x = (x << 8) | in[base + j];
-            pos += total;
-        }
-        bad = bad || (x != L) || (pos != end);
-        if (__any_sync(0xffffffffu, bad) && lane == 0) set_error(err, kErrCorrupt);
     }
+    __syncwarp();
+}
+
+// Decoder: one warp per chunk, kRansWarps chunks of one job per CTA.  The slot->symbol
+// lookup and prob/cum live in shared memory when small; the chunk's byte stream is read
+// through a 4 KB shared-memory window refilled every 32 steps (a step consumes at most
+// 96 bytes).  Every read is bounds-checked against the chunk's byte range; a malformed
+// stream sets kErrCorrupt and the warp stops.
+static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uint32_t* err) {
+    extern __shared__ __align__(16) uint8_t rsm[];
+    __shared__ int s_skip;
+    if (threadIdx.x == 0) s_skip = *err != 0;  // a failed table parse leaves no valid lookup
+    __syncthreads();
+    if (s_skip) return;
+    const RansJob& jb = J.job[job_of_block(J)];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t prec = jb.prec;
+    const uint32_t M = 1u << prec, L = 4u << prec;
+    uint2* tab = reinterpret_cast<uint2*>(rsm);
+    uint16_t* look = reinterpret_cast<uint16_t*>(rsm + kSmemTableSyms * 8);
+    uint8_t* win = rsm + kSmemTableSyms * 8 + kSmemLookupSlots * 2 + warp * kWindow;
+    const bool smem_tab = jb.alphabet <= kSmemTableSyms;
+    const bool smem_look = M <= kSmemLookupSlots && jb.alphabet <= 65536;
+    if (smem_tab)
+        for (uint32_t s = threadIdx.x; s < jb.alphabet; s += blockDim.x) tab[s] = make_uint2(jb.prob[s], jb.cum[s]);
+    if (smem_look)
+        for (uint32_t s = threadIdx.x; s < M; s += blockDim.x) look[s] = static_cast<uint16_t>(jb.lookup[s]);
+    __syncthreads();
+    const uint32_t c = (blockIdx.x - jb.first_block) * kRansWarps + warp;
+    if (c >= jb.chunks) return;
+    const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
+    const uint64_t cend = min(cbeg + jb.S, jb.count);
+    const uint32_t steps = static_cast<uint32_t>((cend - cbeg + 31) / 32);
+    const uint32_t lt = lanemask_lt();
+    uint64_t pos = jb.chunk_off[c];
+    const uint64_t end = jb.chunk_off[c + 1];
+    uint32_t x = jb.states[static_cast<uint64_t>(c) * 32 + lane];
+    bool bad = (x < L) || (static_cast<uint64_t>(x) >= (static_cast<uint64_t>(L) << 8)) || end > jb.bytes_len ||
+               pos > end;
+    if (__any_sync(0xffffffffu, bad)) {
+        if (lane == 0) set_error(err, kErrCorrupt);
+        return;
+    }
+    uint64_t wbase = pos & ~15ull;
+    window_fill(win, jb.bytes, jb.bytes_len, wbase);
+    for (uint32_t t = 0; t < steps; ++t) {
+        if ((t & (kRansTile - 1)) == 0 && pos - wbase > kWindow - 3 * 1024) {
+            __syncwarp();
+            wbase = pos & ~15ull;
+            window_fill(win, jb.bytes, jb.bytes_len, wbase);
+        }
+        const uint64_t k = cbeg + static_cast<uint64_t>(t) * 32 + lane;
+        const bool act = k < cend;
+        uint32_t nb = 0;
+        if (act) {
+            const uint32_t slot = x & (M - 1);
+            const uint32_t s = smem_look ? look[slot] : __ldg(jb.lookup + slot);
+            uint32_t f, cm;
+            if (smem_tab) { const uint2 e = tab[s]; f = e.x; cm = e.y; }
+            else { f = __ldg(jb.prob + s); cm = __ldg(jb.cum + s); }
+            x = f * (x >> prec) + slot - cm;
+            jb.out[k] = s;
+            nb = (x < L) + (x < (L >> 8)) + (x < (L >> 16));
+        }
+        const uint32_t b0 = __ballot_sync(0xffffffffu, nb & 1u), b1 = __ballot_sync(0xffffffffu, nb & 2u);
+        const uint32_t pre = __popc(b0 & lt) + 2 * __popc(b1 & lt);
+        const uint32_t total = __popc(b0) + 2 * __popc(b1);
+        if (pos + total > end) { bad = true; break; }
+        const uint32_t wo = static_cast<uint32_t>(pos - wbase) + pre;
+        for (uint32_t j = 0; j < nb; ++j) x = (x << 8) | win[wo + j];
+        if (act && x < L) bad = true;
+        pos += total;
+        if (__any_sync(0xffffffffu, bad)) break;
+    }
+    bad = bad || (x != L) || (pos != end);
+    if (__any_sync(0xffffffffu, bad) && lane == 0) set_error(err, kErrCorrupt);
 }
 
 }  // namespace chain
