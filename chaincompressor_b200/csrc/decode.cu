@@ -518,6 +518,8 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states, d_states_first);
         T.mark("tables", stream);
         {  // per device, cheap; set on every call
+            CHAIN_CUDA(cudaFuncSetAttribute(rans_decode_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            cudaSharedmemCarveoutMaxShared));
             CHAIN_CUDA(cudaFuncSetAttribute(rans_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             static_cast<int>(kRansDecSmem)));
         }

@@ -1152,6 +1152,8 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     T.mark("serialize_tables", stream);
     if (jobs.total_blocks) {
         {  // per device, cheap; set on every call
+            CHAIN_CUDA(cudaFuncSetAttribute(rans_encode_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            cudaSharedmemCarveoutMaxShared));
             CHAIN_CUDA(cudaFuncSetAttribute(rans_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             static_cast<int>(kRansEncSmem)));
         }
