@@ -42,7 +42,7 @@ class ChainError(RuntimeError):
 class ChainOpts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("bl", ctypes.c_int32), ("l1", ctypes.c_int32),
                 ("l2", ctypes.c_int32), ("rans_bytes_per_lane", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 11)]
+                ("rans_max_steps", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 10)]
 
 
 _LIB = None
@@ -115,11 +115,13 @@ class Codec:
 
     # -------------------------------------------------------------- compress
     def compress_ptr(self, ptr: int, dtype: int, layout: int, n: int, dims: int, eb: float, p: int,
-                     threshold: int, bl=True, l1=True, l2=True, rans_bytes_per_lane: int = 0) -> int:
+                     threshold: int, bl=True, l1=True, l2=True, rans_bytes_per_lane: int = 0,
+                     rans_max_steps: int = 0) -> int:
         o = ChainOpts()
         o.struct_size = ctypes.sizeof(ChainOpts)
         o.bl, o.l1, o.l2 = int(bl), int(l1), int(l2)
         o.rans_bytes_per_lane = rans_bytes_per_lane
+        o.rans_max_steps = rans_max_steps
         out_len = ctypes.c_size_t()
         _check(self.L.chain_compress(self.h, ctypes.c_void_p(ptr), dtype, layout, n, dims, float(eb), int(p),
                                      int(threshold), ctypes.byref(o), ctypes.byref(out_len)))

@@ -140,7 +140,7 @@ chain_status chain_compress(chain_ctx* ctx, const void* points, chain_dtype dtyp
         return set_err(CHAIN_ERR_UNSUPPORTED, "this build supports at most 16 dimensions");
     if (n >= (1ull << 31)) return set_err(CHAIN_ERR_UNSUPPORTED, "this build supports fewer than 2^31 points");
     int bl = 1, l1 = 1, l2 = 1;
-    uint32_t bpl = 0;
+    uint32_t bpl = 0, steps = 0;
     if (opts) {
         if (opts->struct_size < offsetof(chain_opts, reserved))
             return set_err(CHAIN_ERR_INVALID_ARGUMENT, "chain_opts.struct_size too small");
@@ -148,12 +148,13 @@ chain_status chain_compress(chain_ctx* ctx, const void* points, chain_dtype dtyp
         if (opts->l1 >= 0) l1 = opts->l1 != 0;
         if (opts->l2 >= 0) l2 = opts->l2 != 0;
         bpl = opts->rans_bytes_per_lane;
+        steps = opts->rans_max_steps;
     }
     DeviceGuard g(ctx->device);
     ctx->result = nullptr;
     ctx->result_len = 0;
     g_last_error.clear();
-    return encode_frame(ctx, points, dtype, layout, n, dims, eb, p, threshold, bl, l1, l2, bpl, out_len);
+    return encode_frame(ctx, points, dtype, layout, n, dims, eb, p, threshold, bl, l1, l2, bpl, steps, out_len);
 }
 
 chain_status chain_result_copy(chain_ctx* ctx, void* dst, size_t capacity) {

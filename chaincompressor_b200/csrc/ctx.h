@@ -155,7 +155,7 @@ chain_status ensure_state(chain_ctx* ctx, size_t bytes);
 
 chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype, chain_layout layout,
                           uint64_t n, uint32_t dims, double eb, int64_t p, int64_t threshold,
-                          int bl, int l1, int l2, uint32_t bytes_per_lane, size_t* out_len);
+                          int bl, int l1, int l2, uint32_t bytes_per_lane, uint32_t max_steps, size_t* out_len);
 
 chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, chain_dtype out_dtype,
                           chain_layout out_layout, void* out, size_t out_capacity, uint64_t* n,

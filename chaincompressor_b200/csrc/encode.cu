@@ -493,10 +493,15 @@ __device__ inline uint64_t section_overhead(uint32_t table_bytes, uint32_t chunk
     return 1 + 4 + 4 + static_cast<uint64_t>(table_bytes) + 8 + 4 + static_cast<uint64_t>(chunks) * (4 + 128);
 }
 
-__device__ inline void plan_chunks(uint64_t count, double est_payload, uint32_t bytes_per_lane, uint32_t* chunks,
-                                   uint64_t* S) {
+// Chunking of a rANS section: enough lanes that each carries about bytes_per_lane
+// coded bytes (the 4-byte final state per lane is the size overhead), and enough that
+// no lane codes more than max_steps symbols (the serial depth of the kernel).
+__device__ inline void plan_chunks(uint64_t count, double est_payload, uint32_t bytes_per_lane, uint32_t max_steps,
+                                   uint32_t* chunks, uint64_t* S) {
     uint64_t lanes = static_cast<uint64_t>(est_payload / bytes_per_lane) + 1;
     uint64_t ch = (lanes + 31) / 32;
+    const uint64_t ch_depth = (count + 32ull * max_steps - 1) / (32ull * max_steps);
+    if (ch < ch_depth) ch = ch_depth;
     const uint64_t max_ch = (count + 31) / 32;
     if (ch > max_ch) ch = max_ch;
     if (ch < 1) ch = 1;
@@ -509,7 +514,7 @@ __device__ inline void plan_chunks(uint64_t count, double est_payload, uint32_t 
 
 // Chooses each component's encoding: the smallest estimated size among tagged, fixed
 // and raw (ties in that order, as lcps_cpp.cpp:1150-1170), empty when no records.
-__global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane) {
+__global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, uint32_t max_steps) {
     const int s = threadIdx.x;
     if (s >= kStreams || blockIdx.x) return;
     const StreamRef r = refs.s[s];
@@ -546,7 +551,7 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane) {
         const double payload = t.cost_bits / 8.0;
         uint32_t ch;
         uint64_t S;
-        plan_chunks(nrec, payload, bytes_per_lane, &ch, &S);
+        plan_chunks(nrec, payload, bytes_per_lane, max_steps, &ch, &S);
         c.est[kEncTagged] = 13 + 1 + section_overhead(t.table_bytes, ch) + static_cast<uint64_t>(payload) + 1 + 8 +
                             (g.tag_bits + 7) / 8;
     }
@@ -556,7 +561,7 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane) {
         const double payload = t.cost_bits / 8.0;
         uint32_t ch;
         uint64_t S;
-        plan_chunks(nrec * r.dims, payload, bytes_per_lane, &ch, &S);
+        plan_chunks(nrec * r.dims, payload, bytes_per_lane, max_steps, &ch, &S);
         c.est[kEncRaw] = 13 + section_overhead(t.table_bytes, ch) + static_cast<uint64_t>(payload) + 1;
     }
     uint8_t best = kEncTagged;
@@ -565,7 +570,7 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane) {
     c.enc = best;
     if (best == kEncTagged) {
         const RansTableDev& t = st->tag_tab[s];
-        plan_chunks(nrec, t.cost_bits / 8.0, bytes_per_lane, &c.sec_chunks, &c.sec_S);
+        plan_chunks(nrec, t.cost_bits / 8.0, bytes_per_lane, max_steps, &c.sec_chunks, &c.sec_S);
         c.sec_count = nrec;
         c.sec_prec = t.prec;
         c.sec_alphabet = t.alphabet;
@@ -573,7 +578,7 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane) {
         c.max_width = static_cast<uint8_t>(g.maxtag);
     } else if (best == kEncRaw) {
         const RansTableDev& t = st->raw_tab[s];
-        plan_chunks(nrec * r.dims, t.cost_bits / 8.0, bytes_per_lane, &c.sec_chunks, &c.sec_S);
+        plan_chunks(nrec * r.dims, t.cost_bits / 8.0, bytes_per_lane, max_steps, &c.sec_chunks, &c.sec_S);
         c.sec_count = nrec * r.dims;
         c.sec_prec = t.prec;
         c.sec_alphabet = t.alphabet;
@@ -644,6 +649,14 @@ __global__ void __launch_bounds__(256) k_pack_fixed(const uint32_t* __restrict__
         }
         words[w] = acc;
     }
+}
+
+// Encoder symbol entries of every rANS section (blockIdx.y = job).
+__global__ void __launch_bounds__(256) k_enc_symbols(RansJobs J) {
+    const RansJob& jb = J.job[blockIdx.y];
+    uint4* out = const_cast<uint4*>(jb.etab);
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < jb.alphabet; s += gridDim.x * blockDim.x)
+        out[s] = make_enc_symbol(jb.prob[s], jb.cum[s], jb.prec);
 }
 
 // Big-endian words -> bytes in place (so that byte 0 holds the first 8 bits).
@@ -866,12 +879,13 @@ static void launch_minmax(const void* pts, uint64_t n, uint32_t D, EncState* st,
 
 chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype, chain_layout layout, uint64_t n,
                           uint32_t dims, double eb, int64_t p, int64_t threshold, int bl, int l1, int l2,
-                          uint32_t bytes_per_lane, size_t* out_len) {
+                          uint32_t bytes_per_lane, uint32_t max_steps, size_t* out_len) {
     cudaStream_t stream = ctx->stream;
     const size_t esz = dtype == CHAIN_F64 ? 8 : 4;
     const uint64_t nd = n * dims;
     const int64_t p_eff = bl ? p : 1;
     if (bytes_per_lane == 0) bytes_per_lane = 1024;
+    if (max_steps == 0) max_steps = 2048;
 
     chain_status st_ = ensure_state(ctx, sizeof(EncState));
     if (st_ != CHAIN_OK) return st_;
@@ -1010,7 +1024,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     k_value_hist<<<dim3(grid_for(nd, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, hist, hist_stride);
     k_tables<<<dim3(kStreams, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob,
                                                                tag_cum);
-    k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane);
+    k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps);
     CHAIN_LAUNCH_CHECK("plan");
     T.mark("stats+tables+plan", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
@@ -1048,6 +1062,9 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         }
     }
     const uint64_t table_stride = 4 * kRansMaxAlphabet + 64;
+    uint64_t etab_total = 0;
+    for (int s = 0; s < kStreams; ++s)
+        if (hs->ch[s].enc == kEncRaw || hs->ch[s].enc == kEncTagged) etab_total += hs->ch[s].sec_alphabet;
     const uint64_t max_pieces = total_chunks + 64;
     uint64_t bound = header_bytes(dims) + 20 + 16 * hs->ncorr;
     for (int s = 0; s < kStreams; ++s) {
@@ -1061,7 +1078,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     size_t need2 = Arena::need(slots_total, 1) + Arena::need(packed_total, 1) + Arena::need(tags_total + 1, 4) +
                    Arena::need(total_chunks + 1, 4) + Arena::need(total_chunks * 32 + 1, 4) +
                    Arena::need(table_stride * kStreams, 1) + Arena::need(max_pieces, sizeof(Piece)) +
-                   Arena::need(bound, 1) + 8 * 256;
+                   Arena::need(bound, 1) + Arena::need(etab_total + 1, 16) + 9 * 256;
     CHAIN_CUDA(ctx->coded.reserve(need2));
     Arena& C = ctx->coded;
     uint8_t* slots = C.take<uint8_t>(slots_total + 1);
@@ -1072,7 +1089,9 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     uint8_t* tables = C.take<uint8_t>(table_stride * kStreams);
     Piece* pieces = C.take<Piece>(max_pieces);
     uint8_t* container = C.take<uint8_t>(bound);
-    if (!container) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder coding arena too small");
+    uint4* etab = C.take<uint4>(etab_total + 1);
+    if (!container || !etab) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder coding arena too small");
+    uint64_t etab_used = 0;
     if (packed_total) CHAIN_CUDA(cudaMemsetAsync(packed, 0, packed_total, stream));
 
     // exact corrections in increasing index order
@@ -1131,6 +1150,8 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
             jb.cum = c.enc == kEncRaw ? cum + hist_stride * s : tag_cum + 64 * s;
             jb.prec = c.sec_prec;
             jb.alphabet = c.sec_alphabet;
+            jb.etab = etab + etab_used;
+            etab_used += c.sec_alphabet;
             jb.chunks = c.sec_chunks;
             jb.S = c.sec_S;
             jb.bytes = slots + slot_off[s];
@@ -1151,6 +1172,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     k_serialize_tables<<<kStreams, 1024, 0, stream>>>(st, prob, tag_prob, hist_stride, tables, table_stride);
     T.mark("serialize_tables", stream);
     if (jobs.total_blocks) {
+        k_enc_symbols<<<dim3(64, jobs.njobs), 256, 0, stream>>>(jobs);
         {  // per device, cheap; set on every call
             CHAIN_CUDA(cudaFuncSetAttribute(rans_encode_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                             cudaSharedmemCarveoutMaxShared));

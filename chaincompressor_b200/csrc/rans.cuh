@@ -382,7 +382,22 @@ __device__ inline bool parse_table_block(const uint8_t* in, uint32_t len, uint32
 // ----------------------------------------------------------------------------- coding
 // A rANS section is coded as `chunks` chunks of S symbols (S a multiple of 32; the last
 // chunk may be shorter).  Per chunk: 32 final states and one byte stream.
+// Encoder symbol entry (division-free encoding by a precomputed reciprocal, the
+// division-by-invariant-integer method as used in F. Giesen's public-domain rans_byte):
+//   x' = x + bias + q * cmpl_freq,  q = umulhi(x, rcp_freq) >> rcp_shift = floor(x / freq)
+// For freq == 1: rcp_freq = 2^32 - 1, shift 0 (q = x - 1 for x >= 1) and bias = cum + M - 1.
+// Exact for x < 2^31 (here x < 1024 * freq <= 2^30).
+__device__ __forceinline__ uint4 make_enc_symbol(uint32_t freq, uint32_t cum, uint32_t prec) {
+    const uint32_t M = 1u << prec;
+    if (freq < 2) return make_uint4(freq, cum + M - 1, 0xffffffffu, (M - freq));
+    uint32_t shift = 0;
+    while (freq > (1u << shift)) ++shift;
+    const uint32_t rcp = static_cast<uint32_t>(((1ull << (shift + 31)) + freq - 1) / freq);
+    return make_uint4(freq, cum, rcp, (M - freq) | ((shift - 1) << 24));
+}
+
 struct RansJob {
+    const uint4* etab;        // encode: symbol entries [A] (make_enc_symbol)
     const uint32_t* sym;      // encode: symbols
     uint32_t* out;            // decode: symbol output
     uint64_t count;           // symbols
@@ -405,10 +420,11 @@ struct RansJob {
 constexpr int kMaxRansJobs = 16;
 constexpr int kRansWarps = 4;                 // chunks (warps) per CTA
 constexpr int kRansTile = 32;                 // steps per staged tile
-constexpr uint32_t kSmemTableSyms = 4096;     // prob/cum in shared memory up to this alphabet
+constexpr uint32_t kSmemTableSyms = 4096;     // decoder prob/cum in shared memory up to this alphabet
+constexpr uint32_t kSmemEncSyms = 2048;       // encoder entries (16 B) in shared memory up to this alphabet
 constexpr uint32_t kSmemLookupSlots = 16384;  // u16 decode lookup in shared memory up to this M
 constexpr uint32_t kWindow = 4096;            // decoder byte window per warp
-constexpr size_t kRansEncSmem = kSmemTableSyms * 8 + kRansWarps * 2 * kRansTile * 32 * 4;
+constexpr size_t kRansEncSmem = kSmemEncSyms * 16 + kRansWarps * 2 * kRansTile * 32 * 4;
 constexpr size_t kRansDecSmem = kSmemTableSyms * 8 + kSmemLookupSlots * 2 + kRansWarps * kWindow;
 
 struct RansJobs {
@@ -463,14 +479,14 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
     extern __shared__ __align__(16) uint8_t rsm[];
     const RansJob& jb = J.job[job_of_block(J)];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint2* tab = reinterpret_cast<uint2*>(rsm);
-    const bool smem_tab = jb.alphabet <= kSmemTableSyms;
+    uint4* tab = reinterpret_cast<uint4*>(rsm);
+    const bool smem_tab = jb.alphabet <= kSmemEncSyms;
     if (smem_tab)
-        for (uint32_t s = threadIdx.x; s < jb.alphabet; s += blockDim.x) tab[s] = make_uint2(jb.prob[s], jb.cum[s]);
+        for (uint32_t s = threadIdx.x; s < jb.alphabet; s += blockDim.x) tab[s] = jb.etab[s];
     __syncthreads();
     const uint32_t c = (blockIdx.x - jb.first_block) * kRansWarps + warp;
     if (c >= jb.chunks) return;
-    uint32_t* buf = reinterpret_cast<uint32_t*>(rsm + kSmemTableSyms * 8) + warp * 2 * 1024;
+    uint32_t* buf = reinterpret_cast<uint32_t*>(rsm + kSmemEncSyms * 16) + warp * 2 * 1024;
     const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
     const uint64_t cend = min(cbeg + jb.S, jb.count);
     const uint32_t steps = static_cast<uint32_t>((cend - cbeg + 31) / 32);
@@ -500,24 +516,27 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
         for (int t = t_hi; t >= 32 * k; --t) {
             const uint64_t kk = cbeg + static_cast<uint64_t>(t) * 32 + lane;
             const bool act = kk < cend;
-            uint32_t nb = 0, f = 1, cm = 0;
+            uint32_t nb = 0;
+            uint4 e = make_uint4(1, 0, 0, 0);
             if (act) {
                 const uint32_t s = cur[(t - 32 * k) * 32 + lane];
-                if (smem_tab) { const uint2 e = tab[s]; f = e.x; cm = e.y; }
-                else { f = __ldg(jb.prob + s); cm = __ldg(jb.cum + s); }
-                const uint32_t xmax = f << 10;  // ((L >> prec) << 8) * f
-                if (x >= xmax) { nb = 1; if ((x >> 8) >= xmax) { nb = 2; if ((x >> 16) >= xmax) nb = 3; } }
+                e = smem_tab ? tab[s] : __ldg(jb.etab + s);
+                const uint32_t xmax = e.x << 10;  // ((L >> prec) << 8) * freq
+                nb = (x >= xmax) + ((x >> 8) >= xmax) + ((x >> 16) >= xmax);
             }
             const uint32_t b0 = __ballot_sync(0xffffffffu, nb & 1u), b1 = __ballot_sync(0xffffffffu, nb & 2u);
             const uint32_t pre = __popc(b0 & lt) + 2 * __popc(b1 & lt);
             const uint32_t total = __popc(b0) + 2 * __popc(b1);
             if (total > pos) { overflow = true; break; }
-            const uint64_t base = pos - total + pre;
-            for (uint32_t j = 0; j < nb; ++j) out[base + j] = static_cast<uint8_t>(x >> (8 * (nb - 1 - j)));
+            uint8_t* o = out + (pos - total + pre);
+            if (nb == 3) { o[0] = static_cast<uint8_t>(x >> 16); o[1] = static_cast<uint8_t>(x >> 8); o[2] = static_cast<uint8_t>(x); }
+            else if (nb == 2) { o[0] = static_cast<uint8_t>(x >> 8); o[1] = static_cast<uint8_t>(x); }
+            else if (nb == 1) { o[0] = static_cast<uint8_t>(x); }
             pos -= total;
             if (act) {
                 x >>= 8 * nb;
-                x = (x / f) * (1u << prec) + (x % f) + cm;
+                const uint32_t q = __umulhi(x, e.z) >> (e.w >> 24);
+                x = x + e.y + q * (e.w & 0xffffffu);
             }
         }
         if (k > 0) {

@@ -67,8 +67,11 @@ typedef struct chain_opts {
     int32_t bl;                     /* block partitioning (p used as given; else p = 1)   */
     int32_t l1;                     /* level-1 chaining                                   */
     int32_t l2;                     /* level-2 block differencing                         */
-    uint32_t rans_bytes_per_lane;   /* entropy-stage lane sizing; 0 = library default     */
-    uint32_t reserved[11];
+    uint32_t rans_bytes_per_lane;   /* entropy stage: target coded bytes per rANS lane
+                                       (each lane adds a 4-byte state); 0 = default 1024  */
+    uint32_t rans_max_steps;        /* entropy stage: most symbols one lane codes
+                                       (serial depth); 0 = default 2048                   */
+    uint32_t reserved[10];
 } chain_opts;
 
 /* Creates a context bound to CUDA device `device`.  `cuda_stream` is a cudaStream_t
