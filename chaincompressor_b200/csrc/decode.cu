@@ -179,16 +179,34 @@ __global__ void k_check_tagged(const DecState* st_c, DecState* st) {
 }
 
 // ------------------------------------------------------------------- level 2
-// Reset-scan element: bit 63 = "this record is kept" (restart), low 32 bits = offset
-// from wrap_min (kept record) or the modular step -correction (difference record).
+// Reset-scan over the compact block records, three dimensions per pass.  Element j:
+//   kept record       -> restart with its offset from wrap_min
+//   difference record -> add the modular step -correction (mod range)
+// so the inclusive prefix of record j is compact[j] - wrap_min (lcps_cpp.cpp:1890-1934
+// computes the same values sequentially).
+struct L2Vec {
+    uint32_t restart;
+    uint32_t v[3];
+};
 struct ResetAddOp {
-    uint64_t range;
-    __device__ __forceinline__ uint64_t operator()(uint64_t a, uint64_t b) const {
-        if (b >> 63) return b;
-        const uint64_t v = ((a & 0xffffffffull) + (b & 0xffffffffull)) % range;
-        return (a & (1ull << 63)) | v;
+    uint32_t range_lo, range_hi;   // range = wrap_max - wrap_min + 1 <= 2^32
+    __device__ __forceinline__ uint64_t range() const {
+        return static_cast<uint64_t>(range_lo) | (static_cast<uint64_t>(range_hi) << 32);
     }
-    __device__ __forceinline__ static uint64_t identity() { return 0; }
+    __device__ __forceinline__ L2Vec operator()(const L2Vec& a, const L2Vec& b) const {
+        if (b.restart) return b;
+        const uint64_t r = range();
+        L2Vec o;
+        o.restart = a.restart;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            uint64_t s = static_cast<uint64_t>(a.v[k]) + b.v[k];
+            if (s >= r) s -= r;
+            o.v[k] = static_cast<uint32_t>(s);
+        }
+        return o;
+    }
+    __device__ __forceinline__ static L2Vec identity() { return L2Vec{0, {0, 0, 0}}; }
 };
 
 // Choice values are clamped to {0, 1} for the ranks (so every derived index stays in
@@ -208,58 +226,66 @@ struct ChoiceRankOut {
     }
 };
 
+__device__ __forceinline__ int64_t unzigzag(uint64_t sym) {
+    return (sym & 1u) ? -static_cast<int64_t>(sym >> 1) - 1 : static_cast<int64_t>(sym >> 1);
+}
+
 struct Level2TermIn {
-    const uint32_t* choice2;
-    const uint32_t* drank;
-    const uint32_t* keep;
-    const uint32_t* diff;
-    const DecState* st;
-    uint32_t d;
-    __device__ uint64_t operator()(uint64_t j) const {
-        const DecodePlan& P = st->plan;
-        const uint32_t D = P.D;
-        const uint64_t range = static_cast<uint64_t>(P.wrap_max - P.wrap_min) + 1;
-        const uint32_t dr = drank[j];
-        if (choice2[j] == 0) {
-            const int64_t v = keep[static_cast<uint64_t>(j - dr) * D + d];
-            const uint64_t off = static_cast<uint64_t>(v - P.wrap_min);  // validated in Level2TermOut
-            return (1ull << 63) | (off & 0xffffffffull);
-        }
-        const uint64_t sym = diff[static_cast<uint64_t>(dr) * D + d];
-        const int64_t corr = (sym & 1u) ? -static_cast<int64_t>(sym >> 1) - 1 : static_cast<int64_t>(sym >> 1);
-        // offset_j = offset_{j-1} - corr (mod range)
-        const int64_t r = static_cast<int64_t>(range);
-        int64_t step = (-corr) % r;
-        if (step < 0) step += r;
-        return static_cast<uint64_t>(step);
-    }
-};
-struct Level2TermOut {
     const uint32_t* choice2;
     const uint32_t* drank;
     const uint32_t* keep;
     const uint32_t* diff;
     const DecState* stc;
     DecState* st;
-    uint32_t d;
-    uint32_t* compact;   // [B * D]
-    __device__ void operator()(uint64_t j, uint64_t prefix, uint64_t term) const {
+    uint32_t d0;   // first dimension of this pass
+    __device__ L2Vec operator()(uint64_t j) const {
         const DecodePlan& P = stc->plan;
         const uint32_t D = P.D;
-        const uint64_t range = static_cast<uint64_t>(P.wrap_max - P.wrap_min) + 1;
-        // validate the record's raw value (lcps_cpp.cpp:1905-1922)
+        const int64_t r = P.wrap_max - P.wrap_min + 1;
+        const int64_t maxc = r / 2 - ((r & 1) == 0 ? 1 : 0), minc = -(r / 2);
+        const uint32_t dr = drank[j];
+        L2Vec o = ResetAddOp::identity();
+        bool bad = false;
         if (choice2[j] == 0) {
-            const int64_t v = keep[static_cast<uint64_t>(j - drank[j]) * D + d];
-            if (v < P.wrap_min || v > P.wrap_max) set_error(&st->err, kErrCorrupt);
+            o.restart = 1;
+            const uint64_t row = static_cast<uint64_t>(j - dr) * D;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (d0 + k < D) {
+                    const int64_t v = keep[row + d0 + k];
+                    bad |= v < P.wrap_min || v > P.wrap_max;   // lcps_cpp.cpp:1905-1907
+                    o.v[k] = static_cast<uint32_t>(v - P.wrap_min);
+                }
+            }
         } else {
-            const uint64_t sym = diff[static_cast<uint64_t>(drank[j]) * D + d];
-            const int64_t corr = (sym & 1u) ? -static_cast<int64_t>(sym >> 1) - 1 : static_cast<int64_t>(sym >> 1);
-            const int64_t r = static_cast<int64_t>(range);
-            const int64_t maxc = r / 2 - ((r & 1) == 0 ? 1 : 0), minc = -(r / 2);
-            if (corr < minc || corr > maxc) set_error(&st->err, kErrCorrupt);
+            const uint64_t row = static_cast<uint64_t>(dr) * D;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (d0 + k < D) {
+                    const int64_t corr = unzigzag(diff[row + d0 + k]);
+                    bad |= corr < minc || corr > maxc;        // lcps_cpp.cpp:1917-1918
+                    // offset_j = offset_{j-1} - corr (mod range)
+                    o.v[k] = bad ? 0u : static_cast<uint32_t>(corr <= 0 ? -corr : r - corr);
+                }
+            }
         }
-        const uint64_t inc = ResetAddOp{range}(prefix, term);
-        compact[j * D + d] = static_cast<uint32_t>(P.wrap_min + static_cast<int64_t>(inc & 0xffffffffull));
+        if (bad) set_error(&st->err, kErrCorrupt);
+        return o;
+    }
+};
+struct Level2TermOut {
+    const DecState* stc;
+    uint32_t d0;
+    uint32_t* compact;   // [B * D]
+    __device__ void operator()(uint64_t j, const L2Vec& prefix, const L2Vec& term) const {
+        const DecodePlan& P = stc->plan;
+        const uint32_t D = P.D;
+        const ResetAddOp op{static_cast<uint32_t>(P.wrap_max - P.wrap_min + 1),
+                            static_cast<uint32_t>((P.wrap_max - P.wrap_min + 1) >> 32)};
+        const L2Vec inc = op(prefix, term);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (d0 + k < D) compact[j * D + d0 + k] = static_cast<uint32_t>(P.wrap_min + inc.v[k]);
     }
 };
 
@@ -268,31 +294,38 @@ struct ZeroIn {
     const uint32_t* idrel;
     __device__ uint32_t operator()(uint64_t i) const { return idrel[i] == 0 ? 1u : 0u; }
 };
+// Ranks of the explicit points; parents (explicit points are roots and point to
+// themselves); and the list of chained points, whose rank among chained points is
+// i - (explicit points before i).
 struct ZeroRankOut {
     const uint32_t* idrel;
     uint32_t* parent;
     uint32_t* zrank;
+    uint32_t* chained;
     DecState* st;
     uint64_t n;
     __device__ void operator()(uint64_t i, uint32_t pre, uint32_t z) const {
         zrank[i] = pre;
         const uint32_t j = idrel[i];
         if (z) { parent[i] = static_cast<uint32_t>(i); return; }
+        chained[i - pre] = static_cast<uint32_t>(i);
         if (static_cast<uint64_t>(j) >= n - i) { set_error(&st->err, kErrCorrupt); parent[i] = static_cast<uint32_t>(i); return; }
         parent[i] = static_cast<uint32_t>(i + j);
     }
 };
 
-// One pointer-jumping round.  A round that moves no pointer clears jump_active, and every
-// later round returns at once.  Jumps only point forward, so rounds <= ceil(log2 N).
-__global__ void __launch_bounds__(256) k_jump(uint32_t* parent, const uint32_t* idrel, uint64_t n, DecState* st,
-                                               uint32_t* moved) {
+// One pointer-jumping round over the chained points.  A round that moves no pointer
+// clears jump_active, and every later round returns at once.  Jumps only point
+// forward, so ceil(log2 N) rounds reach every root.
+__global__ void __launch_bounds__(256) k_jump(uint32_t* parent, const uint32_t* chained, const uint32_t* zeros,
+                                               uint64_t n, DecState* st, uint32_t* moved) {
     if (!st->jump_active) return;
+    const uint64_t m = n - *zeros;
     bool any = false;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < m;
+         k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t i = chained[k];
         const uint32_t p = parent[i];
-        if (idrel[p] == 0) continue;
         const uint32_t pp = parent[p];
         if (pp != p) { parent[i] = pp; any = true; }
     }
@@ -427,7 +460,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     need += Arena::need(tags_total + 1, 4);
     need += Arena::need(max_prec_slots + 1, 4) + Arena::need(max_alpha + 1, 4) * 2;
     need += Arena::need(total_chunks + kStreams + 1, 8) + Arena::need(total_chunks * 32 + 1, 4);
-    need += Arena::need(scan_tiles(std::max<uint64_t>(nd, N)) + 16, 8);
+    need += Arena::need(scan_scratch_bytes(std::max<uint64_t>(nd, N)), 1);
     need += Arena::need(16, 8);
     need += Arena::need(parse_scratch + 1, 4);
     if (host_out) need += Arena::need(nd, osz);
@@ -459,7 +492,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     uint32_t* cum = A.take<uint32_t>(max_alpha + 1);
     uint64_t* chunk_off = A.take<uint64_t>(total_chunks + kStreams + 1);
     uint32_t* states = A.take<uint32_t>(total_chunks * 32 + 1);
-    uint64_t* scanbuf = A.take<uint64_t>(scan_tiles(std::max<uint64_t>(nd, N)) + 16);
+    uint64_t* scanbuf = reinterpret_cast<uint64_t*>(A.take<uint8_t>(scan_scratch_bytes(std::max<uint64_t>(nd, N))));
     uint64_t* misc = A.take<uint64_t>(16);
     uint32_t* pscratch = A.take<uint32_t>(parse_scratch + 1);
     void* dout = host_out ? A.take<uint8_t>(nd * osz) : out;
@@ -517,13 +550,14 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         k_lookup<<<dim3(256, nsec), 256, 0, stream>>>(refs, st);
         k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states, d_states_first);
         T.mark("tables", stream);
+        rans_plan_smem(jobs, true);
         {  // per device, cheap; set on every call
             CHAIN_CUDA(cudaFuncSetAttribute(rans_decode_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                             cudaSharedmemCarveoutMaxShared));
             CHAIN_CUDA(cudaFuncSetAttribute(rans_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            static_cast<int>(kRansDecSmem)));
+                                            static_cast<int>(rans_dec_smem(jobs))));
         }
-        rans_decode_kernel<<<jobs.total_blocks, 32 * kRansWarps, kRansDecSmem, stream>>>(jobs, &st->err);
+        rans_decode_kernel<<<jobs.total_blocks, 32 * kRansWarps, rans_dec_smem(jobs), stream>>>(jobs, &st->err);
     }
     CHAIN_LAUNCH_CHECK("entropy decode");
     T.mark("rans_decode", stream);
@@ -549,22 +583,23 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     uint32_t* ndiff_dev = reinterpret_cast<uint32_t*>(misc + 1);
     device_exclusive_scan<uint32_t>(ChoiceIn{streams[3]}, ChoiceRankOut{streams[3], drank, st}, B,
                                     reinterpret_cast<uint32_t*>(scanbuf), ndiff_dev, stream);
-    for (uint32_t d = 0; d < D; ++d) {
-        device_exclusive_scan<uint64_t>(
-            Level2TermIn{streams[3], drank, streams[2], streams[1], st, d},
-            Level2TermOut{streams[3], drank, streams[2], streams[1], st, st, d, compact}, B, scanbuf,
-            static_cast<uint64_t*>(nullptr), stream, ResetAddOp{range});
+    const ResetAddOp l2op{static_cast<uint32_t>(range), static_cast<uint32_t>(range >> 32)};
+    for (uint32_t d0 = 0; d0 < D; d0 += 3) {
+        device_exclusive_scan<L2Vec>(Level2TermIn{streams[3], drank, streams[2], streams[1], st, st, d0},
+                                     Level2TermOut{st, d0, compact}, B, reinterpret_cast<L2Vec*>(scanbuf),
+                                     static_cast<L2Vec*>(nullptr), stream, l2op);
     }
     T.mark("level2_inverse", stream);
     // ---- level 1 inverse
     uint32_t* zeros_dev = reinterpret_cast<uint32_t*>(misc + 2);
-    device_exclusive_scan<uint32_t>(ZeroIn{streams[0]}, ZeroRankOut{streams[0], parent, zrank, st, N}, N,
+    uint32_t* chained = drank;  // the choice ranks are no longer needed
+    device_exclusive_scan<uint32_t>(ZeroIn{streams[0]}, ZeroRankOut{streams[0], parent, zrank, chained, st, N}, N,
                                     reinterpret_cast<uint32_t*>(scanbuf), zeros_dev, stream);
     T.mark("zero_ranks", stream);
     int rounds = 1;
     while ((1ull << rounds) < N) ++rounds;
     for (int r = 0; r < rounds + 1; ++r) {
-        k_jump<<<dgrid(N), 256, 0, stream>>>(parent, streams[0], N, st, moved);
+        k_jump<<<dgrid(N), 256, 0, stream>>>(parent, chained, zeros_dev, N, st, moved);
         k_jump_flag<<<1, 1, 0, stream>>>(st, moved);
     }
     CHAIN_LAUNCH_CHECK("levels");

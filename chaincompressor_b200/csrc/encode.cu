@@ -903,7 +903,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     need += Arena::need(n, 8) + Arena::need(nsort, 8) * 2;  // keys (index order), sort ping-pong
     need += Arena::need(nsort, 4) * 2;                      // sort values ping-pong
     need += Arena::need(sort_counts, 4);
-    need += Arena::need(scan_tiles(std::max<uint64_t>(sort_counts, nd)) + 16, 8);
+    need += Arena::need(scan_scratch_bytes(std::max<uint64_t>(sort_counts, nd)), 1);
     need += Arena::need(nd, 4) * 4;           // rel, rec, keep, diff
     need += Arena::need(n, 4) * 2;            // idrel, choice2
     need += Arena::need(corr_cap, 8) * 4;     // corrections idx/val + sorted copies
@@ -927,7 +927,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     uint32_t* val_a = A.take<uint32_t>(nsort);
     uint32_t* val_b = A.take<uint32_t>(nsort);
     uint32_t* counts = A.take<uint32_t>(sort_counts);
-    uint64_t* scanbuf = A.take<uint64_t>(scan_tiles(std::max<uint64_t>(sort_counts, nd)) + 16);
+    uint64_t* scanbuf = reinterpret_cast<uint64_t*>(A.take<uint8_t>(scan_scratch_bytes(std::max<uint64_t>(sort_counts, nd))));
     uint32_t* rel = A.take<uint32_t>(nd);
     uint32_t* rec = A.take<uint32_t>(nd);
     uint32_t* keep = A.take<uint32_t>(nd);
@@ -1173,13 +1173,14 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     T.mark("serialize_tables", stream);
     if (jobs.total_blocks) {
         k_enc_symbols<<<dim3(64, jobs.njobs), 256, 0, stream>>>(jobs);
+        rans_plan_smem(jobs, false);
         {  // per device, cheap; set on every call
             CHAIN_CUDA(cudaFuncSetAttribute(rans_encode_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                             cudaSharedmemCarveoutMaxShared));
             CHAIN_CUDA(cudaFuncSetAttribute(rans_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            static_cast<int>(kRansEncSmem)));
+                                            static_cast<int>(rans_enc_smem(jobs))));
         }
-        rans_encode_kernel<<<jobs.total_blocks, 32 * kRansWarps, kRansEncSmem, stream>>>(jobs, &st->err);
+        rans_encode_kernel<<<jobs.total_blocks, 32 * kRansWarps, rans_enc_smem(jobs), stream>>>(jobs, &st->err);
     }
     CHAIN_LAUNCH_CHECK("entropy coding");
     T.mark("rans_encode", stream);

@@ -7,9 +7,10 @@
 //
 // Each 8-bit pass is three launches: a per-tile digit histogram, a device-wide
 // exclusive scan of the digit-major count table, and a stable scatter.  The scatter
-// ranks keys inside a 4096-key tile with warp match_any + popc (each warp owns a
-// contiguous 512-key slice, processed 32 keys per round in order), so equal digits
-// keep their input order.
+// ranks keys inside a tile with warp match_any + popc (each warp owns a contiguous
+// slice, processed 32 keys per round in order, so equal digits keep their input
+// order), reorders the tile by digit in shared memory, and writes each digit's run
+// to its global position with consecutive threads on consecutive addresses.
 #pragma once
 
 #include "chain_common.cuh"
@@ -18,21 +19,26 @@
 namespace chain {
 
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortBins = 256;
+
+template <typename KT>
+struct SortShape {
+    static constexpr int kItems = sizeof(KT) > 4 ? 8 : 16;
+    static constexpr int kTile = kSortThreads * kItems;
+};
 
 template <typename KT>
 __global__ void __launch_bounds__(kSortThreads)
 radix_hist_kernel(const KT* __restrict__ keys, uint64_t n, int shift, uint32_t* __restrict__ counts,
                   uint32_t num_tiles) {
+    constexpr int I = SortShape<KT>::kItems, TILE = SortShape<KT>::kTile;
     __shared__ uint32_t hist[kSortBins];
     hist[threadIdx.x] = 0;
     __syncthreads();
-    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kSortTile;
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * TILE;
 #pragma unroll
-    for (int k = 0; k < kSortItems; ++k) {
+    for (int k = 0; k < I; ++k) {
         const uint64_t i = base + static_cast<uint64_t>(k) * kSortThreads + threadIdx.x;
         if (i < n) atomicAdd(&hist[static_cast<uint32_t>(keys[i] >> shift) & 0xFFu], 1u);
     }
@@ -45,16 +51,23 @@ __global__ void __launch_bounds__(kSortThreads)
 radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                      KT* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint64_t n, int shift,
                      const uint32_t* __restrict__ offsets, uint32_t num_tiles) {
+    constexpr int I = SortShape<KT>::kItems, TILE = SortShape<KT>::kTile;
     __shared__ uint32_t whist[kSortWarps][kSortBins];
+    __shared__ uint32_t tile_start[kSortBins];   // first tile-local position of each digit
+    __shared__ uint32_t gbase[kSortBins];        // global position of that first key
+    __shared__ uint32_t scratch[33];
+    __shared__ KT skey[TILE];
+    __shared__ uint32_t sval[TILE];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int t = threadIdx.x; t < kSortWarps * kSortBins; t += kSortThreads) (&whist[0][0])[t] = 0;
     __syncthreads();
-    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kSortTile + static_cast<uint64_t>(warp) * (kSortItems * 32);
-    KT key[kSortItems];
-    uint32_t rank[kSortItems];
+    const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * TILE;
+    const uint64_t base = tile0 + static_cast<uint64_t>(warp) * (I * 32);
+    KT key[I];
+    uint32_t rank[I];
     const uint32_t lt = lanemask_lt();
 #pragma unroll
-    for (int r = 0; r < kSortItems; ++r) {
+    for (int r = 0; r < I; ++r) {
         const uint64_t i = base + static_cast<uint64_t>(r) * 32 + lane;
         const bool valid = i < n;
         key[r] = valid ? keys_in[i] : KT(0);
@@ -70,8 +83,16 @@ radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict_
     }
     __syncthreads();
     {
-        const int d = threadIdx.x;  // one thread per digit
-        uint32_t run = offsets[static_cast<uint64_t>(d) * num_tiles + blockIdx.x];
+        // per digit: tile count, then per-warp offsets inside the tile
+        const int d = threadIdx.x;
+        uint32_t cnt = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) cnt += whist[w][d];
+        uint32_t tot;
+        const uint32_t start = block_exclusive_sum(cnt, scratch, &tot);
+        tile_start[d] = start;
+        gbase[d] = offsets[static_cast<uint64_t>(d) * num_tiles + blockIdx.x];
+        uint32_t run = start;
 #pragma unroll
         for (int w = 0; w < kSortWarps; ++w) {
             const uint32_t c = whist[w][d];
@@ -81,14 +102,23 @@ radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict_
     }
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < kSortItems; ++r) {
+    for (int r = 0; r < I; ++r) {
         const uint64_t i = base + static_cast<uint64_t>(r) * 32 + lane;
         if (i < n) {
             const uint32_t digit = static_cast<uint32_t>(key[r] >> shift) & 0xFFu;
-            const uint32_t pos = whist[warp][digit] + rank[r];
-            keys_out[pos] = key[r];
-            vals_out[pos] = vals_in ? vals_in[i] : static_cast<uint32_t>(i);
+            const uint32_t lp = whist[warp][digit] + rank[r];
+            skey[lp] = key[r];
+            sval[lp] = vals_in ? vals_in[i] : static_cast<uint32_t>(i);
         }
+    }
+    __syncthreads();
+    const uint32_t tile_n = static_cast<uint32_t>(min(static_cast<uint64_t>(TILE), n - tile0));
+    for (uint32_t j = threadIdx.x; j < tile_n; j += kSortThreads) {
+        const KT k = skey[j];
+        const uint32_t digit = static_cast<uint32_t>(k >> shift) & 0xFFu;
+        const uint32_t pos = gbase[digit] + (j - tile_start[digit]);
+        keys_out[pos] = k;
+        vals_out[pos] = sval[j];
     }
 }
 
@@ -101,19 +131,22 @@ struct CountOut {
     __device__ void operator()(uint64_t i, uint32_t prefix, uint32_t) const { c[i] = prefix; }
 };
 
-inline uint32_t radix_tiles(uint64_t n) { return static_cast<uint32_t>((n + kSortTile - 1) / kSortTile); }
+template <typename KT>
+inline uint32_t radix_tiles(uint64_t n) {
+    return static_cast<uint32_t>((n + SortShape<KT>::kTile - 1) / SortShape<KT>::kTile);
+}
 
-// Scratch requirement (bytes) of radix_sort_pairs for n keys.
-inline size_t radix_counts_elems(uint64_t n) { return static_cast<size_t>(radix_tiles(n)) * kSortBins; }
+// Count-table entries radix_sort_pairs needs for n keys of either key width.
+inline size_t radix_counts_elems(uint64_t n) { return static_cast<size_t>(radix_tiles<uint64_t>(n)) * kSortBins; }
 
 // Sorts keys_in (values implicitly 0..n-1) by bits [0, key_bits), stably.  Ping-pongs
 // between (keys_a, vals_a) and (keys_b, vals_b); keys_in is only read.  Returns true
 // when the result is in the *_b buffers.  counts: radix_counts_elems(n) u32;
-// scan_buf: scan_tiles(counts) u32.
+// scan_buf: scan_scratch_bytes(counts) bytes.
 template <typename KT>
 bool radix_sort_pairs(const KT* keys_in, KT* keys_a, uint32_t* vals_a, KT* keys_b, uint32_t* vals_b, uint64_t n,
                       int key_bits, uint32_t* counts, uint32_t* scan_buf, cudaStream_t stream) {
-    const uint32_t tiles = radix_tiles(n);
+    const uint32_t tiles = radix_tiles<KT>(n);
     int passes = (key_bits + 7) / 8;
     if (passes == 0) passes = 1;  // one pass produces the identity permutation
     for (int p = 0; p < passes; ++p) {

@@ -424,14 +424,31 @@ constexpr uint32_t kSmemTableSyms = 4096;     // decoder prob/cum in shared memo
 constexpr uint32_t kSmemEncSyms = 2048;       // encoder entries (16 B) in shared memory up to this alphabet
 constexpr uint32_t kSmemLookupSlots = 16384;  // u16 decode lookup in shared memory up to this M
 constexpr uint32_t kWindow = 4096;            // decoder byte window per warp
-constexpr size_t kRansEncSmem = kSmemEncSyms * 16 + kRansWarps * 2 * kRansTile * 32 * 4;
-constexpr size_t kRansDecSmem = kSmemTableSyms * 8 + kSmemLookupSlots * 2 + kRansWarps * kWindow;
 
+// Shared memory is sized per launch: the largest table of this launch that fits the
+// shared-memory limits (tab_cap symbols, look_cap decode slots), plus staging.
 struct RansJobs {
     RansJob job[kMaxRansJobs];
     uint32_t njobs;
     uint32_t total_blocks;
+    uint32_t tab_cap;    // tables with alphabet <= tab_cap live in shared memory
+    uint32_t look_cap;   // decode lookups with M <= look_cap live in shared memory
 };
+
+inline void rans_plan_smem(RansJobs& J, bool decode) {
+    uint32_t tab = 0, look = 0;
+    for (uint32_t j = 0; j < J.njobs; ++j) {
+        const uint32_t A = J.job[j].alphabet, M = 1u << J.job[j].prec;
+        if (A <= (decode ? kSmemTableSyms : kSmemEncSyms) && A > tab) tab = A;
+        if (decode && M <= kSmemLookupSlots && A <= 65536 && M > look) look = M;
+    }
+    J.tab_cap = (tab + 7) & ~7u;
+    J.look_cap = (look + 7) & ~7u;
+}
+inline size_t rans_enc_smem(const RansJobs& J) { return J.tab_cap * 16ull + kRansWarps * 2 * kRansTile * 32 * 4; }
+inline size_t rans_dec_smem(const RansJobs& J) {
+    return J.tab_cap * 8ull + J.look_cap * 2ull + kRansWarps * kWindow;
+}
 
 __device__ __forceinline__ int job_of_block(const RansJobs& J) {
     int j = 0;
@@ -480,13 +497,13 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
     const RansJob& jb = J.job[job_of_block(J)];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint4* tab = reinterpret_cast<uint4*>(rsm);
-    const bool smem_tab = jb.alphabet <= kSmemEncSyms;
+    const bool smem_tab = jb.alphabet <= J.tab_cap;
     if (smem_tab)
         for (uint32_t s = threadIdx.x; s < jb.alphabet; s += blockDim.x) tab[s] = jb.etab[s];
     __syncthreads();
     const uint32_t c = (blockIdx.x - jb.first_block) * kRansWarps + warp;
     if (c >= jb.chunks) return;
-    uint32_t* buf = reinterpret_cast<uint32_t*>(rsm + kSmemEncSyms * 16) + warp * 2 * 1024;
+    uint32_t* buf = reinterpret_cast<uint32_t*>(rsm + J.tab_cap * 16ull) + warp * 2 * 1024;
     const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
     const uint64_t cend = min(cbeg + jb.S, jb.count);
     const uint32_t steps = static_cast<uint32_t>((cend - cbeg + 31) / 32);
@@ -587,10 +604,10 @@ static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uin
     const uint32_t prec = jb.prec;
     const uint32_t M = 1u << prec, L = 4u << prec;
     uint2* tab = reinterpret_cast<uint2*>(rsm);
-    uint16_t* look = reinterpret_cast<uint16_t*>(rsm + kSmemTableSyms * 8);
-    uint8_t* win = rsm + kSmemTableSyms * 8 + kSmemLookupSlots * 2 + warp * kWindow;
-    const bool smem_tab = jb.alphabet <= kSmemTableSyms;
-    const bool smem_look = M <= kSmemLookupSlots && jb.alphabet <= 65536;
+    uint16_t* look = reinterpret_cast<uint16_t*>(rsm + J.tab_cap * 8ull);
+    uint8_t* win = rsm + J.tab_cap * 8ull + J.look_cap * 2ull + warp * kWindow;
+    const bool smem_tab = jb.alphabet <= J.tab_cap;
+    const bool smem_look = M <= J.look_cap && jb.alphabet <= 65536;
     if (smem_tab)
         for (uint32_t s = threadIdx.x; s < jb.alphabet; s += blockDim.x) tab[s] = make_uint2(jb.prob[s], jb.cum[s]);
     if (smem_look)

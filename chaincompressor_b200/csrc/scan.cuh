@@ -1,13 +1,14 @@
 // Device-wide exclusive scan (reduce-then-scan) over a functor-produced sequence with
 // an associative operator.
 //
-//   in(i)  -> T              value of element i (0 <= i < n)
+//   in(i)  -> T              value of element i (0 <= i < n), evaluated once
 //   out(i, prefix, value)    called once per element with its exclusive prefix
 //   Op: T operator()(T a, T b) (a precedes b), static T identity()
 //
 // Three launches: per-tile reduction, a one-CTA scan of the tile aggregates, and the
-// per-tile scan seeded with the tile's prefix.  Tiles are 4096 elements, read and
-// written in a coalesced (striped) order and scanned through shared memory.
+// per-tile scan seeded with the tile's prefix.  A tile is 256 threads x kItems<T>
+// elements; elements are loaded in a coalesced (striped) order into shared memory,
+// each thread scans a contiguous run, and out() is called from that run.
 #pragma once
 
 #include "chain_common.cuh"
@@ -15,8 +16,12 @@
 namespace chain {
 
 constexpr int kScanThreads = 256;
-constexpr int kScanItems = 16;
-constexpr int kScanTile = kScanThreads * kScanItems;
+
+template <typename T>
+struct ScanShape {
+    static constexpr int kItems = sizeof(T) > 8 ? 8 : 16;
+    static constexpr int kTile = kScanThreads * kItems;
+};
 
 template <typename T>
 struct SumOp {
@@ -24,31 +29,46 @@ struct SumOp {
     __device__ __forceinline__ static T identity() { return T(0); }
 };
 
+// Warp shuffle of any trivially copyable type made of 32-bit words.
+template <typename T>
+__device__ __forceinline__ T shfl_up_any(T v, int o) {
+    static_assert(sizeof(T) % 4 == 0, "scan types must be made of 32-bit words");
+    union U {
+        T t;
+        uint32_t w[sizeof(T) / 4];
+        __device__ U() {}
+    } u;
+    u.t = v;
+#pragma unroll
+    for (int k = 0; k < static_cast<int>(sizeof(T) / 4); ++k) u.w[k] = __shfl_up_sync(0xffffffffu, u.w[k], o);
+    return u.t;
+}
+
 template <typename T, typename Op>
 __device__ __forceinline__ T warp_inclusive_scan_op(T v, Op op) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        T t = __shfl_up_sync(0xffffffffu, v, o);
+        T t = shfl_up_any(v, o);
         if (lane >= o) v = op(t, v);
     }
     return v;
 }
 
-// Exclusive scan across the CTA; *total receives the CTA aggregate.
+// Exclusive scan across the CTA; *total (may be null) receives the CTA aggregate.
 template <typename T, typename Op>
 __device__ __forceinline__ T block_exclusive_scan_op(T v, Op op, T* scratch, T* total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nwarps = (blockDim.x + 31) >> 5;
     T inc = warp_inclusive_scan_op(v, op);
-    T exc = __shfl_up_sync(0xffffffffu, inc, 1);
+    T exc = shfl_up_any(inc, 1);
     if (lane == 0) exc = Op::identity();
     if (lane == 31) scratch[warp] = inc;
     __syncthreads();
     if (warp == 0) {
         T w = lane < nwarps ? scratch[lane] : Op::identity();
         T wi = warp_inclusive_scan_op(w, op);
-        T we = __shfl_up_sync(0xffffffffu, wi, 1);
+        T we = shfl_up_any(wi, 1);
         if (lane == 0) we = Op::identity();
         if (lane < nwarps) scratch[lane] = we;
         if (lane == nwarps - 1) scratch[32] = wi;
@@ -60,16 +80,34 @@ __device__ __forceinline__ T block_exclusive_scan_op(T v, Op op, T* scratch, T* 
     return out;
 }
 
+// Padded shared-memory index: one spare slot every 32 elements keeps the per-thread
+// contiguous reads free of bank conflicts.
+__device__ __forceinline__ int scan_pad(int j) { return j + (j >> 5); }
+
+template <typename T, typename InF>
+__device__ __forceinline__ void scan_stage(InF in, uint64_t n, uint64_t base, T* vals) {
+    constexpr int I = ScanShape<T>::kItems;
+#pragma unroll
+    for (int k = 0; k < I; ++k) {
+        const int j = k * kScanThreads + threadIdx.x;
+        const uint64_t i = base + j;
+        if (i < n) vals[scan_pad(j)] = in(i);
+    }
+}
+
 template <typename T, typename InF, typename Op>
 __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(InF in, uint64_t n, T* tile_aggr, Op op) {
+    constexpr int I = ScanShape<T>::kItems, TILE = ScanShape<T>::kTile;
+    __shared__ T vals[TILE + TILE / 32];
     __shared__ T scratch[33];
-    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile + static_cast<uint64_t>(threadIdx.x) * kScanItems;
-    // each thread reduces a contiguous run (order matters for non-commutative ops)
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * TILE;
+    scan_stage<T>(in, n, base, vals);
+    __syncthreads();
     T acc = Op::identity();
-#pragma unroll 4
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint64_t i = base + k;
-        if (i < n) acc = op(acc, in(i));
+#pragma unroll
+    for (int k = 0; k < I; ++k) {
+        const int j = threadIdx.x * I + k;
+        if (base + j < n) acc = op(acc, vals[scan_pad(j)]);
     }
     T tot;
     block_exclusive_scan_op(acc, op, scratch, &tot);
@@ -96,50 +134,42 @@ __global__ void __launch_bounds__(1024) scan_tilesums_kernel(T* aggr, uint64_t c
 template <typename T, typename InF, typename OutF, typename Op>
 __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(InF in, OutF out, uint64_t n,
                                                                   const T* tile_prefix, Op op) {
-    __shared__ T vals[kScanTile + kScanTile / 32];
+    constexpr int I = ScanShape<T>::kItems, TILE = ScanShape<T>::kTile;
+    __shared__ T vals[TILE + TILE / 32];
     __shared__ T scratch[33];
-    // padded index: one extra slot every 32 elements avoids bank conflicts on the
-    // per-thread contiguous reads below
-#define CHAIN_SCAN_PAD(j) ((j) + ((j) >> 5))
-    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile;
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const int j = k * kScanThreads + threadIdx.x;
-        const uint64_t i = base + j;
-        vals[CHAIN_SCAN_PAD(j)] = i < n ? in(i) : Op::identity();
-    }
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * TILE;
+    scan_stage<T>(in, n, base, vals);
     __syncthreads();
-    T local[kScanItems];
+    T local[I];
     T agg = Op::identity();
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        local[k] = vals[CHAIN_SCAN_PAD(threadIdx.x * kScanItems + k)];
+    for (int k = 0; k < I; ++k) {
+        const int j = threadIdx.x * I + k;
+        local[k] = base + j < n ? vals[scan_pad(j)] : Op::identity();
         agg = op(agg, local[k]);
     }
     T ex = op(tile_prefix[blockIdx.x], block_exclusive_scan_op(agg, op, scratch, static_cast<T*>(nullptr)));
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        vals[CHAIN_SCAN_PAD(threadIdx.x * kScanItems + k)] = ex;
+    for (int k = 0; k < I; ++k) {
+        const uint64_t i = base + threadIdx.x * I + k;
+        if (i < n) out(i, ex, local[k]);
         ex = op(ex, local[k]);
     }
-    __syncthreads();
-    // out() also receives the element's own value, re-read through the input functor.
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const int j = k * kScanThreads + threadIdx.x;
-        const uint64_t i = base + j;
-        if (i < n) out(i, vals[CHAIN_SCAN_PAD(j)], in(i));
-    }
-#undef CHAIN_SCAN_PAD
 }
 
-inline uint64_t scan_tiles(uint64_t n) { return (n + kScanTile - 1) / kScanTile; }
+template <typename T>
+inline uint64_t scan_tiles(uint64_t n) {
+    return (n + ScanShape<T>::kTile - 1) / ScanShape<T>::kTile;
+}
+// Bytes of tile-aggregate scratch that any scan over n elements of a type up to 16
+// bytes needs.
+inline uint64_t scan_scratch_bytes(uint64_t n) { return 16 * (n / 2048 + 16); }
 
-// Launches the three scan kernels on `stream`; `tile_buf` holds scan_tiles(n) values.
+// Launches the three scan kernels on `stream`; `tile_buf` holds scan_tiles<T>(n) values.
 template <typename T, typename InF, typename OutF, typename Op = SumOp<T>>
 void device_exclusive_scan(InF in, OutF out, uint64_t n, T* tile_buf, T* total, cudaStream_t stream,
                            Op op = Op()) {
-    const uint64_t tiles = scan_tiles(n);
+    const uint64_t tiles = scan_tiles<T>(n);
     if (tiles == 0) {
         if (total) cudaMemsetAsync(total, 0, sizeof(T), stream);
         return;
