@@ -18,8 +18,13 @@
 //   "LCG2" u32 version=2, u32 D, u64 N, i64 p, f64 eb, i64 wrap_min, i64 wrap_max,
 //   f64 minima[D], u8 input_dtype, u32 stream_count=5,
 //   5 x { char name[4], u64 body_len, body },
-//   "EXC0", u64 body_len, { u64 count, count x u64 flat index (strictly increasing),
-//                           count x f64 original value }.
+//   "EXC0", u64 body_len, { u64 count; when count > 0: u64 ndistinct,
+//                           ndistinct x f64 distinct corrected values (ascending bits),
+//                           u64 len, component body of the index gaps,
+//                           u64 len, component body of the value ids }.
+// Exact corrections (lcps_cpp.cpp:2097-2103) are the points whose FP64 reconstruction
+// would miss eb; they are listed by flat index i*D+d in increasing order.  Gap k is
+// index_k - index_{k-1} - 1 (index_0 itself for k = 0); id k selects the value.
 // Component body:
 //   u8 encoding, u32 dims, u64 records, then
 //   empty (0):  nothing (records == 0)
@@ -44,6 +49,10 @@
 namespace chain {
 
 constexpr uint32_t kFormatVersion = 2;
+// Coded streams: the five components, then the two exact-correction streams.
+constexpr int kCodeStreams = kStreams + 2;
+constexpr int kCorrGaps = kStreams;      // index gaps
+constexpr int kCorrIds = kStreams + 1;   // value ids
 // Component names, in container order (cu/chain/lcps_gpu_cpp.cu:88).
 __host__ __device__ inline void stream_name(int s, char out[4]) {
     const char names[kStreams][4] = {{'I', 'D', 'R', '0'}, {'D', 'I', 'F', '0'}, {'K', 'E', 'P', '0'},
@@ -87,10 +96,10 @@ struct DecodePlan {
     double eb;
     int64_t wrap_min, wrap_max;
     double minima[kMaxDims];
-    CompPlan comp[kStreams];
+    CompPlan comp[kCodeStreams];
     uint64_t exc_count;
-    uint64_t exc_idx_off;
-    uint64_t exc_val_off;
+    uint64_t exc_ndistinct;
+    uint64_t exc_dict_off;
     uint32_t ok;      // 1 = parsed and structurally valid
     uint32_t why;     // failure code (line of the failed check) when ok == 0
 };
@@ -178,6 +187,48 @@ __host__ __device__ inline bool parse_section(ByteReader& r, SectionPlan* s, uin
     return true;
 }
 
+// One component body of body_len bytes (the reader sits at its first byte).
+__host__ __device__ inline bool parse_component(ByteReader& r, uint64_t body_len, CompPlan* c, uint32_t want_dims,
+                                                uint64_t max_records, DecodePlan* plan) {
+    CHAIN_PARSE_REQUIRE(r.need(body_len));
+    const uint64_t body_end = r.pos + body_len;
+    c->enc = r.u8();
+    c->dims = r.u32();
+    c->records = r.u64();
+    CHAIN_PARSE_REQUIRE(r.ok && c->dims == want_dims && c->records <= max_records);
+    CHAIN_PARSE_REQUIRE(c->enc <= kEncRaw);
+    if (c->enc == kEncEmpty) {
+        CHAIN_PARSE_REQUIRE(c->records == 0);
+    } else if (c->enc == kEncFixed) {
+        CHAIN_PARSE_REQUIRE(c->records > 0);
+        for (uint32_t d = 0; d < c->dims; ++d) {
+            c->minv[d] = r.u64();
+            c->width[d] = r.u8();
+            CHAIN_PARSE_REQUIRE(r.ok && c->width[d] >= 1 && c->width[d] <= 32);
+        }
+        for (uint32_t d = 0; d < c->dims; ++d) {
+            c->packed_off[d] = r.pos;
+            CHAIN_PARSE_REQUIRE(r.skip((c->records * c->width[d] + 7) / 8));
+        }
+    } else if (c->enc == kEncTagged) {
+        CHAIN_PARSE_REQUIRE(c->records > 0);
+        c->max_width = r.u8();
+        CHAIN_PARSE_REQUIRE(r.ok && c->max_width >= 1 && c->max_width <= 32);
+        if (!parse_section(r, &c->sec, c->records, plan)) return false;
+        CHAIN_PARSE_REQUIRE(c->sec.alphabet <= 33u);
+        c->packed_bits = r.u64();
+        CHAIN_PARSE_REQUIRE(r.ok && c->packed_bits >= c->records * c->dims &&
+                            c->packed_bits <= c->records * c->dims * 32ull);
+        c->tagged_off = r.pos;
+        CHAIN_PARSE_REQUIRE(r.skip((c->packed_bits + 7) / 8));
+    } else {
+        CHAIN_PARSE_REQUIRE(c->records > 0);
+        if (!parse_section(r, &c->sec, c->records * c->dims, plan)) return false;
+    }
+    CHAIN_PARSE_REQUIRE(r.ok && r.pos == body_end);
+    return true;
+}
+
 // Parses and structurally validates a container.  Semantic validation of the coded
 // integers (ranges, counts, references) happens in the decode kernels.
 __host__ __device__ inline bool parse_container(const uint8_t* data, uint64_t len, DecodePlan* plan) {
@@ -205,61 +256,37 @@ __host__ __device__ inline bool parse_container(const uint8_t* data, uint64_t le
     CHAIN_PARSE_REQUIRE(r.ok && (plan->input_dtype == 4 || plan->input_dtype == 8));
     CHAIN_PARSE_REQUIRE(r.u32() == kStreams);
     for (int s = 0; s < kStreams; ++s) {
-        CompPlan* c = &plan->comp[s];
         char name[5] = {0, 0, 0, 0, 0};
         stream_name(s, name);
         CHAIN_PARSE_REQUIRE(r.magic(name));
         const uint64_t body_len = r.u64();
-        CHAIN_PARSE_REQUIRE(r.need(body_len));
-        const uint64_t body_end = r.pos + body_len;
-        c->enc = r.u8();
-        c->dims = r.u32();
-        c->records = r.u64();
-        const uint32_t want_dims = (s == 0 || s == 3) ? 1u : plan->D;
-        CHAIN_PARSE_REQUIRE(r.ok && c->dims == want_dims && c->records <= plan->N);
-        CHAIN_PARSE_REQUIRE(c->enc <= kEncRaw);
-        if (c->enc == kEncEmpty) {
-            CHAIN_PARSE_REQUIRE(c->records == 0);
-        } else if (c->enc == kEncFixed) {
-            CHAIN_PARSE_REQUIRE(c->records > 0);
-            for (uint32_t d = 0; d < c->dims; ++d) {
-                c->minv[d] = r.u64();
-                c->width[d] = r.u8();
-                CHAIN_PARSE_REQUIRE(r.ok && c->width[d] >= 1 && c->width[d] <= 32);
-            }
-            for (uint32_t d = 0; d < c->dims; ++d) {
-                c->packed_off[d] = r.pos;
-                CHAIN_PARSE_REQUIRE(r.skip((c->records * c->width[d] + 7) / 8));
-            }
-        } else if (c->enc == kEncTagged) {
-            CHAIN_PARSE_REQUIRE(c->records > 0);
-            c->max_width = r.u8();
-            CHAIN_PARSE_REQUIRE(r.ok && c->max_width >= 1 && c->max_width <= 32);
-            if (!parse_section(r, &c->sec, c->records, plan)) return false;
-            CHAIN_PARSE_REQUIRE(c->sec.alphabet <= 33u);
-            c->packed_bits = r.u64();
-            CHAIN_PARSE_REQUIRE(r.ok && c->packed_bits >= c->records * c->dims &&
-                                c->packed_bits <= c->records * c->dims * 32ull);
-            c->tagged_off = r.pos;
-            CHAIN_PARSE_REQUIRE(r.skip((c->packed_bits + 7) / 8));
-        } else {
-            CHAIN_PARSE_REQUIRE(c->records > 0);
-            if (!parse_section(r, &c->sec, c->records * c->dims, plan)) return false;
-        }
-        CHAIN_PARSE_REQUIRE(r.ok && r.pos == body_end);
+        if (!parse_component(r, body_len, &plan->comp[s], (s == 0 || s == 3) ? 1u : plan->D, plan->N, plan))
+            return false;
     }
     CHAIN_PARSE_REQUIRE(plan->comp[0].records == plan->N && plan->comp[4].records == plan->N);
     CHAIN_PARSE_REQUIRE(plan->comp[3].records >= 1 && plan->comp[2].records >= 1);
     CHAIN_PARSE_REQUIRE(plan->comp[1].records + plan->comp[2].records == plan->comp[3].records);
     CHAIN_PARSE_REQUIRE(r.magic("EXC0"));
     const uint64_t exc_len = r.u64();
+    CHAIN_PARSE_REQUIRE(r.need(exc_len));
+    const uint64_t exc_end = r.pos + exc_len;
     plan->exc_count = r.u64();
+    plan->exc_ndistinct = 0;
+    plan->comp[kCorrGaps].enc = plan->comp[kCorrIds].enc = kEncEmpty;
+    plan->comp[kCorrGaps].records = plan->comp[kCorrIds].records = 0;
     CHAIN_PARSE_REQUIRE(r.ok && plan->exc_count <= plan->N * plan->D);
-    CHAIN_PARSE_REQUIRE(exc_len == 8 + 16 * plan->exc_count);
-    plan->exc_idx_off = r.pos;
-    plan->exc_val_off = r.pos + 8 * plan->exc_count;
-    CHAIN_PARSE_REQUIRE(r.skip(16 * plan->exc_count));
-    CHAIN_PARSE_REQUIRE(r.pos == len);
+    if (plan->exc_count) {
+        plan->exc_ndistinct = r.u64();
+        CHAIN_PARSE_REQUIRE(r.ok && plan->exc_ndistinct >= 1 && plan->exc_ndistinct <= plan->exc_count);
+        plan->exc_dict_off = r.pos;
+        CHAIN_PARSE_REQUIRE(r.skip(8 * plan->exc_ndistinct));
+        for (int s = kCorrGaps; s <= kCorrIds; ++s) {
+            const uint64_t body_len = r.u64();
+            if (!parse_component(r, body_len, &plan->comp[s], 1u, plan->exc_count, plan)) return false;
+            CHAIN_PARSE_REQUIRE(plan->comp[s].records == plan->exc_count);
+        }
+    }
+    CHAIN_PARSE_REQUIRE(r.ok && r.pos == exc_end && r.pos == len);
     plan->ok = 1;
     return true;
 }

@@ -26,8 +26,8 @@ struct DecState {
     uint32_t jump_active;   // pointer jumping: 1 while some parent moved in the last round
     uint32_t zeros;         // idrel == 0 count
     uint32_t ndiff_seen;
-    uint64_t tag_bits[kStreams];
-    uint32_t maxtag[kStreams];
+    uint64_t tag_bits[kCodeStreams];
+    uint32_t maxtag[kCodeStreams];
     DecodePlan plan;
 };
 
@@ -37,7 +37,7 @@ __global__ void k_dec_init(DecState* st) {
     st->jump_active = 1;
     st->zeros = 0;
     st->ndiff_seen = 0;
-    for (int s = 0; s < kStreams; ++s) { st->tag_bits[s] = 0; st->maxtag[s] = 0; }
+    for (int s = 0; s < kCodeStreams; ++s) { st->tag_bits[s] = 0; st->maxtag[s] = 0; }
 }
 
 __global__ void k_parse(const uint8_t* data, uint64_t len, DecState* st) {
@@ -55,7 +55,7 @@ struct SectionRef {
     uint64_t* chunk_off;
 };
 struct SectionRefs {
-    SectionRef r[kStreams];
+    SectionRef r[kCodeStreams];
     int count;
 };
 
@@ -171,7 +171,7 @@ struct TagUnpackOut {
 
 __global__ void k_check_tagged(const DecState* st_c, DecState* st) {
     if (threadIdx.x || blockIdx.x) return;
-    for (int s = 0; s < kStreams; ++s) {
+    for (int s = 0; s < kCodeStreams; ++s) {
         const CompPlan& c = st_c->plan.comp[s];
         if (c.enc != kEncTagged) continue;
         if (st->tag_bits[s] != c.packed_bits || st->maxtag[s] != c.max_width) set_error(&st->err, kErrCorrupt);
@@ -368,24 +368,35 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
     }
 }
 
+// Exact corrections: index_k = sum_{m<=k} (gap_m + 1) - 1, value = dictionary[id_k]
+// (lcps_cpp.cpp:1979-1992 applies the same records).  Indices are strictly increasing
+// by construction; each is checked against n * dims, each id against the dictionary.
+struct CorrIn {
+    const uint32_t* gaps;
+    __device__ uint64_t operator()(uint64_t k) const { return static_cast<uint64_t>(gaps[k]) + 1; }
+};
 template <typename OT, bool SOA>
-__global__ void k_corrections(const uint8_t* data, const DecState* stc, DecState* st, OT* out) {
-    const DecodePlan& P = stc->plan;
-    const uint64_t cnt = P.exc_count;
-    const uint64_t nd = P.N * P.D;
-    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < cnt;
-         k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint64_t idx = 0, prev = 0, vb = 0;
-        for (int b = 0; b < 8; ++b) idx |= static_cast<uint64_t>(data[P.exc_idx_off + 8 * k + b]) << (8 * b);
-        if (k) for (int b = 0; b < 8; ++b) prev |= static_cast<uint64_t>(data[P.exc_idx_off + 8 * (k - 1) + b]) << (8 * b);
-        for (int b = 0; b < 8; ++b) vb |= static_cast<uint64_t>(data[P.exc_val_off + 8 * k + b]) << (8 * b);
+struct CorrOut {
+    const uint32_t* ids;
+    const uint8_t* data;
+    const DecState* stc;
+    DecState* st;
+    OT* out;
+    __device__ void operator()(uint64_t k, uint64_t prefix, uint64_t step) const {
+        const DecodePlan& P = stc->plan;
+        const uint64_t idx = prefix + step - 1;
+        const uint32_t id = ids[k];
+        const uint64_t nd = P.N * P.D;
+        if (idx >= nd || id >= P.exc_ndistinct) { set_error(&st->err, kErrCorrupt); return; }
+        uint64_t vb = 0;
+        for (int b = 0; b < 8; ++b) vb |= static_cast<uint64_t>(data[P.exc_dict_off + 8ull * id + b]) << (8 * b);
         double v;
         memcpy(&v, &vb, 8);
-        if (idx >= nd || (k && idx <= prev) || !chain_isfinite(v)) { set_error(&st->err, kErrCorrupt); continue; }
+        if (!chain_isfinite(v)) { set_error(&st->err, kErrCorrupt); return; }
         const uint64_t i = idx / P.D, d = idx - i * P.D;
         out[SOA ? d * P.N + i : idx] = static_cast<OT>(v);
     }
-}
+};
 
 // --------------------------------------------------------------------- host
 static unsigned dgrid(uint64_t n, int threads = 256, unsigned cap = 148u * 16u) {
@@ -438,8 +449,8 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
                                                        " bytes, need " + std::to_string(nd * osz));
     const uint64_t B = plan.comp[3].records;
     uint64_t max_prec_slots = 0, total_chunks = 0, max_alpha = 0, tags_total = 0, parse_scratch = 0;
-    uint64_t tag_off[kStreams] = {0};
-    for (int s = 0; s < kStreams; ++s) {
+    uint64_t tag_off[kCodeStreams] = {0};
+    for (int s = 0; s < kCodeStreams; ++s) {
         const CompPlan& c = plan.comp[s];
         if (c.enc == kEncRaw || c.enc == kEncTagged) {
             max_prec_slots += 1ull << c.sec.prec;
@@ -459,7 +470,8 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     need += Arena::need(N, 4);               // drank
     need += Arena::need(tags_total + 1, 4);
     need += Arena::need(max_prec_slots + 1, 4) + Arena::need(max_alpha + 1, 4) * 2;
-    need += Arena::need(total_chunks + kStreams + 1, 8) + Arena::need(total_chunks * 32 + 1, 4);
+    need += Arena::need(total_chunks + kCodeStreams + 1, 8) + Arena::need(total_chunks * 32 + 1, 4);
+    need += Arena::need(plan.exc_count + 1, 4) * 2;   // correction gaps, ids
     need += Arena::need(scan_scratch_bytes(std::max<uint64_t>(nd, N)), 1);
     need += Arena::need(16, 8);
     need += Arena::need(parse_scratch + 1, 4);
@@ -476,12 +488,14 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         CHAIN_CUDA(cudaMemcpyAsync(&st->plan, &hs->plan, sizeof(DecodePlan), cudaMemcpyHostToDevice, stream));
         T.mark("h2d_container", stream);
     }
-    uint32_t* streams[kStreams];
+    uint32_t* streams[kCodeStreams];
     streams[0] = A.take<uint32_t>(N);
     streams[1] = A.take<uint32_t>(nd);
     streams[2] = A.take<uint32_t>(nd);
     streams[3] = A.take<uint32_t>(N);
     streams[4] = A.take<uint32_t>(nd);
+    streams[kCorrGaps] = A.take<uint32_t>(plan.exc_count + 1);
+    streams[kCorrIds] = A.take<uint32_t>(plan.exc_count + 1);
     uint32_t* compact = A.take<uint32_t>(nd);
     uint32_t* zrank = A.take<uint32_t>(N);
     uint32_t* parent = A.take<uint32_t>(N);
@@ -490,7 +504,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     uint32_t* lookup = A.take<uint32_t>(max_prec_slots + 1);
     uint32_t* prob = A.take<uint32_t>(max_alpha + 1);
     uint32_t* cum = A.take<uint32_t>(max_alpha + 1);
-    uint64_t* chunk_off = A.take<uint64_t>(total_chunks + kStreams + 1);
+    uint64_t* chunk_off = A.take<uint64_t>(total_chunks + kCodeStreams + 1);
     uint32_t* states = A.take<uint32_t>(total_chunks * 32 + 1);
     uint64_t* scanbuf = reinterpret_cast<uint64_t*>(A.take<uint8_t>(scan_scratch_bytes(std::max<uint64_t>(nd, N))));
     uint64_t* misc = A.take<uint64_t>(16);
@@ -503,11 +517,11 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     // ---- entropy sections
     SectionRefs refs{};
     RansJobs jobs{};
-    uint64_t states_first[kStreams] = {0};
+    uint64_t states_first[kCodeStreams] = {0};
     uint64_t slot_base = 0, alpha_base = 0, chunk_base = 0, off_base = 0, pscr_base = 0;
     uint32_t first = 0;
     int nsec = 0;
-    for (int s = 0; s < kStreams; ++s) {
+    for (int s = 0; s < kCodeStreams; ++s) {
         const CompPlan& c = plan.comp[s];
         if (c.enc != kEncRaw && c.enc != kEncTagged) continue;
         SectionRef& R = refs.r[nsec];
@@ -543,8 +557,9 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     }
     refs.count = nsec;
     jobs.total_blocks = first;
-    uint64_t* d_states_first = misc + 8;   // nsec <= 5 entries -> misc[8..12]
-    CHAIN_CUDA(cudaMemcpyAsync(d_states_first, states_first, sizeof(uint64_t) * kStreams, cudaMemcpyHostToDevice, stream));
+    uint64_t* d_states_first = misc + 8;   // nsec <= 7 entries -> misc[8..14]
+    CHAIN_CUDA(cudaMemcpyAsync(d_states_first, states_first, sizeof(uint64_t) * kCodeStreams, cudaMemcpyHostToDevice,
+                               stream));
     if (nsec) {
         k_section_setup<<<nsec, 1024, 0, stream>>>(refs, dcont, st);
         k_lookup<<<dim3(256, nsec), 256, 0, stream>>>(refs, st);
@@ -562,7 +577,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     CHAIN_LAUNCH_CHECK("entropy decode");
     T.mark("rans_decode", stream);
     // ---- tagged and fixed components
-    for (int s = 0; s < kStreams; ++s) {
+    for (int s = 0; s < kCodeStreams; ++s) {
         const CompPlan& c = plan.comp[s];
         const CompPlan* dc = &st->plan.comp[s];
         if (c.enc == kEncFixed) {
@@ -607,19 +622,31 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     // ---- reconstruction
     const bool soa = out_layout == CHAIN_SOA;
     const unsigned g = dgrid(N);
-    const unsigned gc = dgrid(plan.exc_count);
+    const uint64_t ncx = plan.exc_count;
+    const CorrIn cin{streams[kCorrGaps]};
+    uint64_t* sb = scanbuf;
     if (out_dtype == CHAIN_F64) {
         double* o = static_cast<double*>(dout);
-        if (soa) { k_reconstruct<double, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
-                   if (plan.exc_count) k_corrections<double, true><<<gc, 256, 0, stream>>>(dcont, st, st, o); }
-        else { k_reconstruct<double, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
-               if (plan.exc_count) k_corrections<double, false><<<gc, 256, 0, stream>>>(dcont, st, st, o); }
+        if (soa) {
+            k_reconstruct<double, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+            if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<double, true>{streams[kCorrIds], dcont, st, st, o},
+                                                     ncx, sb, static_cast<uint64_t*>(nullptr), stream);
+        } else {
+            k_reconstruct<double, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+            if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<double, false>{streams[kCorrIds], dcont, st, st, o},
+                                                     ncx, sb, static_cast<uint64_t*>(nullptr), stream);
+        }
     } else {
         float* o = static_cast<float*>(dout);
-        if (soa) { k_reconstruct<float, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
-                   if (plan.exc_count) k_corrections<float, true><<<gc, 256, 0, stream>>>(dcont, st, st, o); }
-        else { k_reconstruct<float, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
-               if (plan.exc_count) k_corrections<float, false><<<gc, 256, 0, stream>>>(dcont, st, st, o); }
+        if (soa) {
+            k_reconstruct<float, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+            if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<float, true>{streams[kCorrIds], dcont, st, st, o},
+                                                     ncx, sb, static_cast<uint64_t*>(nullptr), stream);
+        } else {
+            k_reconstruct<float, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+            if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<float, false>{streams[kCorrIds], dcont, st, st, o},
+                                                     ncx, sb, static_cast<uint64_t*>(nullptr), stream);
+        }
     }
     CHAIN_LAUNCH_CHECK("reconstruct");
     T.mark("reconstruct", stream);

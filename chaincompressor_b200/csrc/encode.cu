@@ -65,10 +65,12 @@ struct EncState {
     uint32_t B, nkeep, ndiff, pad0;
     uint32_t rec_min, rec_max, rec_maxdiff, pad1;
     int64_t wrap_min, wrap_max, wrap_range, wrap_min_corr, wrap_max_corr;
-    StreamStats st[kStreams];
-    RansTableDev raw_tab[kStreams];
-    RansTableDev tag_tab[kStreams];
-    StreamChoice ch[kStreams];
+    StreamStats st[kCodeStreams];
+    RansTableDev raw_tab[kCodeStreams];
+    RansTableDev tag_tab[kCodeStreams];
+    StreamChoice ch[kCodeStreams];
+    uint32_t ndistinct;   // distinct exact-correction values
+    uint32_t pad3;
     uint64_t total_bytes;
     uint32_t npieces;
     uint32_t pad2;
@@ -361,7 +363,7 @@ struct StreamRef {
     uint64_t count_const;
 };
 struct StreamRefs {
-    StreamRef s[kStreams];
+    StreamRef s[kCodeStreams];
 };
 
 __device__ __forceinline__ uint64_t stream_records(const StreamRef& r) {
@@ -379,8 +381,8 @@ __device__ __forceinline__ void warp_hist_add(uint32_t* bins, uint32_t v, bool v
 // Per-stream statistics: per-dimension min/max, overall max, record tags
 // (max(1, max_d bitlen v)) histogram and their bit total.  Registers hold the
 // extrema; the tag histogram is warp-aggregated in shared memory.
-__global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState* st) {
-    const int s = blockIdx.y;
+__global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState* st, int s0) {
+    const int s = s0 + blockIdx.y;
     const StreamRef r = refs.s[s];
     const uint64_t nrec = stream_records(r);
     __shared__ uint32_t smin[kMaxDims], smax[kMaxDims], stag[34];
@@ -443,8 +445,8 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
 // warp-aggregated, so a hot value costs one atomic per warp instead of one per lane.
 constexpr int kSmemHistBins = 8192;
 __global__ void __launch_bounds__(256) k_value_hist(StreamRefs refs, const EncState* st, uint32_t* hist,
-                                                     uint64_t hist_stride) {
-    const int s = blockIdx.y;
+                                                     uint64_t hist_stride, int s0) {
+    const int s = s0 + blockIdx.y;
     const StreamRef r = refs.s[s];
     const uint32_t maxall = st->st[s].maxall;
     const uint64_t nrec = stream_records(r);
@@ -474,8 +476,8 @@ __global__ void __launch_bounds__(256) k_value_hist(StreamRefs refs, const EncSt
 // One CTA per (stream, kind): kind 0 = raw value table, kind 1 = tag table.
 __global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncState* st, const uint32_t* hist,
                                                            uint64_t hist_stride, uint32_t* prob, uint32_t* cum,
-                                                           uint32_t* tag_prob, uint32_t* tag_cum) {
-    const int s = blockIdx.x, kind = blockIdx.y;
+                                                           uint32_t* tag_prob, uint32_t* tag_cum, int s0) {
+    const int s = s0 + blockIdx.x, kind = blockIdx.y;
     const StreamRef r = refs.s[s];
     const uint64_t nrec = stream_records(r);
     if (kind == 0) {
@@ -514,9 +516,10 @@ __device__ inline void plan_chunks(uint64_t count, double est_payload, uint32_t 
 
 // Chooses each component's encoding: the smallest estimated size among tagged, fixed
 // and raw (ties in that order, as lcps_cpp.cpp:1150-1170), empty when no records.
-__global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, uint32_t max_steps) {
-    const int s = threadIdx.x;
-    if (s >= kStreams || blockIdx.x) return;
+__global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, uint32_t max_steps, int s0,
+                       int count) {
+    const int s = s0 + threadIdx.x;
+    if (static_cast<int>(threadIdx.x) >= count || blockIdx.x) return;
     const StreamRef r = refs.s[s];
     const uint64_t nrec = stream_records(r);
     StreamChoice& c = st->ch[s];
@@ -679,16 +682,15 @@ __global__ void __launch_bounds__(1024) k_serialize_tables(EncState* st, const u
 
 // --------------------------------------------------------------- assembly
 struct AssemblyIn {
-    const uint8_t* table_bytes;   // [kStreams] x table_stride
+    const uint8_t* table_bytes;   // [kCodeStreams] x table_stride
     uint64_t table_stride;
-    const uint32_t* chunk_len[kStreams];
-    const uint32_t* states[kStreams];
-    const uint8_t* slots[kStreams];
-    uint64_t slot_cap[kStreams];
-    const uint8_t* packed[kStreams];         // fixed/tagged payload (bytes)
-    uint64_t packed_dim_stride[kStreams];    // fixed: bytes between dimension payloads
-    const uint64_t* corr_idx;
-    const double* corr_val;
+    const uint32_t* chunk_len[kCodeStreams];
+    const uint32_t* states[kCodeStreams];
+    const uint8_t* slots[kCodeStreams];
+    uint64_t slot_cap[kCodeStreams];
+    const uint8_t* packed[kCodeStreams];         // fixed/tagged payload (bytes)
+    uint64_t packed_dim_stride[kCodeStreams];    // fixed: bytes between dimension payloads
+    const uint64_t* corr_dict;                   // distinct corrected values (bits)
     uint8_t input_dtype;
 };
 
@@ -734,13 +736,9 @@ __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* piece
     for (uint32_t d = 0; d < D; ++d) w.f64(st->mins[d]);
     w.u8(in.input_dtype);
     w.uint(kStreams, 4);
-    for (int s = 0; s < kStreams; ++s) {
+    // one component body; returns its length
+    auto component = [&](int s) -> uint64_t {
         StreamChoice& c = st->ch[s];
-        char name[4];
-        stream_name(s, name);
-        w.raw(name, 4);
-        const uint64_t len_pos = w.pos;
-        w.pos += 8;
         const uint64_t body0 = w.pos;
         w.u8(c.enc);
         w.uint(c.dims, 4);
@@ -772,16 +770,40 @@ __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* piece
             }
         }
         c.body_bytes = w.pos - body0;
+        return c.body_bytes;
+    };
+    auto sized = [&](int s) {   // u64 length, then the body
+        const uint64_t len_pos = w.pos;
+        w.pos += 8;
+        const uint64_t len = component(s);
         const uint64_t save = w.pos;
         w.pos = len_pos;
-        w.uint(c.body_bytes, 8);
+        w.uint(len, 8);
         w.pos = save;
+    };
+    for (int s = 0; s < kStreams; ++s) {
+        char name[4];
+        stream_name(s, name);
+        w.raw(name, 4);
+        sized(s);
     }
     w.raw("EXC0", 4);
-    w.uint(8 + 16 * st->ncorr, 8);
+    const uint64_t exc_len_pos = w.pos;
+    w.pos += 8;
+    const uint64_t exc0 = w.pos;
     w.uint(st->ncorr, 8);
-    piece(reinterpret_cast<const uint8_t*>(in.corr_idx), 8 * st->ncorr);
-    piece(reinterpret_cast<const uint8_t*>(in.corr_val), 8 * st->ncorr);
+    if (st->ncorr) {
+        w.uint(st->ndistinct, 8);
+        piece(reinterpret_cast<const uint8_t*>(in.corr_dict), 8 * st->ndistinct);
+        sized(kCorrGaps);
+        sized(kCorrIds);
+    }
+    {
+        const uint64_t save = w.pos;
+        w.pos = exc_len_pos;
+        w.uint(save - exc0, 8);
+        w.pos = save;
+    }
     st->total_bytes = w.pos;
     st->npieces = np;
     st->nsegs = segs;
@@ -805,6 +827,30 @@ __global__ void __launch_bounds__(256) k_copy_pieces(const Piece* pieces, const 
         for (uint64_t b = off + threadIdx.x; b < end; b += blockDim.x) dst[b] = pc.src[b];
     }
 }
+
+// Exact corrections as coded streams: index gaps (index_k - index_{k-1} - 1) and ids
+// into the ascending list of distinct values.
+__global__ void k_corr_gaps(const uint64_t* idx, uint64_t count, uint32_t* gaps) {
+    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < count;
+         k += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        gaps[k] = static_cast<uint32_t>(idx[k] - (k ? idx[k - 1] + 1 : 0));
+}
+struct DictIn {
+    const uint64_t* sorted_bits;
+    __device__ uint32_t operator()(uint64_t k) const {
+        return (k == 0 || sorted_bits[k] != sorted_bits[k - 1]) ? 1u : 0u;
+    }
+};
+struct DictOut {
+    const uint64_t* sorted_bits;
+    const uint32_t* sorted_pos;
+    uint64_t* dict;
+    uint32_t* ids;
+    __device__ void operator()(uint64_t k, uint32_t pre, uint32_t first) const {
+        if (first) dict[pre] = sorted_bits[k];
+        ids[sorted_pos[k]] = pre + first - 1;
+    }
+};
 
 __global__ void k_gather_corrections(const uint32_t* perm, const uint64_t* idx_sorted_in, const double* val_in,
                                      uint64_t* idx_out, double* val_out, uint64_t count) {
@@ -833,7 +879,10 @@ __global__ void k_init_state(EncState* st, uint32_t dims, uint64_t n, double eb,
     st->rec_min = 0xffffffffu;
     st->rec_max = 0;
     st->rec_maxdiff = 0;
-    for (int s = 0; s < kStreams; ++s) {
+    st->ndistinct = 0;
+    for (int s = 0; s < kCodeStreams; ++s) {
+        st->ch[s].enc = kEncEmpty;
+        st->ch[s].records = 0;
         StreamStats& g = st->st[s];
         for (int d = 0; d < kMaxDims; ++d) { g.minv[d] = 0xffffffffu; g.maxv[d] = 0; }
         g.maxall = 0;
@@ -907,8 +956,9 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     need += Arena::need(nd, 4) * 4;           // rel, rec, keep, diff
     need += Arena::need(n, 4) * 2;            // idrel, choice2
     need += Arena::need(corr_cap, 8) * 4;     // corrections idx/val + sorted copies
-    need += Arena::need(hist_stride * kStreams, 4) * 3;  // hist, prob, cum
-    need += Arena::need(64 * kStreams, 4) * 2;
+    need += Arena::need(hist_stride * kCodeStreams, 4) * 3;  // hist, prob, cum
+    need += Arena::need(64 * kCodeStreams, 4) * 2;
+    need += Arena::need(corr_cap, 4) * 2 + Arena::need(corr_cap, 8);  // correction gaps, ids, values
     need += 64 * 256;
     CHAIN_CUDA(ctx->frame.reserve(need));
     Arena& A = ctx->frame;
@@ -938,15 +988,18 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     double* corr_val = A.take<double>(corr_cap);
     uint64_t* corr_idx_s = A.take<uint64_t>(corr_cap);
     double* corr_val_s = A.take<double>(corr_cap);
-    uint32_t* hist = A.take<uint32_t>(hist_stride * kStreams);
-    uint32_t* prob = A.take<uint32_t>(hist_stride * kStreams);
-    uint32_t* cum = A.take<uint32_t>(hist_stride * kStreams);
-    uint32_t* tag_prob = A.take<uint32_t>(64 * kStreams);
-    uint32_t* tag_cum = A.take<uint32_t>(64 * kStreams);
+    uint32_t* hist = A.take<uint32_t>(hist_stride * kCodeStreams);
+    uint32_t* prob = A.take<uint32_t>(hist_stride * kCodeStreams);
+    uint32_t* cum = A.take<uint32_t>(hist_stride * kCodeStreams);
+    uint32_t* tag_prob = A.take<uint32_t>(64 * kCodeStreams);
+    uint32_t* tag_cum = A.take<uint32_t>(64 * kCodeStreams);
+    uint32_t* corr_gaps = A.take<uint32_t>(corr_cap);
+    uint32_t* corr_ids = A.take<uint32_t>(corr_cap);
+    uint64_t* corr_dict = A.take<uint64_t>(corr_cap);
     if (!tag_cum) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder frame arena too small");
 
     k_init_state<<<1, 1, 0, stream>>>(st, dims, n, eb, static_cast<uint64_t>(p_eff), threshold);
-    CHAIN_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * hist_stride * kStreams, stream));
+    CHAIN_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * hist_stride * kCodeStreams, stream));
 
     // ---- phase 1: extrema and quantization parameters
     const bool soa = layout == CHAIN_SOA;
@@ -1020,11 +1073,13 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     refs.s[2] = StreamRef{keep, dims, &st->nkeep, 0};
     refs.s[3] = StreamRef{choice2, 1, &st->B, 0};
     refs.s[4] = StreamRef{rel, dims, nullptr, n};
-    k_stream_stats<<<dim3(grid_for(n, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st);
-    k_value_hist<<<dim3(grid_for(nd, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, hist, hist_stride);
+    refs.s[kCorrGaps] = StreamRef{corr_gaps, 1, nullptr, 0};
+    refs.s[kCorrIds] = StreamRef{corr_ids, 1, nullptr, 0};
+    k_stream_stats<<<dim3(grid_for(n, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, 0);
+    k_value_hist<<<dim3(grid_for(nd, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, hist, hist_stride, 0);
     k_tables<<<dim3(kStreams, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob,
-                                                               tag_cum);
-    k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps);
+                                                               tag_cum, 0);
+    k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, 0, kStreams);
     CHAIN_LAUNCH_CHECK("plan");
     T.mark("stats+tables+plan", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
@@ -1035,11 +1090,42 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         return set_err(CHAIN_ERR_UNSUPPORTED, "more exact corrections than this build buffers (" +
                                                   std::to_string(hs->ncorr) + ")");
 
+    // ---- exact corrections: increasing index order, then gaps + value-id streams
+    if (hs->ncorr) {
+        if (nd > 0xffffffffull)
+            return set_err(CHAIN_ERR_UNSUPPORTED, "exact corrections need n * dims < 2^32 in this build");
+        const uint64_t nc = hs->ncorr;
+        const int bits = std::max(1, bitlen64(nd - 1));
+        uint32_t* scan32b = reinterpret_cast<uint32_t*>(scanbuf);
+        bool in_b = radix_sort_pairs<uint64_t>(corr_idx, key_a, val_a, key_b, val_b, nc, bits, counts, scan32b, stream);
+        k_gather_corrections<<<grid_for(nc), 256, 0, stream>>>(in_b ? val_b : val_a, in_b ? key_b : key_a, corr_val,
+                                                               corr_idx_s, corr_val_s, nc);
+        k_corr_gaps<<<grid_for(nc), 256, 0, stream>>>(corr_idx_s, nc, corr_gaps);
+        const uint64_t* vbits = reinterpret_cast<const uint64_t*>(corr_val_s);
+        in_b = radix_sort_pairs<uint64_t>(vbits, key_a, val_a, key_b, val_b, nc, 64, counts, scan32b, stream);
+        device_exclusive_scan<uint32_t>(DictIn{in_b ? key_b : key_a},
+                                        DictOut{in_b ? key_b : key_a, in_b ? val_b : val_a, corr_dict, corr_ids}, nc,
+                                        scan32b, &st->ndistinct, stream);
+        refs.s[kCorrGaps].count_const = nc;
+        refs.s[kCorrIds].count_const = nc;
+        const unsigned g = grid_for(nc, 256, 148u * 4u);
+        k_stream_stats<<<dim3(g, 2), 256, 0, stream>>>(refs, st, kCorrGaps);
+        k_value_hist<<<dim3(g, 2), 256, 0, stream>>>(refs, st, hist, hist_stride, kCorrGaps);
+        k_tables<<<dim3(2, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob, tag_cum,
+                                                          kCorrGaps);
+        k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, kCorrGaps, 2);
+        CHAIN_LAUNCH_CHECK("corrections");
+        CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
+        CHAIN_CUDA(cudaStreamSynchronize(stream));
+        if (hs->err) return status_from_err(hs->err);
+        T.mark("corrections", stream);
+    }
+
     // ---- phase 3: coding buffers
     uint64_t slots_total = 0, packed_total = 0, tags_total = 0, total_chunks = 0;
-    uint64_t slot_cap[kStreams] = {0}, slot_off[kStreams] = {0}, packed_off[kStreams] = {0},
-             packed_stride[kStreams] = {0}, tags_off[kStreams] = {0};
-    for (int s = 0; s < kStreams; ++s) {
+    uint64_t slot_cap[kCodeStreams] = {0}, slot_off[kCodeStreams] = {0}, packed_off[kCodeStreams] = {0},
+             packed_stride[kCodeStreams] = {0}, tags_off[kCodeStreams] = {0};
+    for (int s = 0; s < kCodeStreams; ++s) {
         const StreamChoice& c = hs->ch[s];
         if (c.enc == kEncRaw || c.enc == kEncTagged) {
             slot_cap[s] = ((3 * c.sec_S + 64) + 15) & ~15ull;
@@ -1063,11 +1149,11 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     }
     const uint64_t table_stride = 4 * kRansMaxAlphabet + 64;
     uint64_t etab_total = 0;
-    for (int s = 0; s < kStreams; ++s)
+    for (int s = 0; s < kCodeStreams; ++s)
         if (hs->ch[s].enc == kEncRaw || hs->ch[s].enc == kEncTagged) etab_total += hs->ch[s].sec_alphabet;
     const uint64_t max_pieces = total_chunks + 64;
-    uint64_t bound = header_bytes(dims) + 20 + 16 * hs->ncorr;
-    for (int s = 0; s < kStreams; ++s) {
+    uint64_t bound = header_bytes(dims) + 40 + 8ull * hs->ndistinct;
+    for (int s = 0; s < kCodeStreams; ++s) {
         const StreamChoice& c = hs->ch[s];
         bound += 12 + 13 + 1 + 9ull * c.dims;
         if (c.enc == kEncFixed) bound += packed_stride[s] * c.dims;
@@ -1077,7 +1163,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     }
     size_t need2 = Arena::need(slots_total, 1) + Arena::need(packed_total, 1) + Arena::need(tags_total + 1, 4) +
                    Arena::need(total_chunks + 1, 4) + Arena::need(total_chunks * 32 + 1, 4) +
-                   Arena::need(table_stride * kStreams, 1) + Arena::need(max_pieces, sizeof(Piece)) +
+                   Arena::need(table_stride * kCodeStreams, 1) + Arena::need(max_pieces, sizeof(Piece)) +
                    Arena::need(bound, 1) + Arena::need(etab_total + 1, 16) + 9 * 256;
     CHAIN_CUDA(ctx->coded.reserve(need2));
     Arena& C = ctx->coded;
@@ -1086,7 +1172,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     uint32_t* tags = C.take<uint32_t>(tags_total + 1);
     uint32_t* chunk_len = C.take<uint32_t>(total_chunks + 1);
     uint32_t* states = C.take<uint32_t>(total_chunks * 32 + 1);
-    uint8_t* tables = C.take<uint8_t>(table_stride * kStreams);
+    uint8_t* tables = C.take<uint8_t>(table_stride * kCodeStreams);
     Piece* pieces = C.take<Piece>(max_pieces);
     uint8_t* container = C.take<uint8_t>(bound);
     uint4* etab = C.take<uint4>(etab_total + 1);
@@ -1094,29 +1180,16 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     uint64_t etab_used = 0;
     if (packed_total) CHAIN_CUDA(cudaMemsetAsync(packed, 0, packed_total, stream));
 
-    // exact corrections in increasing index order
-    if (hs->ncorr) {
-        const uint64_t nc = hs->ncorr;
-        const int bits = std::max(1, bitlen64(nd - 1));
-        uint64_t* ka = reinterpret_cast<uint64_t*>(key_a);
-        uint64_t* kb2 = reinterpret_cast<uint64_t*>(key_b);
-        const bool in_b = radix_sort_pairs<uint64_t>(corr_idx, ka, val_a, kb2, val_b, nc, bits, counts,
-                                                     reinterpret_cast<uint32_t*>(scanbuf), stream);
-        k_gather_corrections<<<grid_for(nc), 256, 0, stream>>>(in_b ? val_b : val_a, in_b ? kb2 : ka, corr_val,
-                                                               corr_idx_s, corr_val_s, nc);
-    }
-
     RansJobs jobs{};
     jobs.njobs = 0;
     uint32_t first = 0;
     AssemblyIn ain{};
     ain.table_bytes = tables;
     ain.table_stride = table_stride;
-    ain.corr_idx = corr_idx_s;
-    ain.corr_val = corr_val_s;
+    ain.corr_dict = corr_dict;
     ain.input_dtype = static_cast<uint8_t>(esz);
     uint64_t chunk_base = 0;
-    for (int s = 0; s < kStreams; ++s) {
+    for (int s = 0; s < kCodeStreams; ++s) {
         const StreamChoice& c = hs->ch[s];
         const StreamRef& r = refs.s[s];
         if (c.enc == kEncFixed) {
@@ -1169,7 +1242,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     }
     jobs.total_blocks = first;
     T.mark("corrections+packing", stream);
-    k_serialize_tables<<<kStreams, 1024, 0, stream>>>(st, prob, tag_prob, hist_stride, tables, table_stride);
+    k_serialize_tables<<<kCodeStreams, 1024, 0, stream>>>(st, prob, tag_prob, hist_stride, tables, table_stride);
     T.mark("serialize_tables", stream);
     if (jobs.total_blocks) {
         k_enc_symbols<<<dim3(64, jobs.njobs), 256, 0, stream>>>(jobs);
