@@ -7,10 +7,10 @@
 //
 // Each 8-bit pass is three launches: a per-tile digit histogram, a device-wide
 // exclusive scan of the digit-major count table, and a stable scatter.  The scatter
-// ranks keys inside a tile with warp match_any + popc (each warp owns a contiguous
-// slice, processed 32 keys per round in order, so equal digits keep their input
-// order), reorders the tile by digit in shared memory, and writes each digit's run
-// to its global position with consecutive threads on consecutive addresses.
+// loads its whole tile at once, ranks keys with 8 ballots per 32 keys (each warp owns
+// a contiguous slice, processed 32 keys per round in order, so equal digits keep their
+// input order), reorders the tile by digit in shared memory, and writes each digit's
+// run to its global position with consecutive threads on consecutive addresses.
 #pragma once
 
 #include "chain_common.cuh"
@@ -64,17 +64,29 @@ radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict_
     const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * TILE;
     const uint64_t base = tile0 + static_cast<uint64_t>(warp) * (I * 32);
     KT key[I];
+    uint32_t val[I];
     uint32_t rank[I];
     const uint32_t lt = lanemask_lt();
+    // all loads first, so that they are in flight together
+#pragma unroll
+    for (int r = 0; r < I; ++r) {
+        const uint64_t i = base + static_cast<uint64_t>(r) * 32 + lane;
+        key[r] = i < n ? keys_in[i] : KT(0);
+        val[r] = i < n ? (vals_in ? vals_in[i] : static_cast<uint32_t>(i)) : 0u;
+    }
+    // stable rank within the warp: lanes with an equal digit found with 8 ballots
 #pragma unroll
     for (int r = 0; r < I; ++r) {
         const uint64_t i = base + static_cast<uint64_t>(r) * 32 + lane;
         const bool valid = i < n;
-        key[r] = valid ? keys_in[i] : KT(0);
         const uint32_t digit = static_cast<uint32_t>(key[r] >> shift) & 0xFFu;
-        const uint32_t active = __ballot_sync(0xffffffffu, valid);
-        uint32_t peers = 0;
-        if (valid) peers = __match_any_sync(active, digit);
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const bool bit = (digit >> b) & 1u;
+            const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+            peers &= bit ? bal : ~bal;
+        }
         const uint32_t prior = valid ? whist[warp][digit] : 0u;
         __syncwarp();
         rank[r] = prior + __popc(peers & lt);
@@ -108,7 +120,7 @@ radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict_
             const uint32_t digit = static_cast<uint32_t>(key[r] >> shift) & 0xFFu;
             const uint32_t lp = whist[warp][digit] + rank[r];
             skey[lp] = key[r];
-            sval[lp] = vals_in ? vals_in[i] : static_cast<uint32_t>(i);
+            sval[lp] = val[r];
         }
     }
     __syncthreads();
