@@ -1,30 +1,37 @@
 """Chain compressor benchmark (one JSON line on rank 0).
 
 Workload (default): the large single frame -- 16,777,216 float32 particles in
-[0,100]^3, 80% from 64 Gaussian blobs and 20% uniform, random order, eb = 1e-3 x range,
-p = 4, threshold = 2 (seeded synthetic data; the reference names no public dataset).
-A step = one compress of the frame followed by one decompress of its container.
+[0,100]^3, 80% from 64 Gaussian blobs and 20% uniform, random particle order,
+eb = 1e-3 x range, p = 4, threshold = 2.  Seeded synthetic data (the reference names no
+public dataset).  A step = one compress of the frame; the decompress of its container
+is timed the same way and reported beside it.
 
-  value  : compress throughput, GB/s of uncompressed input, device-resident input
-           (HBM -> container in HBM), max over ranks
-  e2e    : the same through the C ABI with pinned HOST buffers (H2D of the points
-           and D2H of the container inside the timed region)
+  value : compress throughput in GB/s of uncompressed input, input already in HBM,
+          container left in HBM; device time from CUDA events on the library's stream,
+          max over ranks
+  e2e   : the same through the C ABI with pinned HOST buffers: H2D of the points and
+          D2H of the container inside the timed region
   decompress : the same two numbers for the decoder (container -> float64 points)
+  roofline   : the dominant kernel of the compress step (rans_encode_kernel) against
+          the measured HBM copy bandwidth; roofline_decompress likewise for
+          rans_decode_kernel; path_roofline: (input + container bytes) / step time
 
 Multi-GPU: frames are independent, so N ranks compress N independent frames
-(replicas, weak scaling, no collective on the data path).
+(replicas, weak scaling, no collective on the data path; only the timing max-reduce).
 
---impl reference runs the reference CPU Chain (lcps_cpp / lcps_cpu_decompress built
-from the reference sources into oracle/_ref) on a bounded sample of the same workload
-with one process per host core.
+--impl reference: the reference's own CPU Chain (cpp/chain/lcps_cpp.cpp, built from
+the reference sources into oracle/_ref) on a bounded sample of the same workload (its
+first 2^20 particles), one process per host core up to 64, rank 0 only.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import re
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -37,6 +44,7 @@ for _p in (ROOT, ROOT / "oracle"):
 
 METRIC = "compress GB/s (uncompressed bytes/s) at eb=1e-3*range"
 UNIT = "GB/s"
+SAMPLE_N = 1 << 20
 
 
 def _peaks():
@@ -51,30 +59,29 @@ def _frame(config: str, rank: int):
 
     if config == "blobs":
         pts = W.blobs(W.BLOBS_N, seed=1 + rank)
-        return pts, W.eb_for(pts, 1e-3), 4, 2, "blobs-16M-f32"
+        return pts, W.eb_for(pts, 1e-3), 4, 2, "blobs-16M-f32 (64 Gaussian blobs + 20% uniform, random order)"
     if config == "column":
         pts = W.column(seed=rank)
-        return pts, W.eb_for(pts, 1e-3), 4, 2, "column-80703-f32"
+        return pts, W.eb_for(pts, 1e-3), 4, 2, "column-80703-f32 (dam-break-like lattice, random order)"
     if config == "trajectory":
         pts = W.trajectory(0, seed=2 + rank)
-        return pts, W.eb_for(pts, 1e-3), 4, 2, "trajectory-4M-f64"
+        return pts, W.eb_for(pts, 1e-3), 4, 2, "trajectory-4M-f64 (jittered lattice, periodic box)"
     raise SystemExit(f"unknown config {config}")
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.proc = None
-        self.path = None
+        self.path = tempfile.mktemp(suffix=".csv")
         try:
-            import tempfile
-            self.path = tempfile.mktemp(suffix=".csv")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={index}",
-                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 + ",".join("clocks_event_reasons." + f for f in self.FIELDS),
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
@@ -98,10 +105,38 @@ class Clocks:
                     pass
         if not rows:
             return None
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k, v in enumerate(r[2]) if v.lower() == "active"})
-        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": rows[0][1],
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({self.FIELDS[k] for r in rows for k, v in enumerate(r[2]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": rows[0][1], "reasons": reasons,
+                "samples": len(rows)}
+
+
+def _profile_traffic(kernel: str):
+    """dram read+write bytes per launch of `kernel` from the committed ncu summary."""
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        m = re.search(rf"^{kernel} traffic_bytes_per_launch: (\d+)", f.read_text(), re.M)
+        if m:
+            return int(m.group(1)), f.name
+    return None, None
+
+
+def _cpu_baseline(pts, eb, p, t):
+    """Reference CPU compress (oracle/_ref) of the first 2^20 particles, one core."""
+    import oracle
+
+    if not oracle.ref_available():
+        return None
+    sample = np.ascontiguousarray(pts[:SAMPLE_N])
+    oracle.ref_compress(sample[:4096], eb, p, t)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        oracle.ref_compress(sample, eb, p, t)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el > 10.0 or reps >= 4:
+            break
+    return {"value": round(reps * sample.nbytes / el / 1e9, 6), "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"first {len(sample)} particles of the same frame, {reps} compress call(s), "
+                      f"{el:.1f} s; reference lcps_cpp.lcps_compress2 is single-threaded"}
 
 
 def run_ours(args, rank: int, world: int):
@@ -109,14 +144,17 @@ def run_ours(args, rank: int, world: int):
 
     from chaincompressor_b200 import _native as N
 
-    torch.cuda.set_device(rank % max(1, torch.cuda.device_count()))
-    dev = torch.cuda.current_device()
+    ndev = max(1, torch.cuda.device_count())
+    dev = int(os.environ.get("LOCAL_RANK", rank)) % ndev
+    torch.cuda.set_device(dev)
     pts, eb, p, t, wl = _frame(args.config, rank)
     n, d = pts.shape
     esz = pts.dtype.itemsize
+    raw = n * d * esz
     soa_host = torch.from_numpy(np.ascontiguousarray(pts.T)).pin_memory()
     soa_dev = soa_host.to(f"cuda:{dev}")
-    codec = N.Codec(dev)
+    stream = torch.cuda.Stream(device=dev)
+    codec = N.Codec(dev, stream=stream.cuda_stream)
     dist = world > 1
     if dist:
         import torch.distributed as tdist
@@ -127,91 +165,184 @@ def run_ours(args, rank: int, world: int):
         torch.cuda.synchronize()
 
     dtype_code = N.CHAIN_F32 if esz == 4 else N.CHAIN_F64
-    # warm-up (also sizes the arenas)
+    comp = lambda ptr: codec.compress_ptr(ptr, dtype_code, N.CHAIN_SOA, n, d, eb, p, t)  # noqa: E731
     for _ in range(args.warmup):
-        codec.compress_ptr(soa_dev.data_ptr(), dtype_code, N.CHAIN_SOA, n, d, eb, p, t)
-    clen = codec.compress_ptr(soa_dev.data_ptr(), dtype_code, N.CHAIN_SOA, n, d, eb, p, t)
+        comp(soa_dev.data_ptr())
+    clen = comp(soa_dev.data_ptr())
     cont_dev = torch.empty(clen, dtype=torch.uint8, device=f"cuda:{dev}")
     codec.result_copy_to(cont_dev.data_ptr(), clen)
     cont_host = torch.empty(clen, dtype=torch.uint8).pin_memory()
     cont_host.copy_(cont_dev.cpu())
     out_dev = torch.empty((n, d), dtype=torch.float64, device=f"cuda:{dev}")
     out_host = torch.empty((n, d), dtype=torch.float64).pin_memory()
+    decomp = lambda src, dst: codec.decompress_ptr(src, clen, dst, n * d * 8)  # noqa: E731
     for _ in range(args.warmup):
-        codec.decompress_ptr(cont_dev.data_ptr(), clen, out_dev.data_ptr(), out_dev.numel() * 8)
+        decomp(cont_dev.data_ptr(), out_dev.data_ptr())
 
-    def timed(fn):
+    def timed(fn, stages=False):
+        """Device time per step from CUDA events on the library stream (the library
+        calls are synchronous, so the events bracket all of their device work)."""
+        codec.set_stage_timing(stages)
+        acc = {}
         barrier()
-        t0 = time.perf_counter()
+        l0 = N.launch_count()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
         for _ in range(args.steps):
             fn()
+            if stages:
+                for name, ms in codec.stage_times():
+                    acc[name] = acc.get(name, 0.0) + ms
+        ev1.record(stream)
         barrier()
-        return (time.perf_counter() - t0) / args.steps
+        launches = N.launch_count() - l0
+        codec.set_stage_timing(False)
+        return ev0.elapsed_time(ev1) / 1e3 / args.steps, launches, {k: v / args.steps for k, v in acc.items()}
 
-    # The library call is synchronous (it ends with a stream synchronize), so host
-    # time around it brackets the device work; it is cross-checked with CUDA events
-    # recorded on the library stream below.
     clocks = Clocks(dev)
-    t_c = timed(lambda: codec.compress_ptr(soa_dev.data_ptr(), dtype_code, N.CHAIN_SOA, n, d, eb, p, t))
-    t_d = timed(lambda: codec.decompress_ptr(cont_dev.data_ptr(), clen, out_dev.data_ptr(), out_dev.numel() * 8))
+    t_c, launches_c, stages_c = timed(lambda: comp(soa_dev.data_ptr()), stages=True)
+    t_d, launches_d, stages_d = timed(lambda: decomp(cont_dev.data_ptr(), out_dev.data_ptr()), stages=True)
 
     def e2e_c():
-        codec.compress_ptr(soa_host.data_ptr(), dtype_code, N.CHAIN_SOA, n, d, eb, p, t)
+        comp(soa_host.data_ptr())
         codec.result_copy_to(cont_host.data_ptr(), clen)
 
-    def e2e_d():
-        codec.decompress_ptr(cont_host.data_ptr(), clen, out_host.data_ptr(), out_host.numel() * 8)
-
-    t_ce = timed(e2e_c)
-    t_de = timed(e2e_d)
+    t_ce, _, _ = timed(e2e_c)
+    t_de, _, _ = timed(lambda: decomp(cont_host.data_ptr(), out_host.data_ptr()))
     clk = clocks.stop()
     if dist:
         tt = torch.tensor([t_c, t_d, t_ce, t_de], dtype=torch.float64, device=f"cuda:{dev}")
         tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
         t_c, t_d, t_ce, t_de = tt.tolist()
-    # correctness of the measured run
     dec = out_host.numpy()
     err = float(np.abs(dec - pts.astype(np.float64)).max())
-    raw = n * d * esz
-    gbs = lambda sec: world * raw / sec / 1e9  # noqa: E731
+
+    # roofline of the dominant kernels: algorithmic bytes per launch / event-timed duration
+    sys.path.insert(0, str(ROOT / "tests"))
+    import lcg2_inspect
+
+    info = lcg2_inspect.inspect(bytes(cont_host.numpy()))
+    rans_syms = sum(c["section"]["symbols"] for c in info["components"].values() if "section" in c)
+    rans_bytes = sum(c["section"]["payload"] + 132 * c["section"]["chunks"]
+                     for c in info["components"].values() if "section" in c)
     peaks, src = _peaks()
+    peak = float(peaks["hbm_gbs"])
+
+    def roof(kernel, stage_ms, alg_bytes):
+        if not stage_ms:
+            return None
+        ach = alg_bytes / (stage_ms / 1e3) / 1e9
+        traffic, prof = _profile_traffic(kernel)
+        return {"kernel": kernel, "bound": "hbm", "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                "avg_launch_ms": round(stage_ms, 4), "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic_source": prof}
+
+    gbs = lambda sec: world * raw / sec / 1e9  # noqa: E731
     line = {
         "metric": METRIC, "value": round(gbs(t_c), 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round((t_c + t_d) * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64-quantize/u32-codes", "data": "synthetic",
-        "config": {"workload": wl, "n": n, "dims": d, "eb": eb, "eb_frac_of_range": 1e-3, "p": p, "threshold": t,
-                   "l2_flush": "inputs larger than L2 (input %d MB)" % (raw // 2**20),
-                   "parallelism": f"replicas{world}"},
+        "warmup": args.warmup, "ms_per_step": round(t_c * 1e3, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 quantize, u32 codes, u8 rANS", "data": "synthetic (seeded)",
+        "config": {"workload": wl, "n": n, "dims": d, "input_dtype": str(pts.dtype), "eb": eb,
+                   "eb_frac_of_range": 1e-3, "p": p, "threshold": t,
+                   "l2_flush": f"inputs larger than L2 ({raw >> 20} MB input per frame)",
+                   "parallelism": f"replicas x{world} (independent frames)"},
         "e2e": {"value": round(gbs(t_ce), 3), "unit": UNIT, "h2d_bytes_per_step": raw, "d2h_bytes_per_step": clen},
-        "decompress": {"value": round(gbs(t_d), 3), "unit": UNIT,
+        "gpu_launches": launches_c, "gpu_launches_per_step": launches_c // max(1, args.steps),
+        "roofline": roof("rans_encode_kernel", stages_c.get("rans_encode"), 4 * rans_syms + rans_bytes),
+        "decompress": {"value": round(gbs(t_d), 3), "unit": UNIT, "ms_per_step": round(t_d * 1e3, 4),
+                       "gpu_launches": launches_d,
                        "e2e": {"value": round(gbs(t_de), 3), "unit": UNIT, "h2d_bytes_per_step": clen,
-                               "d2h_bytes_per_step": n * d * 8}},
+                               "d2h_bytes_per_step": n * d * 8},
+                       "roofline": roof("rans_decode_kernel", stages_d.get("rans_decode"),
+                                        4 * rans_syms + rans_bytes)},
+        "path_roofline": {"compress_frac": round((raw + clen) / t_c / 1e9 / peak, 4),
+                          "decompress_frac": round((clen + n * d * 8) / t_d / 1e9 / peak, 4),
+                          "note": "algorithmic bytes = input + container (compress), container + "
+                                  "float64 output (decompress), per step / device time"},
         "compressed_bytes": clen, "ratio": round(raw / clen, 4), "max_abs_err_over_eb": err / eb,
+        "exact_corrections": info["corrections"]["count"],
+        "stages_ms": {"compress": {k: round(v, 4) for k, v in stages_c.items()},
+                      "decompress": {k: round(v, 4) for k, v in stages_d.items()}},
         "ms": {"compress": t_c * 1e3, "decompress": t_d * 1e3, "compress_e2e": t_ce * 1e3,
                "decompress_e2e": t_de * 1e3},
-        "peak_source": src,
     }
     if clk:
         line["clocks"] = clk
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = _cpu_baseline(pts, eb, p, t)
     codec.close()
     return line
+
+
+_REF_JOB = None
+
+
+def _ref_init(job):
+    global _REF_JOB
+    _REF_JOB = job
+
+
+def _ref_worker(_):
+    import oracle
+
+    pts, eb, p, t = _REF_JOB
+    t0 = time.perf_counter()
+    oracle.ref_compress(pts, eb, p, t)
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    import multiprocessing as mp
+
+    import oracle
+
+    if not oracle.ref_available():
+        return {"impl": "reference", "unavailable": "reference CPU modules (oracle/_ref) were not built"}
+    pts, eb, p, t, wl = _frame(args.config, 0)
+    sample = np.ascontiguousarray(pts[:SAMPLE_N])
+    cores = max(1, min(os.cpu_count() or 1, 64))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_ref_init, initargs=((sample, eb, p, t),)) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_worker, range(cores))
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            pool.map(_ref_worker, range(cores))
+            times.append(time.perf_counter() - t0)
+    step = float(np.mean(times))
+    value = cores * sample.nbytes / step / 1e9
+    n, d = pts.shape
+    sample_desc = (f"each step: {cores} processes each compress the first {len(sample)} particles "
+                   f"({sample.nbytes >> 20} MB) of the frame with lcps_cpp.lcps_compress2")
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": wl, "n": n, "dims": d, "eb": eb, "eb_frac_of_range": 1e-3, "p": p, "threshold": t},
+        "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": sample_desc},
+        "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="blobs", choices=["blobs", "column", "trajectory"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
-        if rank != 0:
-            return
-        print(json.dumps({"impl": "reference", "unavailable": "not implemented yet"}))
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
         return
     if world > 1:
         import datetime
@@ -224,6 +355,7 @@ def main():
     line = run_ours(args, rank, world)
     if world > 1:
         import torch.distributed as tdist
+
         tdist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))

@@ -30,7 +30,7 @@ CHAIN_SOA, CHAIN_AOS = 0, 1
 # Every entry point declared in include/chain_b200.h.
 EXPORTS = ("chain_ctx_create", "chain_ctx_destroy", "chain_last_error_message", "chain_compress_bound",
            "chain_compress", "chain_result_copy", "chain_result_device_ptr", "chain_peek", "chain_decompress",
-           "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times")
+           "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count")
 
 
 class ChainError(RuntimeError):
@@ -72,7 +72,7 @@ def load() -> ctypes.CDLL:
         L.chain_debug_streams.argtypes = [P, P, P, ctypes.POINTER(u64), P, ctypes.POINTER(u64), P,
                                           ctypes.POINTER(u64), P]
         for f in ("chain_ctx_create", "chain_compress", "chain_result_copy", "chain_peek", "chain_decompress",
-                  "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times"):
+                  "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count"):
             getattr(L, f).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -202,6 +202,11 @@ def peek(data: bytes):
     src = ctypes.create_string_buffer(data, len(data))
     _check(L.chain_peek(ctypes.addressof(src), len(data), ctypes.byref(n), ctypes.byref(d), ctypes.byref(t)))
     return n.value, d.value, t.value
+
+
+def launch_count() -> int:
+    """Kernel launches issued by the library on this thread so far."""
+    return load().chain_launch_count()
 
 
 def compress_bound(n: int, dims: int) -> int:

@@ -13,6 +13,8 @@
 namespace chain {
 
 static thread_local std::string g_last_error;
+static thread_local uint64_t g_launches = 0;
+uint64_t& launch_counter() { return g_launches; }
 
 chain_status set_err(chain_status st, const std::string& msg) {
     g_last_error = msg;
@@ -217,6 +219,8 @@ chain_status chain_debug_streams(chain_ctx* ctx, int64_t* idrel, int64_t* diff, 
     if ((s = fetch(d.rel, d.n * d.dims, rel)) != CHAIN_OK) return s;
     return CHAIN_OK;
 }
+
+uint64_t chain_launch_count(void) { return g_launches; }
 
 chain_status chain_set_stage_timing(chain_ctx* ctx, int enabled) {
     if (!ctx) return set_err(CHAIN_ERR_INVALID_ARGUMENT, "null context");

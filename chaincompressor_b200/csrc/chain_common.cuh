@@ -32,6 +32,11 @@ enum ErrBits : uint32_t {
 // Component encodings of the container (see chain_format.h).
 enum Encoding : uint8_t { kEncEmpty = 0, kEncTagged = 1, kEncFixed = 2, kEncRaw = 3 };
 
+// Host-side count of kernel launches issued by the library (tracing aid: every launch
+// site calls count_launch()).
+uint64_t& launch_counter();
+inline void count_launch() { ++launch_counter(); }
+
 __host__ __device__ inline int bitlen32(uint32_t v) {
 #ifdef __CUDA_ARCH__
     return 32 - __clz(v);

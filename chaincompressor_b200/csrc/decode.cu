@@ -427,8 +427,8 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     const uint8_t* dcont = static_cast<const uint8_t*>(container);
     size_t base_need = host_in ? Arena::need(len + 16, 1) : 0;
     if (!host_in) {
-        k_dec_init<<<1, 1, 0, stream>>>(st);
-        k_parse<<<1, 1, 0, stream>>>(dcont, len, st);
+        k_dec_init<<<1, 1, 0, stream>>>(st); count_launch();
+        k_parse<<<1, 1, 0, stream>>>(dcont, len, st); count_launch();
         CHAIN_LAUNCH_CHECK("parse");
         CHAIN_CUDA(cudaMemcpyAsync(&hs->plan, &st->plan, sizeof(DecodePlan), cudaMemcpyDeviceToHost, stream));
         CHAIN_CUDA(cudaStreamSynchronize(stream));
@@ -484,7 +484,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         CHAIN_CUDA(cudaMemcpyAsync(d, container, len, cudaMemcpyHostToDevice, stream));
         dcont = d;
         hs->plan = plan;
-        k_dec_init<<<1, 1, 0, stream>>>(st);
+        k_dec_init<<<1, 1, 0, stream>>>(st); count_launch();
         CHAIN_CUDA(cudaMemcpyAsync(&st->plan, &hs->plan, sizeof(DecodePlan), cudaMemcpyHostToDevice, stream));
         T.mark("h2d_container", stream);
     }
@@ -561,9 +561,9 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     CHAIN_CUDA(cudaMemcpyAsync(d_states_first, states_first, sizeof(uint64_t) * kCodeStreams, cudaMemcpyHostToDevice,
                                stream));
     if (nsec) {
-        k_section_setup<<<nsec, 1024, 0, stream>>>(refs, dcont, st);
-        k_lookup<<<dim3(256, nsec), 256, 0, stream>>>(refs, st);
-        k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states, d_states_first);
+        k_section_setup<<<nsec, 1024, 0, stream>>>(refs, dcont, st); count_launch();
+        k_lookup<<<dim3(256, nsec), 256, 0, stream>>>(refs, st); count_launch();
+        k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states, d_states_first); count_launch();
         T.mark("tables", stream);
         rans_plan_smem(jobs, true);
         {  // per device, cheap; set on every call
@@ -572,7 +572,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
             CHAIN_CUDA(cudaFuncSetAttribute(rans_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             static_cast<int>(rans_dec_smem(jobs))));
         }
-        rans_decode_kernel<<<jobs.total_blocks, 32 * kRansWarps, rans_dec_smem(jobs), stream>>>(jobs, &st->err);
+        rans_decode_kernel<<<jobs.total_blocks, 32 * kRansWarps, rans_dec_smem(jobs), stream>>>(jobs, &st->err); count_launch();
     }
     CHAIN_LAUNCH_CHECK("entropy decode");
     T.mark("rans_decode", stream);
@@ -581,7 +581,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         const CompPlan& c = plan.comp[s];
         const CompPlan* dc = &st->plan.comp[s];
         if (c.enc == kEncFixed) {
-            k_unpack_fixed<<<dgrid(c.records * c.dims), 256, 0, stream>>>(dcont, dc, streams[s], st);
+            k_unpack_fixed<<<dgrid(c.records * c.dims), 256, 0, stream>>>(dcont, dc, streams[s], st); count_launch();
         } else if (c.enc == kEncTagged) {
             uint32_t* tg = tags + tag_off[s];
             device_exclusive_scan<uint64_t>(TagIn{tg, c.dims},
@@ -589,7 +589,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
                                             scanbuf, static_cast<uint64_t*>(nullptr), stream);
         }
     }
-    if (tags_total) k_check_tagged<<<1, 1, 0, stream>>>(st, st);
+    if (tags_total) k_check_tagged<<<1, 1, 0, stream>>>(st, st); count_launch();
     CHAIN_LAUNCH_CHECK("unpack");
     T.mark("unpack", stream);
 
@@ -614,8 +614,8 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     int rounds = 1;
     while ((1ull << rounds) < N) ++rounds;
     for (int r = 0; r < rounds + 1; ++r) {
-        k_jump<<<dgrid(N), 256, 0, stream>>>(parent, chained, zeros_dev, N, st, moved);
-        k_jump_flag<<<1, 1, 0, stream>>>(st, moved);
+        k_jump<<<dgrid(N), 256, 0, stream>>>(parent, chained, zeros_dev, N, st, moved); count_launch();
+        k_jump_flag<<<1, 1, 0, stream>>>(st, moved); count_launch();
     }
     CHAIN_LAUNCH_CHECK("levels");
     T.mark("pointer_jump", stream);
@@ -628,22 +628,22 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     if (out_dtype == CHAIN_F64) {
         double* o = static_cast<double*>(dout);
         if (soa) {
-            k_reconstruct<double, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+            k_reconstruct<double, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr); count_launch();
             if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<double, true>{streams[kCorrIds], dcont, st, st, o},
                                                      ncx, sb, static_cast<uint64_t*>(nullptr), stream);
         } else {
-            k_reconstruct<double, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+            k_reconstruct<double, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr); count_launch();
             if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<double, false>{streams[kCorrIds], dcont, st, st, o},
                                                      ncx, sb, static_cast<uint64_t*>(nullptr), stream);
         }
     } else {
         float* o = static_cast<float*>(dout);
         if (soa) {
-            k_reconstruct<float, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+            k_reconstruct<float, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr); count_launch();
             if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<float, true>{streams[kCorrIds], dcont, st, st, o},
                                                      ncx, sb, static_cast<uint64_t*>(nullptr), stream);
         } else {
-            k_reconstruct<float, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr);
+            k_reconstruct<float, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr); count_launch();
             if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<float, false>{streams[kCorrIds], dcont, st, st, o},
                                                      ncx, sb, static_cast<uint64_t*>(nullptr), stream);
         }

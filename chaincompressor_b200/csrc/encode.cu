@@ -917,13 +917,13 @@ template <typename FT, bool SOA, typename KT>
 static void launch_quantize(const void* pts, uint64_t n, uint32_t D, EncState* st, void* key, uint32_t* rel,
                             uint64_t* cidx, double* cval, uint64_t cap, cudaStream_t s) {
     k_quantize<FT, SOA, KT><<<grid_for(n), 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st,
-                                                         static_cast<KT*>(key), rel, cidx, cval, cap);
+                                                         static_cast<KT*>(key), rel, cidx, cval, cap); count_launch();
 }
 
 template <typename FT, bool SOA>
 static void launch_minmax(const void* pts, uint64_t n, uint32_t D, EncState* st, cudaStream_t s) {
     dim3 g(grid_for(n, 256, 148u * 8u), D);
-    k_minmax<FT, SOA><<<g, 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st);
+    k_minmax<FT, SOA><<<g, 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st); count_launch();
 }
 
 chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype, chain_layout layout, uint64_t n,
@@ -998,7 +998,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     uint64_t* corr_dict = A.take<uint64_t>(corr_cap);
     if (!tag_cum) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder frame arena too small");
 
-    k_init_state<<<1, 1, 0, stream>>>(st, dims, n, eb, static_cast<uint64_t>(p_eff), threshold);
+    k_init_state<<<1, 1, 0, stream>>>(st, dims, n, eb, static_cast<uint64_t>(p_eff), threshold); count_launch();
     CHAIN_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * hist_stride * kCodeStreams, stream));
 
     // ---- phase 1: extrema and quantization parameters
@@ -1007,7 +1007,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
                             : launch_minmax<float, false>(pts, n, dims, st, stream);
     else soa ? launch_minmax<double, true>(pts, n, dims, st, stream)
              : launch_minmax<double, false>(pts, n, dims, st, stream);
-    k_qparams<<<1, 1, 0, stream>>>(st);
+    k_qparams<<<1, 1, 0, stream>>>(st); count_launch();
     CHAIN_LAUNCH_CHECK("encoder phase 1");
     T.mark("extrema", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
@@ -1034,14 +1034,14 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         if (wide) {
             const bool in_b = radix_sort_pairs<uint64_t>(key_idx, key_a, val_a, key_b, val_b, n, key_bits, counts,
                                                          reinterpret_cast<uint32_t*>(scanbuf), stream);
-            k_level1<uint64_t><<<grid_for(n), 256, 0, stream>>>(in_b ? key_b : key_a, in_b ? val_b : val_a, n, st, idrel);
+            k_level1<uint64_t><<<grid_for(n), 256, 0, stream>>>(in_b ? key_b : key_a, in_b ? val_b : val_a, n, st, idrel); count_launch();
         } else {
             uint32_t* k32 = reinterpret_cast<uint32_t*>(key_idx);
             uint32_t* ka = reinterpret_cast<uint32_t*>(key_a);
             uint32_t* kb = reinterpret_cast<uint32_t*>(key_b);
             const bool in_b = radix_sort_pairs<uint32_t>(k32, ka, val_a, kb, val_b, n, key_bits, counts,
                                                          reinterpret_cast<uint32_t*>(scanbuf), stream);
-            k_level1<uint32_t><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel);
+            k_level1<uint32_t><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel); count_launch();
         }
     } else {
         CHAIN_CUDA(cudaMemsetAsync(idrel, 0, sizeof(uint32_t) * n, stream));
@@ -1057,11 +1057,11 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
                                         ExplicitOut<uint32_t>{reinterpret_cast<uint32_t*>(key_idx), st, rec}, n,
                                         scan32, &st->B, stream);
     T.mark("explicit_records", stream);
-    k_l2_stats<<<grid_for(n), 256, 0, stream>>>(rec, st);
-    k_l2_params<<<1, 1, 0, stream>>>(st);
+    k_l2_stats<<<grid_for(n), 256, 0, stream>>>(rec, st); count_launch();
+    k_l2_params<<<1, 1, 0, stream>>>(st); count_launch();
     device_exclusive_scan<uint32_t>(Level2In{rec, st, l2}, Level2Out{rec, st, choice2, keep, diff}, n, scan32,
                                     &st->ndiff, stream);
-    k_l2_counts<<<1, 1, 0, stream>>>(st);
+    k_l2_counts<<<1, 1, 0, stream>>>(st); count_launch();
     CHAIN_LAUNCH_CHECK("level 2");
     T.mark("level2", stream);
     // The level-2 scan covers n >= B entries; its functors ignore entries j >= B (read
@@ -1075,11 +1075,11 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     refs.s[4] = StreamRef{rel, dims, nullptr, n};
     refs.s[kCorrGaps] = StreamRef{corr_gaps, 1, nullptr, 0};
     refs.s[kCorrIds] = StreamRef{corr_ids, 1, nullptr, 0};
-    k_stream_stats<<<dim3(grid_for(n, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, 0);
-    k_value_hist<<<dim3(grid_for(nd, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, hist, hist_stride, 0);
+    k_stream_stats<<<dim3(grid_for(n, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, 0); count_launch();
+    k_value_hist<<<dim3(grid_for(nd, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, hist, hist_stride, 0); count_launch();
     k_tables<<<dim3(kStreams, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob,
-                                                               tag_cum, 0);
-    k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, 0, kStreams);
+                                                               tag_cum, 0); count_launch();
+    k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, 0, kStreams); count_launch();
     CHAIN_LAUNCH_CHECK("plan");
     T.mark("stats+tables+plan", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
@@ -1099,8 +1099,8 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         uint32_t* scan32b = reinterpret_cast<uint32_t*>(scanbuf);
         bool in_b = radix_sort_pairs<uint64_t>(corr_idx, key_a, val_a, key_b, val_b, nc, bits, counts, scan32b, stream);
         k_gather_corrections<<<grid_for(nc), 256, 0, stream>>>(in_b ? val_b : val_a, in_b ? key_b : key_a, corr_val,
-                                                               corr_idx_s, corr_val_s, nc);
-        k_corr_gaps<<<grid_for(nc), 256, 0, stream>>>(corr_idx_s, nc, corr_gaps);
+                                                               corr_idx_s, corr_val_s, nc); count_launch();
+        k_corr_gaps<<<grid_for(nc), 256, 0, stream>>>(corr_idx_s, nc, corr_gaps); count_launch();
         const uint64_t* vbits = reinterpret_cast<const uint64_t*>(corr_val_s);
         in_b = radix_sort_pairs<uint64_t>(vbits, key_a, val_a, key_b, val_b, nc, 64, counts, scan32b, stream);
         device_exclusive_scan<uint32_t>(DictIn{in_b ? key_b : key_a},
@@ -1109,11 +1109,11 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         refs.s[kCorrGaps].count_const = nc;
         refs.s[kCorrIds].count_const = nc;
         const unsigned g = grid_for(nc, 256, 148u * 4u);
-        k_stream_stats<<<dim3(g, 2), 256, 0, stream>>>(refs, st, kCorrGaps);
-        k_value_hist<<<dim3(g, 2), 256, 0, stream>>>(refs, st, hist, hist_stride, kCorrGaps);
+        k_stream_stats<<<dim3(g, 2), 256, 0, stream>>>(refs, st, kCorrGaps); count_launch();
+        k_value_hist<<<dim3(g, 2), 256, 0, stream>>>(refs, st, hist, hist_stride, kCorrGaps); count_launch();
         k_tables<<<dim3(2, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob, tag_cum,
-                                                          kCorrGaps);
-        k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, kCorrGaps, 2);
+                                                          kCorrGaps); count_launch();
+        k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, kCorrGaps, 2); count_launch();
         CHAIN_LAUNCH_CHECK("corrections");
         CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
         CHAIN_CUDA(cudaStreamSynchronize(stream));
@@ -1197,8 +1197,8 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
                 const uint64_t nwords = (c.records * c.width[d] + 31) / 32;
                 uint32_t* words = reinterpret_cast<uint32_t*>(packed + packed_off[s] + packed_stride[s] * d);
                 k_pack_fixed<<<grid_for(nwords), 256, 0, stream>>>(r.data, c.dims, d, c.records,
-                                                                     hs->st[s].minv[d], c.width[d], words, nwords);
-                k_words_to_bytes<<<grid_for(nwords), 256, 0, stream>>>(words, nwords);
+                                                                     hs->st[s].minv[d], c.width[d], words, nwords); count_launch();
+                k_words_to_bytes<<<grid_for(nwords), 256, 0, stream>>>(words, nwords); count_launch();
             }
             ain.packed[s] = packed + packed_off[s];
             ain.packed_dim_stride[s] = packed_stride[s];
@@ -1206,12 +1206,12 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         const uint32_t* symbols = r.data;
         if (c.enc == kEncTagged) {
             uint32_t* tg = tags + tags_off[s];
-            k_tags<<<grid_for(c.records), 256, 0, stream>>>(r.data, c.dims, c.records, tg);
+            k_tags<<<grid_for(c.records), 256, 0, stream>>>(r.data, c.dims, c.records, tg); count_launch();
             uint32_t* words = reinterpret_cast<uint32_t*>(packed + packed_off[s]);
             device_exclusive_scan<uint64_t>(TagBitsIn{tg, c.dims}, TagPackOut{r.data, tg, c.dims, words}, c.records,
                                             scanbuf, static_cast<uint64_t*>(nullptr), stream);
             const uint64_t nwords = (c.packed_bits + 31) / 32;
-            k_words_to_bytes<<<grid_for(nwords), 256, 0, stream>>>(words, nwords);
+            k_words_to_bytes<<<grid_for(nwords), 256, 0, stream>>>(words, nwords); count_launch();
             ain.packed[s] = packed + packed_off[s];
             symbols = tg;
         }
@@ -1242,10 +1242,10 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     }
     jobs.total_blocks = first;
     T.mark("corrections+packing", stream);
-    k_serialize_tables<<<kCodeStreams, 1024, 0, stream>>>(st, prob, tag_prob, hist_stride, tables, table_stride);
+    k_serialize_tables<<<kCodeStreams, 1024, 0, stream>>>(st, prob, tag_prob, hist_stride, tables, table_stride); count_launch();
     T.mark("serialize_tables", stream);
     if (jobs.total_blocks) {
-        k_enc_symbols<<<dim3(64, jobs.njobs), 256, 0, stream>>>(jobs);
+        k_enc_symbols<<<dim3(64, jobs.njobs), 256, 0, stream>>>(jobs); count_launch();
         rans_plan_smem(jobs, false);
         {  // per device, cheap; set on every call
             CHAIN_CUDA(cudaFuncSetAttribute(rans_encode_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -1253,12 +1253,12 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
             CHAIN_CUDA(cudaFuncSetAttribute(rans_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             static_cast<int>(rans_enc_smem(jobs))));
         }
-        rans_encode_kernel<<<jobs.total_blocks, 32 * kRansWarps, rans_enc_smem(jobs), stream>>>(jobs, &st->err);
+        rans_encode_kernel<<<jobs.total_blocks, 32 * kRansWarps, rans_enc_smem(jobs), stream>>>(jobs, &st->err); count_launch();
     }
     CHAIN_LAUNCH_CHECK("entropy coding");
     T.mark("rans_encode", stream);
-    k_layout<<<1, 1, 0, stream>>>(st, ain, container, pieces, static_cast<uint32_t>(max_pieces));
-    k_copy_pieces<<<148u * 8u, 256, 0, stream>>>(pieces, st, container);
+    k_layout<<<1, 1, 0, stream>>>(st, ain, container, pieces, static_cast<uint32_t>(max_pieces)); count_launch();
+    k_copy_pieces<<<148u * 8u, 256, 0, stream>>>(pieces, st, container); count_launch();
     CHAIN_LAUNCH_CHECK("assembly");
     T.mark("assemble", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));

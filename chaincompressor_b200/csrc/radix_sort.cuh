@@ -167,11 +167,11 @@ bool radix_sort_pairs(const KT* keys_in, KT* keys_a, uint32_t* vals_a, KT* keys_
         const uint32_t* vin = p == 0 ? nullptr : (p % 2 == 1 ? vals_a : vals_b);
         KT* kout = p % 2 == 0 ? keys_a : keys_b;
         uint32_t* vout = p % 2 == 0 ? vals_a : vals_b;
-        radix_hist_kernel<KT><<<tiles, kSortThreads, 0, stream>>>(kin, n, shift, counts, tiles);
+        radix_hist_kernel<KT><<<tiles, kSortThreads, 0, stream>>>(kin, n, shift, counts, tiles); count_launch();
         const uint64_t ncounts = static_cast<uint64_t>(tiles) * kSortBins;
         device_exclusive_scan<uint32_t>(CountIn{counts}, CountOut{counts}, ncounts, scan_buf,
                                         static_cast<uint32_t*>(nullptr), stream);
-        radix_scatter_kernel<KT><<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, shift, counts, tiles);
+        radix_scatter_kernel<KT><<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, shift, counts, tiles); count_launch();
     }
     return passes % 2 == 0;
 }

@@ -174,10 +174,10 @@ void device_exclusive_scan(InF in, OutF out, uint64_t n, T* tile_buf, T* total, 
         if (total) cudaMemsetAsync(total, 0, sizeof(T), stream);
         return;
     }
-    scan_reduce_kernel<T, InF, Op><<<static_cast<unsigned>(tiles), kScanThreads, 0, stream>>>(in, n, tile_buf, op);
-    scan_tilesums_kernel<T, Op><<<1, 1024, 0, stream>>>(tile_buf, tiles, total, op);
+    scan_reduce_kernel<T, InF, Op><<<static_cast<unsigned>(tiles), kScanThreads, 0, stream>>>(in, n, tile_buf, op); count_launch();
+    scan_tilesums_kernel<T, Op><<<1, 1024, 0, stream>>>(tile_buf, tiles, total, op); count_launch();
     scan_apply_kernel<T, InF, OutF, Op><<<static_cast<unsigned>(tiles), kScanThreads, 0, stream>>>(in, out, n,
-                                                                                               tile_buf, op);
+                                                                                               tile_buf, op); count_launch();
 }
 
 }  // namespace chain

@@ -129,6 +129,9 @@ CHAIN_API chain_status chain_debug_streams(chain_ctx* ctx, int64_t* idrel, int64
  * milliseconds since the previous stage) and their count.  Tracing aid only: timing
  * adds one event record per stage. */
 CHAIN_API chain_status chain_set_stage_timing(chain_ctx* ctx, int enabled);
+
+/* Number of CUDA kernels this thread's library calls have launched so far. */
+CHAIN_API uint64_t chain_launch_count(void);
 CHAIN_API int chain_stage_times(const chain_ctx* ctx, const char** names, float* ms, int max);
 
 #ifdef __cplusplus
