@@ -123,3 +123,22 @@ def test_pybind_surface_matches_reference_api():
     assert np.array_equal(soa, out.T)
     with pytest.raises(ValueError):
         chain_caller.chain_gpu(_soa(pts), 0.0, p, t, 0)
+
+
+GOLDEN = sorted((__import__("pathlib").Path(__file__).parent / "golden").glob("*.npz"))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
+def test_gpu_matches_reference_golden(codec, path):
+    """GPU streams and decoded float64 coordinates equal the reference CPU Chain's
+    (fixtures made from the reference modules by tests/golden/make_golden.py)."""
+    g = np.load(path)
+    pts = g["points"]
+    kw = {"bl": bool(g["bl"]), "l1": bool(g["l1"]), "l2": bool(g["l2"])}
+    n, d = pts.shape
+    data = codec.compress(_soa(pts), float(g["eb"]), int(g["p"]), int(g["threshold"]), layout=N.CHAIN_SOA, **kw)
+    got = codec.debug_streams(n, d)
+    for k in ("idrel", "diff", "keep", "choice2", "rel"):
+        assert np.array_equal(got[k], g[k]), k
+    dec = codec.decompress(data)
+    assert np.array_equal(dec.view(np.uint64), g["decoded"].view(np.uint64))
