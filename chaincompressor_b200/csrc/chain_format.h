@@ -37,8 +37,9 @@
 //   raw (3):    rANS section over the record-major values
 // rANS section:
 //   u8 prec, u32 alphabet, u32 table_bytes, table tokens (rans.cuh), u64 symbols per
-//   chunk S (multiple of 32), u32 chunks, chunks x u32 chunk bytes,
-//   chunks x 32 x u32 final lane states, then the chunk byte streams back to back.
+//   chunk S (multiple of 32), u32 chunks, u64 payload bytes (the sum of the chunk
+//   bytes), chunks x u32 chunk bytes, chunks x 32 x u32 final lane states, then the
+//   chunk byte streams back to back.
 #pragma once
 
 #include <stdint.h>
@@ -170,20 +171,14 @@ __host__ __device__ inline bool parse_section(ByteReader& r, SectionPlan* s, uin
     CHAIN_PARSE_REQUIRE(r.ok && s->S >= 32 && (s->S & 31) == 0);
     const uint64_t want = (count + s->S - 1) / s->S;
     CHAIN_PARSE_REQUIRE(want == s->chunks && s->chunks >= 1);
+    s->payload_len = r.u64();
     s->chunk_tab_off = r.pos;
-    uint64_t payload = 0;
-    CHAIN_PARSE_REQUIRE(r.need(4ull * s->chunks));
-    for (uint32_t c = 0; c < s->chunks; ++c) {
-        uint64_t v = 0;
-        for (int i = 0; i < 4; ++i) v |= static_cast<uint64_t>(r.p[r.pos + 4ull * c + i]) << (8 * i);
-        payload += v;
-    }
-    r.pos += 4ull * s->chunks;
+    // the chunk lengths must add up to payload_len; the decoder checks that in parallel
+    CHAIN_PARSE_REQUIRE(r.skip(4ull * s->chunks));
     s->states_off = r.pos;
     CHAIN_PARSE_REQUIRE(r.skip(128ull * s->chunks));
     s->payload_off = r.pos;
-    s->payload_len = payload;
-    CHAIN_PARSE_REQUIRE(r.skip(payload));
+    CHAIN_PARSE_REQUIRE(r.skip(s->payload_len));
     return true;
 }
 

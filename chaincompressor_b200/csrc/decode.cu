@@ -23,7 +23,7 @@ namespace chain {
 
 struct DecState {
     uint32_t err;
-    uint32_t jump_active;   // pointer jumping: 1 while some parent moved in the last round
+    uint32_t pad0;
     uint32_t zeros;         // idrel == 0 count
     uint32_t ndiff_seen;
     uint64_t tag_bits[kCodeStreams];
@@ -34,7 +34,6 @@ struct DecState {
 __global__ void k_dec_init(DecState* st) {
     if (threadIdx.x || blockIdx.x) return;
     st->err = 0;
-    st->jump_active = 1;
     st->zeros = 0;
     st->ndiff_seen = 0;
     for (int s = 0; s < kCodeStreams; ++s) { st->tag_bits[s] = 0; st->maxtag[s] = 0; }
@@ -52,6 +51,7 @@ struct SectionRef {
     uint32_t* prob;
     uint32_t* cum;
     uint32_t* lookup;
+    uint64_t* slots;
     uint64_t* chunk_off;
 };
 struct SectionRefs {
@@ -81,7 +81,10 @@ __global__ void __launch_bounds__(1024) k_section_setup(SectionRefs refs, const 
         if (c < s.chunks) R.chunk_off[c] = carry + ex;
         carry += tot;
     }
-    if (threadIdx.x == 0) R.chunk_off[s.chunks] = carry;
+    if (threadIdx.x == 0) {
+        R.chunk_off[s.chunks] = carry;
+        if (carry != s.payload_off + s.payload_len) set_error(&st->err, kErrCorrupt);
+    }
 }
 
 // slot -> symbol: binary search of the cumulative table (any grid; blockIdx.y = section).
@@ -99,6 +102,7 @@ __global__ void __launch_bounds__(256) k_lookup(SectionRefs refs, const DecState
         // zero-probability symbols share their successor's cum; step back to the owner
         while (R.prob[lo] == 0 && lo > 0) --lo;
         R.lookup[slot] = lo;
+        R.slots[slot] = pack_slot(lo, R.prob[lo], slot - R.cum[lo]);
     }
 }
 
@@ -294,7 +298,11 @@ struct ZeroIn {
     const uint32_t* idrel;
     __device__ uint32_t operator()(uint64_t i) const { return idrel[i] == 0 ? 1u : 0u; }
 };
-// Ranks of the explicit points; parents (explicit points are roots and point to
+// Parent words: bit 31 set = resolved (the low bits are the chain's explicit point).
+constexpr uint32_t kResolved = 0x80000000u;
+constexpr uint32_t kParentMask = 0x7fffffffu;
+
+// Ranks of the explicit points; parents (explicit points are resolved roots pointing to
 // themselves); and the list of chained points, whose rank among chained points is
 // i - (explicit points before i).
 struct ZeroRankOut {
@@ -307,34 +315,36 @@ struct ZeroRankOut {
     __device__ void operator()(uint64_t i, uint32_t pre, uint32_t z) const {
         zrank[i] = pre;
         const uint32_t j = idrel[i];
-        if (z) { parent[i] = static_cast<uint32_t>(i); return; }
+        if (z) { parent[i] = static_cast<uint32_t>(i) | kResolved; return; }
         chained[i - pre] = static_cast<uint32_t>(i);
-        if (static_cast<uint64_t>(j) >= n - i) { set_error(&st->err, kErrCorrupt); parent[i] = static_cast<uint32_t>(i); return; }
+        if (static_cast<uint64_t>(j) >= n - i) {
+            set_error(&st->err, kErrCorrupt);
+            parent[i] = static_cast<uint32_t>(i) | kResolved;
+            return;
+        }
         parent[i] = static_cast<uint32_t>(i + j);
     }
 };
 
-// One pointer-jumping round over the chained points.  A round that moves no pointer
-// clears jump_active, and every later round returns at once.  Jumps only point
-// forward, so ceil(log2 N) rounds reach every root.
+// One pointer-jumping round over the chained points: an unresolved point takes its
+// parent's parent word (and with it the resolved bit).  pending[r] records whether
+// any point is still unresolved after round r; a round whose predecessor left none
+// returns at once.  Jumps only point forward, so ceil(log2 N) rounds resolve all.
 __global__ void __launch_bounds__(256) k_jump(uint32_t* parent, const uint32_t* chained, const uint32_t* zeros,
-                                               uint64_t n, DecState* st, uint32_t* moved) {
-    if (!st->jump_active) return;
+                                               uint64_t n, uint32_t* pending, int round) {
+    if (round > 0 && pending[round - 1] == 0) return;
     const uint64_t m = n - *zeros;
     bool any = false;
     for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < m;
          k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint32_t i = chained[k];
         const uint32_t p = parent[i];
+        if (p & kResolved) continue;
         const uint32_t pp = parent[p];
-        if (pp != p) { parent[i] = pp; any = true; }
+        parent[i] = pp;
+        any |= !(pp & kResolved);
     }
-    if (__syncthreads_or(any) && threadIdx.x == 0) atomicOr(moved, 1u);
-}
-__global__ void k_jump_flag(DecState* st, uint32_t* moved) {
-    if (threadIdx.x || blockIdx.x) return;
-    if (st->jump_active && *moved == 0) st->jump_active = 0;
-    *moved = 0;
+    if (__syncthreads_or(any) && threadIdx.x == 0) atomicOr(&pending[round], 1u);
 }
 
 // q = block(root) * p + offset, then x = fma(q + 0.5, 2 eb, min) (lcps_cpp.cpp:1496-1500).
@@ -351,7 +361,7 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
     const uint32_t B = static_cast<uint32_t>(P.comp[3].records);
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint32_t root = parent[i];
+        const uint32_t root = parent[i] & kParentMask;
         const uint32_t cr = zrank[root];
         bool bad = cr >= B;
         for (uint32_t d = 0; d < D; ++d) {
@@ -469,11 +479,11 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     need += Arena::need(nd, 4) * 4;          // diff, keep, rel, compact
     need += Arena::need(N, 4);               // drank
     need += Arena::need(tags_total + 1, 4);
-    need += Arena::need(max_prec_slots + 1, 4) + Arena::need(max_alpha + 1, 4) * 2;
+    need += Arena::need(max_prec_slots + 1, 4) + Arena::need(max_prec_slots + 1, 8) + Arena::need(max_alpha + 1, 4) * 2;
     need += Arena::need(total_chunks + kCodeStreams + 1, 8) + Arena::need(total_chunks * 32 + 1, 4);
     need += Arena::need(plan.exc_count + 1, 4) * 2;   // correction gaps, ids
     need += Arena::need(scan_scratch_bytes(std::max<uint64_t>(nd, N)), 1);
-    need += Arena::need(16, 8);
+    need += Arena::need(32, 8);
     need += Arena::need(parse_scratch + 1, 4);
     if (host_out) need += Arena::need(nd, osz);
     need += 24 * 256;
@@ -502,17 +512,17 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     uint32_t* drank = A.take<uint32_t>(N);
     uint32_t* tags = A.take<uint32_t>(tags_total + 1);
     uint32_t* lookup = A.take<uint32_t>(max_prec_slots + 1);
+    uint64_t* slots64 = A.take<uint64_t>(max_prec_slots + 1);
     uint32_t* prob = A.take<uint32_t>(max_alpha + 1);
     uint32_t* cum = A.take<uint32_t>(max_alpha + 1);
     uint64_t* chunk_off = A.take<uint64_t>(total_chunks + kCodeStreams + 1);
     uint32_t* states = A.take<uint32_t>(total_chunks * 32 + 1);
     uint64_t* scanbuf = reinterpret_cast<uint64_t*>(A.take<uint8_t>(scan_scratch_bytes(std::max<uint64_t>(nd, N))));
-    uint64_t* misc = A.take<uint64_t>(16);
+    uint64_t* misc = A.take<uint64_t>(32);
     uint32_t* pscratch = A.take<uint32_t>(parse_scratch + 1);
     void* dout = host_out ? A.take<uint8_t>(nd * osz) : out;
     if (!misc || !dout) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "decoder arena too small");
-    uint32_t* moved = reinterpret_cast<uint32_t*>(misc);
-    CHAIN_CUDA(cudaMemsetAsync(misc, 0, 16 * sizeof(uint64_t), stream));
+    CHAIN_CUDA(cudaMemsetAsync(misc, 0, 32 * sizeof(uint64_t), stream));
 
     // ---- entropy sections
     SectionRefs refs{};
@@ -531,6 +541,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         R.prob = prob + alpha_base;
         R.cum = cum + alpha_base;
         R.lookup = lookup + slot_base;
+        R.slots = slots64 + slot_base;
         R.chunk_off = chunk_off + off_base;
         states_first[nsec] = chunk_base * 32;
         RansJob& jb = jobs.job[jobs.njobs++];
@@ -538,6 +549,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         jb.prob = R.prob;
         jb.cum = R.cum;
         jb.lookup = R.lookup;
+        jb.slots = R.slots;
         jb.prec = c.sec.prec;
         jb.alphabet = c.sec.alphabet;
         jb.chunks = c.sec.chunks;
@@ -613,9 +625,9 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     T.mark("zero_ranks", stream);
     int rounds = 1;
     while ((1ull << rounds) < N) ++rounds;
-    for (int r = 0; r < rounds + 1; ++r) {
-        k_jump<<<dgrid(N), 256, 0, stream>>>(parent, chained, zeros_dev, N, st, moved); count_launch();
-        k_jump_flag<<<1, 1, 0, stream>>>(st, moved); count_launch();
+    uint32_t* pending = reinterpret_cast<uint32_t*>(misc + 16);  // misc[16..31]: 32 round flags
+    for (int r = 0; r < rounds; ++r) {
+        k_jump<<<dgrid(N), 256, 0, stream>>>(parent, chained, zeros_dev, N, pending, r); count_launch();
     }
     CHAIN_LAUNCH_CHECK("levels");
     T.mark("pointer_jump", stream);
@@ -656,11 +668,13 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     }
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, offsetof(DecState, plan), cudaMemcpyDeviceToHost, stream));
     uint32_t counts[4] = {0, 0, 0, 0};
+    uint32_t still_pending = 0;
     CHAIN_CUDA(cudaMemcpyAsync(counts, misc + 1, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+    CHAIN_CUDA(cudaMemcpyAsync(&still_pending, pending + rounds - 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     CHAIN_CUDA(cudaStreamSynchronize(stream));
     T.finish();
     const uint32_t ndiff_seen = counts[0], zeros_seen = counts[2];
-    if (hs->err || ndiff_seen != plan.comp[1].records || zeros_seen != B || hs->jump_active)
+    if (hs->err || ndiff_seen != plan.comp[1].records || zeros_seen != B || still_pending)
         return set_err(CHAIN_ERR_CORRUPT_STREAM, "LCG2: invalid integer payload (flags " + std::to_string(hs->err) +
                                                      ")");
     return CHAIN_OK;

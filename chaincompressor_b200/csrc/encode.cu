@@ -42,6 +42,7 @@ struct StreamChoice {
     uint64_t est[4];          // estimated body bytes by encoding (index = Encoding)
     uint32_t sec_prec, sec_alphabet, sec_chunks, table_len;
     uint64_t sec_S, sec_count;
+    uint64_t payload_bytes;   // sum of the chunk bytes (after coding)
     uint64_t packed_bits;
     uint64_t body_bytes;      // exact, after coding
 };
@@ -78,14 +79,35 @@ struct EncState {
 };
 
 // A byte range copied into the container.  Pieces are cut into kCopySeg-byte
-// segments so that large payloads spread over many CTAs.
+// segments so that large payloads spread over many CTAs.  A chunked piece (stream >= 0)
+// is the whole payload of one rANS section: its segments never cross a chunk, and a
+// segment finds its chunk through the stream's per-chunk segment prefix.
 struct Piece {
     const uint8_t* src;
     uint64_t dst;
     uint64_t len;
     uint64_t seg_begin;   // index of this piece's first segment
+    int32_t stream;       // -1: plain byte range; else the coded stream whose chunks these are
+    int32_t pad;
 };
 constexpr uint64_t kCopySeg = 4096;
+
+// Per rANS section: where each chunk's bytes sit in its encoder slot and in the
+// section payload, and how many copy segments precede it.
+struct ChunkMap {
+    const uint8_t* slots;
+    uint64_t slot_cap;
+    const uint32_t* len;   // [chunks]
+    uint64_t* off;         // [chunks] byte offset in the payload
+    uint32_t* seg;         // [chunks + 1] copy segments before the chunk
+    uint32_t chunks;
+    uint32_t pad;
+};
+struct ChunkMaps {
+    ChunkMap m[kCodeStreams];
+    int sec_stream[kCodeStreams];   // coded streams that have a rANS section
+    int nsec;
+};
 
 // --------------------------------------------------------------- quantization
 template <typename FT, bool SOA>
@@ -581,7 +603,11 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
         c.max_width = static_cast<uint8_t>(g.maxtag);
     } else if (best == kEncRaw) {
         const RansTableDev& t = st->raw_tab[s];
-        plan_chunks(nrec * r.dims, t.cost_bits / 8.0, bytes_per_lane, max_steps, &c.sec_chunks, &c.sec_S);
+        // Tables too large for shared memory cost one L2 round trip per coded symbol on
+        // both sides, so their lanes get a shorter serial depth.
+        const bool large = t.alphabet > kSmemEncSyms || (1u << t.prec) > kSmemLookupSlots;
+        const uint32_t steps = large ? min(max_steps, kLargeTableMaxSteps) : max_steps;
+        plan_chunks(nrec * r.dims, t.cost_bits / 8.0, bytes_per_lane, steps, &c.sec_chunks, &c.sec_S);
         c.sec_count = nrec * r.dims;
         c.sec_prec = t.prec;
         c.sec_alphabet = t.alphabet;
@@ -688,6 +714,7 @@ struct AssemblyIn {
     const uint32_t* states[kCodeStreams];
     const uint8_t* slots[kCodeStreams];
     uint64_t slot_cap[kCodeStreams];
+    const uint32_t* chunk_segs[kCodeStreams];    // copy-segment prefix (chunks + 1)
     const uint8_t* packed[kCodeStreams];         // fixed/tagged payload (bytes)
     uint64_t packed_dim_stride[kCodeStreams];    // fixed: bytes between dimension payloads
     const uint64_t* corr_dict;                   // distinct corrected values (bits)
@@ -711,6 +738,32 @@ struct Writer {
     }
 };
 
+// One CTA per rANS section: payload offsets and copy-segment prefix of its chunks.
+__global__ void __launch_bounds__(1024) k_chunk_prefix(ChunkMaps maps, EncState* st) {
+    const int s = maps.sec_stream[blockIdx.x];
+    const ChunkMap M = maps.m[s];
+    __shared__ uint64_t red[33];
+    uint64_t carry_b = 0, carry_s = 0;
+    for (uint32_t base = 0; base < M.chunks; base += blockDim.x) {
+        const uint32_t k = base + threadIdx.x;
+        const uint64_t len = k < M.chunks ? M.len[k] : 0;
+        const uint64_t nseg = (len + kCopySeg - 1) / kCopySeg;
+        uint64_t tb, ts;
+        const uint64_t eb = block_exclusive_sum(len, red, &tb);
+        const uint64_t es = block_exclusive_sum(nseg, red, &ts);
+        if (k < M.chunks) {
+            M.off[k] = carry_b + eb;
+            M.seg[k] = static_cast<uint32_t>(carry_s + es);
+        }
+        carry_b += tb;
+        carry_s += ts;
+    }
+    if (threadIdx.x == 0) {
+        M.seg[M.chunks] = static_cast<uint32_t>(carry_s);
+        st->ch[s].payload_bytes = carry_b;
+    }
+}
+
 // Single thread: writes every header field and emits the list of payload pieces.
 __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* pieces, uint32_t max_pieces) {
     if (threadIdx.x || blockIdx.x) return;
@@ -719,9 +772,16 @@ __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* piece
     uint64_t segs = 0;
     auto piece = [&](const uint8_t* src, uint64_t len) {
         if (len == 0) return;
-        if (np < max_pieces) pieces[np] = Piece{src, w.pos, len, segs};
+        if (np < max_pieces) pieces[np] = Piece{src, w.pos, len, segs, -1, 0};
         ++np;
         segs += (len + kCopySeg - 1) / kCopySeg;
+        w.pos += len;
+    };
+    auto chunked = [&](int s, uint64_t len, uint32_t nseg) {
+        if (len == 0) return;
+        if (np < max_pieces) pieces[np] = Piece{nullptr, w.pos, len, segs, s, 0};
+        ++np;
+        segs += nseg;
         w.pos += len;
     };
     const uint32_t D = st->dims;
@@ -758,12 +818,10 @@ __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* piece
             piece(in.table_bytes + in.table_stride * s, c.table_len);
             w.uint(c.sec_S, 8);
             w.uint(c.sec_chunks, 4);
+            w.uint(c.payload_bytes, 8);
             piece(reinterpret_cast<const uint8_t*>(in.chunk_len[s]), 4ull * c.sec_chunks);
             piece(reinterpret_cast<const uint8_t*>(in.states[s]), 128ull * c.sec_chunks);
-            for (uint32_t k = 0; k < c.sec_chunks; ++k) {
-                const uint32_t len = in.chunk_len[s][k];
-                piece(in.slots[s] + in.slot_cap[s] * k + (in.slot_cap[s] - len), len);
-            }
+            chunked(s, c.payload_bytes, in.chunk_segs[s][c.sec_chunks]);
             if (c.enc == kEncTagged) {
                 w.uint(c.packed_bits, 8);
                 piece(in.packed[s], (c.packed_bits + 7) / 8);
@@ -810,8 +868,10 @@ __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* piece
     if (np > max_pieces) set_error(&st->err, kErrInternal);
 }
 
-// One CTA per 4 KB segment; the piece of a segment is found by binary search.
-__global__ void __launch_bounds__(256) k_copy_pieces(const Piece* pieces, const EncState* st, uint8_t* out) {
+// One CTA per 4 KB segment; the piece of a segment is found by binary search, and for
+// a chunked piece the chunk by a second binary search over its segment prefix.
+__global__ void __launch_bounds__(256) k_copy_pieces(const Piece* pieces, ChunkMaps maps, const EncState* st,
+                                                      uint8_t* out) {
     const uint32_t np = st->npieces;
     const uint64_t nsegs = st->nsegs;
     for (uint64_t g = blockIdx.x; g < nsegs; g += gridDim.x) {
@@ -821,10 +881,29 @@ __global__ void __launch_bounds__(256) k_copy_pieces(const Piece* pieces, const 
             if (pieces[mid].seg_begin <= g) lo = mid; else hi = mid - 1;
         }
         const Piece pc = pieces[lo];
-        const uint64_t off = (g - pc.seg_begin) * kCopySeg;
-        const uint64_t end = min(off + kCopySeg, pc.len);
-        uint8_t* dst = out + pc.dst;
-        for (uint64_t b = off + threadIdx.x; b < end; b += blockDim.x) dst[b] = pc.src[b];
+        const uint8_t* src;
+        uint8_t* dst;
+        uint64_t len;
+        if (pc.stream < 0) {
+            const uint64_t off = (g - pc.seg_begin) * kCopySeg;
+            src = pc.src + off;
+            dst = out + pc.dst + off;
+            len = min(kCopySeg, pc.len - off);
+        } else {
+            const ChunkMap& M = maps.m[pc.stream];
+            const uint32_t ls = static_cast<uint32_t>(g - pc.seg_begin);
+            uint32_t a = 0, b = M.chunks - 1;   // last chunk with seg[k] <= ls
+            while (a < b) {
+                const uint32_t mid = (a + b + 1) >> 1;
+                if (M.seg[mid] <= ls) a = mid; else b = mid - 1;
+            }
+            const uint64_t clen = M.len[a];
+            const uint64_t off = static_cast<uint64_t>(ls - M.seg[a]) * kCopySeg;
+            src = M.slots + M.slot_cap * a + (M.slot_cap - clen) + off;
+            dst = out + pc.dst + M.off[a] + off;
+            len = min(kCopySeg, clen - off);
+        }
+        for (uint64_t b = threadIdx.x; b < len; b += blockDim.x) dst[b] = src[b];
     }
 }
 
@@ -1151,7 +1230,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     uint64_t etab_total = 0;
     for (int s = 0; s < kCodeStreams; ++s)
         if (hs->ch[s].enc == kEncRaw || hs->ch[s].enc == kEncTagged) etab_total += hs->ch[s].sec_alphabet;
-    const uint64_t max_pieces = total_chunks + 64;
+    const uint64_t max_pieces = 128;
     uint64_t bound = header_bytes(dims) + 40 + 8ull * hs->ndistinct;
     for (int s = 0; s < kCodeStreams; ++s) {
         const StreamChoice& c = hs->ch[s];
@@ -1164,7 +1243,8 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     size_t need2 = Arena::need(slots_total, 1) + Arena::need(packed_total, 1) + Arena::need(tags_total + 1, 4) +
                    Arena::need(total_chunks + 1, 4) + Arena::need(total_chunks * 32 + 1, 4) +
                    Arena::need(table_stride * kCodeStreams, 1) + Arena::need(max_pieces, sizeof(Piece)) +
-                   Arena::need(bound, 1) + Arena::need(etab_total + 1, 16) + 9 * 256;
+                   Arena::need(bound, 1) + Arena::need(etab_total + 1, 16) + Arena::need(total_chunks + 1, 8) +
+                   Arena::need(total_chunks + kCodeStreams + 1, 4) + 11 * 256;
     CHAIN_CUDA(ctx->coded.reserve(need2));
     Arena& C = ctx->coded;
     uint8_t* slots = C.take<uint8_t>(slots_total + 1);
@@ -1176,7 +1256,11 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     Piece* pieces = C.take<Piece>(max_pieces);
     uint8_t* container = C.take<uint8_t>(bound);
     uint4* etab = C.take<uint4>(etab_total + 1);
-    if (!container || !etab) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder coding arena too small");
+    uint64_t* chunk_off = C.take<uint64_t>(total_chunks + 1);
+    uint32_t* chunk_seg = C.take<uint32_t>(total_chunks + kCodeStreams + 1);
+    if (!container || !etab || !chunk_seg) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder coding arena too small");
+    ChunkMaps maps{};
+    uint64_t seg_base = 0;
     uint64_t etab_used = 0;
     if (packed_total) CHAIN_CUDA(cudaMemsetAsync(packed, 0, packed_total, stream));
 
@@ -1237,6 +1321,16 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
             ain.states[s] = jb.states;
             ain.slots[s] = jb.bytes;
             ain.slot_cap[s] = slot_cap[s];
+            ChunkMap& cm = maps.m[s];
+            cm.slots = jb.bytes;
+            cm.slot_cap = slot_cap[s];
+            cm.len = jb.chunk_len;
+            cm.off = chunk_off + chunk_base;
+            cm.seg = chunk_seg + seg_base;
+            cm.chunks = c.sec_chunks;
+            ain.chunk_segs[s] = cm.seg;
+            maps.sec_stream[maps.nsec++] = s;
+            seg_base += c.sec_chunks + 1;
             chunk_base += c.sec_chunks;
         }
     }
@@ -1257,8 +1351,11 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     }
     CHAIN_LAUNCH_CHECK("entropy coding");
     T.mark("rans_encode", stream);
+    if (maps.nsec) {
+        k_chunk_prefix<<<maps.nsec, 1024, 0, stream>>>(maps, st); count_launch();
+    }
     k_layout<<<1, 1, 0, stream>>>(st, ain, container, pieces, static_cast<uint32_t>(max_pieces)); count_launch();
-    k_copy_pieces<<<148u * 8u, 256, 0, stream>>>(pieces, st, container); count_launch();
+    k_copy_pieces<<<148u * 16u, 256, 0, stream>>>(pieces, maps, st, container); count_launch();
     CHAIN_LAUNCH_CHECK("assembly");
     T.mark("assemble", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));

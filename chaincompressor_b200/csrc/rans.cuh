@@ -12,9 +12,11 @@
 // consumes them (lane order within a step, most significant byte first).
 //
 // Probability normalisation is this project's own exact-integer scheme (the
-// reference's uses x87 long double): p_s = max(1, round(f_s * M / n)); a deficit goes
-// to the most probable symbol; an excess is removed proportionally from the
-// reducible mass and then one unit at a time from the largest probabilities.
+// reference's uses x87 long double): symbols with f_s * M / n < 1 get probability 1,
+// the others share the remaining mass in proportion (round to nearest), and the
+// rounding residue goes to the most probable symbol.  When that symbol cannot absorb
+// it, an excess is removed proportionally from the reducible mass and then one unit
+// at a time from the largest probabilities.
 #pragma once
 
 #include "chain_common.cuh"
@@ -81,16 +83,57 @@ __device__ inline void build_rans_table(const uint32_t* __restrict__ hist, uint3
     uniq = block_reduce_sum(uniq, red);
     const int prec = rans_precision_bits(uniq);
     const uint64_t M = 1ull << prec;
-    uint64_t sum = 0;
+    // Symbols with f * M / n < 1 are pinned to probability 1; the remaining mass is
+    // shared by the others in proportion (rounded to nearest), re-pinning any that
+    // round to 0.  The rounding residue then goes to the most probable symbol.
+    constexpr uint32_t kPin = 0x80000000u;
+    uint64_t pinned = 0, pinned_f = 0;
     for (uint32_t s = threadIdx.x; s < A; s += blockDim.x) {
         const uint64_t f = hist[s];
-        uint64_t p = f ? (2 * f * M + n) / (2 * n) : 0;
-        if (f && p == 0) p = 1;
-        prob[s] = static_cast<uint32_t>(p);
-        sum += p;
+        const bool pin = f && f * M < n;
+        pinned += pin;
+        pinned_f += pin ? f : 0;
+        prob[s] = pin ? (kPin | 1u) : 0u;
     }
-    sum = block_reduce_sum(sum, red);
+    pinned = block_reduce_sum(pinned, red);
+    pinned_f = block_reduce_sum(pinned_f, red);
+    uint64_t sum = 0;
+    for (int round = 0; round < 16; ++round) {
+        const uint64_t budget = M - pinned, rest = n - pinned_f;
+        uint64_t newly = 0, newly_f = 0, free_sum = 0;
+        for (uint32_t s = threadIdx.x; s < A; s += blockDim.x) {
+            const uint64_t f = hist[s];
+            if (!f || (prob[s] & kPin) || rest == 0) continue;
+            const uint64_t p = (2 * f * budget + rest) / (2 * rest);
+            if (p == 0) {
+                prob[s] = kPin | 1u;
+                ++newly;
+                newly_f += f;
+            } else {
+                prob[s] = static_cast<uint32_t>(p);
+                free_sum += p;
+            }
+        }
+        newly = block_reduce_sum(newly, red);
+        newly_f = block_reduce_sum(newly_f, red);
+        free_sum = block_reduce_sum(free_sum, red);
+        pinned += newly;
+        pinned_f += newly_f;
+        sum = pinned + free_sum;
+        if (newly == 0) break;
+    }
+    for (uint32_t s = threadIdx.x; s < A; s += blockDim.x) prob[s] &= ~kPin;
     __syncthreads();
+    if (sum != M) {
+        table_block_argmax(prob, A, &sh_best);
+        const int64_t fixed = static_cast<int64_t>(prob[sh_best]) + static_cast<int64_t>(M) - static_cast<int64_t>(sum);
+        __syncthreads();
+        if (fixed >= 1) {
+            if (threadIdx.x == 0) prob[sh_best] = static_cast<uint32_t>(fixed);
+            sum = M;
+        }
+        __syncthreads();
+    }
     if (sum < M) {
         table_block_argmax(prob, A, &sh_best);
         if (threadIdx.x == 0) prob[sh_best] += static_cast<uint32_t>(M - sum);
@@ -404,6 +447,7 @@ struct RansJob {
     const uint32_t* prob;     // [A]
     const uint32_t* cum;      // [A]
     const uint32_t* lookup;   // decode: slot -> symbol [M]
+    const uint64_t* slots;    // decode: slot -> pack_slot(symbol, freq, slot - cum) [M]
     uint32_t prec;
     uint32_t alphabet;
     uint32_t chunks;
@@ -424,6 +468,13 @@ constexpr uint32_t kSmemTableSyms = 4096;     // decoder prob/cum in shared memo
 constexpr uint32_t kSmemEncSyms = 2048;       // encoder entries (16 B) in shared memory up to this alphabet
 constexpr uint32_t kSmemLookupSlots = 16384;  // u16 decode lookup in shared memory up to this M
 constexpr uint32_t kWindow = 4096;            // decoder byte window per warp
+constexpr uint32_t kLargeTableMaxSteps = 512; // serial depth of lanes whose tables stay in L2
+
+// Decoder slot entry for tables kept in global memory: one load per step gives the
+// symbol, its frequency and slot - cum[symbol].
+__host__ __device__ inline uint64_t pack_slot(uint32_t sym, uint32_t freq, uint32_t bias) {
+    return static_cast<uint64_t>(sym) | (static_cast<uint64_t>(freq) << 18) | (static_cast<uint64_t>(bias) << 39);
+}
 
 // Shared memory is sized per launch: the largest table of this launch that fits the
 // shared-memory limits (tab_cap symbols, look_cap decode slots), plus staging.
@@ -641,11 +692,18 @@ static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uin
         uint32_t nb = 0;
         if (act) {
             const uint32_t slot = x & (M - 1);
-            const uint32_t s = smem_look ? look[slot] : __ldg(jb.lookup + slot);
-            uint32_t f, cm;
-            if (smem_tab) { const uint2 e = tab[s]; f = e.x; cm = e.y; }
-            else { f = __ldg(jb.prob + s); cm = __ldg(jb.cum + s); }
-            x = f * (x >> prec) + slot - cm;
+            uint32_t s;
+            if (smem_look) {
+                s = look[slot];
+                uint32_t f, cm;
+                if (smem_tab) { const uint2 e = tab[s]; f = e.x; cm = e.y; }
+                else { f = __ldg(jb.prob + s); cm = __ldg(jb.cum + s); }
+                x = f * (x >> prec) + slot - cm;
+            } else {
+                const uint64_t e = __ldg(jb.slots + slot);
+                s = static_cast<uint32_t>(e & 0x3ffffu);
+                x = static_cast<uint32_t>((e >> 18) & 0x1fffffu) * (x >> prec) + static_cast<uint32_t>(e >> 39);
+            }
             jb.out[k] = s;
             nb = (x < L) + (x < (L >> 8)) + (x < (L >> 16));
         }
