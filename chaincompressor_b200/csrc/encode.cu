@@ -605,7 +605,9 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
         const RansTableDev& t = st->raw_tab[s];
         // Tables too large for shared memory cost one L2 round trip per coded symbol on
         // both sides, so their lanes get a shorter serial depth.
-        const bool large = t.alphabet > kSmemEncSyms || (1u << t.prec) > kSmemLookupSlots;
+        // (Only worth its lane overhead on streams long enough to fill the GPU.)
+        const bool large = (t.alphabet > kSmemEncSyms || (1u << t.prec) > kSmemLookupSlots) &&
+                           nrec * r.dims >= kLargeTableMinSymbols;
         const uint32_t steps = large ? min(max_steps, kLargeTableMaxSteps) : max_steps;
         plan_chunks(nrec * r.dims, t.cost_bits / 8.0, bytes_per_lane, steps, &c.sec_chunks, &c.sec_S);
         c.sec_count = nrec * r.dims;
