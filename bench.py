@@ -224,7 +224,7 @@ def run_ours(args, rank: int, world: int):
 
     info = lcg2_inspect.inspect(bytes(cont_host.numpy()))
     rans_syms = sum(c["section"]["symbols"] for c in info["components"].values() if "section" in c)
-    rans_bytes = sum(c["section"]["payload"] + 132 * c["section"]["chunks"]
+    rans_bytes = sum(c["section"]["payload"] + c["section"]["state_bytes"] + 4 * c["section"]["chunks"]
                      for c in info["components"].values() if "section" in c)
     peaks, src = _peaks()
     peak = float(peaks["hbm_gbs"])

@@ -37,9 +37,10 @@
 //   raw (3):    rANS section over the record-major values
 // rANS section:
 //   u8 prec, u32 alphabet, u32 table_bytes, table tokens (rans.cuh), u64 symbols per
-//   chunk S (multiple of 32), u32 chunks, u64 payload bytes (the sum of the chunk
-//   bytes), chunks x u32 chunk bytes, chunks x 32 x u32 final lane states, then the
-//   chunk byte streams back to back.
+//   chunk S, u8 lanes W (1..32, S a multiple of W), u32 chunks, u64 payload bytes (the
+//   sum of the chunk bytes), chunks x u32 chunk bytes, chunks x W x u32 final lane
+//   states, then the chunk byte streams back to back.
+//   Fixed width 0 means a constant component (every value equals its minimum).
 #pragma once
 
 #include <stdint.h>
@@ -67,6 +68,8 @@ struct SectionPlan {
     uint64_t table_off;    // absolute offsets into the container
     uint32_t table_len;
     uint32_t chunks;
+    uint32_t lanes;
+    uint32_t pad;
     uint64_t S;
     uint64_t count;        // symbols
     uint64_t chunk_tab_off;
@@ -167,8 +170,9 @@ __host__ __device__ inline bool parse_section(ByteReader& r, SectionPlan* s, uin
     s->table_off = r.pos;
     CHAIN_PARSE_REQUIRE(r.skip(s->table_len));
     s->S = r.u64();
+    s->lanes = r.u8();
     s->chunks = r.u32();
-    CHAIN_PARSE_REQUIRE(r.ok && s->S >= 32 && (s->S & 31) == 0);
+    CHAIN_PARSE_REQUIRE(r.ok && s->lanes >= 1 && s->lanes <= 32 && s->S >= s->lanes && s->S % s->lanes == 0);
     const uint64_t want = (count + s->S - 1) / s->S;
     CHAIN_PARSE_REQUIRE(want == s->chunks && s->chunks >= 1);
     s->payload_len = r.u64();
@@ -176,7 +180,7 @@ __host__ __device__ inline bool parse_section(ByteReader& r, SectionPlan* s, uin
     // the chunk lengths must add up to payload_len; the decoder checks that in parallel
     CHAIN_PARSE_REQUIRE(r.skip(4ull * s->chunks));
     s->states_off = r.pos;
-    CHAIN_PARSE_REQUIRE(r.skip(128ull * s->chunks));
+    CHAIN_PARSE_REQUIRE(r.skip(4ull * s->lanes * s->chunks));
     s->payload_off = r.pos;
     CHAIN_PARSE_REQUIRE(r.skip(s->payload_len));
     return true;
@@ -199,7 +203,7 @@ __host__ __device__ inline bool parse_component(ByteReader& r, uint64_t body_len
         for (uint32_t d = 0; d < c->dims; ++d) {
             c->minv[d] = r.u64();
             c->width[d] = r.u8();
-            CHAIN_PARSE_REQUIRE(r.ok && c->width[d] >= 1 && c->width[d] <= 32);
+            CHAIN_PARSE_REQUIRE(r.ok && c->width[d] <= 32);
         }
         for (uint32_t d = 0; d < c->dims; ++d) {
             c->packed_off[d] = r.pos;

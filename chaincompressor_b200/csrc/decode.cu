@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(256) k_states(SectionRefs refs, const uint8_t*
     const SectionRef R = refs.r[blockIdx.y];
     const SectionPlan& s = *R.sec;
     uint32_t* out = states_base + states_first[blockIdx.y];
-    const uint64_t words = 32ull * s.chunks;
+    const uint64_t words = static_cast<uint64_t>(s.lanes) * s.chunks;
     for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < words;
          w += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint8_t* q = data + s.states_off + 4 * w;
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(256) k_unpack_fixed(const uint8_t* data, const
         const uint64_t k = j / c.dims;
         const uint32_t d = static_cast<uint32_t>(j - k * c.dims);
         const int w = c.width[d];
-        const uint64_t off = read_bits_msb(data + c.packed_off[d], k * w, w);
+        const uint64_t off = w ? read_bits_msb(data + c.packed_off[d], k * w, w) : 0;
         const uint64_t v = c.minv[d] + off;
         if (v > 0xffffffffull) { set_error(&st->err, kErrCorrupt); continue; }
         out[j] = static_cast<uint32_t>(v);
@@ -553,6 +553,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         jb.prec = c.sec.prec;
         jb.alphabet = c.sec.alphabet;
         jb.chunks = c.sec.chunks;
+        jb.lanes = c.sec.lanes;
         jb.S = c.sec.S;
         jb.bytes = const_cast<uint8_t*>(dcont);
         jb.bytes_len = len;

@@ -40,7 +40,7 @@ struct StreamChoice {
     uint32_t dims;
     uint64_t records;
     uint64_t est[4];          // estimated body bytes by encoding (index = Encoding)
-    uint32_t sec_prec, sec_alphabet, sec_chunks, table_len;
+    uint32_t sec_prec, sec_alphabet, sec_chunks, table_len, sec_lanes, pad_lanes;
     uint64_t sec_S, sec_count;
     uint64_t payload_bytes;   // sum of the chunk bytes (after coding)
     uint64_t packed_bits;
@@ -513,19 +513,29 @@ __global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncSt
     }
 }
 
-__device__ inline uint64_t section_overhead(uint32_t table_bytes, uint32_t chunks) {
-    return 1 + 4 + 4 + static_cast<uint64_t>(table_bytes) + 8 + 4 + static_cast<uint64_t>(chunks) * (4 + 128);
+__device__ inline uint64_t section_overhead(uint32_t table_bytes, uint32_t chunks, uint32_t lanes) {
+    return 1 + 4 + 4 + static_cast<uint64_t>(table_bytes) + 8 + 1 + 4 + 8 +
+           static_cast<uint64_t>(chunks) * (4 + 4ull * lanes);
 }
 
 // Chunking of a rANS section: enough lanes that each carries about bytes_per_lane
 // coded bytes (the 4-byte final state per lane is the size overhead), and enough that
-// no lane codes more than max_steps symbols (the serial depth of the kernel).
+// no lane codes more than max_steps symbols (the serial depth of the kernel).  Below
+// 32 lanes the section is one chunk of W = next power of two lanes.
 __device__ inline void plan_chunks(uint64_t count, double est_payload, uint32_t bytes_per_lane, uint32_t max_steps,
-                                   uint32_t* chunks, uint64_t* S) {
-    uint64_t lanes = static_cast<uint64_t>(est_payload / bytes_per_lane) + 1;
-    uint64_t ch = (lanes + 31) / 32;
-    const uint64_t ch_depth = (count + 32ull * max_steps - 1) / (32ull * max_steps);
-    if (ch < ch_depth) ch = ch_depth;
+                                   uint32_t* chunks, uint64_t* S, uint32_t* lanes) {
+    uint64_t need = static_cast<uint64_t>(est_payload / bytes_per_lane) + 1;
+    const uint64_t depth = (count + max_steps - 1) / max_steps;
+    if (need < depth) need = depth;
+    if (need < 32) {
+        uint32_t w = 1;
+        while (w < need) w <<= 1;
+        *lanes = w;
+        *S = (count + w - 1) / w * w;
+        *chunks = 1;
+        return;
+    }
+    uint64_t ch = (need + 31) / 32;
     const uint64_t max_ch = (count + 31) / 32;
     if (ch > max_ch) ch = max_ch;
     if (ch < 1) ch = 1;
@@ -533,6 +543,7 @@ __device__ inline void plan_chunks(uint64_t count, double est_payload, uint32_t 
     s = (s + 31) & ~31ull;
     if (s < 32) s = 32;
     *S = s;
+    *lanes = 32;
     *chunks = static_cast<uint32_t>((count + s - 1) / s);
 }
 
@@ -561,33 +572,38 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
     }
     if (st->tag_tab[s].alphabet == 0xFFFFFFFFu || st->raw_tab[s].alphabet == 0xFFFFFFFFu)
         set_error(&st->err, kErrInternal);
-    // fixed
+    // fixed (width 0 = constant component)
     uint64_t fixed = 13 + 9ull * r.dims;
     for (uint32_t d = 0; d < r.dims; ++d) {
         const uint32_t span = g.maxv[d] - g.minv[d];
-        const int w = span ? bitlen32(span) : 1;
+        const int w = bitlen32(span);
         c.width[d] = static_cast<uint8_t>(w);
         fixed += (nrec * w + 7) / 8;
     }
     c.est[kEncFixed] = fixed;
     // tagged
+    uint32_t tag_ch = 0, tag_lanes = 0;
+    uint64_t tag_S = 0;
     {
         const RansTableDev& t = st->tag_tab[s];
         const double payload = t.cost_bits / 8.0;
-        uint32_t ch;
-        uint64_t S;
-        plan_chunks(nrec, payload, bytes_per_lane, max_steps, &ch, &S);
-        c.est[kEncTagged] = 13 + 1 + section_overhead(t.table_bytes, ch) + static_cast<uint64_t>(payload) + 1 + 8 +
-                            (g.tag_bits + 7) / 8;
+        plan_chunks(nrec, payload, bytes_per_lane, max_steps, &tag_ch, &tag_S, &tag_lanes);
+        c.est[kEncTagged] = 13 + 1 + section_overhead(t.table_bytes, tag_ch, tag_lanes) +
+                            static_cast<uint64_t>(payload) + 1 + 8 + (g.tag_bits + 7) / 8;
     }
-    // raw
+    // raw.  Tables too large for shared memory cost one L2 round trip per coded symbol on
+    // both sides, so on streams long enough to fill the GPU their lanes get a shorter
+    // serial depth.
+    uint32_t raw_ch = 0, raw_lanes = 0;
+    uint64_t raw_S = 0;
     if (g.maxall < kRansMaxAlphabet && st->raw_tab[s].alphabet != 0) {
         const RansTableDev& t = st->raw_tab[s];
         const double payload = t.cost_bits / 8.0;
-        uint32_t ch;
-        uint64_t S;
-        plan_chunks(nrec * r.dims, payload, bytes_per_lane, max_steps, &ch, &S);
-        c.est[kEncRaw] = 13 + section_overhead(t.table_bytes, ch) + static_cast<uint64_t>(payload) + 1;
+        const bool large = (t.alphabet > kSmemEncSyms || (1u << t.prec) > kSmemLookupSlots) &&
+                           nrec * r.dims >= kLargeTableMinSymbols;
+        const uint32_t steps = large ? min(max_steps, kLargeTableMaxSteps) : max_steps;
+        plan_chunks(nrec * r.dims, payload, bytes_per_lane, steps, &raw_ch, &raw_S, &raw_lanes);
+        c.est[kEncRaw] = 13 + section_overhead(t.table_bytes, raw_ch, raw_lanes) + static_cast<uint64_t>(payload) + 1;
     }
     uint8_t best = kEncTagged;
     if (c.est[kEncFixed] < c.est[best]) best = kEncFixed;
@@ -595,7 +611,9 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
     c.enc = best;
     if (best == kEncTagged) {
         const RansTableDev& t = st->tag_tab[s];
-        plan_chunks(nrec, t.cost_bits / 8.0, bytes_per_lane, max_steps, &c.sec_chunks, &c.sec_S);
+        c.sec_chunks = tag_ch;
+        c.sec_S = tag_S;
+        c.sec_lanes = tag_lanes;
         c.sec_count = nrec;
         c.sec_prec = t.prec;
         c.sec_alphabet = t.alphabet;
@@ -603,13 +621,9 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
         c.max_width = static_cast<uint8_t>(g.maxtag);
     } else if (best == kEncRaw) {
         const RansTableDev& t = st->raw_tab[s];
-        // Tables too large for shared memory cost one L2 round trip per coded symbol on
-        // both sides, so their lanes get a shorter serial depth.
-        // (Only worth its lane overhead on streams long enough to fill the GPU.)
-        const bool large = (t.alphabet > kSmemEncSyms || (1u << t.prec) > kSmemLookupSlots) &&
-                           nrec * r.dims >= kLargeTableMinSymbols;
-        const uint32_t steps = large ? min(max_steps, kLargeTableMaxSteps) : max_steps;
-        plan_chunks(nrec * r.dims, t.cost_bits / 8.0, bytes_per_lane, steps, &c.sec_chunks, &c.sec_S);
+        c.sec_chunks = raw_ch;
+        c.sec_S = raw_S;
+        c.sec_lanes = raw_lanes;
         c.sec_count = nrec * r.dims;
         c.sec_prec = t.prec;
         c.sec_alphabet = t.alphabet;
@@ -819,10 +833,11 @@ __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* piece
             w.uint(c.table_len, 4);
             piece(in.table_bytes + in.table_stride * s, c.table_len);
             w.uint(c.sec_S, 8);
+            w.u8(static_cast<uint8_t>(c.sec_lanes));
             w.uint(c.sec_chunks, 4);
             w.uint(c.payload_bytes, 8);
             piece(reinterpret_cast<const uint8_t*>(in.chunk_len[s]), 4ull * c.sec_chunks);
-            piece(reinterpret_cast<const uint8_t*>(in.states[s]), 128ull * c.sec_chunks);
+            piece(reinterpret_cast<const uint8_t*>(in.states[s]), 4ull * c.sec_lanes * c.sec_chunks);
             chunked(s, c.payload_bytes, in.chunk_segs[s][c.sec_chunks]);
             if (c.enc == kEncTagged) {
                 w.uint(c.packed_bits, 8);
@@ -1014,7 +1029,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     const size_t esz = dtype == CHAIN_F64 ? 8 : 4;
     const uint64_t nd = n * dims;
     const int64_t p_eff = bl ? p : 1;
-    if (bytes_per_lane == 0) bytes_per_lane = 1024;
+    if (bytes_per_lane == 0) bytes_per_lane = 4096;
     if (max_steps == 0) max_steps = 2048;
 
     chain_status st_ = ensure_state(ctx, sizeof(EncState));
@@ -1312,6 +1327,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
             jb.etab = etab + etab_used;
             etab_used += c.sec_alphabet;
             jb.chunks = c.sec_chunks;
+            jb.lanes = c.sec_lanes;
             jb.S = c.sec_S;
             jb.bytes = slots + slot_off[s];
             jb.slot_cap = slot_cap[s];

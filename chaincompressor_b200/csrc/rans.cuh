@@ -6,10 +6,12 @@
 // prec = clamp(3*min(18, bitlen(#unique)+2)/2, 12, 20) (lcps_cpp.cpp:541-552), the
 // state interval [4*2^prec, 1024*2^prec) with byte-wise renormalisation, and the
 // compact probability-table tokens (lcps_cpp.cpp:686-729).  What is new: a symbol
-// stream is cut into chunks; one warp codes one chunk with 32 interleaved states
-// (symbol j of a chunk belongs to lane j % 32), and the lanes' renormalisation bytes
-// are interleaved in one byte stream per chunk in the exact order the decoding warp
-// consumes them (lane order within a step, most significant byte first).
+// stream is cut into chunks; one warp codes one chunk with W interleaved states
+// (W = lanes of the section, 1..32; symbol j of a chunk belongs to lane j % W), and
+// the lanes' renormalisation bytes are interleaved in one byte stream per chunk in the
+// exact order the decoding warp consumes them (lane order within a step, most
+// significant byte first).  Small sections use fewer lanes, since each lane stores a
+// 4-byte final state.
 //
 // Probability normalisation is this project's own exact-integer scheme (the
 // reference's uses x87 long double): symbols with f_s * M / n < 1 get probability 1,
@@ -451,14 +453,16 @@ struct RansJob {
     uint32_t prec;
     uint32_t alphabet;
     uint32_t chunks;
+    uint32_t lanes;           // interleaved states per chunk (1..32)
     uint32_t first_block;     // first CTA of this job (kRansWarps chunks per CTA)
+    uint32_t pad;
     uint64_t S;               // symbols per chunk (multiple of 32)
     uint8_t* bytes;           // encode: chunk slots (slot_cap each); decode: container
     uint64_t bytes_len;       // decode: container length (staged loads stay inside it)
     uint64_t slot_cap;        // encode only
     const uint64_t* chunk_off;  // decode: absolute byte offset of each chunk (chunks + 1)
     uint32_t* chunk_len;      // encode: bytes per chunk
-    uint32_t* states;         // encode: out [chunks * 32]; decode: in
+    uint32_t* states;         // encode: out [chunks * lanes]; decode: in
 };
 
 constexpr int kMaxRansJobs = 16;
@@ -558,8 +562,10 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
     uint32_t* buf = reinterpret_cast<uint32_t*>(rsm + J.tab_cap * 16ull) + warp * 2 * 1024;
     const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
     const uint64_t cend = min(cbeg + jb.S, jb.count);
-    const uint32_t steps = static_cast<uint32_t>((cend - cbeg + 31) / 32);
+    const uint32_t W = jb.lanes;
+    const uint32_t steps = static_cast<uint32_t>((cend - cbeg + W - 1) / W);
     const uint32_t ntiles = (steps + kRansTile - 1) / kRansTile;
+    const uint64_t tile_syms = static_cast<uint64_t>(kRansTile) * W;
     const uint32_t prec = jb.prec;
     const uint32_t L = 4u << prec;
     const uint32_t lt = lanemask_lt();
@@ -570,25 +576,25 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
     uint32_t r[32];
     bool vec;
     {
-        const uint64_t tb = cbeg + 1024ull * (ntiles - 1);
-        tile_load(jb.sym, tb, min(tb + 1024, cend), r, vec);
+        const uint64_t tb = cbeg + tile_syms * (ntiles - 1);
+        tile_load(jb.sym, tb, min(tb + tile_syms, cend), r, vec);
         tile_store(buf + ((ntiles - 1) & 1) * 1024, r, vec);
         __syncwarp();
     }
     for (int k = static_cast<int>(ntiles) - 1; k >= 0 && !overflow; --k) {
         if (k > 0) {
-            const uint64_t tb = cbeg + 1024ull * (k - 1);
-            tile_load(jb.sym, tb, min(tb + 1024, cend), r, vec);
+            const uint64_t tb = cbeg + tile_syms * (k - 1);
+            tile_load(jb.sym, tb, min(tb + tile_syms, cend), r, vec);
         }
         const uint32_t* cur = buf + (k & 1) * 1024;
         const int t_hi = min(static_cast<int>(steps) - 1, 32 * k + 31);
         for (int t = t_hi; t >= 32 * k; --t) {
-            const uint64_t kk = cbeg + static_cast<uint64_t>(t) * 32 + lane;
-            const bool act = kk < cend;
+            const uint64_t kk = cbeg + static_cast<uint64_t>(t) * W + lane;
+            const bool act = static_cast<uint32_t>(lane) < W && kk < cend;
             uint32_t nb = 0;
             uint4 e = make_uint4(1, 0, 0, 0);
             if (act) {
-                const uint32_t s = cur[(t - 32 * k) * 32 + lane];
+                const uint32_t s = cur[(t - 32 * k) * W + lane];
                 e = smem_tab ? tab[s] : __ldg(jb.etab + s);
                 const uint32_t xmax = e.x << 10;  // ((L >> prec) << 8) * freq
                 nb = (x >= xmax) + ((x >> 8) >= xmax) + ((x >> 16) >= xmax);
@@ -618,7 +624,7 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
         if (lane == 0) set_error(err, kErrInternal);
         return;
     }
-    jb.states[static_cast<uint64_t>(c) * 32 + lane] = x;
+    if (static_cast<uint32_t>(lane) < W) jb.states[static_cast<uint64_t>(c) * W + lane] = x;
     if (lane == 0) jb.chunk_len[c] = static_cast<uint32_t>(jb.slot_cap - pos);
 }
 
@@ -669,11 +675,12 @@ static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uin
     if (c >= jb.chunks) return;
     const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
     const uint64_t cend = min(cbeg + jb.S, jb.count);
-    const uint32_t steps = static_cast<uint32_t>((cend - cbeg + 31) / 32);
+    const uint32_t W = jb.lanes;
+    const uint32_t steps = static_cast<uint32_t>((cend - cbeg + W - 1) / W);
     const uint32_t lt = lanemask_lt();
     uint64_t pos = jb.chunk_off[c];
     const uint64_t end = jb.chunk_off[c + 1];
-    uint32_t x = jb.states[static_cast<uint64_t>(c) * 32 + lane];
+    uint32_t x = static_cast<uint32_t>(lane) < W ? jb.states[static_cast<uint64_t>(c) * W + lane] : L;
     bool bad = (x < L) || (static_cast<uint64_t>(x) >= (static_cast<uint64_t>(L) << 8)) || end > jb.bytes_len ||
                pos > end;
     if (__any_sync(0xffffffffu, bad)) {
@@ -688,8 +695,8 @@ static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uin
             wbase = pos & ~15ull;
             window_fill(win, jb.bytes, jb.bytes_len, wbase);
         }
-        const uint64_t k = cbeg + static_cast<uint64_t>(t) * 32 + lane;
-        const bool act = k < cend;
+        const uint64_t k = cbeg + static_cast<uint64_t>(t) * W + lane;
+        const bool act = static_cast<uint32_t>(lane) < W && k < cend;
         uint32_t nb = 0;
         if (act) {
             const uint32_t slot = x & (M - 1);

@@ -68,7 +68,7 @@ typedef struct chain_opts {
     int32_t l1;                     /* level-1 chaining                                   */
     int32_t l2;                     /* level-2 block differencing                         */
     uint32_t rans_bytes_per_lane;   /* entropy stage: target coded bytes per rANS lane
-                                       (each lane adds a 4-byte state); 0 = default 1024  */
+                                       (each lane adds a 4-byte state); 0 = default 4096  */
     uint32_t rans_max_steps;        /* entropy stage: most symbols one lane codes
                                        (serial depth); 0 = default 2048                   */
     uint32_t reserved[10];

@@ -27,14 +27,14 @@ class Reader:
 def _section(r, count):
     prec, alphabet, tlen = r.u("B"), r.u("I"), r.u("I")
     r.take(tlen)
-    S, chunks, payload = r.u("Q"), r.u("I"), r.u("Q")
+    S, lanes, chunks, payload = r.u("Q"), r.u("B"), r.u("I"), r.u("Q")
     lens = struct.unpack("<%dI" % chunks, r.take(4 * chunks))
     if sum(lens) != payload:
         raise ValueError("chunk lengths do not add up to the payload length")
-    r.take(128 * chunks)
+    r.take(4 * lanes * chunks)
     r.take(payload)
-    return {"prec": prec, "alphabet": alphabet, "table_bytes": tlen, "S": S, "chunks": chunks,
-            "payload": sum(lens), "symbols": count}
+    return {"prec": prec, "alphabet": alphabet, "table_bytes": tlen, "S": S, "lanes": lanes, "chunks": chunks,
+            "payload": sum(lens), "symbols": count, "state_bytes": 4 * lanes * chunks}
 
 
 def _component(r, body_len):
