@@ -178,6 +178,11 @@ def run_ours(args, rank: int, world: int):
     decomp = lambda src, dst: codec.decompress_ptr(src, clen, dst, n * d * 8)  # noqa: E731
     for _ in range(args.warmup):
         decomp(cont_dev.data_ptr(), out_dev.data_ptr())
+    # the host-buffer calls stage through the same arenas; warm them too
+    for _ in range(args.warmup):
+        comp(soa_host.data_ptr())
+        codec.result_copy_to(cont_host.data_ptr(), clen)
+        decomp(cont_host.data_ptr(), out_host.data_ptr())
 
     def timed(fn, stages=False):
         """Device time per step from CUDA events on the library stream (the library

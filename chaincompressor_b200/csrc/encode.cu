@@ -400,45 +400,95 @@ __device__ __forceinline__ void warp_hist_add(uint32_t* bins, uint32_t v, bool v
     if ((peers & lanemask_lt()) == 0) atomicAdd(&bins[v], static_cast<uint32_t>(__popc(peers)));
 }
 
-// Per-stream statistics: per-dimension min/max, overall max, record tags
-// (max(1, max_d bitlen v)) histogram and their bit total.  Registers hold the
-// extrema; the tag histogram is warp-aggregated in shared memory.
-__global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState* st, int s0) {
+// Eight 16-bit counters packed into four registers (bins 0..7), for the hot small
+// values of a stream; flushed into shared memory at the end.
+struct PackedCount8 {
+    uint32_t r0 = 0, r1 = 0, r2 = 0, r3 = 0;
+    __device__ __forceinline__ void add(uint32_t v) {   // v < 8
+        const uint32_t inc = 1u << ((v & 1u) << 4);
+        const uint32_t h = v >> 1;
+        r0 += h == 0 ? inc : 0u;
+        r1 += h == 1 ? inc : 0u;
+        r2 += h == 2 ? inc : 0u;
+        r3 += h == 3 ? inc : 0u;
+    }
+    // Warp-sums the counters and adds them to bins[0..7] (lane 0).
+    __device__ __forceinline__ void flush(uint32_t* bins) {
+        uint32_t c[8] = {r0 & 0xffffu, r0 >> 16, r1 & 0xffffu, r1 >> 16,
+                         r2 & 0xffffu, r2 >> 16, r3 & 0xffffu, r3 >> 16};
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t t = warp_sum(c[k]);
+            if ((threadIdx.x & 31) == 0 && t) atomicAdd(&bins[k], t);
+        }
+        r0 = r1 = r2 = r3 = 0;
+    }
+};
+
+// Per-stream statistics in one pass: per-dimension min/max, overall max, the record
+// tags (max(1, max_d bitlen v)) histogram and bit total, and the value histogram of
+// the raw candidate (values < 2^18; a larger max makes the candidate ineligible).
+// Values below 8 count in registers, below kSmemHistBins in shared memory, the rest
+// in global memory with warp aggregation.  Counters flush before they could overflow.
+constexpr int kSmemHistBins = 4096;
+constexpr uint32_t kFlushEvery = 16384;   // values per thread between register flushes
+__global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState* st, uint32_t* hist,
+                                                       uint64_t hist_stride, int s0) {
     const int s = s0 + blockIdx.y;
     const StreamRef r = refs.s[s];
     const uint64_t nrec = stream_records(r);
     __shared__ uint32_t smin[kMaxDims], smax[kMaxDims], stag[34];
+    __shared__ uint32_t sh[kSmemHistBins];
     __shared__ unsigned long long sbits;
     if (threadIdx.x < kMaxDims) { smin[threadIdx.x] = 0xffffffffu; smax[threadIdx.x] = 0; }
     if (threadIdx.x < 34) stag[threadIdx.x] = 0;
+    for (int t = threadIdx.x; t < kSmemHistBins; t += blockDim.x) sh[t] = 0;
     if (threadIdx.x == 0) sbits = 0;
     __syncthreads();
     const uint32_t D = r.dims;
+    uint32_t* gh = hist + hist_stride * s;
     uint32_t mn[kMaxDims], mx[kMaxDims];
 #pragma unroll
     for (int d = 0; d < kMaxDims; ++d) { mn[d] = 0xffffffffu; mx[d] = 0; }
     uint64_t bits = 0;
+    PackedCount8 vc, tc;
+    uint32_t since_flush = 0;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     const uint64_t rounds = (nrec + stride - 1) / stride;
     for (uint64_t rr = 0; rr < rounds; ++rr) {
         const uint64_t j = rr * stride + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
         const bool valid = j < nrec;
         uint32_t tag = 1;
-        if (valid) {
 #pragma unroll
-            for (int d = 0; d < kMaxDims; ++d) {
-                if (d < static_cast<int>(D)) {
-                    const uint32_t v = r.data[j * D + d];
+        for (int d = 0; d < kMaxDims; ++d) {
+            if (d < static_cast<int>(D)) {
+                const uint32_t v = valid ? r.data[j * D + d] : 0u;
+                if (valid) {
                     mn[d] = v < mn[d] ? v : mn[d];
                     mx[d] = v > mx[d] ? v : mx[d];
                     const uint32_t w = bitlen32(v);
                     tag = w > tag ? w : tag;
+                    if (v < 8) vc.add(v);
+                    else if (v < kSmemHistBins) atomicAdd(&sh[v], 1u);
                 }
+                const bool big = valid && v >= kSmemHistBins && v < kRansMaxAlphabet;
+                if (__any_sync(0xffffffffu, big)) warp_hist_add(gh, v, big);
             }
-            bits += static_cast<uint64_t>(D) * tag;
         }
-        warp_hist_add(stag, tag, valid);
+        if (valid) {
+            bits += static_cast<uint64_t>(D) * tag;
+            if (tag < 8) tc.add(tag);
+            else atomicAdd(&stag[tag], 1u);
+        }
+        since_flush += D;
+        if (since_flush >= kFlushEvery) {
+            vc.flush(sh);
+            tc.flush(stag);
+            since_flush = 0;
+        }
     }
+    vc.flush(sh);
+    tc.flush(stag);
 #pragma unroll
     for (int d = 0; d < kMaxDims; ++d) {
         if (d < static_cast<int>(D)) {
@@ -460,39 +510,8 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
         atomicMax(&g.maxtag, threadIdx.x);
     }
     if (threadIdx.x == 0 && sbits) atomicAdd(reinterpret_cast<unsigned long long*>(&g.tag_bits), sbits);
-}
-
-// Value histograms for the raw candidate (alphabet = max + 1 < 2^18).  Values below
-// kSmemHistBins count in shared memory, larger ones in global memory; both paths are
-// warp-aggregated, so a hot value costs one atomic per warp instead of one per lane.
-constexpr int kSmemHistBins = 8192;
-__global__ void __launch_bounds__(256) k_value_hist(StreamRefs refs, const EncState* st, uint32_t* hist,
-                                                     uint64_t hist_stride, int s0) {
-    const int s = s0 + blockIdx.y;
-    const StreamRef r = refs.s[s];
-    const uint32_t maxall = st->st[s].maxall;
-    const uint64_t nrec = stream_records(r);
-    if (nrec == 0 || maxall >= kRansMaxAlphabet) return;
-    const uint32_t A = maxall + 1;
-    uint32_t* h = hist + hist_stride * s;
-    const uint64_t nval = nrec * r.dims;
-    __shared__ uint32_t sh[kSmemHistBins];
-    const uint32_t ns = A < kSmemHistBins ? A : kSmemHistBins;
-    for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) sh[t] = 0;
-    __syncthreads();
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    const uint64_t rounds = (nval + stride - 1) / stride;
-    for (uint64_t rr = 0; rr < rounds; ++rr) {
-        const uint64_t j = rr * stride + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-        const bool valid = j < nval;
-        const uint32_t v = valid ? r.data[j] : 0u;
-        const bool small = v < kSmemHistBins;
-        warp_hist_add(sh, v, valid && small);
-        warp_hist_add(h, v, valid && !small);
-    }
-    __syncthreads();
-    for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x)
-        if (sh[t]) atomicAdd(&h[t], sh[t]);
+    for (int t = threadIdx.x; t < kSmemHistBins; t += blockDim.x)
+        if (sh[t]) atomicAdd(&gh[t], sh[t]);
 }
 
 // One CTA per (stream, kind): kind 0 = raw value table, kind 1 = tag table.
@@ -1171,8 +1190,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     refs.s[4] = StreamRef{rel, dims, nullptr, n};
     refs.s[kCorrGaps] = StreamRef{corr_gaps, 1, nullptr, 0};
     refs.s[kCorrIds] = StreamRef{corr_ids, 1, nullptr, 0};
-    k_stream_stats<<<dim3(grid_for(n, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, 0); count_launch();
-    k_value_hist<<<dim3(grid_for(nd, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, hist, hist_stride, 0); count_launch();
+    k_stream_stats<<<dim3(grid_for(n, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, hist, hist_stride, 0); count_launch();
     k_tables<<<dim3(kStreams, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob,
                                                                tag_cum, 0); count_launch();
     k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, 0, kStreams); count_launch();
@@ -1205,8 +1223,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         refs.s[kCorrGaps].count_const = nc;
         refs.s[kCorrIds].count_const = nc;
         const unsigned g = grid_for(nc, 256, 148u * 4u);
-        k_stream_stats<<<dim3(g, 2), 256, 0, stream>>>(refs, st, kCorrGaps); count_launch();
-        k_value_hist<<<dim3(g, 2), 256, 0, stream>>>(refs, st, hist, hist_stride, kCorrGaps); count_launch();
+        k_stream_stats<<<dim3(g, 2), 256, 0, stream>>>(refs, st, hist, hist_stride, kCorrGaps); count_launch();
         k_tables<<<dim3(2, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob, tag_cum,
                                                           kCorrGaps); count_launch();
         k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, kCorrGaps, 2); count_launch();

@@ -131,11 +131,16 @@ __global__ void __launch_bounds__(1024) scan_tilesums_kernel(T* aggr, uint64_t c
     if (threadIdx.x == 0 && total) *total = carry;
 }
 
-template <typename T, typename InF, typename OutF, typename Op>
+// Scan-then-output kernel.  With Striped = true, out() is called in the coalesced
+// (striped) element order, from prefixes and values staged in shared memory; use it
+// when out() writes element-indexed arrays.  Striped needs two tiles of shared memory,
+// so it is used for 4-byte element types.
+template <typename T, typename InF, typename OutF, typename Op, bool Striped>
 __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(InF in, OutF out, uint64_t n,
                                                                   const T* tile_prefix, Op op) {
     constexpr int I = ScanShape<T>::kItems, TILE = ScanShape<T>::kTile;
-    __shared__ T vals[TILE + TILE / 32];
+    constexpr int PADDED = TILE + TILE / 32;
+    __shared__ T vals[Striped ? 2 * PADDED : PADDED];
     __shared__ T scratch[33];
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * TILE;
     scan_stage<T>(in, n, base, vals);
@@ -149,11 +154,27 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(InF in, OutF o
         agg = op(agg, local[k]);
     }
     T ex = op(tile_prefix[blockIdx.x], block_exclusive_scan_op(agg, op, scratch, static_cast<T*>(nullptr)));
+    if constexpr (Striped) {
+        T* pre = vals + PADDED;
 #pragma unroll
-    for (int k = 0; k < I; ++k) {
-        const uint64_t i = base + threadIdx.x * I + k;
-        if (i < n) out(i, ex, local[k]);
-        ex = op(ex, local[k]);
+        for (int k = 0; k < I; ++k) {
+            pre[scan_pad(threadIdx.x * I + k)] = ex;
+            ex = op(ex, local[k]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < I; ++k) {
+            const int j = k * kScanThreads + threadIdx.x;
+            const uint64_t i = base + j;
+            if (i < n) out(i, pre[scan_pad(j)], vals[scan_pad(j)]);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < I; ++k) {
+            const uint64_t i = base + threadIdx.x * I + k;
+            if (i < n) out(i, ex, local[k]);
+            ex = op(ex, local[k]);
+        }
     }
 }
 
@@ -166,9 +187,11 @@ inline uint64_t scan_tiles(uint64_t n) {
 inline uint64_t scan_scratch_bytes(uint64_t n) { return 16 * (n / 2048 + 16); }
 
 // Launches the three scan kernels on `stream`; `tile_buf` holds scan_tiles<T>(n) values.
+// out() runs in striped (coalesced) element order for 4-byte element types.
 template <typename T, typename InF, typename OutF, typename Op = SumOp<T>>
 void device_exclusive_scan(InF in, OutF out, uint64_t n, T* tile_buf, T* total, cudaStream_t stream,
                            Op op = Op()) {
+    constexpr bool kStriped = sizeof(T) <= 4;
     const uint64_t tiles = scan_tiles<T>(n);
     if (tiles == 0) {
         if (total) cudaMemsetAsync(total, 0, sizeof(T), stream);
@@ -176,8 +199,8 @@ void device_exclusive_scan(InF in, OutF out, uint64_t n, T* tile_buf, T* total, 
     }
     scan_reduce_kernel<T, InF, Op><<<static_cast<unsigned>(tiles), kScanThreads, 0, stream>>>(in, n, tile_buf, op); count_launch();
     scan_tilesums_kernel<T, Op><<<1, 1024, 0, stream>>>(tile_buf, tiles, total, op); count_launch();
-    scan_apply_kernel<T, InF, OutF, Op><<<static_cast<unsigned>(tiles), kScanThreads, 0, stream>>>(in, out, n,
-                                                                                               tile_buf, op); count_launch();
+    scan_apply_kernel<T, InF, OutF, Op, kStriped><<<static_cast<unsigned>(tiles), kScanThreads, 0, stream>>>(
+        in, out, n, tile_buf, op); count_launch();
 }
 
 }  // namespace chain
