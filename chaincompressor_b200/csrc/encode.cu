@@ -388,6 +388,11 @@ struct StreamRefs {
     StreamRef s[kCodeStreams];
 };
 
+// The streams one statistics launch covers (blockIdx.y indexes s[]).
+struct StreamSel {
+    int s[kCodeStreams];
+};
+
 __device__ __forceinline__ uint64_t stream_records(const StreamRef& r) {
     return r.count_dev ? static_cast<uint64_t>(*r.count_dev) : r.count_const;
 }
@@ -425,17 +430,22 @@ struct PackedCount8 {
     }
 };
 
+constexpr int kSmemHistBins = 4096;
+
 // Per-stream statistics in one pass: per-dimension min/max, overall max, the record
 // tags (max(1, max_d bitlen v)) histogram and bit total, and the value histogram of
 // the raw candidate (values < 2^18; a larger max makes the candidate ineligible).
-// Values below 8 count in registers, below kSmemHistBins in shared memory, the rest
-// in global memory with warp aggregation.  Counters flush before they could overflow.
-constexpr int kSmemHistBins = 4096;
-constexpr uint32_t kFlushEvery = 16384;   // values per thread between register flushes
+// Template DIM is the records' dimension count (0 = read it at run time).  Each thread
+// takes groups of 4 records with 16-byte loads; values below 8 count in registers,
+// below kSmemHistBins in shared memory, the rest in global memory.  Register
+// counters flush before they could overflow.  blockIdx.y selects the stream from
+// sel[] (the streams of one launch share DIM).
+template <int DIM>
 __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState* st, uint32_t* hist,
-                                                       uint64_t hist_stride, int s0) {
-    const int s = s0 + blockIdx.y;
+                                                       uint64_t hist_stride, StreamSel sel) {
+    const int s = sel.s[blockIdx.y];
     const StreamRef r = refs.s[s];
+    const uint32_t D = DIM ? DIM : r.dims;
     const uint64_t nrec = stream_records(r);
     __shared__ uint32_t smin[kMaxDims], smax[kMaxDims], stag[34];
     __shared__ uint32_t sh[kSmemHistBins];
@@ -445,53 +455,74 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
     for (int t = threadIdx.x; t < kSmemHistBins; t += blockDim.x) sh[t] = 0;
     if (threadIdx.x == 0) sbits = 0;
     __syncthreads();
-    const uint32_t D = r.dims;
     uint32_t* gh = hist + hist_stride * s;
-    uint32_t mn[kMaxDims], mx[kMaxDims];
+    constexpr int KD = DIM ? DIM : kMaxDims;
+    // 4-record groups per thread between flushes of the 16-bit register counters.
+    constexpr uint32_t kFlushGroups = 16383 / KD;
+    uint32_t mn[KD], mx[KD];
 #pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) { mn[d] = 0xffffffffu; mx[d] = 0; }
+    for (int d = 0; d < KD; ++d) { mn[d] = 0xffffffffu; mx[d] = 0; }
     uint64_t bits = 0;
     PackedCount8 vc, tc;
-    uint32_t since_flush = 0;
+    uint32_t groups_since_flush = 0;
+    auto value = [&](uint32_t v, int d, uint32_t& tag) {
+        mn[d] = v < mn[d] ? v : mn[d];
+        mx[d] = v > mx[d] ? v : mx[d];
+        const uint32_t w = bitlen32(v);
+        tag = w > tag ? w : tag;
+        if (v < 8) vc.add(v);
+        else if (v < kSmemHistBins) atomicAdd(&sh[v], 1u);
+        else if (v < kRansMaxAlphabet) atomicAdd(&gh[v], 1u);
+    };
+    auto record_done = [&](uint32_t tag) {
+        bits += static_cast<uint64_t>(D) * tag;
+        if (tag < 8) tc.add(tag);
+        else atomicAdd(&stag[tag], 1u);
+    };
+    const uint64_t ngroups = (nrec + 3) / 4;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    const uint64_t rounds = (nrec + stride - 1) / stride;
+    const uint64_t rounds = (ngroups + stride - 1) / stride;
+    const bool vec_ok = (reinterpret_cast<uintptr_t>(r.data) & 15) == 0;
     for (uint64_t rr = 0; rr < rounds; ++rr) {
-        const uint64_t j = rr * stride + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-        const bool valid = j < nrec;
-        uint32_t tag = 1;
+        const uint64_t g = rr * stride + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+        if (g < ngroups) {
+            const uint64_t rec0 = 4 * g;
+            if (DIM && vec_ok && rec0 + 4 <= nrec) {
+                uint32_t v[4 * KD];
+                const uint4* p = reinterpret_cast<const uint4*>(r.data + rec0 * D);
 #pragma unroll
-        for (int d = 0; d < kMaxDims; ++d) {
-            if (d < static_cast<int>(D)) {
-                const uint32_t v = valid ? r.data[j * D + d] : 0u;
-                if (valid) {
-                    mn[d] = v < mn[d] ? v : mn[d];
-                    mx[d] = v > mx[d] ? v : mx[d];
-                    const uint32_t w = bitlen32(v);
-                    tag = w > tag ? w : tag;
-                    if (v < 8) vc.add(v);
-                    else if (v < kSmemHistBins) atomicAdd(&sh[v], 1u);
+                for (int q = 0; q < KD; ++q) {
+                    const uint4 t = __ldg(p + q);
+                    v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
                 }
-                const bool big = valid && v >= kSmemHistBins && v < kRansMaxAlphabet;
-                if (__any_sync(0xffffffffu, big)) warp_hist_add(gh, v, big);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    uint32_t tag = 1;
+#pragma unroll
+                    for (int d = 0; d < KD; ++d) value(v[k * KD + d], d, tag);
+                    record_done(tag);
+                }
+            } else {
+                for (uint64_t rec = rec0; rec < rec0 + 4 && rec < nrec; ++rec) {
+                    uint32_t tag = 1;
+#pragma unroll
+                    for (int d = 0; d < KD; ++d)
+                        if (DIM || d < static_cast<int>(D)) value(r.data[rec * D + d], d, tag);
+                    record_done(tag);
+                }
             }
         }
-        if (valid) {
-            bits += static_cast<uint64_t>(D) * tag;
-            if (tag < 8) tc.add(tag);
-            else atomicAdd(&stag[tag], 1u);
-        }
-        since_flush += D;
-        if (since_flush >= kFlushEvery) {
+        if (++groups_since_flush == kFlushGroups) {
             vc.flush(sh);
             tc.flush(stag);
-            since_flush = 0;
+            groups_since_flush = 0;
         }
     }
     vc.flush(sh);
     tc.flush(stag);
 #pragma unroll
-    for (int d = 0; d < kMaxDims; ++d) {
-        if (d < static_cast<int>(D)) {
+    for (int d = 0; d < KD; ++d) {
+        if (DIM || d < static_cast<int>(D)) {
             const uint32_t a = warp_min(mn[d]), b = warp_max(mx[d]);
             if ((threadIdx.x & 31) == 0) { atomicMin(&smin[d], a); atomicMax(&smax[d], b); }
         }
@@ -499,17 +530,17 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
     bits = warp_sum(bits);
     if ((threadIdx.x & 31) == 0 && bits) atomicAdd(&sbits, static_cast<unsigned long long>(bits));
     __syncthreads();
-    StreamStats& g = st->st[s];
+    StreamStats& gs = st->st[s];
     if (threadIdx.x < D && smax[threadIdx.x] >= smin[threadIdx.x]) {
-        atomicMin(&g.minv[threadIdx.x], smin[threadIdx.x]);
-        atomicMax(&g.maxv[threadIdx.x], smax[threadIdx.x]);
-        atomicMax(&g.maxall, smax[threadIdx.x]);
+        atomicMin(&gs.minv[threadIdx.x], smin[threadIdx.x]);
+        atomicMax(&gs.maxv[threadIdx.x], smax[threadIdx.x]);
+        atomicMax(&gs.maxall, smax[threadIdx.x]);
     }
     if (threadIdx.x < 34 && stag[threadIdx.x]) {
-        atomicAdd(&g.tag_hist[threadIdx.x], stag[threadIdx.x]);
-        atomicMax(&g.maxtag, threadIdx.x);
+        atomicAdd(&gs.tag_hist[threadIdx.x], stag[threadIdx.x]);
+        atomicMax(&gs.maxtag, threadIdx.x);
     }
-    if (threadIdx.x == 0 && sbits) atomicAdd(reinterpret_cast<unsigned long long*>(&g.tag_bits), sbits);
+    if (threadIdx.x == 0 && sbits) atomicAdd(reinterpret_cast<unsigned long long*>(&gs.tag_bits), sbits);
     for (int t = threadIdx.x; t < kSmemHistBins; t += blockDim.x)
         if (sh[t]) atomicAdd(&gh[t], sh[t]);
 }
@@ -1028,6 +1059,29 @@ static chain_status status_from_err(uint32_t err) {
     return set_err(CHAIN_ERR_DEVICE, "internal encoder error (flags " + std::to_string(err) + ")");
 }
 
+// Statistics of streams s0 .. s0+count-1: one launch for the one-dimensional streams
+// and one for the D-dimensional ones (templated on D when D <= 4).
+static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, uint64_t hist_stride, uint32_t dims,
+                         uint64_t max_records, int s0, int count, cudaStream_t stream) {
+    StreamSel one{}, many{};
+    int n1 = 0, nd = 0;
+    for (int s = s0; s < s0 + count; ++s) {
+        if (refs.s[s].dims == 1) one.s[n1++] = s;
+        else many.s[nd++] = s;
+    }
+    const unsigned g = grid_for((max_records + 3) / 4, 256, 148u * 4u);
+    if (n1) { k_stream_stats<1><<<dim3(g, n1), 256, 0, stream>>>(refs, st, hist, hist_stride, one); count_launch(); }
+    if (nd) {
+        switch (dims) {
+            case 2: k_stream_stats<2><<<dim3(g, nd), 256, 0, stream>>>(refs, st, hist, hist_stride, many); break;
+            case 3: k_stream_stats<3><<<dim3(g, nd), 256, 0, stream>>>(refs, st, hist, hist_stride, many); break;
+            case 4: k_stream_stats<4><<<dim3(g, nd), 256, 0, stream>>>(refs, st, hist, hist_stride, many); break;
+            default: k_stream_stats<0><<<dim3(g, nd), 256, 0, stream>>>(refs, st, hist, hist_stride, many); break;
+        }
+        count_launch();
+    }
+}
+
 template <typename FT, bool SOA, typename KT>
 static void launch_quantize(const void* pts, uint64_t n, uint32_t D, EncState* st, void* key, uint32_t* rel,
                             uint64_t* cidx, double* cval, uint64_t cap, cudaStream_t s) {
@@ -1190,7 +1244,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     refs.s[4] = StreamRef{rel, dims, nullptr, n};
     refs.s[kCorrGaps] = StreamRef{corr_gaps, 1, nullptr, 0};
     refs.s[kCorrIds] = StreamRef{corr_ids, 1, nullptr, 0};
-    k_stream_stats<<<dim3(grid_for(n, 256, 148u * 4u), kStreams), 256, 0, stream>>>(refs, st, hist, hist_stride, 0); count_launch();
+    launch_stats(refs, st, hist, hist_stride, dims, n, 0, kStreams, stream);
     k_tables<<<dim3(kStreams, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob,
                                                                tag_cum, 0); count_launch();
     k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, 0, kStreams); count_launch();
@@ -1223,7 +1277,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         refs.s[kCorrGaps].count_const = nc;
         refs.s[kCorrIds].count_const = nc;
         const unsigned g = grid_for(nc, 256, 148u * 4u);
-        k_stream_stats<<<dim3(g, 2), 256, 0, stream>>>(refs, st, hist, hist_stride, kCorrGaps); count_launch();
+        launch_stats(refs, st, hist, hist_stride, dims, nc, kCorrGaps, 2, stream);
         k_tables<<<dim3(2, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob, tag_cum,
                                                           kCorrGaps); count_launch();
         k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, kCorrGaps, 2); count_launch();
