@@ -30,7 +30,8 @@ CHAIN_SOA, CHAIN_AOS = 0, 1
 # Every entry point declared in include/chain_b200.h.
 EXPORTS = ("chain_ctx_create", "chain_ctx_destroy", "chain_last_error_message", "chain_compress_bound",
            "chain_compress", "chain_result_copy", "chain_result_device_ptr", "chain_peek", "chain_decompress",
-           "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count")
+           "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count",
+           "chain_decompress_noalloc")
 
 
 class ChainError(RuntimeError):
@@ -71,8 +72,10 @@ def load() -> ctypes.CDLL:
         L.chain_decompress.argtypes = [P, P, sz, i32, i32, P, sz, ctypes.POINTER(u64), ctypes.POINTER(u32)]
         L.chain_debug_streams.argtypes = [P, P, P, ctypes.POINTER(u64), P, ctypes.POINTER(u64), P,
                                           ctypes.POINTER(u64), P]
+        L.chain_decompress_noalloc.argtypes = [P, sz, i32, i32, P, sz, ctypes.POINTER(u64), ctypes.POINTER(u32), P]
         for f in ("chain_ctx_create", "chain_compress", "chain_result_copy", "chain_peek", "chain_decompress",
-                  "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count"):
+                  "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count",
+                  "chain_decompress_noalloc"):
             getattr(L, f).restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -202,6 +205,16 @@ def peek(data: bytes):
     src = ctypes.create_string_buffer(data, len(data))
     _check(L.chain_peek(ctypes.addressof(src), len(data), ctypes.byref(n), ctypes.byref(d), ctypes.byref(t)))
     return n.value, d.value, t.value
+
+
+def decompress_noalloc_ptr(src_ptr: int, length: int, out_ptr: int, capacity: int, dtype: int = CHAIN_F64,
+                           layout: int = CHAIN_AOS, stream: int = 0):
+    """chain_decompress_noalloc on the current CUDA device: no context, no allocation."""
+    L = load()
+    n, d = ctypes.c_uint64(), ctypes.c_uint32()
+    _check(L.chain_decompress_noalloc(ctypes.c_void_p(src_ptr), length, dtype, layout, ctypes.c_void_p(out_ptr),
+                                      capacity, ctypes.byref(n), ctypes.byref(d), ctypes.c_void_p(stream)))
+    return n.value, d.value
 
 
 def launch_count() -> int:

@@ -12,13 +12,21 @@
 namespace chain {
 
 // Bump allocator over one device allocation.  reserve() grows the allocation between
-// calls (never while kernels of the current call are queued on it).
+// calls (never while kernels of the current call are queued on it).  A `fixed` arena
+// lies over memory it does not own: reserve() never allocates or frees, it only
+// reports whether `bytes` fit (and records the request in `requested`).
 struct Arena {
     uint8_t* base = nullptr;
     size_t cap = 0;
     size_t used = 0;
+    bool fixed = false;
+    size_t requested = 0;
     cudaError_t reserve(size_t bytes) {
         used = 0;
+        if (fixed) {
+            requested = bytes;
+            return bytes <= cap ? cudaSuccess : cudaErrorMemoryAllocation;
+        }
         if (bytes <= cap) return cudaSuccess;
         if (base) cudaFree(base);
         base = nullptr;
@@ -160,5 +168,8 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
 chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, chain_dtype out_dtype,
                           chain_layout out_layout, void* out, size_t out_capacity, uint64_t* n,
                           uint32_t* dims);
+
+// Bytes of device state (and of its host mirror) that decode_frame uses.
+size_t decode_state_bytes();
 
 }  // namespace chain

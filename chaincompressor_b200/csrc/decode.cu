@@ -681,4 +681,6 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     return CHAIN_OK;
 }
 
+size_t decode_state_bytes() { return sizeof(DecState); }
+
 }  // namespace chain

@@ -115,6 +115,26 @@ CHAIN_API chain_status chain_decompress(chain_ctx* ctx, const void* container, s
                               chain_dtype out_dtype, chain_layout out_layout, void* out,
                               size_t out_capacity_bytes, uint64_t* n, uint32_t* dims);
 
+/* Decompression that allocates nothing, for callers that cannot allocate memory when
+ * they decode (a plug-in inside an application that owns the device memory pool or
+ * runs under a hard memory cap; a loop that must not pay for cudaMalloc/cudaFree, which
+ * can synchronise the device).  No counterpart in the reference: it is this library's
+ * own addition.  Same arguments, output and errors as chain_decompress, without a
+ * context: it runs on the calling thread's current device, on `cuda_stream` (a
+ * cudaStream_t; NULL = the default stream), and calls no cudaMalloc, cudaFree or any
+ * other allocating routine.  Its working memory is one fixed 64 MiB device array that
+ * every GPU on which the library's module is loaded holds until the process exits;
+ * frames whose decoder working set does not fit are rejected with
+ * CHAIN_ERR_UNSUPPORTED and a message giving the bytes needed.  All calls share that
+ * array and keep the last call's contents (each call clears what must start at zero);
+ * overlapping calls would race on it, so calls are serialised by a process-wide lock
+ * and each returns only after its GPU work has completed.  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress): make it before any stream
+ * capture begins on that device. */
+CHAIN_API chain_status chain_decompress_noalloc(const void* container, size_t len, chain_dtype out_dtype,
+                                                chain_layout out_layout, void* out, size_t out_capacity_bytes,
+                                                uint64_t* n, uint32_t* dims, void* cuda_stream);
+
 /* Debug/parity entry: after chain_compress on this context, copies the encoder's
  * integer streams to host buffers (each may be NULL).  Layout is record-major
  * (point-major) int64, matching the order the reference feeds its entropy stage
