@@ -501,9 +501,11 @@ inline void rans_plan_smem(RansJobs& J, bool decode) {
     J.tab_cap = (tab + 7) & ~7u;
     J.look_cap = (look + 7) & ~7u;
 }
-inline size_t rans_enc_smem(const RansJobs& J) { return J.tab_cap * 16ull + kRansWarps * 2 * kRansTile * 32 * 4; }
+inline size_t rans_enc_smem(const RansJobs& J) {
+    return J.tab_cap * 16ull + kRansWarps * 2 * kRansTile * 32 * 4 + kRansWarps * kWindow;
+}
 inline size_t rans_dec_smem(const RansJobs& J) {
-    return J.tab_cap * 8ull + J.look_cap * 2ull + kRansWarps * kWindow;
+    return J.tab_cap * 8ull + J.look_cap * 2ull + kRansWarps * kWindow + 16;   // +16: 3-byte renorm reads
 }
 
 __device__ __forceinline__ int job_of_block(const RansJobs& J) {
@@ -547,7 +549,11 @@ __device__ __forceinline__ void tile_store(uint32_t* buf, const uint32_t (&r)[32
 // Encoder: one warp per chunk, kRansWarps chunks of one job per CTA.  The job's table
 // sits in shared memory when small; symbols are prefetched one 32-step tile ahead
 // into shared memory; the warp's byte counts are prefix-summed with two ballots
-// (0..3 bytes per lane).
+// (0..3 bytes per lane).  Bytes are written backwards into a kWindow-byte shared-memory
+// window; before each group of kRansTile steps, if fewer than a group's worst case
+// (kRansTile * 96 bytes) are free, the window's 16-byte-aligned written part goes to
+// the chunk's slot in global memory with 16-byte stores and the ragged rest (< 16
+// bytes) moves to the window's top.  Offsets are 32-bit (a chunk slot is < 4 GB).
 static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uint32_t* err) {
     extern __shared__ __align__(16) uint8_t rsm[];
     const RansJob& jb = J.job[job_of_block(J)];
@@ -560,18 +566,24 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
     const uint32_t c = (blockIdx.x - jb.first_block) * kRansWarps + warp;
     if (c >= jb.chunks) return;
     uint32_t* buf = reinterpret_cast<uint32_t*>(rsm + J.tab_cap * 16ull) + warp * 2 * 1024;
+    uint8_t* ow = rsm + J.tab_cap * 16ull + kRansWarps * 2 * kRansTile * 32 * 4 + warp * kWindow;
     const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
     const uint64_t cend = min(cbeg + jb.S, jb.count);
     const uint32_t W = jb.lanes;
-    const uint32_t steps = static_cast<uint32_t>((cend - cbeg + W - 1) / W);
+    const uint32_t cnt = static_cast<uint32_t>(cend - cbeg);
+    const uint32_t steps = (cnt + W - 1) / W;
     const uint32_t ntiles = (steps + kRansTile - 1) / kRansTile;
     const uint64_t tile_syms = static_cast<uint64_t>(kRansTile) * W;
     const uint32_t prec = jb.prec;
     const uint32_t L = 4u << prec;
     const uint32_t lt = lanemask_lt();
+    constexpr uint32_t kGroupBytes = kRansTile * 32 * 3;
     uint32_t x = L;
     uint8_t* out = jb.bytes + static_cast<uint64_t>(c) * jb.slot_cap;
-    uint64_t pos = jb.slot_cap;
+    const bool ovec = (reinterpret_cast<uintptr_t>(out) & 15) == 0 && (jb.slot_cap & 15) == 0;
+    uint32_t pos = static_cast<uint32_t>(jb.slot_cap);   // slot offset of the lowest byte written
+    uint32_t wtop = pos;                                  // slot offset of the window's end
+    uint32_t rel = kWindow;                               // window index of `pos`
     bool overflow = false;
     uint32_t r[32];
     bool vec;
@@ -586,28 +598,41 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
             const uint64_t tb = cbeg + tile_syms * (k - 1);
             tile_load(jb.sym, tb, min(tb + tile_syms, cend), r, vec);
         }
+        if (rel < kGroupBytes) {   // flush the aligned part of the window
+            const uint32_t a = (rel + 15) & ~15u;
+            const int64_t gb = static_cast<int64_t>(wtop) - kWindow;   // window index i <-> slot offset gb + i
+            if (ovec) {
+                for (uint32_t i = a + 16 * lane; i < kWindow; i += 16 * 32)
+                    *reinterpret_cast<uint4*>(out + (gb + i)) = *reinterpret_cast<const uint4*>(ow + i);
+            } else {
+                for (uint32_t i = a + lane; i < kWindow; i += 32) out[gb + i] = ow[i];
+            }
+            const uint32_t h = a - rel;
+            const uint8_t hb = static_cast<uint32_t>(lane) < h ? ow[rel + lane] : 0;
+            __syncwarp();
+            if (static_cast<uint32_t>(lane) < h) ow[kWindow - h + lane] = hb;
+            __syncwarp();
+            wtop -= kWindow - a;
+            rel = kWindow - h;
+        }
         const uint32_t* cur = buf + (k & 1) * 1024;
         const int t_hi = min(static_cast<int>(steps) - 1, 32 * k + 31);
-        for (int t = t_hi; t >= 32 * k; --t) {
-            const uint64_t kk = cbeg + static_cast<uint64_t>(t) * W + lane;
-            const bool act = static_cast<uint32_t>(lane) < W && kk < cend;
-            uint32_t nb = 0;
-            uint4 e = make_uint4(1, 0, 0, 0);
-            if (act) {
-                const uint32_t s = cur[(t - 32 * k) * W + lane];
-                e = smem_tab ? tab[s] : __ldg(jb.etab + s);
-                const uint32_t xmax = e.x << 10;  // ((L >> prec) << 8) * freq
-                nb = (x >= xmax) + ((x >> 8) >= xmax) + ((x >> 16) >= xmax);
-            }
+        uint32_t kl = static_cast<uint32_t>(t_hi) * W + lane;   // symbol index within the chunk
+        for (int t = t_hi; t >= 32 * k; --t, kl -= W) {
+            const bool act = static_cast<uint32_t>(lane) < W && kl < cnt;
+            const uint32_t s = act ? cur[(t - 32 * k) * W + lane] : 0u;
+            const uint4 e = smem_tab ? tab[s] : __ldg(jb.etab + s);
+            const uint32_t xmax = e.x << 10;  // ((L >> prec) << 8) * freq
+            const uint32_t nb = act ? (x >= xmax) + ((x >> 8) >= xmax) + ((x >> 16) >= xmax) : 0u;
             const uint32_t b0 = __ballot_sync(0xffffffffu, nb & 1u), b1 = __ballot_sync(0xffffffffu, nb & 2u);
-            const uint32_t pre = __popc(b0 & lt) + 2 * __popc(b1 & lt);
             const uint32_t total = __popc(b0) + 2 * __popc(b1);
             if (total > pos) { overflow = true; break; }
-            uint8_t* o = out + (pos - total + pre);
-            if (nb == 3) { o[0] = static_cast<uint8_t>(x >> 16); o[1] = static_cast<uint8_t>(x >> 8); o[2] = static_cast<uint8_t>(x); }
-            else if (nb == 2) { o[0] = static_cast<uint8_t>(x >> 8); o[1] = static_cast<uint8_t>(x); }
-            else if (nb == 1) { o[0] = static_cast<uint8_t>(x); }
             pos -= total;
+            rel -= total;
+            uint8_t* o = ow + rel + __popc(b0 & lt) + 2 * __popc(b1 & lt);
+            if (nb > 0) o[nb - 1] = static_cast<uint8_t>(x);
+            if (nb > 1) o[nb - 2] = static_cast<uint8_t>(x >> 8);
+            if (nb > 2) o[0] = static_cast<uint8_t>(x >> 16);
             if (act) {
                 x >>= 8 * nb;
                 const uint32_t q = __umulhi(x, e.z) >> (e.w >> 24);
@@ -623,6 +648,11 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
     if (__any_sync(0xffffffffu, overflow)) {
         if (lane == 0) set_error(err, kErrInternal);
         return;
+    }
+    __syncwarp();
+    {
+        const int64_t gb = static_cast<int64_t>(wtop) - kWindow;
+        for (uint32_t i = rel + lane; i < kWindow; i += 32) out[gb + i] = ow[i];
     }
     if (static_cast<uint32_t>(lane) < W) jb.states[static_cast<uint64_t>(c) * W + lane] = x;
     if (lane == 0) jb.chunk_len[c] = static_cast<uint32_t>(jb.slot_cap - pos);
@@ -648,9 +678,13 @@ __device__ __forceinline__ void window_fill(uint8_t* win, const uint8_t* bytes, 
 
 // Decoder: one warp per chunk, kRansWarps chunks of one job per CTA.  The slot->symbol
 // lookup and prob/cum live in shared memory when small; the chunk's byte stream is read
-// through a 4 KB shared-memory window refilled every 32 steps (a step consumes at most
-// 96 bytes).  Every read is bounds-checked against the chunk's byte range; a malformed
-// stream sets kErrCorrupt and the warp stops.
+// through a kWindow-byte shared-memory window, refilled before each group of kRansTile
+// steps whenever fewer than kRansTile * 96 bytes (the most a group can consume) remain
+// in it.  Offsets inside the group are 32-bit and relative to the window; each lane
+// renormalises by reading 3 bytes unconditionally and shifting in the nb it needs.
+// Every step checks the warp's byte total against the chunk's end; a malformed stream
+// (state out of range, overrun, or a final state or position that does not match) sets
+// kErrCorrupt, checked once per group.
 static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uint32_t* err) {
     extern __shared__ __align__(16) uint8_t rsm[];
     __shared__ int s_skip;
@@ -676,8 +710,10 @@ static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uin
     const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
     const uint64_t cend = min(cbeg + jb.S, jb.count);
     const uint32_t W = jb.lanes;
-    const uint32_t steps = static_cast<uint32_t>((cend - cbeg + W - 1) / W);
+    const uint32_t cnt = static_cast<uint32_t>(cend - cbeg);   // symbols of this chunk (S < 2^32)
+    const uint32_t steps = (cnt + W - 1) / W;
     const uint32_t lt = lanemask_lt();
+    uint32_t* outc = jb.out + cbeg;
     uint64_t pos = jb.chunk_off[c];
     const uint64_t end = jb.chunk_off[c + 1];
     uint32_t x = static_cast<uint32_t>(lane) < W ? jb.states[static_cast<uint64_t>(c) * W + lane] : L;
@@ -687,45 +723,55 @@ static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uin
         if (lane == 0) set_error(err, kErrCorrupt);
         return;
     }
+    constexpr uint32_t kGroupBytes = kRansTile * 32 * 3;   // most bytes one group of steps consumes
+    static_assert(kWindow >= kGroupBytes + 16, "window must hold a group's bytes after a refill");
     uint64_t wbase = pos & ~15ull;
+    uint32_t rel = static_cast<uint32_t>(pos - wbase);
+    uint32_t rel_end = static_cast<uint32_t>(min(end - wbase, static_cast<uint64_t>(1u << 30)));
     window_fill(win, jb.bytes, jb.bytes_len, wbase);
-    for (uint32_t t = 0; t < steps; ++t) {
-        if ((t & (kRansTile - 1)) == 0 && pos - wbase > kWindow - 3 * 1024) {
+    bool overrun = false;
+    uint32_t k = static_cast<uint32_t>(lane);   // symbol index within the chunk: t * W + lane
+    for (uint32_t t0 = 0; t0 < steps && !overrun; t0 += kRansTile) {
+        if (rel > kWindow - kGroupBytes) {
             __syncwarp();
-            wbase = pos & ~15ull;
+            const uint64_t p = wbase + rel;
+            wbase = p & ~15ull;
+            rel = static_cast<uint32_t>(p - wbase);
+            rel_end = static_cast<uint32_t>(min(end - wbase, static_cast<uint64_t>(1u << 30)));
             window_fill(win, jb.bytes, jb.bytes_len, wbase);
         }
-        const uint64_t k = cbeg + static_cast<uint64_t>(t) * W + lane;
-        const bool act = static_cast<uint32_t>(lane) < W && k < cend;
-        uint32_t nb = 0;
-        if (act) {
+        const uint32_t tn = min(static_cast<uint32_t>(kRansTile), steps - t0);
+        for (uint32_t t = 0; t < tn; ++t, k += W) {
+            const bool act = static_cast<uint32_t>(lane) < W && k < cnt;
             const uint32_t slot = x & (M - 1);
-            uint32_t s;
+            uint32_t s, xn;
             if (smem_look) {
                 s = look[slot];
                 uint32_t f, cm;
                 if (smem_tab) { const uint2 e = tab[s]; f = e.x; cm = e.y; }
                 else { f = __ldg(jb.prob + s); cm = __ldg(jb.cum + s); }
-                x = f * (x >> prec) + slot - cm;
+                xn = f * (x >> prec) + slot - cm;
             } else {
                 const uint64_t e = __ldg(jb.slots + slot);
                 s = static_cast<uint32_t>(e & 0x3ffffu);
-                x = static_cast<uint32_t>((e >> 18) & 0x1fffffu) * (x >> prec) + static_cast<uint32_t>(e >> 39);
+                xn = static_cast<uint32_t>((e >> 18) & 0x1fffffu) * (x >> prec) + static_cast<uint32_t>(e >> 39);
             }
-            jb.out[k] = s;
-            nb = (x < L) + (x < (L >> 8)) + (x < (L >> 16));
+            if (act) outc[k] = s;
+            x = act ? xn : x;
+            const uint32_t nb = act ? (x < L) + (x < (L >> 8)) + (x < (L >> 16)) : 0u;
+            const uint32_t b0 = __ballot_sync(0xffffffffu, nb & 1u), b1 = __ballot_sync(0xffffffffu, nb & 2u);
+            const uint32_t total = __popc(b0) + 2 * __popc(b1);
+            if (rel + total > rel_end) { overrun = true; break; }
+            const uint32_t wo = rel + __popc(b0 & lt) + 2 * __popc(b1 & lt);
+            const uint32_t v = (static_cast<uint32_t>(win[wo]) << 16) | (static_cast<uint32_t>(win[wo + 1]) << 8) |
+                               static_cast<uint32_t>(win[wo + 2]);
+            x = static_cast<uint32_t>(((static_cast<uint64_t>(x) << 24) | v) >> (24 - 8 * nb));
+            bad = bad || (act && x < L);
+            rel += total;
         }
-        const uint32_t b0 = __ballot_sync(0xffffffffu, nb & 1u), b1 = __ballot_sync(0xffffffffu, nb & 2u);
-        const uint32_t pre = __popc(b0 & lt) + 2 * __popc(b1 & lt);
-        const uint32_t total = __popc(b0) + 2 * __popc(b1);
-        if (pos + total > end) { bad = true; break; }
-        const uint32_t wo = static_cast<uint32_t>(pos - wbase) + pre;
-        for (uint32_t j = 0; j < nb; ++j) x = (x << 8) | win[wo + j];
-        if (act && x < L) bad = true;
-        pos += total;
         if (__any_sync(0xffffffffu, bad)) break;
     }
-    bad = bad || (x != L) || (pos != end);
+    bad = bad || overrun || (x != L) || (wbase + rel != end);
     if (__any_sync(0xffffffffu, bad) && lane == 0) set_error(err, kErrCorrupt);
 }
 
