@@ -133,21 +133,47 @@ __device__ __forceinline__ uint64_t read_bits_msb(const uint8_t* bytes, uint64_t
     return width == 64 ? acc : (acc & ((1ull << width) - 1));
 }
 
-// Fixed: one thread per value.
-__global__ void __launch_bounds__(256) k_unpack_fixed(const uint8_t* data, const CompPlan* cp, uint32_t* out,
-                                                       DecState* st) {
-    const CompPlan& c = *cp;
-    const uint64_t n = c.records * c.dims;
-    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
-         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t k = j / c.dims;
-        const uint32_t d = static_cast<uint32_t>(j - k * c.dims);
-        const int w = c.width[d];
-        const uint64_t off = w ? read_bits_msb(data + c.packed_off[d], k * w, w) : 0;
-        const uint64_t v = c.minv[d] + off;
-        if (v > 0xffffffffull) { set_error(&st->err, kErrCorrupt); continue; }
-        out[j] = static_cast<uint32_t>(v);
+// Fixed: one thread per record, all dimensions.  Each value is cut from two big-endian
+// 32-bit words of the container when it is 4-byte aligned (and the words lie inside it),
+// else read bytewise.
+__global__ void __launch_bounds__(256) k_unpack_fixed(const uint8_t* data, uint64_t len, const CompPlan* cp,
+                                                       uint32_t* out, DecState* st) {
+    __shared__ uint64_t s_bit[kMaxDims], s_min[kMaxDims];
+    __shared__ uint32_t s_w[kMaxDims];
+    const uint32_t D = cp->dims;
+    const uint64_t R = cp->records;
+    if (threadIdx.x < D) {
+        s_bit[threadIdx.x] = cp->packed_off[threadIdx.x] * 8;
+        s_min[threadIdx.x] = cp->minv[threadIdx.x];
+        s_w[threadIdx.x] = cp->width[threadIdx.x];
     }
+    __syncthreads();
+    const bool words = (reinterpret_cast<uintptr_t>(data) & 3) == 0;
+    const uint32_t* dw = reinterpret_cast<const uint32_t*>(data);
+    const uint64_t nwords = len / 4;
+    bool bad = false;
+    for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < R;
+         r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        for (uint32_t d = 0; d < D; ++d) {
+            const uint32_t w = s_w[d];
+            uint64_t val = 0;
+            if (w) {
+                const uint64_t b = s_bit[d] + r * w;
+                const uint64_t i = b >> 5;
+                if (words && i + 1 < nwords) {
+                    const uint64_t hi = __byte_perm(__ldg(dw + i), 0, 0x0123);
+                    const uint64_t lo = __byte_perm(__ldg(dw + i + 1), 0, 0x0123);
+                    val = (((hi << 32) | lo) << (b & 31)) >> (64 - w);
+                } else {
+                    val = read_bits_msb(data, b, static_cast<int>(w));
+                }
+            }
+            const uint64_t v = s_min[d] + val;
+            bad = bad || v > 0xffffffffull;
+            out[r * D + d] = static_cast<uint32_t>(v);
+        }
+    }
+    if (bad) set_error(&st->err, kErrCorrupt);
 }
 
 struct TagIn {
@@ -594,7 +620,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         const CompPlan& c = plan.comp[s];
         const CompPlan* dc = &st->plan.comp[s];
         if (c.enc == kEncFixed) {
-            k_unpack_fixed<<<dgrid(c.records * c.dims), 256, 0, stream>>>(dcont, dc, streams[s], st); count_launch();
+            k_unpack_fixed<<<dgrid(c.records), 256, 0, stream>>>(dcont, len, dc, streams[s], st); count_launch();
         } else if (c.enc == kEncTagged) {
             uint32_t* tg = tags + tag_off[s];
             device_exclusive_scan<uint64_t>(TagIn{tg, c.dims},

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 #include <vector>
 
 #include "chain_common.cuh"
@@ -115,35 +116,63 @@ __device__ __forceinline__ double load_coord(const FT* p, uint64_t n, uint32_t D
     return static_cast<double>(SOA ? p[static_cast<uint64_t>(d) * n + i] : p[i * D + d]);
 }
 
+// Per-axis extrema (as ordered bits of the double value), the first index of -0.0 and
+// of +0.0, and a non-finite flag.  blockIdx.y is the axis.  Values are compared in their
+// own type (float -> double is exact and order-preserving; the sign of a zero minimum
+// is settled by the first-zero indices).  A contiguous axis (SoA) is read with 16-byte
+// loads, two per thread in flight.
 template <typename FT, bool SOA>
 __global__ void __launch_bounds__(256) k_minmax(const FT* __restrict__ p, uint64_t n, uint32_t D, EncState* st) {
     const uint32_t d = blockIdx.y;
-    uint64_t mn = ~0ull, mx = 0, zneg = ~0ull, zpos = ~0ull;
+    FT mn = static_cast<FT>(INFINITY), mx = static_cast<FT>(-INFINITY);
+    uint64_t zneg = ~0ull, zpos = ~0ull;
     bool bad = false;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const double x = load_coord<FT, SOA>(p, n, D, i, d);
-        if (!chain_isfinite(x)) { bad = true; continue; }
-        const uint64_t o = ordered_bits(x);
-        mn = o < mn ? o : mn;
-        mx = o > mx ? o : mx;
-        if (x == 0.0) {
+    auto visit = [&](FT x, uint64_t i) {
+        bad = bad || !chain_isfinite(static_cast<double>(x));
+        mn = x < mn ? x : mn;
+        mx = x > mx ? x : mx;
+        if (x == static_cast<FT>(0)) {
             if (signbit(x)) zneg = i < zneg ? i : zneg;
             else zpos = i < zpos ? i : zpos;
         }
+    };
+    const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    constexpr int V = 16 / sizeof(FT);
+    const FT* q = SOA ? p + static_cast<uint64_t>(d) * n : p;
+    if (SOA && (reinterpret_cast<uintptr_t>(q) & 15) == 0) {
+        using Vec = typename std::conditional<sizeof(FT) == 4, float4, double2>::type;
+        const Vec* qv = reinterpret_cast<const Vec*>(q);
+        const uint64_t nv = n / V;
+        for (uint64_t g = tid; g < nv; g += 2 * nthreads) {
+            FT a[V], b[V];
+            const bool two = g + nthreads < nv;
+            *reinterpret_cast<Vec*>(a) = __ldg(qv + g);
+            if (two) *reinterpret_cast<Vec*>(b) = __ldg(qv + g + nthreads);
+#pragma unroll
+            for (int k = 0; k < V; ++k) visit(a[k], g * V + k);
+            if (two) {
+#pragma unroll
+                for (int k = 0; k < V; ++k) visit(b[k], (g + nthreads) * V + k);
+            }
+        }
+        for (uint64_t i = nv * V + tid; i < n; i += nthreads) visit(q[i], i);
+    } else {
+        for (uint64_t i = tid; i < n; i += nthreads) visit(SOA ? q[i] : p[i * D + d], i);
     }
-    mn = warp_min(mn); mx = warp_max(mx); zneg = warp_min(zneg); zpos = warp_min(zpos);
+    uint64_t omn = ordered_bits(static_cast<double>(mn)), omx = ordered_bits(static_cast<double>(mx));
+    omn = warp_min(omn); omx = warp_max(omx); zneg = warp_min(zneg); zpos = warp_min(zpos);
     __shared__ uint64_t s[4][8];
     const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) { s[0][w] = mn; s[1][w] = mx; s[2][w] = zneg; s[3][w] = zpos; }
+    if ((threadIdx.x & 31) == 0) { s[0][w] = omn; s[1][w] = omx; s[2][w] = zneg; s[3][w] = zpos; }
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int k = 1; k < static_cast<int>(blockDim.x >> 5); ++k) {
-            mn = s[0][k] < mn ? s[0][k] : mn; mx = s[1][k] > mx ? s[1][k] : mx;
+            omn = s[0][k] < omn ? s[0][k] : omn; omx = s[1][k] > omx ? s[1][k] : omx;
             zneg = s[2][k] < zneg ? s[2][k] : zneg; zpos = s[3][k] < zpos ? s[3][k] : zpos;
         }
-        atomicMin(reinterpret_cast<unsigned long long*>(&st->minbits[d]), mn);
-        atomicMax(reinterpret_cast<unsigned long long*>(&st->maxbits[d]), mx);
+        atomicMin(reinterpret_cast<unsigned long long*>(&st->minbits[d]), omn);
+        atomicMax(reinterpret_cast<unsigned long long*>(&st->maxbits[d]), omx);
         if (zneg != ~0ull) atomicMin(reinterpret_cast<unsigned long long*>(&st->zero_first[d][0]), zneg);
         if (zpos != ~0ull) atomicMin(reinterpret_cast<unsigned long long*>(&st->zero_first[d][1]), zpos);
     }
@@ -191,24 +220,54 @@ __device__ __forceinline__ bool within_error_bound(double restored, double origi
     return difference >= 0.0 ? remainder <= 0.0 : remainder >= 0.0;
 }
 
-template <typename FT, bool SOA, typename KT>
+// Block index b = q / p and rel = q - b*p for q < 2^31: a shift and a mask when p is a
+// power of two, else a double-precision reciprocal estimate corrected to the exact
+// quotient (the estimate is off by at most one).
+struct BlockDiv {
+    uint64_t p;
+    double inv;
+    int shift;   // >= 0: p == 2^shift
+    __device__ __forceinline__ uint32_t div(uint32_t q) const {
+        if (shift >= 0) return shift >= 32 ? 0u : q >> shift;
+        if (p > 0xffffffffull) return 0u;
+        uint32_t b = static_cast<uint32_t>(static_cast<double>(q) * inv);
+        const uint64_t t = static_cast<uint64_t>(b) * p;
+        if (t > q) --b;
+        else if (t + p <= q) ++b;
+        return b;
+    }
+};
+
+// Quantization of every point (lcps_cpp.cpp:2060-2110): q = floor((x - min) / (2 eb)) in
+// IEEE double, the reconstruction fma(q + 0.5, 2 eb, min) checked against eb (values
+// outside go to the exact-correction list), the block index and the offset inside the
+// block, and the point's Z-order block key.  DIM is the dimension count (0 = run time).
+template <typename FT, bool SOA, typename KT, int DIM>
 __global__ void __launch_bounds__(256)
-k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D, EncState* st, KT* __restrict__ key_out,
+k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT* __restrict__ key_out,
            uint32_t* __restrict__ rel_out, uint64_t* __restrict__ corr_idx, double* __restrict__ corr_val,
            uint64_t corr_cap) {
     __shared__ double s_min[kMaxDims];
-    __shared__ double s_eb, s_denom;
+    __shared__ double s_eb;
     __shared__ uint64_t s_p;
     __shared__ int s_kb;
+    const uint32_t D = DIM ? DIM : D_rt;
     if (threadIdx.x < D) s_min[threadIdx.x] = st->mins[threadIdx.x];
-    if (threadIdx.x == 0) { s_eb = st->eb; s_denom = 2.0 * st->eb; s_p = st->p; s_kb = st->kb; }
+    if (threadIdx.x == 0) { s_eb = st->eb; s_p = st->p; s_kb = st->kb; }
     __syncthreads();
-    const double eb = s_eb, denom = s_denom, two_eb = 2.0 * s_eb;
-    const uint64_t pp = s_p;
+    const double eb = s_eb, denom = 2.0 * s_eb, two_eb = 2.0 * s_eb;
+    BlockDiv bd;
+    bd.p = s_p;
+    bd.inv = 1.0 / static_cast<double>(s_p);
+    bd.shift = (s_p & (s_p - 1)) == 0 ? bitlen64(s_p) - 1 : -1;
+    const int kb = s_kb;
+    constexpr int KD = DIM ? DIM : kMaxDims;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint32_t b[kMaxDims];
-        for (uint32_t d = 0; d < D; ++d) {
+        uint32_t b[KD];
+#pragma unroll
+        for (int d = 0; d < KD; ++d) {
+            if (!DIM && d >= static_cast<int>(D)) break;
             const double x = load_coord<FT, SOA>(p, n, D, i, d);
             const double qv = floor(__ddiv_rn(__dsub_rn(x, s_min[d]), denom));
             const uint32_t q = static_cast<uint32_t>(qv);
@@ -220,11 +279,11 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D, EncState* st, KT* _
                     corr_val[slot] = x;
                 }
             }
-            const uint32_t bb = static_cast<uint32_t>(static_cast<uint64_t>(q) / pp);
+            const uint32_t bb = bd.div(q);
             b[d] = bb;
-            rel_out[i * D + d] = static_cast<uint32_t>(q - static_cast<uint64_t>(bb) * pp);
+            rel_out[i * D + d] = static_cast<uint32_t>(q - static_cast<uint64_t>(bb) * bd.p);
         }
-        key_out[i] = static_cast<KT>(block_key(b, static_cast<int>(D), s_kb));
+        key_out[i] = static_cast<KT>(block_key(b, static_cast<int>(D), kb));
     }
 }
 
@@ -723,26 +782,54 @@ struct TagPackOut {
     }
 };
 
-// Fixed-width packing of one dimension: one thread per output 32-bit word.
-__global__ void __launch_bounds__(256) k_pack_fixed(const uint32_t* __restrict__ data, uint32_t D, uint32_t d,
-                                                     uint64_t nrec, uint32_t minv, int width,
-                                                     uint32_t* __restrict__ words, uint64_t nwords) {
-    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < nwords;
-         w += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t b0 = w * 32, b1 = b0 + 32;
-        uint64_t first = b0 / width;
-        uint64_t last = (b1 - 1) / width;
-        if (last >= nrec) last = nrec - 1;
-        uint32_t acc = 0;
-        for (uint64_t k = first; k <= last; ++k) {
-            const uint64_t v = static_cast<uint64_t>(data[k * D + d] - minv);
-            const int64_t start = static_cast<int64_t>(k * width) - static_cast<int64_t>(b0);  // bit pos in word
-            // value occupies [start, start + width) relative to word start (MSB = bit 0)
-            const int64_t shift = 32 - (start + width);
-            if (shift >= 0) acc |= static_cast<uint32_t>(v << shift);
-            else acc |= static_cast<uint32_t>(v >> (-shift));
+// Fixed-width packing of every dimension of one stream.  Per dimension d, value k takes
+// bits [k*w, (k+1)*w) of an MSB-first bit stream (w = width[d] <= 32), written as
+// big-endian 32-bit words so that byte 0 holds the first 8 bits.  Each warp packs a tile
+// of 1024 records: it stages the tile's values of dimension d in shared memory
+// (coalesced reads), then lane l packs records [32l, 32l+32) into exactly w words.
+struct FixedPack {
+    uint32_t* words[kMaxDims];   // per-dimension output (nwords[d] words)
+    uint64_t nwords[kMaxDims];
+    uint32_t minv[kMaxDims];
+    uint32_t width[kMaxDims];
+};
+constexpr int kPackWarps = 8;
+__global__ void __launch_bounds__(32 * kPackWarps) k_pack_fixed(const uint32_t* __restrict__ data, uint32_t D,
+                                                                 uint64_t nrec, FixedPack fp) {
+    __shared__ uint32_t stage[kPackWarps][33 * 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t* sw = stage[warp];
+    const uint64_t ntiles = (nrec + 1023) / 1024;
+    for (uint64_t tile = static_cast<uint64_t>(blockIdx.x) * kPackWarps + warp; tile < ntiles;
+         tile += static_cast<uint64_t>(gridDim.x) * kPackWarps) {
+        const uint64_t r0 = tile * 1024;
+        for (uint32_t d = 0; d < D; ++d) {
+            const uint32_t w = fp.width[d];
+            if (w == 0) continue;
+            const uint32_t mv = fp.minv[d];
+#pragma unroll 8
+            for (int j = 0; j < 32; ++j) {
+                const uint64_t k = r0 + 32 * j + lane;
+                sw[33 * j + lane] = k < nrec ? __ldg(data + k * D + d) - mv : 0u;
+            }
+            __syncwarp();
+            uint64_t acc = 0;
+            uint32_t nacc = 0, m = 0;
+            uint32_t* out = fp.words[d];
+            const uint64_t wbase = (r0 / 32 + lane) * w;
+            const uint64_t nw = fp.nwords[d];
+#pragma unroll 4
+            for (int j = 0; j < 32; ++j) {
+                acc = (acc << w) | sw[33 * lane + j];
+                nacc += w;
+                if (nacc >= 32) {
+                    nacc -= 32;
+                    if (wbase + m < nw) out[wbase + m] = __byte_perm(static_cast<uint32_t>(acc >> nacc), 0, 0x0123);
+                    ++m;
+                }
+            }
+            __syncwarp();
         }
-        words[w] = acc;
     }
 }
 
@@ -935,6 +1022,39 @@ __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* piece
     if (np > max_pieces) set_error(&st->err, kErrInternal);
 }
 
+// Copies len bytes with the CTA: head bytes up to a 16-byte-aligned destination, then
+// 16-byte stores, each assembled from aligned 4-byte source words with funnel shifts
+// (any source alignment), then tail bytes.  Source words are read only where they hold
+// at least one byte of the range.
+__device__ __forceinline__ void block_copy(uint8_t* dst, const uint8_t* src, uint32_t len) {
+    const uint32_t head = min(len, static_cast<uint32_t>((16 - (reinterpret_cast<uintptr_t>(dst) & 15)) & 15));
+    if (threadIdx.x < head) dst[threadIdx.x] = src[threadIdx.x];
+    const uint32_t body = (len - head) & ~15u;
+    const uint8_t* s = src + head;
+    uint8_t* d = dst + head;
+    const uint32_t o = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(s) & 3);
+    if (o == 0 && (reinterpret_cast<uintptr_t>(s) & 15) == 0) {
+        for (uint32_t i = 16 * threadIdx.x; i < body; i += 16 * blockDim.x)
+            *reinterpret_cast<uint4*>(d + i) = *reinterpret_cast<const uint4*>(s + i);
+    } else if (o == 0) {
+        for (uint32_t i = 16 * threadIdx.x; i < body; i += 16 * blockDim.x) {
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(s + i);
+            *reinterpret_cast<uint4*>(d + i) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    } else {
+        const uint32_t* sa = reinterpret_cast<const uint32_t*>(s - o);   // aligned word holding s[0]
+        const uint32_t sh = 8 * o;
+        for (uint32_t i = 16 * threadIdx.x; i < body; i += 16 * blockDim.x) {
+            const uint32_t* w = sa + i / 4;
+            // bytes s[i .. i+16) lie in words w[0..4]; w[4] holds s[i+16-o .. ], needed since o > 0
+            const uint32_t w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3], w4 = w[4];
+            *reinterpret_cast<uint4*>(d + i) = make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh),
+                                                          __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh));
+        }
+    }
+    for (uint32_t i = head + body + threadIdx.x; i < len; i += blockDim.x) dst[i] = src[i];
+}
+
 // One CTA per 4 KB segment; the piece of a segment is found by binary search, and for
 // a chunked piece the chunk by a second binary search over its segment prefix.
 __global__ void __launch_bounds__(256) k_copy_pieces(const Piece* pieces, ChunkMaps maps, const EncState* st,
@@ -970,7 +1090,7 @@ __global__ void __launch_bounds__(256) k_copy_pieces(const Piece* pieces, ChunkM
             dst = out + pc.dst + M.off[a] + off;
             len = min(kCopySeg, clen - off);
         }
-        for (uint64_t b = threadIdx.x; b < len; b += blockDim.x) dst[b] = src[b];
+        block_copy(dst, src, static_cast<uint32_t>(len));
     }
 }
 
@@ -1085,8 +1205,13 @@ static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, u
 template <typename FT, bool SOA, typename KT>
 static void launch_quantize(const void* pts, uint64_t n, uint32_t D, EncState* st, void* key, uint32_t* rel,
                             uint64_t* cidx, double* cval, uint64_t cap, cudaStream_t s) {
-    k_quantize<FT, SOA, KT><<<grid_for(n), 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st,
-                                                         static_cast<KT*>(key), rel, cidx, cval, cap); count_launch();
+    if (D == 3)
+        k_quantize<FT, SOA, KT, 3><<<grid_for(n), 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st,
+                                                                static_cast<KT*>(key), rel, cidx, cval, cap);
+    else
+        k_quantize<FT, SOA, KT, 0><<<grid_for(n), 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st,
+                                                                static_cast<KT*>(key), rel, cidx, cval, cap);
+    count_launch();
 }
 
 template <typename FT, bool SOA>
@@ -1365,13 +1490,16 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         const StreamChoice& c = hs->ch[s];
         const StreamRef& r = refs.s[s];
         if (c.enc == kEncFixed) {
+            FixedPack fp{};
             for (uint32_t d = 0; d < c.dims; ++d) {
-                const uint64_t nwords = (c.records * c.width[d] + 31) / 32;
-                uint32_t* words = reinterpret_cast<uint32_t*>(packed + packed_off[s] + packed_stride[s] * d);
-                k_pack_fixed<<<grid_for(nwords), 256, 0, stream>>>(r.data, c.dims, d, c.records,
-                                                                     hs->st[s].minv[d], c.width[d], words, nwords); count_launch();
-                k_words_to_bytes<<<grid_for(nwords), 256, 0, stream>>>(words, nwords); count_launch();
+                fp.words[d] = reinterpret_cast<uint32_t*>(packed + packed_off[s] + packed_stride[s] * d);
+                fp.nwords[d] = (c.records * c.width[d] + 31) / 32;
+                fp.minv[d] = hs->st[s].minv[d];
+                fp.width[d] = c.width[d];
             }
+            const uint64_t tiles = (c.records + 1023) / 1024;
+            k_pack_fixed<<<grid_for(tiles, kPackWarps, 148u * 16u), 32 * kPackWarps, 0, stream>>>(r.data, c.dims,
+                                                                                                 c.records, fp); count_launch();
             ain.packed[s] = packed + packed_off[s];
             ain.packed_dim_stride[s] = packed_stride[s];
         }
