@@ -133,45 +133,87 @@ __device__ __forceinline__ uint64_t read_bits_msb(const uint8_t* bytes, uint64_t
     return width == 64 ? acc : (acc & ((1ull << width) - 1));
 }
 
-// Fixed: one thread per record, all dimensions.  Each value is cut from two big-endian
-// 32-bit words of the container when it is 4-byte aligned (and the words lie inside it),
-// else read bytewise.
-__global__ void __launch_bounds__(256) k_unpack_fixed(const uint8_t* data, uint64_t len, const CompPlan* cp,
-                                                       uint32_t* out, DecState* st) {
-    __shared__ uint64_t s_bit[kMaxDims], s_min[kMaxDims];
-    __shared__ uint32_t s_w[kMaxDims];
+// Big-endian 32-bit word at byte offset off of the container (bytes past len read as 0).
+__device__ __forceinline__ uint32_t load_be32(const uint8_t* data, uint64_t len, uint64_t off) {
+    if (off + 4 <= len && (reinterpret_cast<uintptr_t>(data + off) & 3) == 0)
+        return __byte_perm(__ldg(reinterpret_cast<const uint32_t*>(data + off)), 0, 0x0123);
+    uint32_t v = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v = (v << 8) | (off + k < len ? static_cast<uint32_t>(data[off + k]) : 0u);
+    return v;
+}
+
+// Fixed: one warp per tile of 32*G records.  For dimension d (width w) a group of 32
+// records fills exactly w 32-bit words of that dimension's MSB-first bit stream, so the
+// tile's words of every dimension (G * sum w <= 512) are loaded at once into shared
+// memory; each lane then cuts its records' values out of them.  Values pass through
+// shared memory (32*G*D <= 512) so that the tile's outputs are stored contiguously.
+constexpr int kUnpackWarps = 8;
+constexpr uint32_t kUnpackWords = 512;
+__global__ void __launch_bounds__(32 * kUnpackWarps) k_unpack_fixed(const uint8_t* data, uint64_t len,
+                                                                     const CompPlan* cp, uint32_t* out,
+                                                                     DecState* st, uint32_t G) {
+    __shared__ uint64_t s_byte[kMaxDims], s_min[kMaxDims];
+    __shared__ uint32_t s_w[kMaxDims], s_pre[kMaxDims + 1];
+    __shared__ __align__(16) uint32_t wbuf[kUnpackWarps][kUnpackWords];
+    __shared__ __align__(16) uint32_t stage[kUnpackWarps][kUnpackWords];
     const uint32_t D = cp->dims;
     const uint64_t R = cp->records;
     if (threadIdx.x < D) {
-        s_bit[threadIdx.x] = cp->packed_off[threadIdx.x] * 8;
+        s_byte[threadIdx.x] = cp->packed_off[threadIdx.x];
         s_min[threadIdx.x] = cp->minv[threadIdx.x];
         s_w[threadIdx.x] = cp->width[threadIdx.x];
     }
     __syncthreads();
-    const bool words = (reinterpret_cast<uintptr_t>(data) & 3) == 0;
-    const uint32_t* dw = reinterpret_cast<const uint32_t*>(data);
-    const uint64_t nwords = len / 4;
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (uint32_t d = 0; d < D; ++d) { s_pre[d] = acc; acc += G * s_w[d]; }
+        s_pre[D] = acc;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t* wb = wbuf[warp];
+    uint32_t* sg = stage[warp];
+    const uint32_t TR = 32 * G;
+    const uint64_t ntiles = (R + TR - 1) / TR;
     bool bad = false;
-    for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < R;
-         r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    for (uint64_t tile = static_cast<uint64_t>(blockIdx.x) * kUnpackWarps + warp; tile < ntiles;
+         tile += static_cast<uint64_t>(gridDim.x) * kUnpackWarps) {
+        const uint64_t r0 = tile * TR;
+        const uint32_t nr = static_cast<uint32_t>(min(static_cast<uint64_t>(TR), R - r0));
         for (uint32_t d = 0; d < D; ++d) {
-            const uint32_t w = s_w[d];
-            uint64_t val = 0;
-            if (w) {
-                const uint64_t b = s_bit[d] + r * w;
-                const uint64_t i = b >> 5;
-                if (words && i + 1 < nwords) {
-                    const uint64_t hi = __byte_perm(__ldg(dw + i), 0, 0x0123);
-                    const uint64_t lo = __byte_perm(__ldg(dw + i + 1), 0, 0x0123);
-                    val = (((hi << 32) | lo) << (b & 31)) >> (64 - w);
-                } else {
-                    val = read_bits_msb(data, b, static_cast<int>(w));
-                }
-            }
-            const uint64_t v = s_min[d] + val;
-            bad = bad || v > 0xffffffffull;
-            out[r * D + d] = static_cast<uint32_t>(v);
+            const uint32_t nw = G * s_w[d];
+            const uint64_t base = s_byte[d] + 4 * tile * nw;
+            for (uint32_t j = lane; j < nw; j += 32) wb[s_pre[d] + j] = load_be32(data, len, base + 4 * j);
         }
+        __syncwarp();
+        for (uint32_t g = 0; g < G; ++g) {
+            const uint32_t rec = g * 32 + lane;
+            for (uint32_t d = 0; d < D; ++d) {
+                const uint32_t w = s_w[d];
+                uint32_t val = 0;
+                if (w) {
+                    const uint32_t bit = rec * w, j = bit >> 5, o = bit & 31;
+                    const uint32_t hi = wb[s_pre[d] + j];
+                    const uint32_t lo = j + 1 < G * w ? wb[s_pre[d] + j + 1] : 0u;
+                    val = static_cast<uint32_t>((((static_cast<uint64_t>(hi) << 32) | lo) << o) >> (64 - w));
+                }
+                const uint64_t v = s_min[d] + val;
+                bad = bad || (rec < nr && v > 0xffffffffull);
+                sg[rec * D + d] = static_cast<uint32_t>(v);
+            }
+        }
+        __syncwarp();
+        uint32_t* o = out + r0 * D;
+        const uint32_t nv = nr * D;
+        if ((reinterpret_cast<uintptr_t>(o) & 15) == 0) {
+            for (uint32_t m = 4 * lane; m + 4 <= nv; m += 128)
+                *reinterpret_cast<uint4*>(o + m) = *reinterpret_cast<const uint4*>(sg + m);
+            for (uint32_t m = (nv & ~3u) + lane; m < nv; m += 32) o[m] = sg[m];
+        } else {
+            for (uint32_t m = lane; m < nv; m += 32) o[m] = sg[m];
+        }
+        __syncwarp();
     }
     if (bad) set_error(&st->err, kErrCorrupt);
 }
@@ -328,37 +370,70 @@ struct ZeroIn {
 constexpr uint32_t kResolved = 0x80000000u;
 constexpr uint32_t kParentMask = 0x7fffffffu;
 
-// Ranks of the explicit points; parents (explicit points are resolved roots pointing to
-// themselves); and the list of chained points, whose rank among chained points is
-// i - (explicit points before i).
+// Parents of all points and the list of chained points.  An explicit point is a
+// resolved root whose word holds its rank among explicit points (its block's record in
+// the compact level-2 output); a chained point i points at i + idrel[i], and its rank
+// among chained points is i - (explicit points before i).
 struct ZeroRankOut {
     const uint32_t* idrel;
     uint32_t* parent;
-    uint32_t* zrank;
     uint32_t* chained;
     DecState* st;
     uint64_t n;
     __device__ void operator()(uint64_t i, uint32_t pre, uint32_t z) const {
-        zrank[i] = pre;
         const uint32_t j = idrel[i];
-        if (z) { parent[i] = static_cast<uint32_t>(i) | kResolved; return; }
+        if (z) { parent[i] = pre | kResolved; return; }
         chained[i - pre] = static_cast<uint32_t>(i);
         if (static_cast<uint64_t>(j) >= n - i) {
             set_error(&st->err, kErrCorrupt);
-            parent[i] = static_cast<uint32_t>(i) | kResolved;
+            parent[i] = kResolved;
             return;
         }
         parent[i] = static_cast<uint32_t>(i + j);
     }
 };
 
+// One pass of concurrent pointer jumping over the chained points, highest index first:
+// a point repeatedly replaces its parent word by its parent's current word (which that
+// parent's own thread keeps advancing the same way), so pointers double while threads
+// run side by side, and points reached later (lower indices; parents point forward)
+// mostly find resolved parents.  Warps claim 32 points at a time from *next (zero at
+// launch), so the pass follows descending index order however the CTAs are scheduled.
+// Every word written is an ancestor of the point, so any interleaving is correct.  A
+// point stops after kResolveHops hops; any point left unresolved sets *pending, and the
+// k_jump rounds finish the work.
+constexpr int kResolveHops = 64;
+__global__ void __launch_bounds__(256) k_resolve(uint32_t* parent, const uint32_t* chained, const uint32_t* zeros,
+                                                  uint64_t n, unsigned long long* next, uint32_t* pending) {
+    const uint64_t m = n - *zeros;
+    const int lane = threadIdx.x & 31;
+    bool left = false;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(next, 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= m) break;
+        const uint64_t t = base + lane;
+        if (t < m) {
+            const uint32_t i = chained[m - 1 - t];
+            uint32_t p = parent[i];
+            for (int h = 0; h < kResolveHops && !(p & kResolved); ++h) {
+                p = parent[p];
+                parent[i] = p;
+            }
+            left = left || !(p & kResolved);
+        }
+    }
+    if (__syncthreads_or(left) && threadIdx.x == 0) atomicOr(pending, 1u);
+}
+
 // One pointer-jumping round over the chained points: an unresolved point takes its
-// parent's parent word (and with it the resolved bit).  pending[r] records whether
-// any point is still unresolved after round r; a round whose predecessor left none
-// returns at once.  Jumps only point forward, so ceil(log2 N) rounds resolve all.
+// parent's parent word (and with it the resolved bit).  Round r runs only if
+// pending[r] is set and sets pending[r + 1] if any point is still unresolved after it.
+// Jumps only point forward, so ceil(log2 N) rounds resolve all.
 __global__ void __launch_bounds__(256) k_jump(uint32_t* parent, const uint32_t* chained, const uint32_t* zeros,
                                                uint64_t n, uint32_t* pending, int round) {
-    if (round > 0 && pending[round - 1] == 0) return;
+    if (pending[round] == 0) return;
     const uint64_t m = n - *zeros;
     bool any = false;
     for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < m;
@@ -370,33 +445,37 @@ __global__ void __launch_bounds__(256) k_jump(uint32_t* parent, const uint32_t* 
         parent[i] = pp;
         any |= !(pp & kResolved);
     }
-    if (__syncthreads_or(any) && threadIdx.x == 0) atomicOr(&pending[round], 1u);
+    if (__syncthreads_or(any) && threadIdx.x == 0) atomicOr(&pending[round + 1], 1u);
 }
 
 // q = block(root) * p + offset, then x = fma(q + 0.5, 2 eb, min) (lcps_cpp.cpp:1496-1500).
+// A resolved parent word holds the index of the point's block record in `compact`.
+// Points whose parent word is not resolved yet are skipped: the caller runs the
+// pointer-jumping rounds and this kernel again (or reports them unresolved).
 template <typename OT, bool SOA>
 __global__ void __launch_bounds__(256)
-k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ zrank,
-              const uint32_t* __restrict__ compact, const uint32_t* __restrict__ rel, const DecState* stc,
-              DecState* st, OT* __restrict__ out, int64_t* __restrict__ q_out) {
+k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ compact,
+              const uint32_t* __restrict__ rel, const DecState* stc, DecState* st, OT* __restrict__ out) {
     const DecodePlan& P = stc->plan;
     const uint32_t D = P.D;
     const uint64_t n = P.N;
     const int64_t p = P.p;
     const double two_eb = 2.0 * P.eb;
     const uint32_t B = static_cast<uint32_t>(P.comp[3].records);
+    // blk * p + off <= INT64_MAX for every off < p whenever blk <= safe_blk
+    const int64_t safe_blk = (INT64_MAX - (p - 1)) / p;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint32_t root = parent[i] & kParentMask;
-        const uint32_t cr = zrank[root];
+        const uint32_t pw = parent[i];
+        if (!(pw & kResolved)) continue;
+        const uint32_t cr = pw & kParentMask;
         bool bad = cr >= B;
         for (uint32_t d = 0; d < D; ++d) {
             const int64_t off = rel[i * D + d];
             if (off >= p) bad = true;
             const int64_t blk = bad ? 0 : compact[static_cast<uint64_t>(cr) * D + d];
-            if (blk > (INT64_MAX - off) / p) bad = true;
+            if (blk > safe_blk && blk > (INT64_MAX - off) / p) bad = true;
             const int64_t q = bad ? 0 : blk * p + off;
-            if (q_out) q_out[static_cast<uint64_t>(d) * n + i] = q;
             const double x = fma(__dadd_rn(static_cast<double>(q), 0.5), two_eb, P.minima[d]);
             out[SOA ? static_cast<uint64_t>(d) * n + i : i * D + d] = static_cast<OT>(x);
         }
@@ -501,7 +580,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     }
     const bool host_out = !is_device_ptr(out);
     size_t need = base_need;
-    need += Arena::need(N, 4) * 4;           // idrel, choice2, zrank, parent
+    need += Arena::need(N, 4) * 3;           // idrel, choice2, parent
     need += Arena::need(nd, 4) * 4;          // diff, keep, rel, compact
     need += Arena::need(N, 4);               // drank
     need += Arena::need(tags_total + 1, 4);
@@ -533,7 +612,6 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     streams[kCorrGaps] = A.take<uint32_t>(plan.exc_count + 1);
     streams[kCorrIds] = A.take<uint32_t>(plan.exc_count + 1);
     uint32_t* compact = A.take<uint32_t>(nd);
-    uint32_t* zrank = A.take<uint32_t>(N);
     uint32_t* parent = A.take<uint32_t>(N);
     uint32_t* drank = A.take<uint32_t>(N);
     uint32_t* tags = A.take<uint32_t>(tags_total + 1);
@@ -620,7 +698,12 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         const CompPlan& c = plan.comp[s];
         const CompPlan* dc = &st->plan.comp[s];
         if (c.enc == kEncFixed) {
-            k_unpack_fixed<<<dgrid(c.records), 256, 0, stream>>>(dcont, len, dc, streams[s], st); count_launch();
+            uint32_t wsum = 0;
+            for (uint32_t d = 0; d < c.dims; ++d) wsum += c.width[d];
+            const uint32_t G = std::max<uint32_t>(
+                1, std::min<uint32_t>({16u, kUnpackWords / std::max<uint32_t>(wsum, 1), kUnpackWords / (32 * c.dims)}));
+            k_unpack_fixed<<<dgrid((c.records + 32 * G - 1) / (32 * G), kUnpackWarps), 32 * kUnpackWarps, 0, stream>>>(
+                dcont, len, dc, streams[s], st, G); count_launch();
         } else if (c.enc == kEncTagged) {
             uint32_t* tg = tags + tag_off[s];
             device_exclusive_scan<uint64_t>(TagIn{tg, c.dims},
@@ -647,61 +730,78 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     // ---- level 1 inverse
     uint32_t* zeros_dev = reinterpret_cast<uint32_t*>(misc + 2);
     uint32_t* chained = drank;  // the choice ranks are no longer needed
-    device_exclusive_scan<uint32_t>(ZeroIn{streams[0]}, ZeroRankOut{streams[0], parent, zrank, chained, st, N}, N,
+    device_exclusive_scan<uint32_t>(ZeroIn{streams[0]}, ZeroRankOut{streams[0], parent, chained, st, N}, N,
                                     reinterpret_cast<uint32_t*>(scanbuf), zeros_dev, stream);
     T.mark("zero_ranks", stream);
     int rounds = 1;
     while ((1ull << rounds) < N) ++rounds;
-    uint32_t* pending = reinterpret_cast<uint32_t*>(misc + 16);  // misc[16..31]: 32 round flags
-    for (int r = 0; r < rounds; ++r) {
-        k_jump<<<dgrid(N), 256, 0, stream>>>(parent, chained, zeros_dev, N, pending, r); count_launch();
-    }
+    // misc[16..31]: 32 flags; [0] = left unresolved by k_resolve, [r + 1] = after round r
+    uint32_t* pending = reinterpret_cast<uint32_t*>(misc + 16);
+    unsigned long long* resolve_next = reinterpret_cast<unsigned long long*>(misc + 3);   // zeroed above
+    k_resolve<<<dgrid(N), 256, 0, stream>>>(parent, chained, zeros_dev, N, resolve_next, pending); count_launch();
     CHAIN_LAUNCH_CHECK("levels");
     T.mark("pointer_jump", stream);
-    // ---- reconstruction
+    // ---- reconstruction (and exact corrections, and the copy to host memory)
     const bool soa = out_layout == CHAIN_SOA;
     const unsigned g = dgrid(N);
     const uint64_t ncx = plan.exc_count;
     const CorrIn cin{streams[kCorrGaps]};
     uint64_t* sb = scanbuf;
-    if (out_dtype == CHAIN_F64) {
-        double* o = static_cast<double*>(dout);
-        if (soa) {
-            k_reconstruct<double, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr); count_launch();
-            if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<double, true>{streams[kCorrIds], dcont, st, st, o},
-                                                     ncx, sb, static_cast<uint64_t*>(nullptr), stream);
+    auto reconstruct = [&]() -> chain_status {
+        if (out_dtype == CHAIN_F64) {
+            double* o = static_cast<double*>(dout);
+            if (soa) {
+                k_reconstruct<double, true><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o); count_launch();
+                if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<double, true>{streams[kCorrIds], dcont, st, st, o},
+                                                         ncx, sb, static_cast<uint64_t*>(nullptr), stream);
+            } else {
+                k_reconstruct<double, false><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o); count_launch();
+                if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<double, false>{streams[kCorrIds], dcont, st, st, o},
+                                                         ncx, sb, static_cast<uint64_t*>(nullptr), stream);
+            }
         } else {
-            k_reconstruct<double, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr); count_launch();
-            if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<double, false>{streams[kCorrIds], dcont, st, st, o},
-                                                     ncx, sb, static_cast<uint64_t*>(nullptr), stream);
+            float* o = static_cast<float*>(dout);
+            if (soa) {
+                k_reconstruct<float, true><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o); count_launch();
+                if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<float, true>{streams[kCorrIds], dcont, st, st, o},
+                                                         ncx, sb, static_cast<uint64_t*>(nullptr), stream);
+            } else {
+                k_reconstruct<float, false><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o); count_launch();
+                if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<float, false>{streams[kCorrIds], dcont, st, st, o},
+                                                         ncx, sb, static_cast<uint64_t*>(nullptr), stream);
+            }
         }
-    } else {
-        float* o = static_cast<float*>(dout);
-        if (soa) {
-            k_reconstruct<float, true><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr); count_launch();
-            if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<float, true>{streams[kCorrIds], dcont, st, st, o},
-                                                     ncx, sb, static_cast<uint64_t*>(nullptr), stream);
-        } else {
-            k_reconstruct<float, false><<<g, 256, 0, stream>>>(parent, zrank, compact, streams[4], st, st, o, nullptr); count_launch();
-            if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<float, false>{streams[kCorrIds], dcont, st, st, o},
-                                                     ncx, sb, static_cast<uint64_t*>(nullptr), stream);
+        CHAIN_LAUNCH_CHECK("reconstruct");
+        T.mark("reconstruct", stream);
+        if (host_out) {
+            CHAIN_CUDA(cudaMemcpyAsync(out, dout, nd * osz, cudaMemcpyDeviceToHost, stream));
+            T.mark("d2h_points", stream);
         }
-    }
-    CHAIN_LAUNCH_CHECK("reconstruct");
-    T.mark("reconstruct", stream);
-    if (host_out) {
-        CHAIN_CUDA(cudaMemcpyAsync(out, dout, nd * osz, cudaMemcpyDeviceToHost, stream));
-        T.mark("d2h_points", stream);
+        return CHAIN_OK;
+    };
+    chain_status rs = reconstruct();
+    if (rs != CHAIN_OK) return rs;
+    uint32_t flags[2] = {0, 0};   // [0]: left unresolved by k_resolve; [1]: after the last round
+    CHAIN_CUDA(cudaMemcpyAsync(flags, pending, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    CHAIN_CUDA(cudaStreamSynchronize(stream));
+    if (flags[0]) {
+        // Chains too long for one pass: pointer-jumping rounds, then reconstruct again.
+        for (int r = 0; r < rounds; ++r) {
+            k_jump<<<dgrid(N), 256, 0, stream>>>(parent, chained, zeros_dev, N, pending, r); count_launch();
+        }
+        CHAIN_LAUNCH_CHECK("levels");
+        T.mark("pointer_jump_rounds", stream);
+        rs = reconstruct();
+        if (rs != CHAIN_OK) return rs;
+        CHAIN_CUDA(cudaMemcpyAsync(flags + 1, pending + rounds, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     }
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, offsetof(DecState, plan), cudaMemcpyDeviceToHost, stream));
     uint32_t counts[4] = {0, 0, 0, 0};
-    uint32_t still_pending = 0;
     CHAIN_CUDA(cudaMemcpyAsync(counts, misc + 1, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
-    CHAIN_CUDA(cudaMemcpyAsync(&still_pending, pending + rounds - 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     CHAIN_CUDA(cudaStreamSynchronize(stream));
     T.finish();
     const uint32_t ndiff_seen = counts[0], zeros_seen = counts[2];
-    if (hs->err || ndiff_seen != plan.comp[1].records || zeros_seen != B || still_pending)
+    if (hs->err || ndiff_seen != plan.comp[1].records || zeros_seen != B || flags[1])
         return set_err(CHAIN_ERR_CORRUPT_STREAM, "LCG2: invalid integer payload (flags " + std::to_string(hs->err) +
                                                      ")");
     return CHAIN_OK;

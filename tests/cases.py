@@ -33,6 +33,15 @@ def case(name):
         rng = np.random.default_rng(9)
         pts = rng.uniform(0, 1, size=(5000, 3)).astype(np.float32)
         return pts, 0.01, 1 << 20, 0, {}
+    if name == "long_chain":
+        # a few blocks holding almost every point: level-1 chains of tens of thousands of
+        # links, longer than the decoder's one-pass resolution follows (exercises the
+        # pointer-jumping rounds); block coordinates far from the frame minimum make
+        # chaining pay off
+        rng = np.random.default_rng(14)
+        pts = rng.uniform(1000.0, 1001.2, size=(300_000, 3)).astype(np.float32)
+        pts[0] = 0.0
+        return pts, 0.01, 64, 2, {}
     if name == "p1_big_threshold":
         pts = W.column(20_000, 3)
         return pts, W.eb_for(pts, 1e-3), 1, 1000, {}
@@ -76,5 +85,5 @@ def case(name):
 
 
 GPU_CASES = ["column", "column_qb11", "blobs200k", "blobs_clipped", "traj_f64_e4_p1", "traj_f64_e2",
-             "uniform_p64_t25", "single_point", "one_block", "p1_big_threshold", "neg_threshold", "dims1", "dims2",
+             "uniform_p64_t25", "single_point", "one_block", "long_chain", "p1_big_threshold", "neg_threshold", "dims1", "dims2",
              "dims4", "no_l1", "no_l2", "no_bl", "big_values_tagged", "wide_jump", "negative_zero"]
