@@ -397,12 +397,14 @@ struct ZeroRankOut {
 // a point repeatedly replaces its parent word by its parent's current word (which that
 // parent's own thread keeps advancing the same way), so pointers double while threads
 // run side by side, and points reached later (lower indices; parents point forward)
-// mostly find resolved parents.  Warps claim 32 points at a time from *next (zero at
-// launch), so the pass follows descending index order however the CTAs are scheduled.
-// Every word written is an ancestor of the point, so any interleaving is correct.  A
-// point stops after kResolveHops hops; any point left unresolved sets *pending, and the
-// k_jump rounds finish the work.
+// mostly find resolved parents.  Warps claim 32 * kResolvePer points at a time from
+// *next (zero at launch), so the pass follows descending index order however the CTAs
+// are scheduled; each lane advances its kResolvePer points together, keeping that many
+// independent loads in flight.  Every word written is an ancestor of the point, so any
+// interleaving is correct.  A point stops after kResolveHops hops; any point left
+// unresolved sets *pending, and the k_jump rounds finish the work.
 constexpr int kResolveHops = 64;
+constexpr int kResolvePer = 4;
 __global__ void __launch_bounds__(256) k_resolve(uint32_t* parent, const uint32_t* chained, const uint32_t* zeros,
                                                   uint64_t n, unsigned long long* next, uint32_t* pending) {
     const uint64_t m = n - *zeros;
@@ -410,19 +412,30 @@ __global__ void __launch_bounds__(256) k_resolve(uint32_t* parent, const uint32_
     bool left = false;
     for (;;) {
         unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(next, 32ull);
+        if (lane == 0) base = atomicAdd(next, 32ull * kResolvePer);
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= m) break;
-        const uint64_t t = base + lane;
-        if (t < m) {
-            const uint32_t i = chained[m - 1 - t];
-            uint32_t p = parent[i];
-            for (int h = 0; h < kResolveHops && !(p & kResolved); ++h) {
-                p = parent[p];
-                parent[i] = p;
-            }
-            left = left || !(p & kResolved);
+        uint32_t idx[kResolvePer], p[kResolvePer];
+#pragma unroll
+        for (int k = 0; k < kResolvePer; ++k) {
+            const uint64_t t = base + 32 * k + lane;
+            idx[k] = t < m ? chained[m - 1 - t] : 0u;
+            p[k] = t < m ? parent[idx[k]] : kResolved;
         }
+        for (int h = 0; h < kResolveHops; ++h) {
+            bool open = false;
+#pragma unroll
+            for (int k = 0; k < kResolvePer; ++k) {
+                if (!(p[k] & kResolved)) {
+                    p[k] = parent[p[k]];
+                    parent[idx[k]] = p[k];
+                    open = true;
+                }
+            }
+            if (!open) break;
+        }
+#pragma unroll
+        for (int k = 0; k < kResolvePer; ++k) left = left || !(p[k] & kResolved);
     }
     if (__syncthreads_or(left) && threadIdx.x == 0) atomicOr(pending, 1u);
 }
@@ -451,7 +464,24 @@ __global__ void __launch_bounds__(256) k_jump(uint32_t* parent, const uint32_t* 
 // q = block(root) * p + offset, then x = fma(q + 0.5, 2 eb, min) (lcps_cpp.cpp:1496-1500).
 // A resolved parent word holds the index of the point's block record in `compact`.
 // Points whose parent word is not resolved yet are skipped: the caller runs the
-// pointer-jumping rounds and this kernel again (or reports them unresolved).
+// pointer-jumping rounds and this kernel again (or reports them unresolved).  Each
+// thread takes kReconPer consecutive points and issues their block-record gathers
+// together.
+constexpr int kReconPer = 4;
+struct ReconCtx {
+    const uint32_t* compact;
+    uint32_t D, B;
+    int64_t p, safe_blk;   // blk * p + off <= INT64_MAX for every off < p whenever blk <= safe_blk
+    double two_eb;
+    const double* minima;
+    __device__ __forceinline__ double coord(uint32_t cr, uint32_t d, int64_t off, bool& bad) const {
+        if (off >= p) bad = true;
+        const int64_t blk = bad ? 0 : compact[static_cast<uint64_t>(cr) * D + d];
+        if (blk > safe_blk && blk > (INT64_MAX - off) / p) bad = true;
+        const int64_t q = bad ? 0 : blk * p + off;
+        return fma(__dadd_rn(static_cast<double>(q), 0.5), two_eb, minima[d]);
+    }
+};
 template <typename OT, bool SOA>
 __global__ void __launch_bounds__(256)
 k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ compact,
@@ -459,28 +489,125 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
     const DecodePlan& P = stc->plan;
     const uint32_t D = P.D;
     const uint64_t n = P.N;
-    const int64_t p = P.p;
-    const double two_eb = 2.0 * P.eb;
-    const uint32_t B = static_cast<uint32_t>(P.comp[3].records);
-    // blk * p + off <= INT64_MAX for every off < p whenever blk <= safe_blk
-    const int64_t safe_blk = (INT64_MAX - (p - 1)) / p;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint32_t pw = parent[i];
-        if (!(pw & kResolved)) continue;
-        const uint32_t cr = pw & kParentMask;
-        bool bad = cr >= B;
-        for (uint32_t d = 0; d < D; ++d) {
-            const int64_t off = rel[i * D + d];
-            if (off >= p) bad = true;
-            const int64_t blk = bad ? 0 : compact[static_cast<uint64_t>(cr) * D + d];
-            if (blk > safe_blk && blk > (INT64_MAX - off) / p) bad = true;
-            const int64_t q = bad ? 0 : blk * p + off;
-            const double x = fma(__dadd_rn(static_cast<double>(q), 0.5), two_eb, P.minima[d]);
-            out[SOA ? static_cast<uint64_t>(d) * n + i : i * D + d] = static_cast<OT>(x);
+    ReconCtx R;
+    R.compact = compact;
+    R.D = D;
+    R.B = static_cast<uint32_t>(P.comp[3].records);
+    R.p = P.p;
+    R.safe_blk = (INT64_MAX - (P.p - 1)) / P.p;
+    R.two_eb = 2.0 * P.eb;
+    R.minima = P.minima;
+    bool bad = false;
+    const bool vec = ((reinterpret_cast<uintptr_t>(parent) | reinterpret_cast<uintptr_t>(rel) |
+                       reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+    const uint64_t ng = (n + kReconPer - 1) / kReconPer;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < ng;
+         g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint32_t pw[kReconPer];
+        const bool full = g * kReconPer + kReconPer <= n;
+        if (full && vec) {
+            *reinterpret_cast<uint4*>(pw) = __ldg(reinterpret_cast<const uint4*>(parent + g * kReconPer));
+        } else {
+#pragma unroll
+            for (int k = 0; k < kReconPer; ++k) {
+                const uint64_t i = g * kReconPer + k;
+                pw[k] = i < n ? parent[i] : 0u;
+            }
         }
-        if (bad) set_error(&st->err, kErrCorrupt);
+        if (D == 3 && full && vec) {
+            // four whole points: 16-byte loads of rel, 16-byte stores of the output
+            uint32_t rl[12];
+            const uint4* rp = reinterpret_cast<const uint4*>(rel + g * 12);
+            *reinterpret_cast<uint4*>(rl) = __ldg(rp);
+            *reinterpret_cast<uint4*>(rl + 4) = __ldg(rp + 1);
+            *reinterpret_cast<uint4*>(rl + 8) = __ldg(rp + 2);
+            uint32_t blk[kReconPer][3];
+#pragma unroll
+            for (int k = 0; k < kReconPer; ++k) {
+                const uint32_t cr = pw[k] & kParentMask;
+                const bool ok = (pw[k] & kResolved) && cr < R.B;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) blk[k][d] = ok ? compact[static_cast<uint64_t>(cr) * 3 + d] : 0u;
+            }
+            OT x[12];
+            bool all = true;
+#pragma unroll
+            for (int k = 0; k < kReconPer; ++k) {
+                all = all && (pw[k] & kResolved);
+                bool b = (pw[k] & kParentMask) >= R.B;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const int64_t off = rl[3 * k + d];
+                    if (off >= R.p) b = true;
+                    const int64_t bk = b ? 0 : static_cast<int64_t>(blk[k][d]);
+                    if (bk > R.safe_blk && bk > (INT64_MAX - off) / R.p) b = true;
+                    const int64_t q = b ? 0 : bk * R.p + off;
+                    x[3 * k + d] = static_cast<OT>(fma(__dadd_rn(static_cast<double>(q), 0.5), R.two_eb, R.minima[d]));
+                }
+                bad = bad || (b && (pw[k] & kResolved));
+            }
+            const uint64_t i0 = g * kReconPer;
+            if (!SOA && all) {
+                if constexpr (sizeof(OT) == 8) {
+                    double2* o = reinterpret_cast<double2*>(out + i0 * 3);
+#pragma unroll
+                    for (int v = 0; v < 6; ++v) o[v] = make_double2(x[2 * v], x[2 * v + 1]);
+                } else {
+                    float4* o = reinterpret_cast<float4*>(out + i0 * 3);
+#pragma unroll
+                    for (int v = 0; v < 3; ++v) o[v] = make_float4(x[4 * v], x[4 * v + 1], x[4 * v + 2], x[4 * v + 3]);
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < kReconPer; ++k) {
+                    if (!(pw[k] & kResolved)) continue;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        out[SOA ? static_cast<uint64_t>(d) * n + i0 + k : (i0 + k) * 3 + d] = x[3 * k + d];
+                }
+            }
+        } else if (D == 3) {
+            uint32_t blk[kReconPer][3];
+#pragma unroll
+            for (int k = 0; k < kReconPer; ++k) {
+                const uint32_t cr = pw[k] & kParentMask;
+                const bool ok = (pw[k] & kResolved) && cr < R.B;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) blk[k][d] = ok ? compact[static_cast<uint64_t>(cr) * 3 + d] : 0u;
+            }
+#pragma unroll
+            for (int k = 0; k < kReconPer; ++k) {
+                const uint64_t i = g * kReconPer + k;
+                if (i >= n || !(pw[k] & kResolved)) continue;
+                bool b = (pw[k] & kParentMask) >= R.B;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const int64_t off = rel[i * 3 + d];
+                    if (off >= R.p) b = true;
+                    const int64_t bk = b ? 0 : static_cast<int64_t>(blk[k][d]);
+                    if (bk > R.safe_blk && bk > (INT64_MAX - off) / R.p) b = true;
+                    const int64_t q = b ? 0 : bk * R.p + off;
+                    const double x = fma(__dadd_rn(static_cast<double>(q), 0.5), R.two_eb, R.minima[d]);
+                    out[SOA ? static_cast<uint64_t>(d) * n + i : i * 3 + d] = static_cast<OT>(x);
+                }
+                bad = bad || b;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kReconPer; ++k) {
+                const uint64_t i = g * kReconPer + k;
+                if (i >= n || !(pw[k] & kResolved)) continue;
+                const uint32_t cr = pw[k] & kParentMask;
+                bool b = cr >= R.B;
+                for (uint32_t d = 0; d < D; ++d) {
+                    const double x = R.coord(cr, d, rel[i * D + d], b);
+                    out[SOA ? static_cast<uint64_t>(d) * n + i : i * D + d] = static_cast<OT>(x);
+                }
+                bad = bad || b;
+            }
+        }
     }
+    if (bad) set_error(&st->err, kErrCorrupt);
 }
 
 // Exact corrections: index_k = sum_{m<=k} (gap_m + 1) - 1, value = dictionary[id_k]
