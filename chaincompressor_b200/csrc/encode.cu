@@ -1296,7 +1296,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     const uint64_t nd = n * dims;
     const int64_t p_eff = bl ? p : 1;
     if (bytes_per_lane == 0) bytes_per_lane = 4096;
-    if (max_steps == 0) max_steps = 2048;
+    if (max_steps == 0) max_steps = 1024;
 
     chain_status st_ = ensure_state(ctx, sizeof(EncState));
     if (st_ != CHAIN_OK) return st_;

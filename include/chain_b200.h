@@ -70,7 +70,7 @@ typedef struct chain_opts {
     uint32_t rans_bytes_per_lane;   /* entropy stage: target coded bytes per rANS lane
                                        (each lane adds a 4-byte state); 0 = default 4096  */
     uint32_t rans_max_steps;        /* entropy stage: most symbols one lane codes
-                                       (serial depth); 0 = default 2048                   */
+                                       (serial depth); 0 = default 1024                   */
     uint32_t reserved[10];
 } chain_opts;
 
