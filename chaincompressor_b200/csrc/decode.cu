@@ -845,8 +845,8 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     // ---- level 2 inverse: choice ranks, then one reset-scan per dimension
     const uint64_t range = static_cast<uint64_t>(plan.wrap_max - plan.wrap_min) + 1;
     uint32_t* ndiff_dev = reinterpret_cast<uint32_t*>(misc + 1);
-    device_exclusive_scan<uint32_t>(ChoiceIn{streams[3]}, ChoiceRankOut{streams[3], drank, st}, B,
-                                    reinterpret_cast<uint32_t*>(scanbuf), ndiff_dev, stream);
+    device_flag_scan(ChoiceIn{streams[3]}, ChoiceRankOut{streams[3], drank, st}, B,
+                     reinterpret_cast<uint32_t*>(scanbuf), ndiff_dev, stream);
     const ResetAddOp l2op{static_cast<uint32_t>(range), static_cast<uint32_t>(range >> 32)};
     for (uint32_t d0 = 0; d0 < D; d0 += 3) {
         device_exclusive_scan<L2Vec>(Level2TermIn{streams[3], drank, streams[2], streams[1], st, st, d0},
@@ -857,8 +857,8 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     // ---- level 1 inverse
     uint32_t* zeros_dev = reinterpret_cast<uint32_t*>(misc + 2);
     uint32_t* chained = drank;  // the choice ranks are no longer needed
-    device_exclusive_scan<uint32_t>(ZeroIn{streams[0]}, ZeroRankOut{streams[0], parent, chained, st, N}, N,
-                                    reinterpret_cast<uint32_t*>(scanbuf), zeros_dev, stream);
+    device_flag_scan(ZeroIn{streams[0]}, ZeroRankOut{streams[0], parent, chained, st, N}, N,
+                     reinterpret_cast<uint32_t*>(scanbuf), zeros_dev, stream);
     T.mark("zero_ranks", stream);
     int rounds = 1;
     while ((1ull << rounds) < N) ++rounds;

@@ -472,16 +472,26 @@ struct Level2In {
         return value_bits >= diff_bits ? 1u : 0u;
     }
 };
+// choice2[j] for every record (1 = difference from the previous record).
+__global__ void __launch_bounds__(256) k_l2_choice(Level2In f, uint32_t* choice2) {
+    const uint32_t B = f.st->B;
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < B;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        choice2[j] = f(j);
+}
+struct Level2Flag {
+    const uint32_t* choice2;
+    const EncState* st;
+    __device__ bool operator()(uint64_t j) const { return j < st->B && choice2[j] != 0; }
+};
 struct Level2Out {
     const uint32_t* rec;
     const EncState* st;
-    uint32_t* choice2;
     uint32_t* keep;
     uint32_t* diff;
     __device__ void operator()(uint64_t j, uint32_t drank, uint32_t use_diff) const {
         if (j >= st->B) return;
         const uint32_t D = st->dims;
-        choice2[j] = use_diff;
         if (!use_diff) {
             const uint64_t k = j - drank;
             for (uint32_t d = 0; d < D; ++d) keep[k * D + d] = rec[j * D + d];
@@ -1412,17 +1422,17 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     T.mark("sort+level1", stream);
     uint32_t* scan32 = reinterpret_cast<uint32_t*>(scanbuf);
     if (wide)
-        device_exclusive_scan<uint32_t>(ExplicitIn<uint64_t>{idrel}, ExplicitOut<uint64_t>{key_idx, st, rec}, n,
-                                        scan32, &st->B, stream);
+        device_flag_scan(ExplicitIn<uint64_t>{idrel}, ExplicitOut<uint64_t>{key_idx, st, rec}, n, scan32, &st->B,
+                         stream);
     else
-        device_exclusive_scan<uint32_t>(ExplicitIn<uint32_t>{idrel},
-                                        ExplicitOut<uint32_t>{reinterpret_cast<uint32_t*>(key_idx), st, rec}, n,
-                                        scan32, &st->B, stream);
+        device_flag_scan(ExplicitIn<uint32_t>{idrel},
+                         ExplicitOut<uint32_t>{reinterpret_cast<uint32_t*>(key_idx), st, rec}, n, scan32, &st->B,
+                         stream);
     T.mark("explicit_records", stream);
     k_l2_stats<<<grid_for(n), 256, 0, stream>>>(rec, st); count_launch();
     k_l2_params<<<1, 1, 0, stream>>>(st); count_launch();
-    device_exclusive_scan<uint32_t>(Level2In{rec, st, l2}, Level2Out{rec, st, choice2, keep, diff}, n, scan32,
-                                    &st->ndiff, stream);
+    k_l2_choice<<<grid_for(n), 256, 0, stream>>>(Level2In{rec, st, l2}, choice2); count_launch();
+    device_flag_scan(Level2Flag{choice2, st}, Level2Out{rec, st, keep, diff}, n, scan32, &st->ndiff, stream);
     k_l2_counts<<<1, 1, 0, stream>>>(st); count_launch();
     CHAIN_LAUNCH_CHECK("level 2");
     T.mark("level2", stream);

@@ -203,4 +203,78 @@ void device_exclusive_scan(InF in, OutF out, uint64_t n, T* tile_buf, T* total, 
         in, out, n, tile_buf, op); count_launch();
 }
 
+// ------------------------------------------------------------ flag scans
+// Exclusive count of set flags: pred(i) -> bool for 0 <= i < n, and out(i, rank, flag)
+// called once per element with rank = number of set flags before i.  A tile is
+// kFlagThreads x kFlagItems elements; warp w of a tile handles 32 * kFlagItems
+// consecutive elements in rounds of 32 (element = base + 32 k + lane), so ranks come
+// from ballots and popcounts and every out() call is coalesced.  Three launches: tile
+// counts, a one-CTA scan of the counts, and the ranked pass (pred is evaluated twice).
+constexpr int kFlagThreads = 256;
+constexpr int kFlagItems = 16;
+constexpr int kFlagTile = kFlagThreads * kFlagItems;
+
+template <typename Pred>
+__global__ void __launch_bounds__(kFlagThreads) flag_count_kernel(Pred pred, uint64_t n, uint32_t* tile_counts) {
+    __shared__ uint32_t wsum[kFlagThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * kFlagItems;
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < kFlagItems; ++k) {
+        const uint64_t i = base + 32 * k + lane;
+        c += __popc(__ballot_sync(0xffffffffu, i < n && pred(i)));
+    }
+    if (lane == 0) wsum[warp] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kFlagThreads / 32; ++w) t += wsum[w];
+        tile_counts[blockIdx.x] = t;
+    }
+}
+
+template <typename Pred, typename OutF>
+__global__ void __launch_bounds__(kFlagThreads) flag_apply_kernel(Pred pred, OutF out, uint64_t n,
+                                                                   const uint32_t* tile_prefix) {
+    __shared__ uint32_t wsum[kFlagThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * kFlagItems;
+    uint32_t m[kFlagItems];
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < kFlagItems; ++k) {
+        const uint64_t i = base + 32 * k + lane;
+        m[k] = __ballot_sync(0xffffffffu, i < n && pred(i));
+        c += __popc(m[k]);
+    }
+    if (lane == 0) wsum[warp] = c;
+    __syncthreads();
+    uint32_t run = tile_prefix[blockIdx.x];
+    for (int w = 0; w < warp; ++w) run += wsum[w];
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < kFlagItems; ++k) {
+        const uint64_t i = base + 32 * k + lane;
+        if (i < n) out(i, run + __popc(m[k] & lt), (m[k] >> lane) & 1u);
+        run += __popc(m[k]);
+    }
+}
+
+inline uint64_t flag_tiles(uint64_t n) { return (n + kFlagTile - 1) / kFlagTile; }
+
+// `tile_buf` holds flag_tiles(n) u32 (scan_scratch_bytes(n) bytes suffice); *total
+// (may be null) receives the number of set flags.
+template <typename Pred, typename OutF>
+void device_flag_scan(Pred pred, OutF out, uint64_t n, uint32_t* tile_buf, uint32_t* total, cudaStream_t stream) {
+    const uint64_t tiles = flag_tiles(n);
+    if (tiles == 0) {
+        if (total) cudaMemsetAsync(total, 0, sizeof(uint32_t), stream);
+        return;
+    }
+    flag_count_kernel<Pred><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, n, tile_buf); count_launch();
+    scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(tile_buf, tiles, total, SumOp<uint32_t>()); count_launch();
+    flag_apply_kernel<Pred, OutF><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, out, n, tile_buf); count_launch();
+}
+
 }  // namespace chain
