@@ -287,79 +287,183 @@ struct ChoiceIn {
     const uint32_t* choice2;
     __device__ uint32_t operator()(uint64_t j) const { return choice2[j] ? 1u : 0u; }
 };
-struct ChoiceRankOut {
-    const uint32_t* choice2;
-    uint32_t* drank;
-    DecState* st;
-    __device__ void operator()(uint64_t j, uint32_t pre, uint32_t) const {
-        const uint32_t c = choice2[j];
-        if (c > 1 || (j == 0 && c != 0)) set_error(&st->err, kErrCorrupt);
-        drank[j] = pre;
-    }
-};
 
 __device__ __forceinline__ int64_t unzigzag(uint64_t sym) {
     return (sym & 1u) ? -static_cast<int64_t>(sym >> 1) - 1 : static_cast<int64_t>(sym >> 1);
 }
 
-struct Level2TermIn {
+// Level-2 inverse over tiles of kFlagTile block records (the tiles of the flag scan that
+// counted the difference records): 16 warps per tile, each warp kL2Rounds rounds of 32
+// consecutive records.  A record's row in `diff` is its rank among difference records
+// (tile offset + earlier warps + ballot popcount); a kept record's row in `keep` is its
+// index minus that rank.  Three dimensions per pass, starting at d0.
+constexpr int kL2Warps = 16;
+constexpr int kL2Rounds = kFlagTile / (32 * kL2Warps);
+static_assert(kL2Rounds * 32 * kL2Warps == kFlagTile, "level-2 tiles are flag-scan tiles");
+struct L2Geo {
     const uint32_t* choice2;
-    const uint32_t* drank;
     const uint32_t* keep;
     const uint32_t* diff;
-    const DecState* stc;
-    DecState* st;
-    uint32_t d0;   // first dimension of this pass
-    __device__ L2Vec operator()(uint64_t j) const {
-        const DecodePlan& P = stc->plan;
-        const uint32_t D = P.D;
-        const int64_t r = P.wrap_max - P.wrap_min + 1;
-        const int64_t maxc = r / 2 - ((r & 1) == 0 ? 1 : 0), minc = -(r / 2);
-        const uint32_t dr = drank[j];
-        L2Vec o = ResetAddOp::identity();
-        bool bad = false;
-        if (choice2[j] == 0) {
-            o.restart = 1;
-            const uint64_t row = static_cast<uint64_t>(j - dr) * D;
+    const uint32_t* tile_diff;   // exclusive count of difference records before each tile
+    uint64_t B;
+    uint32_t D, d0;
+    uint64_t range;
+    int64_t wrap_min, wrap_max, minc, maxc;
+    // Difference-record masks of this warp's rounds and the warp's first diff rank.
+    // Contains a __syncthreads: every thread of the CTA calls it.
+    __device__ __forceinline__ uint32_t ranks(uint32_t (&m)[kL2Rounds], uint32_t* s_cnt) const {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * kL2Rounds;
+        uint32_t c = 0;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                if (d0 + k < D) {
-                    const int64_t v = keep[row + d0 + k];
-                    bad |= v < P.wrap_min || v > P.wrap_max;   // lcps_cpp.cpp:1905-1907
-                    o.v[k] = static_cast<uint32_t>(v - P.wrap_min);
-                }
-            }
-        } else {
-            const uint64_t row = static_cast<uint64_t>(dr) * D;
+        for (int k = 0; k < kL2Rounds; ++k) {
+            const uint64_t j = base + 32 * k + lane;
+            m[k] = __ballot_sync(0xffffffffu, j < B && choice2[j] != 0);
+            c += __popc(m[k]);
+        }
+        if (lane == 0) s_cnt[warp] = c;
+        __syncthreads();
+        uint32_t off = tile_diff[blockIdx.x];
+        for (int w = 0; w < warp; ++w) off += s_cnt[w];
+        return off;
+    }
+    // Difference term of dimension d0 + kk: offset_j = offset_{j-1} - corr (mod range).
+    __device__ __forceinline__ uint32_t diff_term(uint64_t rank, uint32_t kk, bool& bad) const {
+        const int64_t corr = unzigzag(diff[rank * D + d0 + kk]);
+        const bool ok = corr >= minc && corr <= maxc;   // lcps_cpp.cpp:1917-1918
+        bad = bad || !ok;
+        return ok ? static_cast<uint32_t>(corr <= 0 ? -corr : static_cast<int64_t>(range) - corr) : 0u;
+    }
+    __device__ __forceinline__ uint32_t keep_value(uint64_t row, uint32_t kk, bool& bad) const {
+        const int64_t v = keep[row * D + d0 + kk];
+        const bool ok = v >= wrap_min && v <= wrap_max;   // lcps_cpp.cpp:1905-1907
+        bad = bad || !ok;
+        return ok ? static_cast<uint32_t>(v - wrap_min) : 0u;
+    }
+};
+
+// Tile aggregate of the reset-scan: the value at the tile's end when the tile holds a
+// kept record (restart), else the modular sum of its difference terms.  Only the terms
+// after the tile's last kept record are read.
+__global__ void __launch_bounds__(32 * kL2Warps) k_l2_tail(L2Geo g, L2Vec* tile_aggr) {
+    __shared__ uint32_t s_cnt[kL2Warps];
+    __shared__ int s_last[kL2Warps];
+    __shared__ unsigned long long s_sum[kL2Warps][3];
+    __shared__ uint32_t s_keep[3];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile;
+    const uint32_t wbase = warp * 32 * kL2Rounds;   // warp's first record within the tile
+    uint32_t m[kL2Rounds];
+    const uint32_t off = g.ranks(m, s_cnt);
+    int last = -1;   // last kept record of this warp (index within the tile)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                if (d0 + k < D) {
-                    const int64_t corr = unzigzag(diff[row + d0 + k]);
-                    bad |= corr < minc || corr > maxc;        // lcps_cpp.cpp:1917-1918
-                    // offset_j = offset_{j-1} - corr (mod range)
-                    o.v[k] = bad ? 0u : static_cast<uint32_t>(corr <= 0 ? -corr : r - corr);
-                }
+    for (int k = 0; k < kL2Rounds; ++k) {
+        const uint64_t j0 = tile0 + wbase + 32 * k;
+        const uint32_t valid = j0 >= g.B ? 0u : (g.B - j0 >= 32 ? 0xffffffffu : (1u << (g.B - j0)) - 1u);
+        const uint32_t km = valid & ~m[k];
+        if (km) last = static_cast<int>(wbase + 32 * k + 31 - __clz(km));
+    }
+    if (lane == 0) s_last[warp] = last;
+    __syncthreads();
+    int tl = -1;
+    for (int w = 0; w < kL2Warps; ++w) tl = s_last[w] > tl ? s_last[w] : tl;
+    bool bad = false;
+    unsigned long long acc[3] = {0, 0, 0};
+    uint32_t run = off;
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < kL2Rounds; ++k) {
+        const uint32_t r = wbase + 32 * k + lane;
+        const uint64_t rank = run + __popc(m[k] & lt);
+        if (((m[k] >> lane) & 1u) && static_cast<int>(r) > tl) {
+#pragma unroll
+            for (uint32_t kk = 0; kk < 3; ++kk)
+                if (g.d0 + kk < g.D) acc[kk] += g.diff_term(rank, kk, bad);
+        }
+        if (static_cast<int>(r) == tl) {
+#pragma unroll
+            for (uint32_t kk = 0; kk < 3; ++kk)
+                s_keep[kk] = g.d0 + kk < g.D ? g.keep_value(tile0 + r - rank, kk, bad) : 0u;
+        }
+        run += __popc(m[k]);
+    }
+#pragma unroll
+    for (int kk = 0; kk < 3; ++kk) {
+        unsigned long long a = warp_sum(acc[kk] % g.range);   // < 32 * 2^32
+        if (lane == 0) s_sum[warp][kk] = a % g.range;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        L2Vec o;
+        o.restart = tl >= 0 ? 1u : 0u;
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) {
+            unsigned long long t = o.restart ? s_keep[kk] : 0ull;
+            for (int w = 0; w < kL2Warps; ++w) t = (t + s_sum[w][kk]) % g.range;
+            o.v[kk] = static_cast<uint32_t>(t);
+        }
+        tile_aggr[blockIdx.x] = o;
+    }
+}
+
+// The reset-scan proper: every record's offset from wrap_min, seeded with the tile's
+// exclusive prefix; writes compact[j * D + d0 + kk] = wrap_min + offset.  Also checks
+// the choice values (lcps_cpp.cpp:1899-1900, 1911-1912) and the value ranges.
+__global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec* tile_prefix, uint32_t* compact,
+                                                             DecState* st) {
+    __shared__ uint32_t s_cnt[kL2Warps];
+    __shared__ L2Vec s_tot[kL2Warps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile;
+    const uint32_t wbase = warp * 32 * kL2Rounds;
+    const ResetAddOp op{static_cast<uint32_t>(g.range), static_cast<uint32_t>(g.range >> 32)};
+    uint32_t m[kL2Rounds];
+    const uint32_t off = g.ranks(m, s_cnt);
+    bool bad = false;
+    L2Vec incl[kL2Rounds];
+    L2Vec wtot = ResetAddOp::identity();
+    uint32_t run = off;
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < kL2Rounds; ++k) {
+        const uint64_t j = tile0 + wbase + 32 * k + lane;
+        const uint64_t rank = run + __popc(m[k] & lt);
+        L2Vec t = ResetAddOp::identity();
+        if (j < g.B) {
+            const uint32_t c = g.choice2[j];
+            bad = bad || c > 1 || (j == 0 && c != 0);
+            if ((m[k] >> lane) & 1u) {
+#pragma unroll
+                for (uint32_t kk = 0; kk < 3; ++kk)
+                    if (g.d0 + kk < g.D) t.v[kk] = g.diff_term(rank, kk, bad);
+            } else {
+                t.restart = 1;
+#pragma unroll
+                for (uint32_t kk = 0; kk < 3; ++kk)
+                    if (g.d0 + kk < g.D) t.v[kk] = g.keep_value(j - rank, kk, bad);
             }
         }
-        if (bad) set_error(&st->err, kErrCorrupt);
-        return o;
+        incl[k] = warp_inclusive_scan_op(t, op);
+        wtot = op(wtot, shfl_idx_any(incl[k], 31));
+        run += __popc(m[k]);
     }
-};
-struct Level2TermOut {
-    const DecState* stc;
-    uint32_t d0;
-    uint32_t* compact;   // [B * D]
-    __device__ void operator()(uint64_t j, const L2Vec& prefix, const L2Vec& term) const {
-        const DecodePlan& P = stc->plan;
-        const uint32_t D = P.D;
-        const ResetAddOp op{static_cast<uint32_t>(P.wrap_max - P.wrap_min + 1),
-                            static_cast<uint32_t>((P.wrap_max - P.wrap_min + 1) >> 32)};
-        const L2Vec inc = op(prefix, term);
+    if (lane == 0) s_tot[warp] = wtot;
+    __syncthreads();
+    L2Vec carry = tile_prefix[blockIdx.x];
+    for (int w = 0; w < warp; ++w) carry = op(carry, s_tot[w]);
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
-            if (d0 + k < D) compact[j * D + d0 + k] = static_cast<uint32_t>(P.wrap_min + inc.v[k]);
+    for (int k = 0; k < kL2Rounds; ++k) {
+        const uint64_t j = tile0 + wbase + 32 * k + lane;
+        const L2Vec v = op(carry, incl[k]);
+        if (j < g.B) {
+#pragma unroll
+            for (uint32_t kk = 0; kk < 3; ++kk)
+                if (g.d0 + kk < g.D) compact[j * g.D + g.d0 + kk] = static_cast<uint32_t>(g.wrap_min + v.v[kk]);
+        }
+        carry = op(carry, shfl_idx_any(incl[k], 31));
     }
-};
+    if (__syncthreads_or(bad) && threadIdx.x == 0) set_error(&st->err, kErrCorrupt);
+}
 
 // ------------------------------------------------------------------- level 1
 struct ZeroIn {
@@ -842,16 +946,41 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     CHAIN_LAUNCH_CHECK("unpack");
     T.mark("unpack", stream);
 
-    // ---- level 2 inverse: choice ranks, then one reset-scan per dimension
+    // ---- level 2 inverse: difference-record counts per tile, then per three dimensions
+    // the tiles' reset-scan aggregates, their exclusive scan, and the records
     const uint64_t range = static_cast<uint64_t>(plan.wrap_max - plan.wrap_min) + 1;
     uint32_t* ndiff_dev = reinterpret_cast<uint32_t*>(misc + 1);
-    device_flag_scan(ChoiceIn{streams[3]}, ChoiceRankOut{streams[3], drank, st}, B,
-                     reinterpret_cast<uint32_t*>(scanbuf), ndiff_dev, stream);
-    const ResetAddOp l2op{static_cast<uint32_t>(range), static_cast<uint32_t>(range >> 32)};
-    for (uint32_t d0 = 0; d0 < D; d0 += 3) {
-        device_exclusive_scan<L2Vec>(Level2TermIn{streams[3], drank, streams[2], streams[1], st, st, d0},
-                                     Level2TermOut{st, d0, compact}, B, reinterpret_cast<L2Vec*>(scanbuf),
-                                     static_cast<L2Vec*>(nullptr), stream, l2op);
+    const uint64_t l2tiles = flag_tiles(B);
+    uint32_t* tile_diff = reinterpret_cast<uint32_t*>(scanbuf);
+    L2Vec* tile_l2 = reinterpret_cast<L2Vec*>(reinterpret_cast<uint8_t*>(scanbuf) + ((4 * l2tiles + 15) & ~15ull));
+    if (l2tiles) {
+        flag_count_kernel<ChoiceIn><<<static_cast<unsigned>(l2tiles), kFlagThreads, 0, stream>>>(ChoiceIn{streams[3]}, B,
+                                                                                                 tile_diff); count_launch();
+        scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(tile_diff, l2tiles, ndiff_dev,
+                                                                                SumOp<uint32_t>()); count_launch();
+        const ResetAddOp l2op{static_cast<uint32_t>(range), static_cast<uint32_t>(range >> 32)};
+        L2Geo g;
+        g.choice2 = streams[3];
+        g.keep = streams[2];
+        g.diff = streams[1];
+        g.tile_diff = tile_diff;
+        g.B = B;
+        g.D = D;
+        g.range = range;
+        g.wrap_min = plan.wrap_min;
+        g.wrap_max = plan.wrap_max;
+        const int64_t r = static_cast<int64_t>(range);
+        g.maxc = r / 2 - ((r & 1) == 0 ? 1 : 0);
+        g.minc = -(r / 2);
+        for (uint32_t d0 = 0; d0 < D; d0 += 3) {
+            g.d0 = d0;
+            k_l2_tail<<<static_cast<unsigned>(l2tiles), 32 * kL2Warps, 0, stream>>>(g, tile_l2); count_launch();
+            scan_tilesums_kernel<L2Vec, ResetAddOp><<<1, 1024, 0, stream>>>(tile_l2, l2tiles, static_cast<L2Vec*>(nullptr),
+                                                                           l2op); count_launch();
+            k_l2_apply<<<static_cast<unsigned>(l2tiles), 32 * kL2Warps, 0, stream>>>(g, tile_l2, compact, st); count_launch();
+        }
+    } else {
+        CHAIN_CUDA(cudaMemsetAsync(ndiff_dev, 0, sizeof(uint32_t), stream));
     }
     T.mark("level2_inverse", stream);
     // ---- level 1 inverse

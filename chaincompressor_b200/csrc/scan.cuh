@@ -44,6 +44,20 @@ __device__ __forceinline__ T shfl_up_any(T v, int o) {
     return u.t;
 }
 
+template <typename T>
+__device__ __forceinline__ T shfl_idx_any(T v, int src) {
+    static_assert(sizeof(T) % 4 == 0, "shuffled types must be made of 32-bit words");
+    union U {
+        T t;
+        uint32_t w[sizeof(T) / 4];
+        __device__ U() {}
+    } u;
+    u.t = v;
+#pragma unroll
+    for (int k = 0; k < static_cast<int>(sizeof(T) / 4); ++k) u.w[k] = __shfl_sync(0xffffffffu, u.w[k], src);
+    return u.t;
+}
+
 template <typename T, typename Op>
 __device__ __forceinline__ T warp_inclusive_scan_op(T v, Op op) {
     const int lane = threadIdx.x & 31;
