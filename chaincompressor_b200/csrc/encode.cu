@@ -363,7 +363,6 @@ __global__ void __launch_bounds__(256)
 k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_t n, const EncState* st,
          uint32_t* __restrict__ idrel) {
     const int D = static_cast<int>(st->dims);
-    const int kb = st->kb;
     const int64_t maxb_bits = st->maxb_bits;
     const int64_t thr = st->threshold;
     for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
@@ -373,11 +372,9 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
         uint32_t out = 0;
         if (k + 1 < n && skey[k + 1] == key) {
             const uint32_t dist = sidx[k + 1] - i;
-            uint32_t b[kMaxDims];
-            block_unkey(static_cast<uint64_t>(key), D, kb, b);
-            uint32_t mx = b[0];
-            for (int d = 1; d < D; ++d) mx = b[d] > mx ? b[d] : mx;
-            const int local_bits = bitlen32(mx);
+            // bit j of block coordinate d sits at key bit j * D + d, so the widest
+            // coordinate of the block has ceil(bitlen(key) / D) bits
+            const int local_bits = (bitlen64(static_cast<uint64_t>(key)) + D - 1) / D;
             const int tag_bits = bitlen32(static_cast<uint32_t>(local_bits));
             const int64_t a = static_cast<int64_t>(local_bits) * D + tag_bits;
             const int64_t c = static_cast<int64_t>(D) * maxb_bits;
