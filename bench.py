@@ -281,6 +281,101 @@ def run_ours(args, rank: int, world: int):
     return line
 
 
+def run_batch_bench(args):
+    """The uneven collection (256 frames, N log-uniform in [1e4, 2e6], column / blobs /
+    uniform content, eb in {1e-2, 1e-3, 1e-4} x range, float32), device-resident: one
+    frame per chain_compress call on one context, against chain_batch_compress with
+    `--workers` contexts.  Frames run on several streams, so the time of a pass is the
+    host wall clock between device synchronisations around the whole collection."""
+    import torch
+
+    from chaincompressor_b200 import _native as N
+    from chaincompressor_b200 import workloads as W
+
+    torch.cuda.set_device(0)
+    specs = W.uneven_specs(256, seed=3)
+    frames = []
+    for n, kind, frac, seed in specs:
+        pts = W.make_frame(n, kind, seed)
+        eb = W.eb_for(pts, frac)
+        frames.append((torch.from_numpy(np.ascontiguousarray(pts.T)).cuda(), n, eb))
+    raw = sum(n * 3 * 4 for _, n, _ in frames)
+    caps = [N.compress_bound(n, 3) for _, n, _ in frames]
+    outbuf = torch.empty(sum(caps), dtype=torch.uint8, device="cuda")
+    offs = np.concatenate([[0], np.cumsum(caps)[:-1]]).astype(np.int64)
+    codec = N.Codec(0)
+
+    def seq_compress():
+        lens = []
+        for (x, n, eb), off, cap in zip(frames, offs, caps):
+            ln = codec.compress_ptr(x.data_ptr(), N.CHAIN_F32, N.CHAIN_SOA, n, 3, eb, 4, 2)
+            codec.result_copy_to(outbuf.data_ptr() + int(off), cap)
+            lens.append(ln)
+        return lens
+
+    items = [N.BatchItem(input=x.data_ptr(), dtype=N.CHAIN_F32, layout=N.CHAIN_SOA, n=n, dims=3, eb=eb, p=4,
+                         threshold=2, output=outbuf.data_ptr() + int(off), output_capacity=cap)
+             for (x, n, eb), off, cap in zip(frames, offs, caps)]
+    batch = N.Batch(0, workers=args.workers)
+
+    def bat_compress():
+        arr = batch.compress_items(items)
+        return [arr[i].output_bytes for i in range(len(items))]
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        l0 = N.launch_count()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            out = fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / args.steps, out, (N.launch_count() - l0) // args.steps
+
+    t_seq, lens_seq, l_seq = timed(seq_compress)
+    t_bat, lens_bat, l_bat = timed(bat_compress)
+    assert lens_seq == lens_bat
+    # decompression of the same containers into float64 AoS device buffers
+    outs = torch.empty(sum(n * 3 for _, n, _ in frames), dtype=torch.float64, device="cuda")
+    ooffs = np.concatenate([[0], np.cumsum([n * 3 for _, n, _ in frames])[:-1]]).astype(np.int64)
+
+    def seq_decompress():
+        for (x, n, eb), off, ln, oo in zip(frames, offs, lens_seq, ooffs):
+            codec.decompress_ptr(outbuf.data_ptr() + int(off), ln, outs.data_ptr() + 8 * int(oo), n * 3 * 8)
+        return None
+
+    ditems = [N.BatchItem(input=outbuf.data_ptr() + int(off), input_bytes=ln, dtype=N.CHAIN_F64, layout=N.CHAIN_AOS,
+                          output=outs.data_ptr() + 8 * int(oo), output_capacity=n * 3 * 8)
+              for (x, n, eb), off, ln, oo in zip(frames, offs, lens_seq, ooffs)]
+
+    def bat_decompress():
+        batch.decompress_items(ditems)
+        return None
+
+    td_seq, _, ld_seq = timed(seq_decompress)
+    td_bat, _, ld_bat = timed(bat_decompress)
+    batch.close()
+    codec.close()
+    gbs = lambda s: raw / s / 1e9  # noqa: E731
+    return {
+        "metric": "batch compress GB/s (uncompressed bytes/s) over 256 uneven frames", "value": round(gbs(t_bat), 3),
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t_bat * 1e3, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 quantize, u32 codes, u8 rANS", "data": "synthetic (seeded)",
+        "config": {"workload": "uneven-256 (N log-uniform 1e4..2e6; column/blobs/uniform; eb 1e-2/1e-3/1e-4 x range;"
+                               " f32)", "frames": len(frames), "points": sum(n for _, n, _ in frames),
+                   "workers": args.workers, "timing": "host wall clock per pass, device synchronised on both sides",
+                   "l2_flush": "inputs larger than L2 (whole collection > 1 GB)"},
+        "sequential": {"value": round(gbs(t_seq), 3), "ms_per_step": round(t_seq * 1e3, 3), "gpu_launches": l_seq},
+        "speedup_vs_sequential": round(t_seq / t_bat, 3), "gpu_launches": l_bat,
+        "decompress": {"value": round(gbs(td_bat), 3), "ms_per_step": round(td_bat * 1e3, 3),
+                       "sequential": round(gbs(td_seq), 3), "speedup_vs_sequential": round(td_seq / td_bat, 3),
+                       "gpu_launches": ld_bat},
+        "compressed_bytes": int(sum(lens_bat)),
+    }
+
+
 _REF_JOB = None
 
 
@@ -362,7 +457,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="blobs", choices=["blobs", "column", "trajectory"])
+    ap.add_argument("--config", default="blobs", choices=["blobs", "column", "trajectory", "batch"])
+    ap.add_argument("--workers", type=int, default=8, help="contexts of the batch path (--config batch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--once", action="store_true",
                     help="one warm-up and one measured compress + decompress, no timing (for ncu launch lists)")
@@ -376,6 +472,10 @@ def main():
         return
     if args.once:
         run_once(args)
+        return
+    if args.config == "batch":
+        if rank == 0:
+            print(json.dumps(run_batch_bench(args)))
         return
     if world > 1:
         import datetime

@@ -31,7 +31,8 @@ CHAIN_SOA, CHAIN_AOS = 0, 1
 EXPORTS = ("chain_ctx_create", "chain_ctx_destroy", "chain_last_error_message", "chain_compress_bound",
            "chain_compress", "chain_result_copy", "chain_result_device_ptr", "chain_peek", "chain_decompress",
            "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count",
-           "chain_decompress_noalloc")
+           "chain_decompress_noalloc", "chain_batch_create", "chain_batch_destroy", "chain_batch_compress",
+           "chain_batch_decompress")
 
 
 class ChainError(RuntimeError):
@@ -44,6 +45,13 @@ class ChainOpts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("bl", ctypes.c_int32), ("l1", ctypes.c_int32),
                 ("l2", ctypes.c_int32), ("rans_bytes_per_lane", ctypes.c_uint32),
                 ("rans_max_steps", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 10)]
+
+
+class BatchItem(ctypes.Structure):
+    _fields_ = [("input", ctypes.c_void_p), ("input_bytes", ctypes.c_size_t), ("dtype", ctypes.c_int),
+                ("layout", ctypes.c_int), ("n", ctypes.c_uint64), ("dims", ctypes.c_uint32), ("eb", ctypes.c_double),
+                ("p", ctypes.c_int64), ("threshold", ctypes.c_int64), ("output", ctypes.c_void_p),
+                ("output_capacity", ctypes.c_size_t), ("output_bytes", ctypes.c_size_t), ("status", ctypes.c_int)]
 
 
 _LIB = None
@@ -73,10 +81,16 @@ def load() -> ctypes.CDLL:
         L.chain_debug_streams.argtypes = [P, P, P, ctypes.POINTER(u64), P, ctypes.POINTER(u64), P,
                                           ctypes.POINTER(u64), P]
         L.chain_decompress_noalloc.argtypes = [P, sz, i32, i32, P, sz, ctypes.POINTER(u64), ctypes.POINTER(u32), P]
+        L.chain_batch_create.argtypes = [i32, i32, ctypes.POINTER(P)]
+        L.chain_batch_destroy.argtypes = [P]
+        L.chain_batch_destroy.restype = None
+        L.chain_batch_compress.argtypes = [P, ctypes.POINTER(BatchItem), sz, ctypes.POINTER(ChainOpts)]
+        L.chain_batch_decompress.argtypes = [P, ctypes.POINTER(BatchItem), sz]
         for f in ("chain_ctx_create", "chain_compress", "chain_result_copy", "chain_peek", "chain_decompress",
-                  "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count",
-                  "chain_decompress_noalloc"):
+                  "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_decompress_noalloc",
+                  "chain_batch_create", "chain_batch_compress", "chain_batch_decompress"):
             getattr(L, f).restype = ctypes.c_int
+        L.chain_launch_count.restype = ctypes.c_uint64
         _LIB = L
     return _LIB
 
@@ -217,8 +231,69 @@ def decompress_noalloc_ptr(src_ptr: int, length: int, out_ptr: int, capacity: in
     return n.value, d.value
 
 
+class Batch:
+    """chain_batch: `workers` contexts on one device, driven by host threads."""
+
+    def __init__(self, device: int = 0, workers: int = 4):
+        self.L = load()
+        h = ctypes.c_void_p()
+        _check(self.L.chain_batch_create(device, workers, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.chain_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def compress_items(self, items, opts: ChainOpts | None = None):
+        arr = (BatchItem * len(items))(*items)
+        _check(self.L.chain_batch_compress(self.h, arr, len(items), ctypes.byref(opts) if opts else None))
+        return arr
+
+    def decompress_items(self, items):
+        arr = (BatchItem * len(items))(*items)
+        _check(self.L.chain_batch_decompress(self.h, arr, len(items)))
+        return arr
+
+    def compress(self, frames, layout: int = CHAIN_SOA) -> list[bytes]:
+        """frames: list of (points, eb, p, threshold) with numpy points ((D, N) for SoA)."""
+        keep, items, outs = [], [], []
+        for pts, eb, p, t in frames:
+            pts = np.ascontiguousarray(pts)
+            n, d = (pts.shape[1], pts.shape[0]) if layout == CHAIN_SOA else pts.shape
+            cap = compress_bound(n, d)
+            out = np.empty(cap, np.uint8)
+            keep.append(pts)
+            outs.append(out)
+            items.append(BatchItem(input=pts.ctypes.data, dtype=CHAIN_F32 if pts.dtype == np.float32 else CHAIN_F64,
+                                   layout=layout, n=n, dims=d, eb=float(eb), p=int(p), threshold=int(t),
+                                   output=out.ctypes.data, output_capacity=cap))
+        arr = self.compress_items(items)
+        return [outs[i][: arr[i].output_bytes].tobytes() for i in range(len(items))]
+
+    def decompress(self, containers, dtype=np.float64, layout: int = CHAIN_AOS) -> list[np.ndarray]:
+        keep, items, outs = [], [], []
+        for data in containers:
+            n, d, _ = peek(data)
+            out = np.empty((n, d) if layout == CHAIN_AOS else (d, n), dtype)
+            src = np.frombuffer(data, np.uint8)
+            keep.append(src)
+            outs.append(out)
+            items.append(BatchItem(input=src.ctypes.data, input_bytes=len(data),
+                                   dtype=CHAIN_F64 if out.dtype == np.float64 else CHAIN_F32, layout=layout,
+                                   output=out.ctypes.data, output_capacity=out.nbytes))
+        self.decompress_items(items)
+        return outs
+
+
 def launch_count() -> int:
-    """Kernel launches issued by the library on this thread so far."""
+    """Kernel launches issued by the library in this process so far."""
     return load().chain_launch_count()
 
 

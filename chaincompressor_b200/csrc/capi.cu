@@ -1,6 +1,7 @@
 // C ABI of libchain_b200 (declared in include/chain_b200.h).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -13,8 +14,9 @@
 namespace chain {
 
 static thread_local std::string g_last_error;
-static thread_local uint64_t g_launches = 0;
-uint64_t& launch_counter() { return g_launches; }
+static std::atomic<uint64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t launch_count_total() { return g_launches.load(std::memory_order_relaxed); }
 
 chain_status set_err(chain_status st, const std::string& msg) {
     g_last_error = msg;
@@ -220,7 +222,7 @@ chain_status chain_debug_streams(chain_ctx* ctx, int64_t* idrel, int64_t* diff, 
     return CHAIN_OK;
 }
 
-uint64_t chain_launch_count(void) { return g_launches; }
+uint64_t chain_launch_count(void) { return launch_count_total(); }
 
 chain_status chain_set_stage_timing(chain_ctx* ctx, int enabled) {
     if (!ctx) return set_err(CHAIN_ERR_INVALID_ARGUMENT, "null context");

@@ -34,8 +34,8 @@ enum Encoding : uint8_t { kEncEmpty = 0, kEncTagged = 1, kEncFixed = 2, kEncRaw 
 
 // Host-side count of kernel launches issued by the library (tracing aid: every launch
 // site calls count_launch()).
-uint64_t& launch_counter();
-inline void count_launch() { ++launch_counter(); }
+void count_launch();          // process-wide, thread-safe
+uint64_t launch_count_total();
 
 __host__ __device__ inline int bitlen32(uint32_t v) {
 #ifdef __CUDA_ARCH__

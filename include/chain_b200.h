@@ -115,6 +115,48 @@ CHAIN_API chain_status chain_decompress(chain_ctx* ctx, const void* container, s
                               chain_dtype out_dtype, chain_layout out_layout, void* out,
                               size_t out_capacity_bytes, uint64_t* n, uint32_t* dims);
 
+/* ---- batches of independent frames ------------------------------------------------
+ * A batch object owns `workers` contexts on one device (each with its own stream and
+ * arenas, kept between batches).  chain_batch_compress / chain_batch_decompress run
+ * the items on those contexts from `workers` host threads, so that many frames'
+ * kernels and host round trips overlap; each item's result is identical to the
+ * one-frame call's.  Items of one call must not share output buffers.  This is the
+ * batched form of the path for collections of frames (for instance 256 frames of
+ * 1e4..2e6 particles each); the reference processes such collections one frame per
+ * call (chain_caller.py:33-40 in a loop).
+ *
+ * Item fields, compress:   input = points, dtype/layout/n/dims/eb/p/threshold as for
+ *                          chain_compress; output = container buffer (host or device)
+ *                          of output_capacity bytes (chain_compress_bound is enough).
+ * Item fields, decompress: input = container of input_bytes bytes; dtype/layout = the
+ *                          output's; output = points buffer of output_capacity bytes;
+ *                          n and dims are returned.
+ * Returned in every item:  output_bytes and status.  The call returns CHAIN_OK when
+ * every item succeeded, else the first failing item's status, with its index in
+ * chain_last_error_message(). */
+typedef struct chain_batch chain_batch;
+typedef struct chain_batch_item {
+    const void* input;
+    size_t input_bytes;
+    chain_dtype dtype;
+    chain_layout layout;
+    uint64_t n;
+    uint32_t dims;
+    double eb;
+    int64_t p;
+    int64_t threshold;
+    void* output;
+    size_t output_capacity;
+    size_t output_bytes;
+    chain_status status;
+} chain_batch_item;
+
+CHAIN_API chain_status chain_batch_create(int device, int workers, chain_batch** out);
+CHAIN_API void chain_batch_destroy(chain_batch* batch);
+CHAIN_API chain_status chain_batch_compress(chain_batch* batch, chain_batch_item* items, size_t count,
+                                            const chain_opts* opts);
+CHAIN_API chain_status chain_batch_decompress(chain_batch* batch, chain_batch_item* items, size_t count);
+
 /* Decompression that allocates nothing, for callers that cannot allocate memory when
  * they decode (a plug-in inside an application that owns the device memory pool or
  * runs under a hard memory cap; a loop that must not pay for cudaMalloc/cudaFree, which
@@ -150,7 +192,8 @@ CHAIN_API chain_status chain_debug_streams(chain_ctx* ctx, int64_t* idrel, int64
  * adds one event record per stage. */
 CHAIN_API chain_status chain_set_stage_timing(chain_ctx* ctx, int enabled);
 
-/* Number of CUDA kernels this thread's library calls have launched so far. */
+/* Number of CUDA kernels the library has launched in this process so far (all threads,
+ * batch workers included). */
 CHAIN_API uint64_t chain_launch_count(void);
 CHAIN_API int chain_stage_times(const chain_ctx* ctx, const char** names, float* ms, int max);
 
