@@ -376,6 +376,120 @@ def run_batch_bench(args):
     }
 
 
+def run_serve_bench(args):
+    """Serving loop: `--requests` requests (50% compress, 50% decompress of containers
+    made beforehand) over a seeded pool of 48 frames (N log-uniform in [1e3, 8e6];
+    column / blobs / uniform content; eb in {1e-2, 1e-3, 1e-4} x range; 70% float32,
+    30% float64; device-resident) through chain_server with `--workers` contexts and a
+    40 GB admission budget.  First the capacity (all requests queued at once), then
+    Poisson arrivals at 0.5, 0.8 and 0.95 of it; latency = queueing + service time as
+    stamped by the server.  Requests on the same pool frame share its output buffers
+    (the bench reads no results; tests/test_gpu_server.py checks them)."""
+    import threading
+
+    import torch
+
+    from chaincompressor_b200 import _native as N
+    from chaincompressor_b200 import workloads as W
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(4)
+    pool = []
+    codec = N.Codec(0)
+    for k in range(48):
+        n = int(np.floor(np.exp(rng.uniform(np.log(1e3), np.log(8e6)))))
+        kind = ("column", "blobs", "uniform")[int(rng.integers(0, 3))]
+        frac = float((1e-2, 1e-3, 1e-4)[int(rng.integers(0, 3))])
+        dt = np.float32 if rng.random() < 0.7 else np.float64
+        pts = W.make_frame(n, kind, int(rng.integers(0, 2**31 - 1)), dt)
+        eb = W.eb_for(pts, frac)
+        x = torch.from_numpy(np.ascontiguousarray(pts.T)).cuda()
+        code = N.CHAIN_F32 if dt == np.float32 else N.CHAIN_F64
+        ln = codec.compress_ptr(x.data_ptr(), code, N.CHAIN_SOA, n, 3, eb, 4, 2)
+        cont = torch.empty(ln, dtype=torch.uint8, device="cuda")
+        codec.result_copy_to(cont.data_ptr(), ln)
+        cap = N.compress_bound(n, 3)
+        cout = torch.empty(cap, dtype=torch.uint8, device="cuda")
+        dout = torch.empty(n * 3, dtype=torch.float64, device="cuda")
+        pool.append(dict(x=x, n=n, eb=eb, code=code, cont=cont, ln=ln, cout=cout, cap=cap, dout=dout,
+                         raw=n * 3 * pts.dtype.itemsize))
+    codec.close()
+    torch.cuda.synchronize()
+    R = args.requests
+    picks = rng.integers(0, len(pool), size=R)
+    ops = rng.integers(0, 2, size=R)
+    items = []
+    for f, op in zip(picks, ops):
+        P = pool[int(f)]
+        if op == 0:
+            items.append(N.BatchItem(input=P["x"].data_ptr(), dtype=P["code"], layout=N.CHAIN_SOA, n=P["n"], dims=3,
+                                     eb=P["eb"], p=4, threshold=2, output=P["cout"].data_ptr(),
+                                     output_capacity=P["cap"]))
+        else:
+            items.append(N.BatchItem(input=P["cont"].data_ptr(), input_bytes=P["ln"], dtype=N.CHAIN_F64,
+                                     layout=N.CHAIN_AOS, output=P["dout"].data_ptr(), output_capacity=P["n"] * 24))
+    raw_total = sum(pool[int(f)]["raw"] for f in picks)
+    srv = N.Server(0, workers=args.workers, memory_budget_bytes=40 << 30)
+
+    def run(arrivals):
+        """Submit item i at t0 + arrivals[i] (seconds); returns (latencies ms, wall s)."""
+        tickets = [None] * R
+        lat = np.zeros(R)
+        failed = [0]
+
+        def waiter():
+            for i in range(R):
+                while tickets[i] is None:
+                    time.sleep(2e-5)
+                st, q, s, _ = srv.wait(tickets[i], check=False)
+                lat[i] = q + s
+                failed[0] += st != 0
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        t0 = time.perf_counter()
+        for i in range(R):
+            target = t0 + arrivals[i]
+            while True:
+                d = target - time.perf_counter()
+                if d <= 0:
+                    break
+                time.sleep(min(d, 5e-4) if d > 1e-3 else 0)
+            tickets[i] = srv.submit(int(ops[i]), items[i])
+        th.join()
+        torch.cuda.synchronize()
+        if failed[0]:
+            raise RuntimeError(f"{failed[0]} of {R} requests failed")
+        return lat, time.perf_counter() - t0
+
+    run(np.zeros(R))   # warm-up: the resident arenas reach their sizes
+    lat0, wall0 = run(np.zeros(R))
+    capacity = R / wall0
+    loads = []
+    for f in (0.5, 0.8, 0.95):
+        lam = f * capacity
+        arr = np.cumsum(np.random.default_rng(5).exponential(1.0 / lam, size=R))
+        lat, wall = run(arr)
+        loads.append({"load": f, "offered_rps": round(lam, 1), "achieved_rps": round(R / wall, 1),
+                      "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                      "mean_ms": round(float(lat.mean()), 3)})
+    srv.close()
+    return {
+        "metric": "serving capacity (requests/s), mixed compress/decompress", "value": round(capacity, 1),
+        "unit": "requests/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": round(wall0 * 1e3, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 quantize, u32 codes, u8 rANS", "data": "synthetic (seeded)",
+        "config": {"workload": "serving mix: 48-frame pool, N log-uniform 1e3..8e6, 70% f32 / 30% f64, "
+                               "50% compress / 50% decompress", "requests": R, "workers": args.workers,
+                   "memory_budget_gb": 40, "timing": "server-stamped queueing + service time per request; "
+                                                     "capacity = requests / wall time with all queued at once"},
+        "capacity_gbs": round(raw_total / wall0 / 1e9, 3),
+        "saturated": {"p50_ms": round(float(np.percentile(lat0, 50)), 3),
+                      "p99_ms": round(float(np.percentile(lat0, 99)), 3)},
+        "loads": loads,
+    }
+
+
 _REF_JOB = None
 
 
@@ -457,7 +571,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="blobs", choices=["blobs", "column", "trajectory", "batch"])
+    ap.add_argument("--config", default="blobs", choices=["blobs", "column", "trajectory", "batch", "serve"])
+    ap.add_argument("--requests", type=int, default=20000, help="requests of the serving run (--config serve)")
     ap.add_argument("--workers", type=int, default=8, help="contexts of the batch path (--config batch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--once", action="store_true",
@@ -476,6 +591,10 @@ def main():
     if args.config == "batch":
         if rank == 0:
             print(json.dumps(run_batch_bench(args)))
+        return
+    if args.config == "serve":
+        if rank == 0:
+            print(json.dumps(run_serve_bench(args)))
         return
     if world > 1:
         import datetime

@@ -32,7 +32,8 @@ EXPORTS = ("chain_ctx_create", "chain_ctx_destroy", "chain_last_error_message", 
            "chain_compress", "chain_result_copy", "chain_result_device_ptr", "chain_peek", "chain_decompress",
            "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count",
            "chain_decompress_noalloc", "chain_batch_create", "chain_batch_destroy", "chain_batch_compress",
-           "chain_batch_decompress")
+           "chain_batch_decompress", "chain_server_create", "chain_server_destroy", "chain_server_submit",
+           "chain_server_wait")
 
 
 class ChainError(RuntimeError):
@@ -86,9 +87,15 @@ def load() -> ctypes.CDLL:
         L.chain_batch_destroy.restype = None
         L.chain_batch_compress.argtypes = [P, ctypes.POINTER(BatchItem), sz, ctypes.POINTER(ChainOpts)]
         L.chain_batch_decompress.argtypes = [P, ctypes.POINTER(BatchItem), sz]
+        L.chain_server_create.argtypes = [i32, i32, sz, ctypes.POINTER(ChainOpts), ctypes.POINTER(P)]
+        L.chain_server_destroy.argtypes = [P]
+        L.chain_server_destroy.restype = None
+        L.chain_server_submit.argtypes = [P, i32, ctypes.POINTER(BatchItem), ctypes.POINTER(u64)]
+        L.chain_server_wait.argtypes = [P, u64, ctypes.POINTER(dbl), ctypes.POINTER(dbl)]
         for f in ("chain_ctx_create", "chain_compress", "chain_result_copy", "chain_peek", "chain_decompress",
                   "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_decompress_noalloc",
-                  "chain_batch_create", "chain_batch_compress", "chain_batch_decompress"):
+                  "chain_batch_create", "chain_batch_compress", "chain_batch_decompress", "chain_server_create",
+                  "chain_server_submit", "chain_server_wait"):
             getattr(L, f).restype = ctypes.c_int
         L.chain_launch_count.restype = ctypes.c_uint64
         _LIB = L
@@ -290,6 +297,47 @@ class Batch:
                                    output=out.ctypes.data, output_capacity=out.nbytes))
         self.decompress_items(items)
         return outs
+
+
+class Server:
+    """chain_server: FIFO admission of compress (op 0) / decompress (op 1) requests onto
+    `workers` resident contexts under a device-memory budget."""
+
+    COMPRESS, DECOMPRESS = 0, 1
+
+    def __init__(self, device: int = 0, workers: int = 8, memory_budget_bytes: int = 40 << 30):
+        self.L = load()
+        h = ctypes.c_void_p()
+        _check(self.L.chain_server_create(device, workers, memory_budget_bytes, None, ctypes.byref(h)))
+        self.h = h
+        self._items = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.chain_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, op: int, item: BatchItem) -> int:
+        """The item (and the buffers it points to) must stay alive until wait()."""
+        t = ctypes.c_uint64()
+        _check(self.L.chain_server_submit(self.h, op, ctypes.byref(item), ctypes.byref(t)))
+        self._items[t.value] = item
+        return t.value
+
+    def wait(self, ticket: int, check: bool = True):
+        """-> (status, queue_ms, service_ms, item)"""
+        q, s = ctypes.c_double(), ctypes.c_double()
+        st = self.L.chain_server_wait(self.h, ticket, ctypes.byref(q), ctypes.byref(s))
+        item = self._items.pop(ticket, None)
+        if check:
+            _check(st)
+        return st, q.value, s.value, item
 
 
 def launch_count() -> int:

@@ -914,11 +914,13 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states, d_states_first); count_launch();
         T.mark("tables", stream);
         rans_plan_smem(jobs, true);
-        {  // per device, cheap; set on every call
+        if (rans_dec_smem(jobs) > kRansDecSmemMax)
+            return set_err(CHAIN_ERR_DEVICE, "internal: rANS decoder shared memory above its fixed maximum");
+        {  // per device, cheap; set on every call, always to the same values
             CHAIN_CUDA(cudaFuncSetAttribute(rans_decode_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                             cudaSharedmemCarveoutMaxShared));
             CHAIN_CUDA(cudaFuncSetAttribute(rans_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            static_cast<int>(rans_dec_smem(jobs))));
+                                            static_cast<int>(kRansDecSmemMax)));
         }
         rans_decode_kernel<<<jobs.total_blocks, 32 * kRansWarps, rans_dec_smem(jobs), stream>>>(jobs, &st->err); count_launch();
     }

@@ -1633,11 +1633,13 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     if (jobs.total_blocks) {
         k_enc_symbols<<<dim3(64, jobs.njobs), 256, 0, stream>>>(jobs); count_launch();
         rans_plan_smem(jobs, false);
-        {  // per device, cheap; set on every call
+        if (rans_enc_smem(jobs) > kRansEncSmemMax)
+            return set_err(CHAIN_ERR_DEVICE, "internal: rANS encoder shared memory above its fixed maximum");
+        {  // per device, cheap; set on every call, always to the same values
             CHAIN_CUDA(cudaFuncSetAttribute(rans_encode_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                             cudaSharedmemCarveoutMaxShared));
             CHAIN_CUDA(cudaFuncSetAttribute(rans_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            static_cast<int>(rans_enc_smem(jobs))));
+                                            static_cast<int>(kRansEncSmemMax)));
         }
         rans_encode_kernel<<<jobs.total_blocks, 32 * kRansWarps, rans_enc_smem(jobs), stream>>>(jobs, &st->err); count_launch();
     }

@@ -508,6 +508,14 @@ inline size_t rans_dec_smem(const RansJobs& J) {
     return J.tab_cap * 8ull + J.look_cap * 2ull + kRansWarps * kWindow + 16;   // +16: 3-byte renorm reads
 }
 
+// Largest dynamic shared memory any launch of the two kernels can request.  The kernels'
+// MaxDynamicSharedMemorySize attribute is set to exactly these values: the attribute is
+// global to the process, so contexts used from several threads at once must never set
+// different values (a smaller one set between another thread's set and launch would make
+// that launch fail).
+constexpr size_t kRansEncSmemMax = kSmemEncSyms * 16ull + kRansWarps * 2 * kRansTile * 32 * 4 + kRansWarps * kWindow;
+constexpr size_t kRansDecSmemMax = kSmemTableSyms * 8ull + kSmemLookupSlots * 2ull + kRansWarps * kWindow + 16;
+
 __device__ __forceinline__ int job_of_block(const RansJobs& J) {
     int j = 0;
     while (j + 1 < static_cast<int>(J.njobs) && blockIdx.x >= J.job[j + 1].first_block) ++j;

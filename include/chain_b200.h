@@ -157,6 +157,26 @@ CHAIN_API chain_status chain_batch_compress(chain_batch* batch, chain_batch_item
                                             const chain_opts* opts);
 CHAIN_API chain_status chain_batch_decompress(chain_batch* batch, chain_batch_item* items, size_t count);
 
+/* ---- request server ---------------------------------------------------------------
+ * A server owns `workers` contexts on one device, each driven by its own host thread.
+ * Submitted requests (op 0 = compress, 1 = decompress; the item as for the batch calls,
+ * owned by the caller until chain_server_wait returns) wait in one FIFO queue; a free
+ * worker admits the head request when its estimated device working set fits in
+ * memory_budget_bytes next to the running requests (a request larger than the budget
+ * runs alone).  Contexts, arenas and streams stay resident between requests.
+ * chain_server_wait blocks until the request has finished and returns its status, its
+ * queueing time (submit -> start) and its service time (start -> end), in milliseconds.
+ * Every submitted ticket must be waited for once.  No counterpart in the reference,
+ * which compresses one frame per synchronous call (chain_caller.py:33-40). */
+typedef struct chain_server chain_server;
+CHAIN_API chain_status chain_server_create(int device, int workers, size_t memory_budget_bytes,
+                                           const chain_opts* opts, chain_server** out);
+CHAIN_API void chain_server_destroy(chain_server* server);
+CHAIN_API chain_status chain_server_submit(chain_server* server, int op, chain_batch_item* item,
+                                           uint64_t* ticket);
+CHAIN_API chain_status chain_server_wait(chain_server* server, uint64_t ticket, double* queue_ms,
+                                         double* service_ms);
+
 /* Decompression that allocates nothing, for callers that cannot allocate memory when
  * they decode (a plug-in inside an application that owns the device memory pool or
  * runs under a hard memory cap; a loop that must not pay for cudaMalloc/cudaFree, which

@@ -93,3 +93,23 @@ def test_batch_small_output_buffer(codec, frames):
     assert st == N.CHAIN_ERR_BUFFER_TOO_SMALL
     assert arr[0].output_bytes == len(codec.compress(pts, eb, p, t, layout=N.CHAIN_SOA))
     batch.close()
+
+
+def test_many_small_frames_many_workers(codec):
+    """Contexts used from several threads at once, on frames whose entropy tables (and so
+    the shared memory of their rANS launches) differ widely."""
+    frames = []
+    rng = np.random.default_rng(23)
+    for k in range(64):
+        n = int(rng.integers(1000, 50_000))
+        pts = W.make_frame(n, ("column", "blobs", "uniform")[k % 3], int(rng.integers(0, 2**31 - 1)))
+        frames.append((np.ascontiguousarray(pts.T), W.eb_for(pts, float(10.0 ** -rng.integers(2, 6))), 4, 2))
+    want = [codec.compress(pts, eb, p, t, layout=N.CHAIN_SOA) for pts, eb, p, t in frames]
+    batch = N.Batch(0, workers=8)
+    for _ in range(3):
+        got = batch.compress(frames, layout=N.CHAIN_SOA)
+        assert got == want
+        dec = batch.decompress(got)
+        for g, c in zip(dec, got):
+            assert np.array_equal(g.view(np.uint64), codec.decompress(c).view(np.uint64))
+    batch.close()
