@@ -33,7 +33,7 @@ EXPORTS = ("chain_ctx_create", "chain_ctx_destroy", "chain_last_error_message", 
            "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count",
            "chain_decompress_noalloc", "chain_batch_create", "chain_batch_destroy", "chain_batch_compress",
            "chain_batch_decompress", "chain_server_create", "chain_server_destroy", "chain_server_submit",
-           "chain_server_wait")
+           "chain_server_wait", "chain_transcode_lcp2")
 
 
 class ChainError(RuntimeError):
@@ -92,10 +92,11 @@ def load() -> ctypes.CDLL:
         L.chain_server_destroy.restype = None
         L.chain_server_submit.argtypes = [P, i32, ctypes.POINTER(BatchItem), ctypes.POINTER(u64)]
         L.chain_server_wait.argtypes = [P, u64, ctypes.POINTER(dbl), ctypes.POINTER(dbl)]
+        L.chain_transcode_lcp2.argtypes = [P, sz, P, sz, ctypes.POINTER(sz)]
         for f in ("chain_ctx_create", "chain_compress", "chain_result_copy", "chain_peek", "chain_decompress",
                   "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_decompress_noalloc",
                   "chain_batch_create", "chain_batch_compress", "chain_batch_decompress", "chain_server_create",
-                  "chain_server_submit", "chain_server_wait"):
+                  "chain_server_submit", "chain_server_wait", "chain_transcode_lcp2"):
             getattr(L, f).restype = ctypes.c_int
         L.chain_launch_count.restype = ctypes.c_uint64
         _LIB = L
@@ -338,6 +339,19 @@ class Server:
         if check:
             _check(st)
         return st, q.value, s.value, item
+
+
+def transcode_lcp2(data: bytes) -> bytes:
+    """LCG2 container -> the reference CPU Chain's LCP2 bitstream (chain_transcode_lcp2)."""
+    L = load()
+    src = np.frombuffer(data, np.uint8)
+    need = ctypes.c_size_t()
+    st = L.chain_transcode_lcp2(src.ctypes.data, src.nbytes, None, 0, ctypes.byref(need))
+    if st not in (CHAIN_OK, CHAIN_ERR_BUFFER_TOO_SMALL):
+        _check(st)
+    out = np.empty(max(1, need.value), np.uint8)
+    _check(L.chain_transcode_lcp2(src.ctypes.data, src.nbytes, out.ctypes.data, out.nbytes, ctypes.byref(need)))
+    return out[: need.value].tobytes()
 
 
 def launch_count() -> int:

@@ -32,7 +32,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
                      "-ftz=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
                      "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
-LIB_SOURCES = ["capi.cu", "encode.cu", "decode.cu", "noalloc.cu", "batch.cu", "server.cu"]
+LIB_SOURCES = ["capi.cu", "encode.cu", "decode.cu", "noalloc.cu", "batch.cu", "server.cu", "transcode.cu"]
 HEADERS = ["chain_common.cuh", "chain_format.h", "ctx.h", "radix_sort.cuh", "rans.cuh", "scan.cuh"]
 LIB = PKG / "libchain_b200.so"
 PYMODS = {"lcps_gpu_cpp": "pymod_compress.cpp", "lcps_gpu_decompress_ans": "pymod_decompress.cpp"}

@@ -157,6 +157,17 @@ CHAIN_API chain_status chain_batch_compress(chain_batch* batch, chain_batch_item
                                             const chain_opts* opts);
 CHAIN_API chain_status chain_batch_decompress(chain_batch* batch, chain_batch_item* items, size_t count);
 
+/* Rewrites an LCG2 container as the reference CPU Chain's LCP2 bitstream, which the
+ * reference decoder (lcps_cpu_decompress.lcps_decompress_serial, chain_caller.py:23-30)
+ * reads directly and decodes to the same points.  Host buffers only; no GPU is used.
+ * Components become RVMX (values below 2^18) or RTG4 and the exact corrections a Zstd
+ * frame of stored blocks, so the result is larger than the reference's own output.
+ * With out == NULL or too small a capacity it returns CHAIN_ERR_BUFFER_TOO_SMALL and
+ * the needed size in *out_len.  Replaces nothing in the reference (its GPU output,
+ * LCG2 v1, has no LCP2 conversion); it is the on-disk bridge between the two formats. */
+CHAIN_API chain_status chain_transcode_lcp2(const void* container, size_t len, void* out, size_t capacity,
+                                            size_t* out_len);
+
 /* ---- request server ---------------------------------------------------------------
  * A server owns `workers` contexts on one device, each driven by its own host thread.
  * Submitted requests (op 0 = compress, 1 = decompress; the item as for the batch calls,
