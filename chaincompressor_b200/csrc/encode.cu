@@ -356,8 +356,9 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
 }
 
 // ------------------------------------------------------------------- level 1
-// One thread per sorted position: the sorted neighbour with an equal key is the next
-// point of the same block (stable sort keeps indices increasing within a block).
+// Sorted position k: the sorted neighbour with an equal key is the next point of the
+// same block (stable sort keeps indices increasing within a block).  Each thread takes
+// four consecutive positions and loads them, and the fifth neighbour, before using any.
 template <typename KT>
 __global__ void __launch_bounds__(256)
 k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_t n, const EncState* st,
@@ -365,24 +366,35 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
     const int D = static_cast<int>(st->dims);
     const int64_t maxb_bits = st->maxb_bits;
     const int64_t thr = st->threshold;
-    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
-         k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const KT key = skey[k];
-        const uint32_t i = sidx[k];
-        uint32_t out = 0;
-        if (k + 1 < n && skey[k + 1] == key) {
-            const uint32_t dist = sidx[k + 1] - i;
-            // bit j of block coordinate d sits at key bit j * D + d, so the widest
-            // coordinate of the block has ceil(bitlen(key) / D) bits
-            const int local_bits = (bitlen64(static_cast<uint64_t>(key)) + D - 1) / D;
-            const int tag_bits = bitlen32(static_cast<uint32_t>(local_bits));
-            const int64_t a = static_cast<int64_t>(local_bits) * D + tag_bits;
-            const int64_t c = static_cast<int64_t>(D) * maxb_bits;
-            const int64_t smaller = a < c ? a : c;
-            const int dl = bitlen32(dist);
-            if (static_cast<int64_t>(dl + bitlen32(static_cast<uint32_t>(dl))) < smaller - thr) out = dist;
+    const int64_t c = static_cast<int64_t>(D) * maxb_bits;
+    const uint64_t ng = (n + 3) / 4;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < ng;
+         g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        KT key[5];
+        uint32_t idx[5];
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+            const uint64_t k = 4 * g + j;
+            key[j] = k < n ? skey[k] : KT(0);
+            idx[j] = k < n ? sidx[k] : 0u;
         }
-        idrel[i] = out;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint64_t k = 4 * g + j;
+            uint32_t out = 0;
+            if (k + 1 < n && key[j + 1] == key[j]) {
+                const uint32_t dist = idx[j + 1] - idx[j];
+                // bit j of block coordinate d sits at key bit j * D + d, so the widest
+                // coordinate of the block has ceil(bitlen(key) / D) bits
+                const int local_bits = (bitlen64(static_cast<uint64_t>(key[j])) + D - 1) / D;
+                const int tag_bits = bitlen32(static_cast<uint32_t>(local_bits));
+                const int64_t a = static_cast<int64_t>(local_bits) * D + tag_bits;
+                const int64_t smaller = a < c ? a : c;
+                const int dl = bitlen32(dist);
+                if (static_cast<int64_t>(dl + bitlen32(static_cast<uint32_t>(dl))) < smaller - thr) out = dist;
+            }
+            if (k < n) idrel[idx[j]] = out;
+        }
     }
 }
 

@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(kFlagThreads) flag_apply_kernel(Pred pred, Out
     uint32_t run = tile_prefix[blockIdx.x];
     for (int w = 0; w < warp; ++w) run += wsum[w];
     const uint32_t lt = lanemask_lt();
-#pragma unroll
+#pragma unroll 4
     for (int k = 0; k < kFlagItems; ++k) {
         const uint64_t i = base + 32 * k + lane;
         if (i < n) out(i, run + __popc(m[k] & lt), (m[k] >> lane) & 1u);
