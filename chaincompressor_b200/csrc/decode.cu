@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(32 * kUnpackWarps) k_unpack_fixed(const uint8_
                                                                      const CompPlan* cp, uint32_t* out,
                                                                      DecState* st, uint32_t G) {
     __shared__ uint64_t s_byte[kMaxDims], s_min[kMaxDims];
-    __shared__ uint32_t s_w[kMaxDims], s_pre[kMaxDims + 1];
+    __shared__ uint32_t s_w[kMaxDims], s_pre[kMaxDims + 1], s_fits[kMaxDims];
     __shared__ __align__(16) uint32_t wbuf[kUnpackWarps][kUnpackWords];
     __shared__ __align__(16) uint32_t stage[kUnpackWarps][kUnpackWords];
     const uint32_t D = cp->dims;
@@ -163,6 +163,8 @@ __global__ void __launch_bounds__(32 * kUnpackWarps) k_unpack_fixed(const uint8_
         s_byte[threadIdx.x] = cp->packed_off[threadIdx.x];
         s_min[threadIdx.x] = cp->minv[threadIdx.x];
         s_w[threadIdx.x] = cp->width[threadIdx.x];
+        // every value of this dimension fits 32 bits: no per-value check needed
+        s_fits[threadIdx.x] = cp->minv[threadIdx.x] + ((1ull << cp->width[threadIdx.x]) - 1) <= 0xffffffffull;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -187,20 +189,21 @@ __global__ void __launch_bounds__(32 * kUnpackWarps) k_unpack_fixed(const uint8_
             for (uint32_t j = lane; j < nw; j += 32) wb[s_pre[d] + j] = load_be32(data, len, base + 4 * j);
         }
         __syncwarp();
-        for (uint32_t g = 0; g < G; ++g) {
-            const uint32_t rec = g * 32 + lane;
-            for (uint32_t d = 0; d < D; ++d) {
-                const uint32_t w = s_w[d];
+        for (uint32_t d = 0; d < D; ++d) {
+            const uint32_t w = s_w[d], pre = s_pre[d], nw = G * w;
+            const uint32_t mn = static_cast<uint32_t>(s_min[d]);
+            const bool fits = s_fits[d];
+            for (uint32_t g = 0; g < G; ++g) {
+                const uint32_t rec = g * 32 + lane;
                 uint32_t val = 0;
                 if (w) {
-                    const uint32_t bit = rec * w, j = bit >> 5, o = bit & 31;
-                    const uint32_t hi = wb[s_pre[d] + j];
-                    const uint32_t lo = j + 1 < G * w ? wb[s_pre[d] + j + 1] : 0u;
-                    val = static_cast<uint32_t>((((static_cast<uint64_t>(hi) << 32) | lo) << o) >> (64 - w));
+                    const uint32_t bit = rec * w, j = bit >> 5;
+                    const uint32_t hi = wb[pre + j];
+                    const uint32_t lo = j + 1 < nw ? wb[pre + j + 1] : 0u;
+                    val = __funnelshift_l(lo, hi, bit & 31) >> (32 - w);
                 }
-                const uint64_t v = s_min[d] + val;
-                bad = bad || (rec < nr && v > 0xffffffffull);
-                sg[rec * D + d] = static_cast<uint32_t>(v);
+                if (!fits) bad = bad || (rec < nr && s_min[d] + val > 0xffffffffull);
+                sg[rec * D + d] = mn + val;
             }
         }
         __syncwarp();
@@ -508,7 +511,7 @@ struct ZeroRankOut {
 // interleaving is correct.  A point stops after kResolveHops hops; any point left
 // unresolved sets *pending, and the k_jump rounds finish the work.
 constexpr int kResolveHops = 64;
-constexpr int kResolvePer = 4;
+constexpr int kResolvePer = 8;
 __global__ void __launch_bounds__(256) k_resolve(uint32_t* parent, const uint32_t* chained, const uint32_t* zeros,
                                                   uint64_t n, unsigned long long* next, uint32_t* pending) {
     const uint64_t m = n - *zeros;
