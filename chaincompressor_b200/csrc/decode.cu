@@ -380,8 +380,12 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_tail(L2Geo g, L2Vec* tile_
         const uint64_t rank = run + __popc(m[k] & lt);
         if (((m[k] >> lane) & 1u) && static_cast<int>(r) > tl) {
 #pragma unroll
-            for (uint32_t kk = 0; kk < 3; ++kk)
-                if (g.d0 + kk < g.D) acc[kk] += g.diff_term(rank, kk, bad);
+            for (uint32_t kk = 0; kk < 3; ++kk) {
+                if (g.d0 + kk < g.D) {
+                    acc[kk] += g.diff_term(rank, kk, bad);   // terms < range: one subtraction keeps acc < range
+                    if (acc[kk] >= g.range) acc[kk] -= g.range;
+                }
+            }
         }
         if (static_cast<int>(r) == tl) {
 #pragma unroll
@@ -392,7 +396,7 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_tail(L2Geo g, L2Vec* tile_
     }
 #pragma unroll
     for (int kk = 0; kk < 3; ++kk) {
-        unsigned long long a = warp_sum(acc[kk] % g.range);   // < 32 * 2^32
+        unsigned long long a = warp_sum(acc[kk]);   // < 32 * 2^32
         if (lane == 0) s_sum[warp][kk] = a % g.range;
     }
     __syncthreads();
@@ -410,60 +414,97 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_tail(L2Geo g, L2Vec* tile_
 }
 
 // The reset-scan proper: every record's offset from wrap_min, seeded with the tile's
-// exclusive prefix; writes compact[j * D + d0 + kk] = wrap_min + offset.  Also checks
-// the choice values (lcps_cpp.cpp:1899-1900, 1911-1912) and the value ranges.
+// exclusive prefix; writes compact[j * D + d0 + kk] = wrap_min + offset.  Blocked
+// layout: lane l of warp w owns the kL2Rounds consecutive records starting at
+// tile + w * 32 * kL2Rounds + l * kL2Rounds, combines them in order, and one warp scan
+// of the lane aggregates (then the CTA's warp totals and the tile prefix) seeds them.
+// Also checks the choice values (lcps_cpp.cpp:1899-1900, 1911-1912) and the value ranges.
 __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec* tile_prefix, uint32_t* compact,
                                                              DecState* st) {
+    constexpr int P = kL2Rounds;   // records per lane
     __shared__ uint32_t s_cnt[kL2Warps];
     __shared__ L2Vec s_tot[kL2Warps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile;
-    const uint32_t wbase = warp * 32 * kL2Rounds;
+    const uint64_t j0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * P +
+                        static_cast<uint64_t>(lane) * P;
     const ResetAddOp op{static_cast<uint32_t>(g.range), static_cast<uint32_t>(g.range >> 32)};
-    uint32_t m[kL2Rounds];
-    const uint32_t off = g.ranks(m, s_cnt);
-    bool bad = false;
-    L2Vec incl[kL2Rounds];
-    L2Vec wtot = ResetAddOp::identity();
-    uint32_t run = off;
-    const uint32_t lt = lanemask_lt();
+    uint32_t c[P];
+    if (j0 + P <= g.B && (reinterpret_cast<uintptr_t>(g.choice2 + j0) & 15) == 0) {
+        const uint4* q = reinterpret_cast<const uint4*>(g.choice2 + j0);
 #pragma unroll
-    for (int k = 0; k < kL2Rounds; ++k) {
-        const uint64_t j = tile0 + wbase + 32 * k + lane;
-        const uint64_t rank = run + __popc(m[k] & lt);
-        L2Vec t = ResetAddOp::identity();
-        if (j < g.B) {
-            const uint32_t c = g.choice2[j];
-            bad = bad || c > 1 || (j == 0 && c != 0);
-            if ((m[k] >> lane) & 1u) {
-#pragma unroll
-                for (uint32_t kk = 0; kk < 3; ++kk)
-                    if (g.d0 + kk < g.D) t.v[kk] = g.diff_term(rank, kk, bad);
-            } else {
-                t.restart = 1;
-#pragma unroll
-                for (uint32_t kk = 0; kk < 3; ++kk)
-                    if (g.d0 + kk < g.D) t.v[kk] = g.keep_value(j - rank, kk, bad);
-            }
+        for (int v = 0; v < P / 4; ++v) {
+            const uint4 w4 = __ldg(q + v);
+            c[4 * v] = w4.x; c[4 * v + 1] = w4.y; c[4 * v + 2] = w4.z; c[4 * v + 3] = w4.w;
         }
-        incl[k] = warp_inclusive_scan_op(t, op);
-        wtot = op(wtot, shfl_idx_any(incl[k], 31));
-        run += __popc(m[k]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < P; ++k) c[k] = j0 + k < g.B ? g.choice2[j0 + k] : 0u;
     }
-    if (lane == 0) s_tot[warp] = wtot;
+    bool bad = false;
+    uint32_t dmask = 0;
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+        const uint64_t j = j0 + k;
+        if (j < g.B) {
+            bad = bad || c[k] > 1 || (j == 0 && c[k] != 0);
+            if (c[k]) dmask |= 1u << k;
+        }
+    }
+    const uint32_t cnt = __popc(dmask);
+    const uint32_t incl_cnt = warp_inclusive_sum(cnt);
+    if (lane == 31) s_cnt[warp] = incl_cnt;
+    __syncthreads();
+    uint64_t rank = g.tile_diff[blockIdx.x] + incl_cnt - cnt;   // diff records before j0
+    for (int w = 0; w < warp; ++w) rank += s_cnt[w];
+    L2Vec t[P];
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+        const uint64_t j = j0 + k;
+        t[k] = ResetAddOp::identity();
+        if (j >= g.B) continue;
+        if ((dmask >> k) & 1u) {
+#pragma unroll
+            for (uint32_t kk = 0; kk < 3; ++kk)
+                if (g.d0 + kk < g.D) t[k].v[kk] = g.diff_term(rank, kk, bad);
+            ++rank;
+        } else {
+            t[k].restart = 1;
+#pragma unroll
+            for (uint32_t kk = 0; kk < 3; ++kk)
+                if (g.d0 + kk < g.D) t[k].v[kk] = g.keep_value(j - rank, kk, bad);
+        }
+    }
+    L2Vec agg = t[0];
+#pragma unroll
+    for (int k = 1; k < P; ++k) agg = op(agg, t[k]);
+    const L2Vec inc = warp_inclusive_scan_op(agg, op);
+    L2Vec exc = shfl_up_any(inc, 1);
+    if (lane == 0) exc = ResetAddOp::identity();
+    if (lane == 31) s_tot[warp] = inc;
     __syncthreads();
     L2Vec carry = tile_prefix[blockIdx.x];
     for (int w = 0; w < warp; ++w) carry = op(carry, s_tot[w]);
+    carry = op(carry, exc);
+    uint32_t o[3 * P];
 #pragma unroll
-    for (int k = 0; k < kL2Rounds; ++k) {
-        const uint64_t j = tile0 + wbase + 32 * k + lane;
-        const L2Vec v = op(carry, incl[k]);
-        if (j < g.B) {
+    for (int k = 0; k < P; ++k) {
+        carry = op(carry, t[k]);
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) o[3 * k + kk] = static_cast<uint32_t>(g.wrap_min + carry.v[kk]);
+    }
+    uint32_t* dst = compact + j0 * g.D;
+    if (g.D == 3 && j0 + P <= g.B && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+        uint4* q = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+        for (int v = 0; v < 3 * P / 4; ++v) q[v] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            if (j0 + k >= g.B) break;
 #pragma unroll
             for (uint32_t kk = 0; kk < 3; ++kk)
-                if (g.d0 + kk < g.D) compact[j * g.D + g.d0 + kk] = static_cast<uint32_t>(g.wrap_min + v.v[kk]);
+                if (g.d0 + kk < g.D) dst[static_cast<uint64_t>(k) * g.D + g.d0 + kk] = o[3 * k + kk];
         }
-        carry = op(carry, shfl_idx_any(incl[k], 31));
     }
     if (__syncthreads_or(bad) && threadIdx.x == 0) set_error(&st->err, kErrCorrupt);
 }
