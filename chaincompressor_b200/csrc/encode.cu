@@ -419,12 +419,37 @@ struct ExplicitOut {
 };
 
 // ------------------------------------------------------------------- level 2
+// Record minimum, maximum and largest per-dimension difference between consecutive
+// records.  Three-dimensional records are read four per thread with 16-byte loads.
 __global__ void __launch_bounds__(256) k_l2_stats(const uint32_t* __restrict__ rec, EncState* st) {
     const uint32_t B = st->B;
     const uint32_t D = st->dims;
     uint32_t mn = 0xffffffffu, mx = 0, md = 0;
-    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < B;
-         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    uint64_t first_scalar = 0;
+    if (D == 3 && (reinterpret_cast<uintptr_t>(rec) & 15) == 0) {
+        const uint64_t ng = B / 4;
+        for (uint64_t g = tid; g < ng; g += nthreads) {
+            uint32_t v[15];   // the previous record, then four records
+            const uint4* q = reinterpret_cast<const uint4*>(rec + 12 * g);
+            const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+            v[3] = a.x; v[4] = a.y; v[5] = a.z; v[6] = a.w; v[7] = b.x; v[8] = b.y;
+            v[9] = b.z; v[10] = b.w; v[11] = c.x; v[12] = c.y; v[13] = c.z; v[14] = c.w;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) v[d] = g ? __ldg(rec + 12 * g - 3 + d) : v[3 + d];
+#pragma unroll
+            for (int k = 3; k < 15; ++k) {
+                mn = v[k] < mn ? v[k] : mn;
+                mx = v[k] > mx ? v[k] : mx;
+                const uint32_t u = v[k - 3];
+                const uint32_t df = v[k] >= u ? v[k] - u : u - v[k];
+                md = df > md ? df : md;
+            }
+        }
+        first_scalar = ng * 4;
+    }
+    for (uint64_t j = first_scalar + tid; j < B; j += nthreads) {
         for (uint32_t d = 0; d < D; ++d) {
             const uint32_t v = rec[j * D + d];
             mn = v < mn ? v : mn;
@@ -481,12 +506,50 @@ struct Level2In {
         return value_bits >= diff_bits ? 1u : 0u;
     }
 };
-// choice2[j] for every record (1 = difference from the previous record).
+// choice2[j] for every record (1 = difference from the previous record).  Three-
+// dimensional records are read four per thread with 16-byte loads (the rule of
+// Level2In, lcps_cpp.cpp:1305-1454, applied in registers).
 __global__ void __launch_bounds__(256) k_l2_choice(Level2In f, uint32_t* choice2) {
-    const uint32_t B = f.st->B;
-    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < B;
-         j += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        choice2[j] = f(j);
+    const EncState* st = f.st;
+    const uint32_t B = st->B, D = st->dims;
+    const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    uint64_t first_scalar = 0;
+    if (f.l2 && D == 3 && ((reinterpret_cast<uintptr_t>(f.rec) | reinterpret_cast<uintptr_t>(choice2)) & 15) == 0) {
+        const uint64_t fvb = 3ull * bitlen32(st->rec_max);
+        const uint64_t fdb = 3ull * bitlen32(st->rec_maxdiff);
+        const uint64_t ng = B / 4;
+        for (uint64_t g = tid; g < ng; g += nthreads) {
+            uint32_t v[15];
+            const uint4* q = reinterpret_cast<const uint4*>(f.rec + 12 * g);
+            const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+            v[3] = a.x; v[4] = a.y; v[5] = a.z; v[6] = a.w; v[7] = b.x; v[8] = b.y;
+            v[9] = b.z; v[10] = b.w; v[11] = c.x; v[12] = c.y; v[13] = c.z; v[14] = c.w;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) v[d] = g ? __ldg(f.rec + 12 * g - 3 + d) : 0u;
+            uint32_t ch[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                uint32_t mv = 0, mdd = 0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const uint32_t x = v[3 + 3 * k + d], u = v[3 * k + d];
+                    mv = x > mv ? x : mv;
+                    const uint32_t df = x >= u ? x - u : u - x;
+                    mdd = df > mdd ? df : mdd;
+                }
+                const int tvw = bitlen32(mv), tdw = bitlen32(mdd);
+                const uint64_t tvb = 3ull * tvw + bitlen32(static_cast<uint32_t>(tvw));
+                const uint64_t tdb = 3ull * tdw + bitlen32(static_cast<uint32_t>(tdw));
+                const uint64_t value_bits = tvb < fvb ? tvb : fvb;
+                const uint64_t diff_bits = tdb > fdb ? tdb : fdb;
+                ch[k] = (4 * g + k == 0) ? 0u : (value_bits >= diff_bits ? 1u : 0u);
+            }
+            *reinterpret_cast<uint4*>(choice2 + 4 * g) = make_uint4(ch[0], ch[1], ch[2], ch[3]);
+        }
+        first_scalar = ng * 4;
+    }
+    for (uint64_t j = first_scalar + tid; j < B; j += nthreads) choice2[j] = f(j);
 }
 struct Level2Flag {
     const uint32_t* choice2;
@@ -598,7 +661,8 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
     __shared__ unsigned long long sbits;
     if (threadIdx.x < kMaxDims) { smin[threadIdx.x] = 0xffffffffu; smax[threadIdx.x] = 0; }
     if (threadIdx.x < 34) stag[threadIdx.x] = 0;
-    for (int t = threadIdx.x; t < kSmemHistBins; t += blockDim.x) sh[t] = 0;
+    constexpr int HB = kSmemHistBins;
+    for (int t = threadIdx.x; t < HB; t += blockDim.x) sh[t] = 0;
     if (threadIdx.x == 0) sbits = 0;
     __syncthreads();
     uint32_t* gh = hist + hist_stride * s;
@@ -617,7 +681,7 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
         const uint32_t w = bitlen32(v);
         tag = w > tag ? w : tag;
         if (v < 8) vc.add(v);
-        else if (v < kSmemHistBins) atomicAdd(&sh[v], 1u);
+        else if (v < HB) atomicAdd(&sh[v], 1u);
         else if (v < kRansMaxAlphabet) atomicAdd(&gh[v], 1u);
     };
     auto record_done = [&](uint32_t tag) {
@@ -687,7 +751,7 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
         atomicMax(&gs.maxtag, threadIdx.x);
     }
     if (threadIdx.x == 0 && sbits) atomicAdd(reinterpret_cast<unsigned long long*>(&gs.tag_bits), sbits);
-    for (int t = threadIdx.x; t < kSmemHistBins; t += blockDim.x)
+    for (int t = threadIdx.x; t < HB; t += blockDim.x)
         if (sh[t]) atomicAdd(&gh[t], sh[t]);
 }
 
@@ -1279,11 +1343,12 @@ static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, u
     const unsigned g = grid_for((max_records + 3) / 4, 256, 148u * 4u);
     if (n1) { k_stream_stats<1><<<dim3(g, n1), 256, 0, stream>>>(refs, st, hist, hist_stride, one); count_launch(); }
     if (nd) {
+        constexpr size_t smem = 0;
         switch (dims) {
-            case 2: k_stream_stats<2><<<dim3(g, nd), 256, 0, stream>>>(refs, st, hist, hist_stride, many); break;
-            case 3: k_stream_stats<3><<<dim3(g, nd), 256, 0, stream>>>(refs, st, hist, hist_stride, many); break;
-            case 4: k_stream_stats<4><<<dim3(g, nd), 256, 0, stream>>>(refs, st, hist, hist_stride, many); break;
-            default: k_stream_stats<0><<<dim3(g, nd), 256, 0, stream>>>(refs, st, hist, hist_stride, many); break;
+            case 2: k_stream_stats<2><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many); break;
+            case 3: k_stream_stats<3><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many); break;
+            case 4: k_stream_stats<4><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many); break;
+            default: k_stream_stats<0><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many); break;
         }
         count_launch();
     }
