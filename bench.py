@@ -110,6 +110,17 @@ class Clocks:
                 "samples": len(rows)}
 
 
+def max_over_ranks(values, device="cpu"):
+    """Element-wise maximum of per-rank timings over the process group (the job's time
+    is its slowest rank's).  Every rank calls it once, in the same place."""
+    import torch
+    import torch.distributed as tdist
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def _profile_traffic(kernel: str):
     """dram read+write bytes per launch of `kernel` from the committed ncu summary."""
     for f in sorted((ROOT / "profiles").glob("*.md")):
@@ -217,9 +228,7 @@ def run_ours(args, rank: int, world: int):
     t_de, _, _ = timed(lambda: decomp(cont_host.data_ptr(), out_host.data_ptr()))
     clk = clocks.stop()
     if dist:
-        tt = torch.tensor([t_c, t_d, t_ce, t_de], dtype=torch.float64, device=f"cuda:{dev}")
-        tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
-        t_c, t_d, t_ce, t_de = tt.tolist()
+        t_c, t_d, t_ce, t_de = max_over_ranks([t_c, t_d, t_ce, t_de], f"cuda:{dev}")
     dec = out_host.numpy()
     err = float(np.abs(dec - pts.astype(np.float64)).max())
 
