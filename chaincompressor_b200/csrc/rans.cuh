@@ -182,25 +182,26 @@ __device__ inline void build_rans_table(const uint32_t* __restrict__ hist, uint3
         }
     }
     __syncthreads();
-    // cumulative frequencies (exclusive prefix) and the cost estimate
-    uint64_t carry = 0;
+    // cumulative frequencies (exclusive prefix) and the cost estimate: each thread takes
+    // a contiguous run of symbols, one block scan gives the runs' offsets
     double cost = 0.0;
     uint64_t tbytes = 0;
-    for (uint32_t base = 0; base < A; base += blockDim.x) {
-        const uint32_t s = base + threadIdx.x;
-        const uint64_t p = s < A ? prob[s] : 0;
-        uint64_t tot;
-        const uint64_t ex = block_exclusive_sum(p, red, &tot);
-        if (s < A) {
-            cum[s] = static_cast<uint32_t>(carry + ex);
-            if (p) {
-                cost += static_cast<double>(hist[s]) * (static_cast<double>(prec) - log2(static_cast<double>(p)));
-                tbytes += rans_token_bytes(static_cast<uint32_t>(p));
-            } else if (s == 0 || prob[s - 1] != 0) {
-                tbytes += 1;  // start of a zero run (runs longer than 64 are counted below)
-            }
+    const uint32_t per = (A + blockDim.x - 1) / blockDim.x;
+    const uint32_t s0 = threadIdx.x * per, s1 = min(A, s0 + per);
+    uint64_t run = 0;
+    for (uint32_t s = s0; s < s1; ++s) run += prob[s];
+    uint64_t carry;
+    uint64_t c = block_exclusive_sum(run, red, &carry);
+    for (uint32_t s = s0; s < s1; ++s) {
+        const uint64_t p = prob[s];
+        cum[s] = static_cast<uint32_t>(c);
+        c += p;
+        if (p) {
+            cost += static_cast<double>(hist[s]) * (static_cast<double>(prec) - log2(static_cast<double>(p)));
+            tbytes += rans_token_bytes(static_cast<uint32_t>(p));
+        } else if (s == 0 || prob[s - 1] != 0) {
+            tbytes += 1;  // start of a zero run (runs longer than 64 are counted below)
         }
-        carry += tot;
     }
     uint64_t zeros = 0;
     for (uint32_t s = threadIdx.x; s < A; s += blockDim.x) zeros += prob[s] == 0;
@@ -411,17 +412,19 @@ __device__ inline bool parse_table_block(const uint8_t* in, uint32_t len, uint32
     }
     __syncthreads();
     if (!s_ok) return false;
-    // cumulative table and total
-    carry = 0;
-    for (uint32_t base = 0; base < A; base += blockDim.x) {
-        const uint32_t s = base + threadIdx.x;
-        const uint64_t p = s < A ? prob[s] : 0;
-        uint64_t tot;
-        const uint64_t e = block_exclusive_sum(p, sscratch, &tot);
-        if (s < A) cum[s] = static_cast<uint32_t>(carry + e > 0xffffffffull ? 0xffffffffu : carry + e);
-        carry += tot;
+    // cumulative table and total: each thread sums a contiguous run of symbols, one
+    // block scan gives the runs' offsets
+    const uint32_t per = (A + blockDim.x - 1) / blockDim.x;
+    const uint32_t s0 = threadIdx.x * per, s1 = min(A, s0 + per);
+    uint64_t run = 0;
+    for (uint32_t s = s0; s < s1; ++s) run += prob[s];
+    uint64_t total;
+    uint64_t c = block_exclusive_sum(run, sscratch, &total);
+    for (uint32_t s = s0; s < s1; ++s) {
+        cum[s] = static_cast<uint32_t>(c > 0xffffffffull ? 0xffffffffu : c);
+        c += prob[s];
     }
-    return carry == M;
+    return total == M;
 }
 
 // ----------------------------------------------------------------------------- coding
