@@ -1542,12 +1542,14 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         const uint64_t nc = hs->ncorr;
         const int bits = std::max(1, bitlen64(nd - 1));
         uint32_t* scan32b = reinterpret_cast<uint32_t*>(scanbuf);
-        bool in_b = radix_sort_pairs<uint64_t>(corr_idx, key_a, val_a, key_b, val_b, nc, bits, counts, scan32b, stream);
+        // flat indices are unique, and equal values need no order for the dictionary,
+        // so the small unstable sort serves both sorts here
+        bool in_b = sort_pairs<uint64_t>(corr_idx, key_a, val_a, key_b, val_b, nc, bits, counts, scan32b, stream);
         k_gather_corrections<<<grid_for(nc), 256, 0, stream>>>(in_b ? val_b : val_a, in_b ? key_b : key_a, corr_val,
                                                                corr_idx_s, corr_val_s, nc); count_launch();
         k_corr_gaps<<<grid_for(nc), 256, 0, stream>>>(corr_idx_s, nc, corr_gaps); count_launch();
         const uint64_t* vbits = reinterpret_cast<const uint64_t*>(corr_val_s);
-        in_b = radix_sort_pairs<uint64_t>(vbits, key_a, val_a, key_b, val_b, nc, 64, counts, scan32b, stream);
+        in_b = sort_pairs<uint64_t>(vbits, key_a, val_a, key_b, val_b, nc, 64, counts, scan32b, stream);
         device_exclusive_scan<uint32_t>(DictIn{in_b ? key_b : key_a},
                                         DictOut{in_b ? key_b : key_a, in_b ? val_b : val_a, corr_dict, corr_ids}, nc,
                                         scan32b, &st->ndistinct, stream);

@@ -176,4 +176,58 @@ bool radix_sort_pairs(const KT* keys_in, KT* keys_a, uint32_t* vals_a, KT* keys_
     return passes % 2 == 0;
 }
 
+// ------------------------------------------------------------- small sorts
+// Up to kSmallSort (key, index) pairs sorted by one CTA: a bitonic sort in shared
+// memory (keys padded with the largest value).  Not stable: used where keys are unique
+// or where the order of equal keys does not matter.
+constexpr uint32_t kSmallSort = 2048;
+template <typename KT>
+__global__ void __launch_bounds__(1024) small_sort_kernel(const KT* __restrict__ keys_in, KT* __restrict__ keys_out,
+                                                          uint32_t* __restrict__ vals_out, uint32_t n) {
+    __shared__ KT sk[kSmallSort];
+    __shared__ uint32_t sv[kSmallSort];
+    uint32_t n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    for (uint32_t i = threadIdx.x; i < n2; i += blockDim.x) {
+        sk[i] = i < n ? keys_in[i] : static_cast<KT>(~static_cast<KT>(0));
+        sv[i] = i;
+    }
+    __syncthreads();
+    for (uint32_t k = 2; k <= n2; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < n2; i += blockDim.x) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const bool up = (i & k) == 0;
+                    const KT a = sk[i], b = sk[ixj];
+                    if ((a > b) == up) {
+                        sk[i] = b;
+                        sk[ixj] = a;
+                        const uint32_t t = sv[i];
+                        sv[i] = sv[ixj];
+                        sv[ixj] = t;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        keys_out[i] = sk[i];
+        vals_out[i] = sv[i];
+    }
+}
+
+// radix_sort_pairs for any n, except that up to kSmallSort keys are sorted by one CTA
+// (not stable; the result is then in the *_a buffers).
+template <typename KT>
+bool sort_pairs(const KT* keys_in, KT* keys_a, uint32_t* vals_a, KT* keys_b, uint32_t* vals_b, uint64_t n,
+                int key_bits, uint32_t* counts, uint32_t* scan_buf, cudaStream_t stream) {
+    if (n <= kSmallSort) {
+        small_sort_kernel<KT><<<1, 1024, 0, stream>>>(keys_in, keys_a, vals_a, static_cast<uint32_t>(n)); count_launch();
+        return false;
+    }
+    return radix_sort_pairs<KT>(keys_in, keys_a, vals_a, keys_b, vals_b, n, key_bits, counts, scan_buf, stream);
+}
+
 }  // namespace chain

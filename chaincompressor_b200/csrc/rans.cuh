@@ -476,7 +476,7 @@ constexpr uint32_t kSmemEncSyms = 2048;       // encoder entries (16 B) in share
 constexpr uint32_t kSmemLookupSlots = 16384;  // u16 decode lookup in shared memory up to this M
 constexpr uint32_t kWindow = 4096;            // decoder byte window per warp
 constexpr uint32_t kLargeTableMaxSteps = 512; // serial depth of lanes whose tables stay in L2
-constexpr uint64_t kLargeTableMinSymbols = 1ull << 22;  // ... on streams at least this long
+constexpr uint64_t kLargeTableMinSymbols = 1ull << 18;  // ... on streams at least this long
 
 // Decoder slot entry for tables kept in global memory: one load per step gives the
 // symbol, its frequency and slot - cum[symbol].
