@@ -38,8 +38,10 @@
 // rANS section:
 //   u8 prec, u32 alphabet, u32 table_bytes, table tokens (rans.cuh), u64 symbols per
 //   chunk S, u8 lanes W (1..32, S a multiple of W), u32 chunks, u64 payload bytes (the
-//   sum of the chunk bytes), chunks x u32 chunk bytes, chunks x W x u32 final lane
-//   states, then the chunk byte streams back to back.
+//   sum of the chunk bytes), chunks x u32 chunk bytes, the chunks x W final lane states
+//   (chunk-major) packed MSB-first at prec + 10 bits each (a final state lies in
+//   [4 * 2^prec, 1024 * 2^prec)) and padded to a byte, then the chunk byte streams back
+//   to back.
 //   Fixed width 0 means a constant component (every value equals its minimum).
 #pragma once
 
@@ -60,6 +62,12 @@ __host__ __device__ inline void stream_name(int s, char out[4]) {
     const char names[kStreams][4] = {{'I', 'D', 'R', '0'}, {'D', 'I', 'F', '0'}, {'K', 'E', 'P', '0'},
                                      {'C', 'H', '2', '0'}, {'R', 'E', 'L', '0'}};
     for (int i = 0; i < 4; ++i) out[i] = names[s][i];
+}
+
+// Bits of one packed final lane state, and the bytes of a section's packed states.
+__host__ __device__ inline uint32_t state_bits(uint32_t prec) { return prec + 10; }
+__host__ __device__ inline uint64_t state_bytes(uint32_t lanes, uint32_t chunks, uint32_t prec) {
+    return (static_cast<uint64_t>(lanes) * chunks * state_bits(prec) + 7) / 8;
 }
 
 struct SectionPlan {
@@ -180,7 +188,7 @@ __host__ __device__ inline bool parse_section(ByteReader& r, SectionPlan* s, uin
     // the chunk lengths must add up to payload_len; the decoder checks that in parallel
     CHAIN_PARSE_REQUIRE(r.skip(4ull * s->chunks));
     s->states_off = r.pos;
-    CHAIN_PARSE_REQUIRE(r.skip(4ull * s->lanes * s->chunks));
+    CHAIN_PARSE_REQUIRE(r.skip(state_bytes(s->lanes, s->chunks, s->prec)));
     s->payload_off = r.pos;
     CHAIN_PARSE_REQUIRE(r.skip(s->payload_len));
     return true;

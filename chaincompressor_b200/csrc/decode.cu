@@ -106,18 +106,20 @@ __global__ void __launch_bounds__(256) k_lookup(SectionRefs refs, const DecState
     }
 }
 
-// Copies the u32 little-endian state words of every chunk (unaligned in the container).
+// Unpacks the final lane states of every chunk (prec + 10 bits each, MSB-first).
 __global__ void __launch_bounds__(256) k_states(SectionRefs refs, const uint8_t* data, uint32_t* states_base,
                                                  const uint64_t* states_first) {
     const SectionRef R = refs.r[blockIdx.y];
     const SectionPlan& s = *R.sec;
     uint32_t* out = states_base + states_first[blockIdx.y];
     const uint64_t words = static_cast<uint64_t>(s.lanes) * s.chunks;
+    const uint32_t B = state_bits(s.prec);
+    const uint8_t* q = data + s.states_off;
     for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < words;
          w += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint8_t* q = data + s.states_off + 4 * w;
-        out[w] = static_cast<uint32_t>(q[0]) | (static_cast<uint32_t>(q[1]) << 8) | (static_cast<uint32_t>(q[2]) << 16) |
-                 (static_cast<uint32_t>(q[3]) << 24);
+        uint64_t bit = w * B, v = 0;
+        for (uint32_t k = 0; k < B; ++k, ++bit) v = (v << 1) | ((q[bit >> 3] >> (7 - (bit & 7))) & 1u);
+        out[w] = static_cast<uint32_t>(v);
     }
 }
 

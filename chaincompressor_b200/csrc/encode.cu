@@ -773,13 +773,13 @@ __global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncSt
     }
 }
 
-__device__ inline uint64_t section_overhead(uint32_t table_bytes, uint32_t chunks, uint32_t lanes) {
-    return 1 + 4 + 4 + static_cast<uint64_t>(table_bytes) + 8 + 1 + 4 + 8 +
-           static_cast<uint64_t>(chunks) * (4 + 4ull * lanes);
+__device__ inline uint64_t section_overhead(uint32_t table_bytes, uint32_t chunks, uint32_t lanes, uint32_t prec) {
+    return 1 + 4 + 4 + static_cast<uint64_t>(table_bytes) + 8 + 1 + 4 + 8 + 4ull * chunks +
+           state_bytes(lanes, chunks, prec);
 }
 
 // Chunking of a rANS section: enough lanes that each carries about bytes_per_lane
-// coded bytes (the 4-byte final state per lane is the size overhead), and enough that
+// coded bytes (the packed final state per lane is the size overhead), and enough that
 // no lane codes more than max_steps symbols (the serial depth of the kernel).  Below
 // 32 lanes the section is one chunk of W = next power of two lanes.
 __device__ inline void plan_chunks(uint64_t count, double est_payload, uint32_t bytes_per_lane, uint32_t max_steps,
@@ -848,7 +848,7 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
         const RansTableDev& t = st->tag_tab[s];
         const double payload = t.cost_bits / 8.0;
         plan_chunks(nrec, payload, bytes_per_lane, max_steps, &tag_ch, &tag_S, &tag_lanes);
-        c.est[kEncTagged] = 13 + 1 + section_overhead(t.table_bytes, tag_ch, tag_lanes) +
+        c.est[kEncTagged] = 13 + 1 + section_overhead(t.table_bytes, tag_ch, tag_lanes, t.prec) +
                             static_cast<uint64_t>(payload) + 1 + 8 + (g.tag_bits + 7) / 8;
     }
     // raw.  Tables too large for shared memory cost one L2 round trip per coded symbol on
@@ -863,7 +863,7 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
                            nrec * r.dims >= kLargeTableMinSymbols;
         const uint32_t steps = large ? min(max_steps, kLargeTableMaxSteps) : max_steps;
         plan_chunks(nrec * r.dims, payload, bytes_per_lane, steps, &raw_ch, &raw_S, &raw_lanes);
-        c.est[kEncRaw] = 13 + section_overhead(t.table_bytes, raw_ch, raw_lanes) + static_cast<uint64_t>(payload) + 1;
+        c.est[kEncRaw] = 13 + section_overhead(t.table_bytes, raw_ch, raw_lanes, t.prec) + static_cast<uint64_t>(payload) + 1;
     }
     uint8_t best = kEncTagged;
     if (c.est[kEncFixed] < c.est[best]) best = kEncFixed;
@@ -984,6 +984,35 @@ __global__ void __launch_bounds__(32 * kPackWarps) k_pack_fixed(const uint32_t* 
     }
 }
 
+// Final lane states of every rANS section (blockIdx.y = section) packed MSB-first at
+// prec + 10 bits each, as big-endian 32-bit words (so byte 0 holds the first bits).
+struct StatePacks {
+    const uint32_t* in[kCodeStreams];
+    uint32_t* out[kCodeStreams];   // 4-byte aligned; room for whole words
+    uint32_t count[kCodeStreams];
+    uint32_t bits[kCodeStreams];
+};
+__global__ void __launch_bounds__(256) k_pack_states(StatePacks sp) {
+    const int k = blockIdx.y;
+    const uint32_t B = sp.bits[k];
+    const uint64_t count = sp.count[k];
+    const uint64_t nwords = (count * B + 31) / 32;
+    const uint32_t* in = sp.in[k];
+    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < nwords;
+         w += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t b0 = w * 32;
+        uint32_t acc = 0;
+        for (uint64_t i = b0 / B; i < count && i * B < b0 + 32; ++i) {
+            // the state's most significant bit sits `start` bits after the word's
+            const int64_t start = static_cast<int64_t>(i * B) - static_cast<int64_t>(b0);
+            const int64_t shift = 32 - (start + static_cast<int64_t>(B));
+            const uint64_t v = in[i];
+            acc |= shift >= 0 ? static_cast<uint32_t>(v << shift) : static_cast<uint32_t>(v >> (-shift));
+        }
+        sp.out[k][w] = __byte_perm(acc, 0, 0x0123);
+    }
+}
+
 // Encoder symbol entries of every rANS section (blockIdx.y = job).
 __global__ void __launch_bounds__(256) k_enc_symbols(RansJobs J) {
     const RansJob& jb = J.job[blockIdx.y];
@@ -1015,7 +1044,7 @@ struct AssemblyIn {
     const uint8_t* table_bytes;   // [kCodeStreams] x table_stride
     uint64_t table_stride;
     const uint32_t* chunk_len[kCodeStreams];
-    const uint32_t* states[kCodeStreams];
+    const uint8_t* states[kCodeStreams];         // packed final lane states
     const uint8_t* slots[kCodeStreams];
     uint64_t slot_cap[kCodeStreams];
     const uint32_t* chunk_segs[kCodeStreams];    // copy-segment prefix (chunks + 1)
@@ -1125,7 +1154,7 @@ __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* piece
             w.uint(c.sec_chunks, 4);
             w.uint(c.payload_bytes, 8);
             piece(reinterpret_cast<const uint8_t*>(in.chunk_len[s]), 4ull * c.sec_chunks);
-            piece(reinterpret_cast<const uint8_t*>(in.states[s]), 4ull * c.sec_lanes * c.sec_chunks);
+            piece(in.states[s], state_bytes(c.sec_lanes, c.sec_chunks, c.sec_prec));
             chunked(s, c.payload_bytes, in.chunk_segs[s][c.sec_chunks]);
             if (c.enc == kEncTagged) {
                 w.uint(c.packed_bits, 8);
@@ -1608,7 +1637,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         if (c.enc == kEncTagged) bound += 8 + (c.packed_bits + 7) / 8;
     }
     size_t need2 = Arena::need(slots_total, 1) + Arena::need(packed_total, 1) + Arena::need(tags_total + 1, 4) +
-                   Arena::need(total_chunks + 1, 4) + Arena::need(total_chunks * 32 + 1, 4) +
+                   Arena::need(total_chunks + 1, 4) + Arena::need(total_chunks * 32 + 1, 4) * 2 +
                    Arena::need(table_stride * kCodeStreams, 1) + Arena::need(max_pieces, sizeof(Piece)) +
                    Arena::need(bound, 1) + Arena::need(etab_total + 1, 16) + Arena::need(total_chunks + 1, 8) +
                    Arena::need(total_chunks + kCodeStreams + 1, 4) + 11 * 256;
@@ -1619,6 +1648,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     uint32_t* tags = C.take<uint32_t>(tags_total + 1);
     uint32_t* chunk_len = C.take<uint32_t>(total_chunks + 1);
     uint32_t* states = C.take<uint32_t>(total_chunks * 32 + 1);
+    uint32_t* packed_states = C.take<uint32_t>(total_chunks * 32 + 1);   // 128 bytes per chunk
     uint8_t* tables = C.take<uint8_t>(table_stride * kCodeStreams);
     Piece* pieces = C.take<Piece>(max_pieces);
     uint8_t* container = C.take<uint8_t>(bound);
@@ -1631,6 +1661,8 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     uint64_t etab_used = 0;
     if (packed_total) CHAIN_CUDA(cudaMemsetAsync(packed, 0, packed_total, stream));
 
+    StatePacks sp{};
+    int sp_n = 0;
     RansJobs jobs{};
     jobs.njobs = 0;
     uint32_t first = 0;
@@ -1689,7 +1721,12 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
             jb.first_block = first;
             first += (c.sec_chunks + kRansWarps - 1) / kRansWarps;
             ain.chunk_len[s] = jb.chunk_len;
-            ain.states[s] = jb.states;
+            ain.states[s] = reinterpret_cast<const uint8_t*>(packed_states + chunk_base * 32);
+            sp.in[sp_n] = jb.states;
+            sp.out[sp_n] = packed_states + chunk_base * 32;
+            sp.count[sp_n] = c.sec_lanes * c.sec_chunks;
+            sp.bits[sp_n] = state_bits(c.sec_prec);
+            ++sp_n;
             ain.slots[s] = jb.bytes;
             ain.slot_cap[s] = slot_cap[s];
             ChunkMap& cm = maps.m[s];
@@ -1721,6 +1758,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
                                             static_cast<int>(kRansEncSmemMax)));
         }
         rans_encode_kernel<<<jobs.total_blocks, 32 * kRansWarps, rans_enc_smem(jobs), stream>>>(jobs, &st->err); count_launch();
+        k_pack_states<<<dim3(16, sp_n), 256, 0, stream>>>(sp); count_launch();
     }
     CHAIN_LAUNCH_CHECK("entropy coding");
     T.mark("rans_encode", stream);

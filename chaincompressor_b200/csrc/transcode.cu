@@ -39,6 +39,12 @@ struct Fail {
 
 uint32_t le32(const uint8_t* p) { return p[0] | (p[1] << 8) | (p[2] << 16) | (static_cast<uint32_t>(p[3]) << 24); }
 
+uint64_t read_msb(const uint8_t* p, uint64_t bit, uint32_t width) {
+    uint64_t v = 0;
+    for (uint32_t k = 0; k < width; ++k, ++bit) v = (v << 1) | ((p[bit >> 3] >> (7 - (bit & 7))) & 1u);
+    return v;
+}
+
 // Probability table of an LCG2 rANS section (token scheme shared with LCP2).
 std::vector<uint32_t> section_table(const uint8_t* data, const SectionPlan& s) {
     std::vector<uint32_t> prob(s.alphabet, 0);
@@ -86,7 +92,8 @@ std::vector<uint32_t> decode_section(const uint8_t* data, const SectionPlan& s) 
         uint64_t pos = 0;
         uint32_t x[32];
         for (uint32_t l = 0; l < s.lanes; ++l) {
-            x[l] = le32(data + s.states_off + 4ull * (static_cast<uint64_t>(c) * s.lanes + l));
+            const uint32_t B = state_bits(s.prec);
+            x[l] = static_cast<uint32_t>(read_msb(data + s.states_off, (static_cast<uint64_t>(c) * s.lanes + l) * B, B));
             if (x[l] < L || static_cast<uint64_t>(x[l]) >= (static_cast<uint64_t>(L) << 8))
                 throw Fail{"rANS lane state out of range"};
         }
@@ -109,11 +116,6 @@ std::vector<uint32_t> decode_section(const uint8_t* data, const SectionPlan& s) 
     return out;
 }
 
-uint64_t read_msb(const uint8_t* p, uint64_t bit, uint32_t width) {
-    uint64_t v = 0;
-    for (uint32_t k = 0; k < width; ++k, ++bit) v = (v << 1) | ((p[bit >> 3] >> (7 - (bit & 7))) & 1u);
-    return v;
-}
 
 // Record-major values of one component.
 std::vector<uint64_t> decode_component(const uint8_t* data, const CompPlan& c) {

@@ -31,10 +31,11 @@ def _section(r, count):
     lens = struct.unpack("<%dI" % chunks, r.take(4 * chunks))
     if sum(lens) != payload:
         raise ValueError("chunk lengths do not add up to the payload length")
-    r.take(4 * lanes * chunks)
+    state_bytes = (lanes * chunks * (prec + 10) + 7) // 8   # final states, prec + 10 bits each
+    r.take(state_bytes)
     r.take(payload)
     return {"prec": prec, "alphabet": alphabet, "table_bytes": tlen, "S": S, "lanes": lanes, "chunks": chunks,
-            "payload": sum(lens), "symbols": count, "state_bytes": 4 * lanes * chunks}
+            "payload": sum(lens), "symbols": count, "state_bytes": state_bytes}
 
 
 def _component(r, body_len):
