@@ -10,8 +10,8 @@
 // (W = lanes of the section, 1..32; symbol j of a chunk belongs to lane j % W), and
 // the lanes' renormalisation bytes are interleaved in one byte stream per chunk in the
 // exact order the decoding warp consumes them (lane order within a step, most
-// significant byte first).  Small sections use fewer lanes, since each lane stores a
-// 4-byte final state.
+// significant byte first).  Small sections use fewer lanes, since each lane stores its
+// final state (prec + 10 bits).
 //
 // Probability normalisation is this project's own exact-integer scheme (the
 // reference's uses x87 long double): symbols with f_s * M / n < 1 get probability 1,
@@ -429,7 +429,7 @@ __device__ inline bool parse_table_block(const uint8_t* in, uint32_t len, uint32
 
 // ----------------------------------------------------------------------------- coding
 // A rANS section is coded as `chunks` chunks of S symbols (S a multiple of 32; the last
-// chunk may be shorter).  Per chunk: 32 final states and one byte stream.
+// chunk may be shorter).  Per chunk: W final states and one byte stream.
 // Encoder symbol entry (division-free encoding by a precomputed reciprocal, the
 // division-by-invariant-integer method as used in F. Giesen's public-domain rans_byte):
 //   x' = x + bias + q * cmpl_freq,  q = umulhi(x, rcp_freq) >> rcp_shift = floor(x / freq)
@@ -557,6 +557,53 @@ __device__ __forceinline__ void tile_store(uint32_t* buf, const uint32_t (&r)[32
     }
 }
 
+// Encoder entry of symbol s (from shared memory when the table is there).
+template <bool kSmem>
+__device__ __forceinline__ uint4 enc_entry(const uint4* tab, const uint4* etab, uint32_t s) {
+    return kSmem ? tab[s] : __ldg(etab + s);
+}
+
+// One encoding step of a lane with entry e: renormalise (0..3 bytes, written at the
+// warp's descending window position in lane order) and push the symbol.
+__device__ __forceinline__ uint32_t rans_encode_step(uint32_t x, const uint4& e, bool act, uint8_t* ow,
+                                                     uint32_t& rel, uint32_t lt) {
+    const uint32_t xmax = e.x << 10;  // ((L >> prec) << 8) * freq
+    const uint32_t nb = act ? (x >= xmax) + ((x >> 8) >= xmax) + ((x >> 16) >= xmax) : 0u;
+    const uint32_t b0 = __ballot_sync(0xffffffffu, nb & 1u), b1 = __ballot_sync(0xffffffffu, nb & 2u);
+    rel -= __popc(b0) + 2 * __popc(b1);
+    uint8_t* o = ow + rel + __popc(b0 & lt) + 2 * __popc(b1 & lt);
+    if (nb > 0) o[nb - 1] = static_cast<uint8_t>(x);
+    if (nb > 1) o[nb - 2] = static_cast<uint8_t>(x >> 8);
+    if (nb > 2) o[0] = static_cast<uint8_t>(x >> 16);
+    if (act) {
+        x >>= 8 * nb;
+        const uint32_t q = __umulhi(x, e.z) >> (e.w >> 24);
+        x = x + e.y + q * (e.w & 0xffffffu);
+    }
+    return x;
+}
+
+// A full tile (kRansTile steps, every lane active, W == 32), steps in descending order.
+// Symbol entries do not depend on the state, so they are fetched four steps ahead.
+template <bool kSmem>
+__device__ __forceinline__ uint32_t rans_encode_full_tile(uint32_t x, const uint32_t* cur, const uint4* tab,
+                                                          const uint4* etab, uint8_t* ow, uint32_t& rel,
+                                                          uint32_t lt) {
+    const int lane = threadIdx.x & 31;
+    constexpr int kAhead = 4;
+    uint4 pf[kAhead];
+#pragma unroll
+    for (int i = 0; i < kAhead; ++i) pf[i] = enc_entry<kSmem>(tab, etab, cur[(kRansTile - 1 - i) * 32 + lane]);
+#pragma unroll
+    for (int i = 0; i < kRansTile; ++i) {
+        const int j = kRansTile - 1 - i;   // step within the tile
+        const uint4 e = pf[i % kAhead];
+        if (j >= kAhead) pf[i % kAhead] = enc_entry<kSmem>(tab, etab, cur[(j - kAhead) * 32 + lane]);
+        x = rans_encode_step(x, e, true, ow, rel, lt);
+    }
+    return x;
+}
+
 // Encoder: one warp per chunk, kRansWarps chunks of one job per CTA.  The job's table
 // sits in shared memory when small; symbols are prefetched one 32-step tile ahead
 // into shared memory; the warp's byte counts are prefix-summed with two ballots
@@ -564,7 +611,9 @@ __device__ __forceinline__ void tile_store(uint32_t* buf, const uint32_t (&r)[32
 // window; before each group of kRansTile steps, if fewer than a group's worst case
 // (kRansTile * 96 bytes) are free, the window's 16-byte-aligned written part goes to
 // the chunk's slot in global memory with 16-byte stores and the ragged rest (< 16
-// bytes) moves to the window's top.  Offsets are 32-bit (a chunk slot is < 4 GB).
+// bytes) moves to the window's top.  A chunk whose bytes exceed its slot is detected
+// after the group that overflowed, before anything reaches global memory.  Offsets are
+// 32-bit (a chunk slot is < 4 GB).
 static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uint32_t* err) {
     extern __shared__ __align__(16) uint8_t rsm[];
     const RansJob& jb = J.job[job_of_block(J)];
@@ -583,6 +632,7 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
     const uint32_t W = jb.lanes;
     const uint32_t cnt = static_cast<uint32_t>(cend - cbeg);
     const uint32_t steps = (cnt + W - 1) / W;
+    const uint32_t full_steps = W == 32 ? cnt / 32 : 0;   // steps in which every lane codes a symbol
     const uint32_t ntiles = (steps + kRansTile - 1) / kRansTile;
     const uint64_t tile_syms = static_cast<uint64_t>(kRansTile) * W;
     const uint32_t prec = jb.prec;
@@ -592,9 +642,8 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
     uint32_t x = L;
     uint8_t* out = jb.bytes + static_cast<uint64_t>(c) * jb.slot_cap;
     const bool ovec = (reinterpret_cast<uintptr_t>(out) & 15) == 0 && (jb.slot_cap & 15) == 0;
-    uint32_t pos = static_cast<uint32_t>(jb.slot_cap);   // slot offset of the lowest byte written
-    uint32_t wtop = pos;                                  // slot offset of the window's end
-    uint32_t rel = kWindow;                               // window index of `pos`
+    uint32_t wtop = static_cast<uint32_t>(jb.slot_cap);   // slot offset of the window's end
+    uint32_t rel = kWindow;                               // window index of the lowest byte written
     bool overflow = false;
     uint32_t r[32];
     bool vec;
@@ -604,7 +653,7 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
         tile_store(buf + ((ntiles - 1) & 1) * 1024, r, vec);
         __syncwarp();
     }
-    for (int k = static_cast<int>(ntiles) - 1; k >= 0 && !overflow; --k) {
+    for (int k = static_cast<int>(ntiles) - 1; k >= 0; --k) {
         if (k > 0) {
             const uint64_t tb = cbeg + tile_syms * (k - 1);
             tile_load(jb.sym, tb, min(tb + tile_syms, cend), r, vec);
@@ -627,28 +676,22 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
             rel = kWindow - h;
         }
         const uint32_t* cur = buf + (k & 1) * 1024;
-        const int t_hi = min(static_cast<int>(steps) - 1, 32 * k + 31);
-        uint32_t kl = static_cast<uint32_t>(t_hi) * W + lane;   // symbol index within the chunk
-        for (int t = t_hi; t >= 32 * k; --t, kl -= W) {
-            const bool act = static_cast<uint32_t>(lane) < W && kl < cnt;
-            const uint32_t s = act ? cur[(t - 32 * k) * W + lane] : 0u;
-            const uint4 e = smem_tab ? tab[s] : __ldg(jb.etab + s);
-            const uint32_t xmax = e.x << 10;  // ((L >> prec) << 8) * freq
-            const uint32_t nb = act ? (x >= xmax) + ((x >> 8) >= xmax) + ((x >> 16) >= xmax) : 0u;
-            const uint32_t b0 = __ballot_sync(0xffffffffu, nb & 1u), b1 = __ballot_sync(0xffffffffu, nb & 2u);
-            const uint32_t total = __popc(b0) + 2 * __popc(b1);
-            if (total > pos) { overflow = true; break; }
-            pos -= total;
-            rel -= total;
-            uint8_t* o = ow + rel + __popc(b0 & lt) + 2 * __popc(b1 & lt);
-            if (nb > 0) o[nb - 1] = static_cast<uint8_t>(x);
-            if (nb > 1) o[nb - 2] = static_cast<uint8_t>(x >> 8);
-            if (nb > 2) o[0] = static_cast<uint8_t>(x >> 16);
-            if (act) {
-                x >>= 8 * nb;
-                const uint32_t q = __umulhi(x, e.z) >> (e.w >> 24);
-                x = x + e.y + q * (e.w & 0xffffffu);
+        if (static_cast<uint32_t>(32 * k + 32) <= full_steps) {
+            x = smem_tab ? rans_encode_full_tile<true>(x, cur, tab, jb.etab, ow, rel, lt)
+                         : rans_encode_full_tile<false>(x, cur, tab, jb.etab, ow, rel, lt);
+        } else {
+            const int t_hi = min(static_cast<int>(steps) - 1, 32 * k + 31);
+            uint32_t kl = static_cast<uint32_t>(t_hi) * W + lane;   // symbol index within the chunk
+            for (int t = t_hi; t >= 32 * k; --t, kl -= W) {
+                const bool act = static_cast<uint32_t>(lane) < W && kl < cnt;
+                const uint32_t s = act ? cur[(t - 32 * k) * W + lane] : 0u;
+                const uint4 e = smem_tab ? tab[s] : __ldg(jb.etab + s);
+                x = rans_encode_step(x, e, act, ow, rel, lt);
             }
+        }
+        if (kWindow - rel > wtop) {   // the chunk's bytes no longer fit its slot
+            overflow = true;
+            break;
         }
         if (k > 0) {
             __syncwarp();
@@ -661,12 +704,10 @@ static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uin
         return;
     }
     __syncwarp();
-    {
-        const int64_t gb = static_cast<int64_t>(wtop) - kWindow;
-        for (uint32_t i = rel + lane; i < kWindow; i += 32) out[gb + i] = ow[i];
-    }
+    const int64_t gb = static_cast<int64_t>(wtop) - kWindow;
+    for (uint32_t i = rel + lane; i < kWindow; i += 32) out[gb + i] = ow[i];
     if (static_cast<uint32_t>(lane) < W) jb.states[static_cast<uint64_t>(c) * W + lane] = x;
-    if (lane == 0) jb.chunk_len[c] = static_cast<uint32_t>(jb.slot_cap - pos);
+    if (lane == 0) jb.chunk_len[c] = static_cast<uint32_t>(jb.slot_cap - (gb + rel));
 }
 
 // Refills a warp's byte window so that it starts at `pos` rounded down to 16 bytes.
@@ -687,15 +728,98 @@ __device__ __forceinline__ void window_fill(uint8_t* win, const uint8_t* bytes, 
     __syncwarp();
 }
 
+// Where a decoder reads its tables: slot lookup and prob/cum in shared memory; lookup
+// in shared memory and prob/cum in global memory; or one packed global slot entry.
+enum RansDecMode { kDecSmemAll = 0, kDecSmemLook = 1, kDecGlobalSlots = 2 };
+
+// Decodes steps [t0, t0 + tn) of a chunk (all lanes active when kFull; then tn ==
+// kRansTile).  The state stays in [L, 256 L) for any byte stream: a step leaves
+// f * (x >> prec) + (slot - cum) >= 4 and renormalisation shifts in the fewest bytes
+// that restore x >= L; so no per-step range check is needed.  Reads stay inside the
+// window (plus its 16-byte tail) because a group starts with at least kRansTile * 96
+// bytes left in it; running past the chunk's end is detected once per group.
+template <int kMode, bool kFull>
+__device__ __forceinline__ uint32_t rans_decode_group(uint32_t x, uint32_t& rel, uint32_t& k, uint32_t tn,
+                                                      const uint8_t* __restrict__ win,
+                                                      const uint16_t* __restrict__ look,
+                                                      const uint2* __restrict__ tab, const RansJob& jb,
+                                                      uint32_t* __restrict__ outc, uint32_t W, uint32_t cnt,
+                                                      uint32_t prec, uint32_t L, uint32_t lt) {
+    const uint32_t mask = (1u << prec) - 1;
+    const bool lane_in = (threadIdx.x & 31) < W;
+#pragma unroll 4
+    for (uint32_t t = 0; t < (kFull ? static_cast<uint32_t>(kRansTile) : tn); ++t, k += W) {
+        const uint32_t slot = x & mask;
+        uint32_t s, xn;
+        if (kMode == kDecSmemAll) {
+            s = look[slot];
+            const uint2 e = tab[s];
+            xn = e.x * (x >> prec) + slot - e.y;
+        } else if (kMode == kDecSmemLook) {
+            s = look[slot];
+            xn = __ldg(jb.prob + s) * (x >> prec) + slot - __ldg(jb.cum + s);
+        } else {
+            const uint64_t e = __ldg(jb.slots + slot);
+            s = static_cast<uint32_t>(e & 0x3ffffu);
+            xn = static_cast<uint32_t>((e >> 18) & 0x1fffffu) * (x >> prec) + static_cast<uint32_t>(e >> 39);
+        }
+        if (kFull) {
+            outc[k] = s;
+        } else {
+            const bool act = lane_in && k < cnt;
+            if (act) outc[k] = s;
+            xn = act ? xn : x;   // an idle lane keeps x >= L and so reads nothing
+        }
+        const uint32_t nb = (xn < L) + (xn < (L >> 8)) + (xn < (L >> 16));
+        const uint32_t b0 = __ballot_sync(0xffffffffu, nb & 1u), b1 = __ballot_sync(0xffffffffu, nb & 2u);
+        const uint32_t wo = rel + __popc(b0 & lt) + 2 * __popc(b1 & lt);
+        rel += __popc(b0) + 2 * __popc(b1);
+        const uint32_t v = (static_cast<uint32_t>(win[wo]) << 16) | (static_cast<uint32_t>(win[wo + 1]) << 8) |
+                           static_cast<uint32_t>(win[wo + 2]);
+        x = (xn << (8 * nb)) | (v >> (24 - 8 * nb));
+    }
+    return x;
+}
+
+// Decodes one chunk: groups of kRansTile steps, the window refilled before a group
+// whenever fewer than kRansTile * 96 bytes (the most a group can consume) remain in it.
+// Returns false when the byte stream ran past the chunk's end.
+template <int kMode>
+__device__ __forceinline__ bool rans_decode_chunk(uint32_t& x, uint64_t& wbase, uint32_t& rel, uint64_t end,
+                                                  uint8_t* win, const uint16_t* look, const uint2* tab,
+                                                  const RansJob& jb, uint32_t* outc, uint32_t W, uint32_t cnt,
+                                                  uint32_t steps, uint32_t prec, uint32_t L) {
+    constexpr uint32_t kGroupBytes = kRansTile * 32 * 3;   // most bytes one group of steps consumes
+    static_assert(kWindow >= kGroupBytes + 16, "window must hold a group's bytes after a refill");
+    const uint32_t lt = lanemask_lt();
+    const uint32_t full_steps = W == 32 ? cnt / 32 : 0;   // steps in which every lane codes a symbol
+    uint32_t rel_end = static_cast<uint32_t>(min(end - wbase, static_cast<uint64_t>(1u << 30)));
+    uint32_t k = threadIdx.x & 31;   // symbol index within the chunk: t * W + lane
+    for (uint32_t t0 = 0; t0 < steps; t0 += kRansTile) {
+        if (rel > kWindow - kGroupBytes) {
+            __syncwarp();
+            const uint64_t p = wbase + rel;
+            wbase = p & ~15ull;
+            rel = static_cast<uint32_t>(p - wbase);
+            rel_end = static_cast<uint32_t>(min(end - wbase, static_cast<uint64_t>(1u << 30)));
+            window_fill(win, jb.bytes, jb.bytes_len, wbase);
+        }
+        if (t0 + kRansTile <= full_steps)
+            x = rans_decode_group<kMode, true>(x, rel, k, kRansTile, win, look, tab, jb, outc, W, cnt, prec, L, lt);
+        else
+            x = rans_decode_group<kMode, false>(x, rel, k, min(static_cast<uint32_t>(kRansTile), steps - t0), win,
+                                                look, tab, jb, outc, W, cnt, prec, L, lt);
+        if (rel > rel_end) return false;
+    }
+    return true;
+}
+
 // Decoder: one warp per chunk, kRansWarps chunks of one job per CTA.  The slot->symbol
 // lookup and prob/cum live in shared memory when small; the chunk's byte stream is read
-// through a kWindow-byte shared-memory window, refilled before each group of kRansTile
-// steps whenever fewer than kRansTile * 96 bytes (the most a group can consume) remain
-// in it.  Offsets inside the group are 32-bit and relative to the window; each lane
-// renormalises by reading 3 bytes unconditionally and shifting in the nb it needs.
-// Every step checks the warp's byte total against the chunk's end; a malformed stream
-// (state out of range, overrun, or a final state or position that does not match) sets
-// kErrCorrupt, checked once per group.
+// through a kWindow-byte shared-memory window.  Offsets inside a group are 32-bit and
+// relative to the window; each lane renormalises by reading 3 bytes unconditionally and
+// shifting in the nb it needs.  A malformed stream (initial state out of range, overrun,
+// or a final state or position that does not match) sets kErrCorrupt.
 static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uint32_t* err) {
     extern __shared__ __align__(16) uint8_t rsm[];
     __shared__ int s_skip;
@@ -723,9 +847,8 @@ static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uin
     const uint32_t W = jb.lanes;
     const uint32_t cnt = static_cast<uint32_t>(cend - cbeg);   // symbols of this chunk (S < 2^32)
     const uint32_t steps = (cnt + W - 1) / W;
-    const uint32_t lt = lanemask_lt();
     uint32_t* outc = jb.out + cbeg;
-    uint64_t pos = jb.chunk_off[c];
+    const uint64_t pos = jb.chunk_off[c];
     const uint64_t end = jb.chunk_off[c + 1];
     uint32_t x = static_cast<uint32_t>(lane) < W ? jb.states[static_cast<uint64_t>(c) * W + lane] : L;
     bool bad = (x < L) || (static_cast<uint64_t>(x) >= (static_cast<uint64_t>(L) << 8)) || end > jb.bytes_len ||
@@ -734,55 +857,17 @@ static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uin
         if (lane == 0) set_error(err, kErrCorrupt);
         return;
     }
-    constexpr uint32_t kGroupBytes = kRansTile * 32 * 3;   // most bytes one group of steps consumes
-    static_assert(kWindow >= kGroupBytes + 16, "window must hold a group's bytes after a refill");
     uint64_t wbase = pos & ~15ull;
     uint32_t rel = static_cast<uint32_t>(pos - wbase);
-    uint32_t rel_end = static_cast<uint32_t>(min(end - wbase, static_cast<uint64_t>(1u << 30)));
     window_fill(win, jb.bytes, jb.bytes_len, wbase);
-    bool overrun = false;
-    uint32_t k = static_cast<uint32_t>(lane);   // symbol index within the chunk: t * W + lane
-    for (uint32_t t0 = 0; t0 < steps && !overrun; t0 += kRansTile) {
-        if (rel > kWindow - kGroupBytes) {
-            __syncwarp();
-            const uint64_t p = wbase + rel;
-            wbase = p & ~15ull;
-            rel = static_cast<uint32_t>(p - wbase);
-            rel_end = static_cast<uint32_t>(min(end - wbase, static_cast<uint64_t>(1u << 30)));
-            window_fill(win, jb.bytes, jb.bytes_len, wbase);
-        }
-        const uint32_t tn = min(static_cast<uint32_t>(kRansTile), steps - t0);
-        for (uint32_t t = 0; t < tn; ++t, k += W) {
-            const bool act = static_cast<uint32_t>(lane) < W && k < cnt;
-            const uint32_t slot = x & (M - 1);
-            uint32_t s, xn;
-            if (smem_look) {
-                s = look[slot];
-                uint32_t f, cm;
-                if (smem_tab) { const uint2 e = tab[s]; f = e.x; cm = e.y; }
-                else { f = __ldg(jb.prob + s); cm = __ldg(jb.cum + s); }
-                xn = f * (x >> prec) + slot - cm;
-            } else {
-                const uint64_t e = __ldg(jb.slots + slot);
-                s = static_cast<uint32_t>(e & 0x3ffffu);
-                xn = static_cast<uint32_t>((e >> 18) & 0x1fffffu) * (x >> prec) + static_cast<uint32_t>(e >> 39);
-            }
-            if (act) outc[k] = s;
-            x = act ? xn : x;
-            const uint32_t nb = act ? (x < L) + (x < (L >> 8)) + (x < (L >> 16)) : 0u;
-            const uint32_t b0 = __ballot_sync(0xffffffffu, nb & 1u), b1 = __ballot_sync(0xffffffffu, nb & 2u);
-            const uint32_t total = __popc(b0) + 2 * __popc(b1);
-            if (rel + total > rel_end) { overrun = true; break; }
-            const uint32_t wo = rel + __popc(b0 & lt) + 2 * __popc(b1 & lt);
-            const uint32_t v = (static_cast<uint32_t>(win[wo]) << 16) | (static_cast<uint32_t>(win[wo + 1]) << 8) |
-                               static_cast<uint32_t>(win[wo + 2]);
-            x = static_cast<uint32_t>(((static_cast<uint64_t>(x) << 24) | v) >> (24 - 8 * nb));
-            bad = bad || (act && x < L);
-            rel += total;
-        }
-        if (__any_sync(0xffffffffu, bad)) break;
-    }
-    bad = bad || overrun || (x != L) || (wbase + rel != end);
+    bool ok;
+    if (smem_look && smem_tab)
+        ok = rans_decode_chunk<kDecSmemAll>(x, wbase, rel, end, win, look, tab, jb, outc, W, cnt, steps, prec, L);
+    else if (smem_look)
+        ok = rans_decode_chunk<kDecSmemLook>(x, wbase, rel, end, win, look, tab, jb, outc, W, cnt, steps, prec, L);
+    else
+        ok = rans_decode_chunk<kDecGlobalSlots>(x, wbase, rel, end, win, look, tab, jb, outc, W, cnt, steps, prec, L);
+    bad = !ok || (x != L) || (wbase + rel != end);
     if (__any_sync(0xffffffffu, bad) && lane == 0) set_error(err, kErrCorrupt);
 }
 
