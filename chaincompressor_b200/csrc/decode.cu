@@ -50,8 +50,8 @@ struct SectionRef {
     uint32_t* scratch;        // table-parse scratch: 8 * (table_len / 64 + 2) u32
     uint32_t* prob;
     uint32_t* cum;
-    uint32_t* lookup;
-    uint64_t* slots;
+    uint8_t* image;     // the rANS decoder's shared-memory tables (dec_image_bytes), or null
+    uint64_t* slots;    // packed slot entries when the section has no image, or null
     uint64_t* chunk_off;
 };
 struct SectionRefs {
@@ -87,22 +87,47 @@ __global__ void __launch_bounds__(1024) k_section_setup(SectionRefs refs, const 
     }
 }
 
-// slot -> symbol: binary search of the cumulative table (any grid; blockIdx.y = section).
+// The rANS decoder's tables of every section (any grid; blockIdx.y = section): its
+// shared-memory image (layout at dec_image_bytes), or the packed global slot entries.
+// A slot's owner is found by binary search of the cumulative table.
 __global__ void __launch_bounds__(256) k_lookup(SectionRefs refs, const DecState* st) {
     if (st->err) return;
     const SectionRef R = refs.r[blockIdx.y];
     const SectionPlan& s = *R.sec;
-    const uint32_t M = 1u << s.prec;
-    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < M; slot += gridDim.x * blockDim.x) {
-        uint32_t lo = 0, hi = s.alphabet - 1;   // last symbol with cum <= slot and prob > 0
+    const uint32_t M = 1u << s.prec, A = s.alphabet;
+    const bool bucketed = rans_dec_bucketed(s.prec, A);
+    const bool smem_look = rans_dec_smem_look(s.prec, A);
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+    uint16_t* owners = nullptr;
+    if (bucketed) {
+        uint32_t* cum = reinterpret_cast<uint32_t*>(R.image);
+        for (uint32_t i = tid; i <= A; i += nthreads) cum[i] = i < A ? R.cum[i] : M;
+        owners = reinterpret_cast<uint16_t*>(R.image + dec_cum_bytes(A));
+    } else if (smem_look) {
+        if (A <= kSmemTableSyms) {
+            uint2* tab = reinterpret_cast<uint2*>(R.image);
+            for (uint32_t i = tid; i < A; i += nthreads) tab[i] = make_uint2(R.prob[i], R.cum[i]);
+        }
+        owners = reinterpret_cast<uint16_t*>(R.image + dec_tab_bytes(A));
+    }
+    // bucketed: entry b < 2^kBucketBits = owner of slot b << (prec - kBucketBits), the last
+    // entry = the last symbol; direct lookup and packed entries: one per slot
+    const uint32_t n = bucketed ? kBucketCount + 1 : M;
+    for (uint32_t i = tid; i < n; i += nthreads) {
+        if (bucketed && i == kBucketCount) {
+            owners[i] = static_cast<uint16_t>(A - 1);
+            continue;
+        }
+        const uint32_t slot = bucketed ? i << (s.prec - kBucketBits) : i;
+        uint32_t lo = 0, hi = A - 1;   // last symbol with cum <= slot and prob > 0
         while (lo < hi) {
             const uint32_t mid = (lo + hi + 1) >> 1;
             if (R.cum[mid] <= slot) lo = mid; else hi = mid - 1;
         }
         // zero-probability symbols share their successor's cum; step back to the owner
         while (R.prob[lo] == 0 && lo > 0) --lo;
-        R.lookup[slot] = lo;
-        R.slots[slot] = pack_slot(lo, R.prob[lo], slot - R.cum[lo]);
+        if (owners) owners[i] = static_cast<uint16_t>(lo);
+        else R.slots[slot] = pack_slot(lo, R.prob[lo], slot - R.cum[lo]);
     }
 }
 
@@ -840,12 +865,14 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         return set_err(CHAIN_ERR_BUFFER_TOO_SMALL, "output buffer holds " + std::to_string(out_capacity) +
                                                        " bytes, need " + std::to_string(nd * osz));
     const uint64_t B = plan.comp[3].records;
-    uint64_t max_prec_slots = 0, total_chunks = 0, max_alpha = 0, tags_total = 0, parse_scratch = 0;
+    uint64_t max_prec_slots = 0, total_chunks = 0, max_alpha = 0, tags_total = 0, parse_scratch = 0, images = 0;
     uint64_t tag_off[kCodeStreams] = {0};
     for (int s = 0; s < kCodeStreams; ++s) {
         const CompPlan& c = plan.comp[s];
         if (c.enc == kEncRaw || c.enc == kEncTagged) {
-            max_prec_slots += 1ull << c.sec.prec;
+            const uint32_t img = dec_image_bytes(c.sec.prec, c.sec.alphabet);
+            images += img;
+            if (img == 0) max_prec_slots += 1ull << c.sec.prec;
             total_chunks += c.sec.chunks;
             max_alpha += c.sec.alphabet;
             parse_scratch += 8ull * (c.sec.table_len / kParseSeg + 2);
@@ -861,7 +888,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     need += Arena::need(nd, 4) * 4;          // diff, keep, rel, compact
     need += Arena::need(N, 4);               // drank
     need += Arena::need(tags_total + 1, 4);
-    need += Arena::need(max_prec_slots + 1, 4) + Arena::need(max_prec_slots + 1, 8) + Arena::need(max_alpha + 1, 4) * 2;
+    need += Arena::need(images + 16, 1) + Arena::need(max_prec_slots + 1, 8) + Arena::need(max_alpha + 1, 4) * 2;
     need += Arena::need(total_chunks + kCodeStreams + 1, 8) + Arena::need(total_chunks * 32 + 1, 4);
     need += Arena::need(plan.exc_count + 1, 4) * 2;   // correction gaps, ids
     need += Arena::need(scan_scratch_bytes(std::max<uint64_t>(nd, N)), 1);
@@ -892,7 +919,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     uint32_t* parent = A.take<uint32_t>(N);
     uint32_t* drank = A.take<uint32_t>(N);
     uint32_t* tags = A.take<uint32_t>(tags_total + 1);
-    uint32_t* lookup = A.take<uint32_t>(max_prec_slots + 1);
+    uint8_t* image_buf = A.take<uint8_t>(images + 16);
     uint64_t* slots64 = A.take<uint64_t>(max_prec_slots + 1);
     uint32_t* prob = A.take<uint32_t>(max_alpha + 1);
     uint32_t* cum = A.take<uint32_t>(max_alpha + 1);
@@ -909,7 +936,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     SectionRefs refs{};
     RansJobs jobs{};
     uint64_t states_first[kCodeStreams] = {0};
-    uint64_t slot_base = 0, alpha_base = 0, chunk_base = 0, off_base = 0, pscr_base = 0;
+    uint64_t slot_base = 0, image_base = 0, alpha_base = 0, chunk_base = 0, off_base = 0, pscr_base = 0;
     uint32_t first = 0;
     int nsec = 0;
     for (int s = 0; s < kCodeStreams; ++s) {
@@ -921,15 +948,16 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         pscr_base += 8ull * (c.sec.table_len / kParseSeg + 2);
         R.prob = prob + alpha_base;
         R.cum = cum + alpha_base;
-        R.lookup = lookup + slot_base;
-        R.slots = slots64 + slot_base;
+        const uint32_t img = dec_image_bytes(c.sec.prec, c.sec.alphabet);
+        R.image = img ? image_buf + image_base : nullptr;
+        R.slots = img ? nullptr : slots64 + slot_base;
         R.chunk_off = chunk_off + off_base;
         states_first[nsec] = chunk_base * 32;
         RansJob& jb = jobs.job[jobs.njobs++];
         jb.count = c.sec.count;
         jb.prob = R.prob;
         jb.cum = R.cum;
-        jb.lookup = R.lookup;
+        jb.image = reinterpret_cast<const uint4*>(R.image);
         jb.slots = R.slots;
         jb.prec = c.sec.prec;
         jb.alphabet = c.sec.alphabet;
@@ -942,8 +970,9 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         jb.states = states + chunk_base * 32;
         jb.out = c.enc == kEncRaw ? streams[s] : tags + tag_off[s];
         jb.first_block = first;
-        first += (c.sec.chunks + kRansWarps - 1) / kRansWarps;
-        slot_base += 1ull << c.sec.prec;
+        first += (c.sec.chunks + kRansDecWarps - 1) / kRansDecWarps;
+        if (img) image_base += img;
+        else slot_base += 1ull << c.sec.prec;
         alpha_base += c.sec.alphabet;
         chunk_base += c.sec.chunks;
         off_base += c.sec.chunks + 1;
@@ -968,7 +997,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
             CHAIN_CUDA(cudaFuncSetAttribute(rans_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             static_cast<int>(kRansDecSmemMax)));
         }
-        rans_decode_kernel<<<jobs.total_blocks, 32 * kRansWarps, rans_dec_smem(jobs), stream>>>(jobs, &st->err); count_launch();
+        rans_decode_kernel<<<jobs.total_blocks, 32 * kRansDecWarps, rans_dec_smem(jobs), stream>>>(jobs, &st->err); count_launch();
     }
     CHAIN_LAUNCH_CHECK("entropy decode");
     T.mark("rans_decode", stream);

@@ -1719,7 +1719,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
             jb.chunk_len = chunk_len + chunk_base;
             jb.states = states + chunk_base * 32;
             jb.first_block = first;
-            first += (c.sec_chunks + kRansWarps - 1) / kRansWarps;
+            first += (c.sec_chunks + kRansEncWarps - 1) / kRansEncWarps;
             ain.chunk_len[s] = jb.chunk_len;
             ain.states[s] = reinterpret_cast<const uint8_t*>(packed_states + chunk_base * 32);
             sp.in[sp_n] = jb.states;
@@ -1757,7 +1757,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
             CHAIN_CUDA(cudaFuncSetAttribute(rans_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             static_cast<int>(kRansEncSmemMax)));
         }
-        rans_encode_kernel<<<jobs.total_blocks, 32 * kRansWarps, rans_enc_smem(jobs), stream>>>(jobs, &st->err); count_launch();
+        rans_encode_kernel<<<jobs.total_blocks, 32 * kRansEncWarps, rans_enc_smem(jobs), stream>>>(jobs, &st->err); count_launch();
         k_pack_states<<<dim3(16, sp_n), 256, 0, stream>>>(sp); count_launch();
     }
     CHAIN_LAUNCH_CHECK("entropy coding");

@@ -451,13 +451,13 @@ struct RansJob {
     uint64_t count;           // symbols
     const uint32_t* prob;     // [A]
     const uint32_t* cum;      // [A]
-    const uint32_t* lookup;   // decode: slot -> symbol [M]
-    const uint64_t* slots;    // decode: slot -> pack_slot(symbol, freq, slot - cum) [M]
+    const uint4* image;       // decode: the job's shared-memory tables (dec_image_bytes), 16-byte aligned
+    const uint64_t* slots;    // decode, tables without an image: slot -> pack_slot(symbol, freq, slot - cum) [M]
     uint32_t prec;
     uint32_t alphabet;
     uint32_t chunks;
     uint32_t lanes;           // interleaved states per chunk (1..32)
-    uint32_t first_block;     // first CTA of this job (kRansWarps chunks per CTA)
+    uint32_t first_block;     // first CTA of this job (kRansEncWarps / kRansDecWarps chunks per CTA)
     uint32_t pad;
     uint64_t S;               // symbols per chunk (multiple of 32)
     uint8_t* bytes;           // encode: chunk slots (slot_cap each); decode: container
@@ -469,11 +469,14 @@ struct RansJob {
 };
 
 constexpr int kMaxRansJobs = 16;
-constexpr int kRansWarps = 4;                 // chunks (warps) per CTA
+constexpr int kRansEncWarps = 4;              // chunks (warps) per encoder CTA
+constexpr int kRansDecWarps = 8;              // chunks (warps) per decoder CTA (shares its table image)
 constexpr int kRansTile = 32;                 // steps per staged tile
 constexpr uint32_t kSmemTableSyms = 4096;     // decoder prob/cum in shared memory up to this alphabet
 constexpr uint32_t kSmemEncSyms = 2048;       // encoder entries (16 B) in shared memory up to this alphabet
 constexpr uint32_t kSmemLookupSlots = 16384;  // u16 decode lookup in shared memory up to this M
+constexpr uint32_t kBucketBits = 13;          // bucketed decode: 2^13 buckets of slots ...
+constexpr uint32_t kBucketMaxSyms = 16384;    // ... for M above kSmemLookupSlots and alphabets up to this
 constexpr uint32_t kWindow = 4096;            // decoder byte window per warp
 constexpr uint32_t kLargeTableMaxSteps = 512; // serial depth of lanes whose tables stay in L2
 constexpr uint64_t kLargeTableMinSymbols = 1ull << 18;  // ... on streams at least this long
@@ -484,31 +487,82 @@ __host__ __device__ inline uint64_t pack_slot(uint32_t sym, uint32_t freq, uint3
     return static_cast<uint64_t>(sym) | (static_cast<uint64_t>(freq) << 18) | (static_cast<uint64_t>(bias) << 39);
 }
 
+// Bucketed decode (tables too large for a shared-memory slot lookup): the slot range is
+// cut into 2^kBucketBits buckets; bucket b's first-slot owner and the cumulative table
+// sit in shared memory, and a step binary-searches the symbols between the owners of
+// bucket b's and bucket b+1's first slots.  The same rule decides it on every side.
+__host__ __device__ inline bool rans_dec_bucketed(uint32_t prec, uint32_t alphabet) {
+    return (1u << prec) > kSmemLookupSlots && alphabet <= kBucketMaxSyms;
+}
+constexpr uint32_t kBucketCount = 1u << kBucketBits;
+
+// A decoder job's shared-memory tables, built once per section in global memory by the
+// table stage and copied verbatim by every CTA of the job:
+//   bucketed:        u32 cum[A + 1] (cum[A] = M), padded to 16 B; u16 owner[2^kBucketBits + 1]
+//   M <= 16384, A <= 65536 (u16 symbols):
+//                    A <= kSmemTableSyms: uint2 {prob, cum}[A], padded to 64 B; u16 look[M]
+//                    else:                u16 look[M] (prob and cum read from global memory)
+//   otherwise:       none (one packed global slot entry per step)
+__host__ __device__ inline bool rans_dec_smem_look(uint32_t prec, uint32_t alphabet) {
+    return (1u << prec) <= kSmemLookupSlots && alphabet <= 65536;
+}
+__host__ __device__ inline uint32_t dec_cum_bytes(uint32_t alphabet) { return ((alphabet + 1 + 3) & ~3u) * 4; }
+__host__ __device__ inline uint32_t dec_tab_bytes(uint32_t alphabet) {
+    return alphabet <= kSmemTableSyms ? ((alphabet + 7) & ~7u) * 8 : 0;
+}
+__host__ __device__ inline uint32_t dec_image_bytes(uint32_t prec, uint32_t alphabet) {
+    if (rans_dec_bucketed(prec, alphabet)) return (dec_cum_bytes(alphabet) + (kBucketCount + 1) * 2 + 15) & ~15u;
+    if (rans_dec_smem_look(prec, alphabet)) return (dec_tab_bytes(alphabet) + (2u << prec) + 15) & ~15u;
+    return 0;
+}
+
+// Copies n16 16-byte words global -> shared with the whole CTA, eight loads in flight
+// per thread.
+__device__ __forceinline__ void block_copy16(uint4* __restrict__ dst, const uint4* __restrict__ src, uint32_t n16) {
+    constexpr int kDepth = 8;
+    for (uint32_t i0 = threadIdx.x; i0 < n16; i0 += blockDim.x * kDepth) {
+        uint4 v[kDepth];
+#pragma unroll
+        for (int u = 0; u < kDepth; ++u) {
+            const uint32_t i = i0 + u * blockDim.x;
+            if (i < n16) v[u] = __ldg(src + i);
+        }
+#pragma unroll
+        for (int u = 0; u < kDepth; ++u) {
+            const uint32_t i = i0 + u * blockDim.x;
+            if (i < n16) dst[i] = v[u];
+        }
+    }
+}
+
 // Shared memory is sized per launch: the largest table of this launch that fits the
-// shared-memory limits (tab_cap symbols, look_cap decode slots), plus staging.
+// shared-memory limits, plus staging.
 struct RansJobs {
     RansJob job[kMaxRansJobs];
     uint32_t njobs;
     uint32_t total_blocks;
-    uint32_t tab_cap;    // tables with alphabet <= tab_cap live in shared memory
-    uint32_t look_cap;   // decode lookups with M <= look_cap live in shared memory
+    uint32_t tab_cap;      // encode: tables with alphabet <= tab_cap live in shared memory
+    uint32_t table_bytes;  // decode: the largest job image (shared-memory bytes before the windows)
 };
 
 inline void rans_plan_smem(RansJobs& J, bool decode) {
-    uint32_t tab = 0, look = 0;
+    uint32_t tab = 0, image = 0;
     for (uint32_t j = 0; j < J.njobs; ++j) {
-        const uint32_t A = J.job[j].alphabet, M = 1u << J.job[j].prec;
-        if (A <= (decode ? kSmemTableSyms : kSmemEncSyms) && A > tab) tab = A;
-        if (decode && M <= kSmemLookupSlots && A <= 65536 && M > look) look = M;
+        const uint32_t A = J.job[j].alphabet;
+        if (!decode && A <= kSmemEncSyms && A > tab) tab = A;
+        if (decode) {
+            const uint32_t b = dec_image_bytes(J.job[j].prec, A);
+            if (b > image) image = b;
+        }
     }
     J.tab_cap = (tab + 7) & ~7u;
-    J.look_cap = (look + 7) & ~7u;
+    J.table_bytes = image;
 }
 inline size_t rans_enc_smem(const RansJobs& J) {
-    return J.tab_cap * 16ull + kRansWarps * 2 * kRansTile * 32 * 4 + kRansWarps * kWindow;
+    return J.tab_cap * 16ull + kRansEncWarps * (2 * kRansTile * 32 * 4 + kWindow);
 }
 inline size_t rans_dec_smem(const RansJobs& J) {
-    return J.tab_cap * 8ull + J.look_cap * 2ull + kRansWarps * kWindow + 16;   // +16: 3-byte renorm reads
+    return J.table_bytes + kRansDecWarps * kWindow + 16;   // +16: 3-byte renorm reads
 }
 
 // Largest dynamic shared memory any launch of the two kernels can request.  The kernels'
@@ -516,8 +570,14 @@ inline size_t rans_dec_smem(const RansJobs& J) {
 // global to the process, so contexts used from several threads at once must never set
 // different values (a smaller one set between another thread's set and launch would make
 // that launch fail).
-constexpr size_t kRansEncSmemMax = kSmemEncSyms * 16ull + kRansWarps * 2 * kRansTile * 32 * 4 + kRansWarps * kWindow;
-constexpr size_t kRansDecSmemMax = kSmemTableSyms * 8ull + kSmemLookupSlots * 2ull + kRansWarps * kWindow + 16;
+// Two decoder CTAs of the largest size still fit one SM (228 KB less 1 KB per CTA).
+constexpr size_t kRansEncSmemMax =
+    kSmemEncSyms * 16ull + kRansEncWarps * 2 * kRansTile * 32 * 4 + kRansEncWarps * kWindow;
+constexpr size_t kDecDirectBytes = kSmemTableSyms * 8ull + kSmemLookupSlots * 2ull;
+constexpr size_t kDecBucketBytes = (((kBucketMaxSyms + 1 + 3) & ~3ull) * 4 + (kBucketCount + 1) * 2 + 15) & ~15ull;
+constexpr size_t kRansDecSmemMax =
+    (kDecDirectBytes > kDecBucketBytes ? kDecDirectBytes : kDecBucketBytes) + kRansDecWarps * kWindow + 16;
+static_assert(2 * (kRansDecSmemMax + 1024 + 16) <= 228 * 1024, "two decoder CTAs per SM");
 
 __device__ __forceinline__ int job_of_block(const RansJobs& J) {
     int j = 0;
@@ -604,7 +664,7 @@ __device__ __forceinline__ uint32_t rans_encode_full_tile(uint32_t x, const uint
     return x;
 }
 
-// Encoder: one warp per chunk, kRansWarps chunks of one job per CTA.  The job's table
+// Encoder: one warp per chunk, kRansEncWarps chunks of one job per CTA.  The job's table
 // sits in shared memory when small; symbols are prefetched one 32-step tile ahead
 // into shared memory; the warp's byte counts are prefix-summed with two ballots
 // (0..3 bytes per lane).  Bytes are written backwards into a kWindow-byte shared-memory
@@ -614,19 +674,18 @@ __device__ __forceinline__ uint32_t rans_encode_full_tile(uint32_t x, const uint
 // bytes) moves to the window's top.  A chunk whose bytes exceed its slot is detected
 // after the group that overflowed, before anything reaches global memory.  Offsets are
 // 32-bit (a chunk slot is < 4 GB).
-static __global__ void __launch_bounds__(128) rans_encode_kernel(RansJobs J, uint32_t* err) {
+static __global__ void __launch_bounds__(32 * kRansEncWarps) rans_encode_kernel(RansJobs J, uint32_t* err) {
     extern __shared__ __align__(16) uint8_t rsm[];
     const RansJob& jb = J.job[job_of_block(J)];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint4* tab = reinterpret_cast<uint4*>(rsm);
     const bool smem_tab = jb.alphabet <= J.tab_cap;
-    if (smem_tab)
-        for (uint32_t s = threadIdx.x; s < jb.alphabet; s += blockDim.x) tab[s] = jb.etab[s];
+    if (smem_tab) block_copy16(tab, jb.etab, jb.alphabet);
     __syncthreads();
-    const uint32_t c = (blockIdx.x - jb.first_block) * kRansWarps + warp;
+    const uint32_t c = (blockIdx.x - jb.first_block) * kRansEncWarps + warp;
     if (c >= jb.chunks) return;
     uint32_t* buf = reinterpret_cast<uint32_t*>(rsm + J.tab_cap * 16ull) + warp * 2 * 1024;
-    uint8_t* ow = rsm + J.tab_cap * 16ull + kRansWarps * 2 * kRansTile * 32 * 4 + warp * kWindow;
+    uint8_t* ow = rsm + J.tab_cap * 16ull + kRansEncWarps * 2 * kRansTile * 32 * 4 + warp * kWindow;
     const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
     const uint64_t cend = min(cbeg + jb.S, jb.count);
     const uint32_t W = jb.lanes;
@@ -730,7 +789,7 @@ __device__ __forceinline__ void window_fill(uint8_t* win, const uint8_t* bytes, 
 
 // Where a decoder reads its tables: slot lookup and prob/cum in shared memory; lookup
 // in shared memory and prob/cum in global memory; or one packed global slot entry.
-enum RansDecMode { kDecSmemAll = 0, kDecSmemLook = 1, kDecGlobalSlots = 2 };
+enum RansDecMode { kDecSmemAll = 0, kDecSmemLook = 1, kDecBucket = 2, kDecGlobalSlots = 3 };
 
 // Decodes steps [t0, t0 + tn) of a chunk (all lanes active when kFull; then tn ==
 // kRansTile).  The state stays in [L, 256 L) for any byte stream: a step leaves
@@ -758,6 +817,18 @@ __device__ __forceinline__ uint32_t rans_decode_group(uint32_t x, uint32_t& rel,
         } else if (kMode == kDecSmemLook) {
             s = look[slot];
             xn = __ldg(jb.prob + s) * (x >> prec) + slot - __ldg(jb.cum + s);
+        } else if (kMode == kDecBucket) {
+            // look = bucket owners [kBucketCount + 1], tab = cumulative table [A + 1]
+            const uint32_t* cum = reinterpret_cast<const uint32_t*>(tab);
+            const uint32_t b = slot >> (prec - kBucketBits);
+            uint32_t lo = look[b], hi = look[b + 1];
+            while (lo < hi) {   // last symbol with cum <= slot: the owner
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (cum[mid] <= slot) lo = mid; else hi = mid - 1;
+            }
+            s = lo;
+            const uint32_t c0 = cum[lo];
+            xn = (cum[lo + 1] - c0) * (x >> prec) + slot - c0;
         } else {
             const uint64_t e = __ldg(jb.slots + slot);
             s = static_cast<uint32_t>(e & 0x3ffffu);
@@ -814,13 +885,14 @@ __device__ __forceinline__ bool rans_decode_chunk(uint32_t& x, uint64_t& wbase, 
     return true;
 }
 
-// Decoder: one warp per chunk, kRansWarps chunks of one job per CTA.  The slot->symbol
-// lookup and prob/cum live in shared memory when small; the chunk's byte stream is read
+// Decoder: one warp per chunk, kRansDecWarps chunks of one job per CTA.  The slot->symbol
+// lookup and prob/cum live in shared memory when small, the bucket owners and the
+// cumulative table when the lookup is too large; the chunk's byte stream is read
 // through a kWindow-byte shared-memory window.  Offsets inside a group are 32-bit and
 // relative to the window; each lane renormalises by reading 3 bytes unconditionally and
 // shifting in the nb it needs.  A malformed stream (initial state out of range, overrun,
 // or a final state or position that does not match) sets kErrCorrupt.
-static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uint32_t* err) {
+static __global__ void __launch_bounds__(32 * kRansDecWarps) rans_decode_kernel(RansJobs J, uint32_t* err) {
     extern __shared__ __align__(16) uint8_t rsm[];
     __shared__ int s_skip;
     if (threadIdx.x == 0) s_skip = *err != 0;  // a failed table parse leaves no valid lookup
@@ -830,17 +902,16 @@ static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uin
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t prec = jb.prec;
     const uint32_t M = 1u << prec, L = 4u << prec;
-    uint2* tab = reinterpret_cast<uint2*>(rsm);
-    uint16_t* look = reinterpret_cast<uint16_t*>(rsm + J.tab_cap * 8ull);
-    uint8_t* win = rsm + J.tab_cap * 8ull + J.look_cap * 2ull + warp * kWindow;
-    const bool smem_tab = jb.alphabet <= J.tab_cap;
-    const bool smem_look = M <= J.look_cap && jb.alphabet <= 65536;
-    if (smem_tab)
-        for (uint32_t s = threadIdx.x; s < jb.alphabet; s += blockDim.x) tab[s] = make_uint2(jb.prob[s], jb.cum[s]);
-    if (smem_look)
-        for (uint32_t s = threadIdx.x; s < M; s += blockDim.x) look[s] = static_cast<uint16_t>(jb.lookup[s]);
+    uint8_t* win = rsm + J.table_bytes + warp * kWindow;
+    const bool bucketed = rans_dec_bucketed(prec, jb.alphabet);
+    const bool smem_look = rans_dec_smem_look(prec, jb.alphabet);
+    const bool smem_tab = smem_look && jb.alphabet <= kSmemTableSyms;
+    const uint2* tab = reinterpret_cast<const uint2*>(rsm);   // bucketed: the u32 cumulative table
+    const uint16_t* look = reinterpret_cast<const uint16_t*>(
+        rsm + (bucketed ? dec_cum_bytes(jb.alphabet) : dec_tab_bytes(jb.alphabet)));
+    block_copy16(reinterpret_cast<uint4*>(rsm), jb.image, dec_image_bytes(prec, jb.alphabet) / 16);
     __syncthreads();
-    const uint32_t c = (blockIdx.x - jb.first_block) * kRansWarps + warp;
+    const uint32_t c = (blockIdx.x - jb.first_block) * kRansDecWarps + warp;
     if (c >= jb.chunks) return;
     const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
     const uint64_t cend = min(cbeg + jb.S, jb.count);
@@ -861,7 +932,9 @@ static __global__ void __launch_bounds__(128) rans_decode_kernel(RansJobs J, uin
     uint32_t rel = static_cast<uint32_t>(pos - wbase);
     window_fill(win, jb.bytes, jb.bytes_len, wbase);
     bool ok;
-    if (smem_look && smem_tab)
+    if (bucketed)
+        ok = rans_decode_chunk<kDecBucket>(x, wbase, rel, end, win, look, tab, jb, outc, W, cnt, steps, prec, L);
+    else if (smem_look && smem_tab)
         ok = rans_decode_chunk<kDecSmemAll>(x, wbase, rel, end, win, look, tab, jb, outc, W, cnt, steps, prec, L);
     else if (smem_look)
         ok = rans_decode_chunk<kDecSmemLook>(x, wbase, rel, end, win, look, tab, jb, outc, W, cnt, steps, prec, L);
