@@ -12,9 +12,10 @@ is timed the same way and reported beside it.
   e2e   : the same through the C ABI with pinned HOST buffers: H2D of the points and
           D2H of the container inside the timed region
   decompress : the same two numbers for the decoder (container -> float64 points)
-  roofline   : the dominant kernel of the compress step (rans_encode_kernel) against
-          the measured HBM copy bandwidth; roofline_decompress likewise for
-          rans_decode_kernel; path_roofline: (input + container bytes) / step time
+  roofline   : the dominant kernel of the compress step (radix_scatter_kernel, one
+          launch per 8-bit sort pass) against the measured HBM copy bandwidth;
+          roofline_rans_encode for the encoder's entropy kernel; decompress.roofline
+          for rans_decode_kernel; path_roofline: (input + container bytes) / step time
 
 Multi-GPU: frames are independent, so N ranks compress N independent frames
 (replicas, weak scaling, no collective on the data path; only the timing max-reduce).
@@ -195,11 +196,13 @@ def run_ours(args, rank: int, world: int):
         codec.result_copy_to(cont_host.data_ptr(), clen)
         decomp(cont_host.data_ptr(), out_host.data_ptr())
 
+    counts = {}   # stage marks per step (a stage named more than once is summed)
+
     def timed(fn, stages=False):
         """Device time per step from CUDA events on the library stream (the library
         calls are synchronous, so the events bracket all of their device work)."""
         codec.set_stage_timing(stages)
-        acc = {}
+        acc, occ = {}, {}
         barrier()
         l0 = N.launch_count()
         ev0 = torch.cuda.Event(enable_timing=True)
@@ -210,10 +213,12 @@ def run_ours(args, rank: int, world: int):
             if stages:
                 for name, ms in codec.stage_times():
                     acc[name] = acc.get(name, 0.0) + ms
+                    occ[name] = occ.get(name, 0) + 1
         ev1.record(stream)
         barrier()
         launches = N.launch_count() - l0
         codec.set_stage_timing(False)
+        counts.update({k: v // args.steps for k, v in occ.items()})
         return ev0.elapsed_time(ev1) / 1e3 / args.steps, launches, {k: v / args.steps for k, v in acc.items()}
 
     clocks = Clocks(dev)
@@ -243,15 +248,28 @@ def run_ours(args, rank: int, world: int):
     peaks, src = _peaks()
     peak = float(peaks["hbm_gbs"])
 
-    def roof(kernel, stage_ms, alg_bytes):
+    def roof(kernel, stage_ms, alg_bytes, launches=1):
         if not stage_ms:
             return None
+        stage_ms = stage_ms / launches
         ach = alg_bytes / (stage_ms / 1e3) / 1e9
         traffic, prof = _profile_traffic(kernel)
         return {"kernel": kernel, "bound": "hbm", "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
                 "avg_launch_ms": round(stage_ms, 4), "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)",
                 "traffic_source": prof}
+
+    # radix scatter: pass 0 reads keys (indices are implicit) and writes keys + indices;
+    # later passes read and write both
+    scatter_roof = None
+    for kw in (4, 8):
+        name = f"sort_scatter_k{kw * 8}"
+        passes = counts.get(name, 0)
+        if passes:
+            alg = (n * (kw + kw + 4) + (passes - 1) * n * 2 * (kw + 4)) // passes
+            scatter_roof = roof("radix_scatter_kernel", stages_c.get(name), alg, passes)
+            if scatter_roof:
+                scatter_roof["launches_per_step"] = passes
 
     gbs = lambda sec: world * raw / sec / 1e9  # noqa: E731
     line = {
@@ -264,7 +282,8 @@ def run_ours(args, rank: int, world: int):
                    "parallelism": f"replicas x{world} (independent frames)"},
         "e2e": {"value": round(gbs(t_ce), 3), "unit": UNIT, "h2d_bytes_per_step": raw, "d2h_bytes_per_step": clen},
         "gpu_launches": launches_c, "gpu_launches_per_step": launches_c // max(1, args.steps),
-        "roofline": roof("rans_encode_kernel", stages_c.get("rans_encode"), 4 * rans_syms + rans_bytes),
+        "roofline": scatter_roof,
+        "roofline_rans_encode": roof("rans_encode_kernel", stages_c.get("rans_encode"), 4 * rans_syms + rans_bytes),
         "decompress": {"value": round(gbs(t_d), 3), "unit": UNIT, "ms_per_step": round(t_d * 1e3, 4),
                        "gpu_launches": launches_d,
                        "e2e": {"value": round(gbs(t_de), 3), "unit": UNIT, "h2d_bytes_per_step": clen,

@@ -1506,23 +1506,27 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     T.mark("quantize", stream);
 
     if (l1) {
+        // stage marks around every scatter pass; the key width is in the name
+        const auto sort_marks = [&](bool after) {
+            T.mark(after ? (wide ? "sort_scatter_k64" : "sort_scatter_k32") : "sort_hist_scan", stream);
+        };
         if (wide) {
             const bool in_b = radix_sort_pairs<uint64_t>(key_idx, key_a, val_a, key_b, val_b, n, key_bits, counts,
-                                                         reinterpret_cast<uint32_t*>(scanbuf), stream);
+                                                         reinterpret_cast<uint32_t*>(scanbuf), stream, sort_marks);
             k_level1<uint64_t><<<grid_for(n), 256, 0, stream>>>(in_b ? key_b : key_a, in_b ? val_b : val_a, n, st, idrel); count_launch();
         } else {
             uint32_t* k32 = reinterpret_cast<uint32_t*>(key_idx);
             uint32_t* ka = reinterpret_cast<uint32_t*>(key_a);
             uint32_t* kb = reinterpret_cast<uint32_t*>(key_b);
             const bool in_b = radix_sort_pairs<uint32_t>(k32, ka, val_a, kb, val_b, n, key_bits, counts,
-                                                         reinterpret_cast<uint32_t*>(scanbuf), stream);
+                                                         reinterpret_cast<uint32_t*>(scanbuf), stream, sort_marks);
             k_level1<uint32_t><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel); count_launch();
         }
     } else {
         CHAIN_CUDA(cudaMemsetAsync(idrel, 0, sizeof(uint32_t) * n, stream));
     }
     CHAIN_LAUNCH_CHECK("level 1");
-    T.mark("sort+level1", stream);
+    T.mark("level1", stream);
     uint32_t* scan32 = reinterpret_cast<uint32_t*>(scanbuf);
     if (wide)
         device_flag_scan(ExplicitIn<uint64_t>{idrel}, ExplicitOut<uint64_t>{key_idx, st, rec}, n, scan32, &st->B,

@@ -151,13 +151,19 @@ inline uint32_t radix_tiles(uint64_t n) {
 // Count-table entries radix_sort_pairs needs for n keys of either key width.
 inline size_t radix_counts_elems(uint64_t n) { return static_cast<size_t>(radix_tiles<uint64_t>(n)) * kSortBins; }
 
+struct NoSortHook {
+    void operator()(bool /*after_scatter*/) const {}
+};
+
 // Sorts keys_in (values implicitly 0..n-1) by bits [0, key_bits), stably.  Ping-pongs
 // between (keys_a, vals_a) and (keys_b, vals_b); keys_in is only read.  Returns true
 // when the result is in the *_b buffers.  counts: radix_counts_elems(n) u32;
-// scan_buf: scan_scratch_bytes(counts) bytes.
-template <typename KT>
+// scan_buf: scan_scratch_bytes(counts) bytes.  hook(false) runs before each pass's
+// scatter launch and hook(true) after it (stage timing).
+template <typename KT, typename Hook = NoSortHook>
 bool radix_sort_pairs(const KT* keys_in, KT* keys_a, uint32_t* vals_a, KT* keys_b, uint32_t* vals_b, uint64_t n,
-                      int key_bits, uint32_t* counts, uint32_t* scan_buf, cudaStream_t stream) {
+                      int key_bits, uint32_t* counts, uint32_t* scan_buf, cudaStream_t stream,
+                      const Hook& hook = Hook()) {
     const uint32_t tiles = radix_tiles<KT>(n);
     int passes = (key_bits + 7) / 8;
     if (passes == 0) passes = 1;  // one pass produces the identity permutation
@@ -171,7 +177,9 @@ bool radix_sort_pairs(const KT* keys_in, KT* keys_a, uint32_t* vals_a, KT* keys_
         const uint64_t ncounts = static_cast<uint64_t>(tiles) * kSortBins;
         device_exclusive_scan<uint32_t>(CountIn{counts}, CountOut{counts}, ncounts, scan_buf,
                                         static_cast<uint32_t*>(nullptr), stream);
+        hook(false);
         radix_scatter_kernel<KT><<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, shift, counts, tiles); count_launch();
+        hook(true);
     }
     return passes % 2 == 0;
 }
