@@ -7,10 +7,11 @@
 //
 // Each 8-bit pass is three launches: a per-tile digit histogram, a device-wide
 // exclusive scan of the digit-major count table, and a stable scatter.  The scatter
-// loads its whole tile at once, ranks keys with 8 ballots per 32 keys (each warp owns
-// a contiguous slice, processed 32 keys per round in order, so equal digits keep their
-// input order), reorders the tile by digit in shared memory, and writes each digit's
-// run to its global position with consecutive threads on consecutive addresses.
+// loads its whole tile at once (indices wait in shared memory in input order), ranks
+// keys with 8 ballots per 32 keys (each warp owns a contiguous slice, processed 32 keys
+// per round in order, so equal digits keep their input order), reorders the tile by
+// digit in shared memory, and writes each digit's run to its global position with
+// consecutive threads on consecutive addresses.
 #pragma once
 
 #include "chain_common.cuh"
@@ -24,7 +25,7 @@ constexpr int kSortBins = 256;
 
 template <typename KT>
 struct SortShape {
-    static constexpr int kItems = sizeof(KT) > 4 ? 8 : 16;
+    static constexpr int kItems = sizeof(KT) > 4 ? 8 : 12;
     static constexpr int kTile = kSortThreads * kItems;
 };
 
@@ -46,39 +47,70 @@ radix_hist_kernel(const KT* __restrict__ keys, uint64_t n, int shift, uint32_t* 
     counts[static_cast<uint64_t>(threadIdx.x) * num_tiles + blockIdx.x] = hist[threadIdx.x];
 }
 
+// Shared-memory staging of a tile's reordered pairs: one 8-byte word per pair for
+// 32-bit keys, separate arrays for 64-bit keys.
 template <typename KT>
-__global__ void __launch_bounds__(kSortThreads)
+struct ScatterStage {
+    KT key[SortShape<KT>::kTile];
+    uint32_t val[SortShape<KT>::kTile];
+    __device__ __forceinline__ void put(uint32_t i, KT k, uint32_t v) { key[i] = k; val[i] = v; }
+    __device__ __forceinline__ void get(uint32_t i, KT& k, uint32_t& v) const { k = key[i]; v = val[i]; }
+};
+template <>
+struct ScatterStage<uint32_t> {
+    uint2 kv[SortShape<uint32_t>::kTile];
+    __device__ __forceinline__ void put(uint32_t i, uint32_t k, uint32_t v) { kv[i] = make_uint2(k, v); }
+    __device__ __forceinline__ void get(uint32_t i, uint32_t& k, uint32_t& v) const {
+        const uint2 t = kv[i];
+        k = t.x;
+        v = t.y;
+    }
+};
+
+// Four CTAs per SM (63 registers, <= 46 KB of shared memory): the ranking loop is
+// latency-bound, so resident warps matter more than registers.
+template <typename KT>
+__global__ void __launch_bounds__(kSortThreads, 4)
 radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                      KT* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint64_t n, int shift,
                      const uint32_t* __restrict__ offsets, uint32_t num_tiles) {
-    constexpr int I = SortShape<KT>::kItems, TILE = SortShape<KT>::kTile;
+    constexpr int I = SortShape<KT>::kItems;
     __shared__ uint32_t whist[kSortWarps][kSortBins];
-    __shared__ uint32_t tile_start[kSortBins];   // first tile-local position of each digit
-    __shared__ uint32_t gbase[kSortBins];        // global position of that first key
+    __shared__ int32_t delta[kSortBins];         // global position - tile-local position, per digit
     __shared__ uint32_t scratch[33];
-    __shared__ KT skey[TILE];
-    __shared__ uint32_t sval[TILE];
+    __shared__ ScatterStage<KT> stage;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int t = threadIdx.x; t < kSortWarps * kSortBins; t += kSortThreads) (&whist[0][0])[t] = 0;
     __syncthreads();
-    const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * TILE;
+    const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * SortShape<KT>::kTile;
     const uint64_t base = tile0 + static_cast<uint64_t>(warp) * (I * 32);
+    // keys of this warp's slice that exist (the slice is [base, base + 32 I))
+    const uint32_t rem = base >= n ? 0u : static_cast<uint32_t>(min(n - base, static_cast<uint64_t>(I * 32)));
+    const KT* kin = keys_in + base;
+    const uint32_t* vin = vals_in ? vals_in + base : nullptr;
     KT key[I];
-    uint32_t val[I];
-    uint32_t rank[I];
+    uint32_t rd[I];   // rank within the warp's digit run (bits 0..15) | digit << 16
     const uint32_t lt = lanemask_lt();
-    // all loads first, so that they are in flight together
+    // all loads first, so that they are in flight together (indices are implicit on
+    // the first pass); the indices wait in shared memory, in input order, until the
+    // tile's positions are known
+    __shared__ uint32_t sval_in[SortShape<KT>::kTile];
+    uint32_t* my_val = sval_in + warp * (I * 32) + lane;
+    {
+        uint32_t val[I];
 #pragma unroll
-    for (int r = 0; r < I; ++r) {
-        const uint64_t i = base + static_cast<uint64_t>(r) * 32 + lane;
-        key[r] = i < n ? keys_in[i] : KT(0);
-        val[r] = i < n ? (vals_in ? vals_in[i] : static_cast<uint32_t>(i)) : 0u;
+        for (int r = 0; r < I; ++r) {
+            const uint32_t i = r * 32 + lane;
+            key[r] = i < rem ? kin[i] : KT(0);
+            val[r] = i < rem ? (vin ? vin[i] : static_cast<uint32_t>(base) + i) : 0u;
+        }
+#pragma unroll
+        for (int r = 0; r < I; ++r) my_val[r * 32] = val[r];
     }
     // stable rank within the warp: lanes with an equal digit found with 8 ballots
 #pragma unroll
     for (int r = 0; r < I; ++r) {
-        const uint64_t i = base + static_cast<uint64_t>(r) * 32 + lane;
-        const bool valid = i < n;
+        const bool valid = static_cast<uint32_t>(r * 32 + lane) < rem;
         const uint32_t digit = static_cast<uint32_t>(key[r] >> shift) & 0xFFu;
         uint32_t peers = __ballot_sync(0xffffffffu, valid);
 #pragma unroll
@@ -89,7 +121,7 @@ radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict_
         }
         const uint32_t prior = valid ? whist[warp][digit] : 0u;
         __syncwarp();
-        rank[r] = prior + __popc(peers & lt);
+        rd[r] = (prior + __popc(peers & lt)) | (digit << 16);
         if (valid && (peers & lt) == 0) whist[warp][digit] = prior + __popc(peers);
         __syncwarp();
     }
@@ -102,8 +134,7 @@ radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict_
         for (int w = 0; w < kSortWarps; ++w) cnt += whist[w][d];
         uint32_t tot;
         const uint32_t start = block_exclusive_sum(cnt, scratch, &tot);
-        tile_start[d] = start;
-        gbase[d] = offsets[static_cast<uint64_t>(d) * num_tiles + blockIdx.x];
+        delta[d] = static_cast<int32_t>(offsets[static_cast<uint64_t>(d) * num_tiles + blockIdx.x] - start);
         uint32_t run = start;
 #pragma unroll
         for (int w = 0; w < kSortWarps; ++w) {
@@ -115,22 +146,19 @@ radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict_
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < I; ++r) {
-        const uint64_t i = base + static_cast<uint64_t>(r) * 32 + lane;
-        if (i < n) {
-            const uint32_t digit = static_cast<uint32_t>(key[r] >> shift) & 0xFFu;
-            const uint32_t lp = whist[warp][digit] + rank[r];
-            skey[lp] = key[r];
-            sval[lp] = val[r];
-        }
+        const uint32_t v = my_val[r * 32];
+        if (static_cast<uint32_t>(r * 32 + lane) < rem) stage.put(whist[warp][rd[r] >> 16] + (rd[r] & 0xFFFFu), key[r], v);
     }
     __syncthreads();
-    const uint32_t tile_n = static_cast<uint32_t>(min(static_cast<uint64_t>(TILE), n - tile0));
+    const uint32_t tile_n = static_cast<uint32_t>(min(static_cast<uint64_t>(SortShape<KT>::kTile), n - tile0));
     for (uint32_t j = threadIdx.x; j < tile_n; j += kSortThreads) {
-        const KT k = skey[j];
+        KT k;
+        uint32_t v;
+        stage.get(j, k, v);
         const uint32_t digit = static_cast<uint32_t>(k >> shift) & 0xFFu;
-        const uint32_t pos = gbase[digit] + (j - tile_start[digit]);
+        const uint32_t pos = static_cast<uint32_t>(delta[digit] + static_cast<int32_t>(j));
         keys_out[pos] = k;
-        vals_out[pos] = sval[j];
+        vals_out[pos] = v;
     }
 }
 
