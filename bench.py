@@ -463,6 +463,7 @@ def run_serve_bench(args):
         """Submit item i at t0 + arrivals[i] (seconds); returns (latencies ms, wall s)."""
         tickets = [None] * R
         lat = np.zeros(R)
+        qs = np.zeros(R)
         failed = [0]
 
         def waiter():
@@ -471,6 +472,7 @@ def run_serve_bench(args):
                     time.sleep(2e-5)
                 st, q, s, _ = srv.wait(tickets[i], check=False)
                 lat[i] = q + s
+                qs[i] = q
                 failed[0] += st != 0
 
         th = threading.Thread(target=waiter)
@@ -488,9 +490,24 @@ def run_serve_bench(args):
         torch.cuda.synchronize()
         if failed[0]:
             raise RuntimeError(f"{failed[0]} of {R} requests failed")
+        run.queue = qs
         return lat, time.perf_counter() - t0
 
     run(np.zeros(R))   # warm-up: the resident arenas reach their sizes
+    # isolated latency of every (pool frame, operation): the request served alone on the
+    # idle server, median of three
+    iso_tab = np.zeros((len(pool), 2))
+    first = {}
+    for i, (f, op) in enumerate(zip(picks, ops)):
+        first.setdefault((int(f), int(op)), i)
+    for (f, op), i in first.items():
+        ts = []
+        for _ in range(3):
+            st, q, s, _ = srv.wait(srv.submit(op, items[i]), check=True)
+            ts.append(q + s)
+        iso_tab[f, op] = float(np.median(ts))
+    iso = iso_tab[picks, ops]
+    big = iso >= np.percentile(iso, 90)   # the slowest tenth of the mix when served alone
     lat0, wall0 = run(np.zeros(R))
     capacity = R / wall0
     loads = []
@@ -498,9 +515,17 @@ def run_serve_bench(args):
         lam = f * capacity
         arr = np.cumsum(np.random.default_rng(5).exponential(1.0 / lam, size=R))
         lat, wall = run(arr)
+        p99 = float(np.percentile(lat, 99))
         loads.append({"load": f, "offered_rps": round(lam, 1), "achieved_rps": round(R / wall, 1),
-                      "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
-                      "mean_ms": round(float(lat.mean()), 3)})
+                      "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(p99, 3),
+                      "mean_ms": round(float(lat.mean()), 3),
+                      "p99_over_isolated_p99": round(p99 / float(np.percentile(iso, 99)), 3),
+                      "slowdown_p50": round(float(np.percentile(lat / iso, 50)), 3),
+                      "slowdown_p99": round(float(np.percentile(lat / iso, 99)), 3),
+                      "queue_p99_ms": round(float(np.percentile(run.queue, 99)), 3),
+                      "service_p99_ms": round(float(np.percentile(lat - run.queue, 99)), 3),
+                      "p99_large_ms": round(float(np.percentile(lat[big], 99)), 3),
+                      "p99_small_ms": round(float(np.percentile(lat[~big], 99)), 3)})
     srv.close()
     return {
         "metric": "serving capacity (requests/s), mixed compress/decompress", "value": round(capacity, 1),
@@ -514,6 +539,9 @@ def run_serve_bench(args):
         "capacity_gbs": round(raw_total / wall0 / 1e9, 3),
         "saturated": {"p50_ms": round(float(np.percentile(lat0, 50)), 3),
                       "p99_ms": round(float(np.percentile(lat0, 99)), 3)},
+        "isolated": {"p50_ms": round(float(np.percentile(iso, 50)), 3), "p99_ms": round(float(np.percentile(iso, 99)), 3),
+                     "note": "each request's latency served alone on the idle server (median of 3), over the "
+                             "same request mix; slowdown = served latency / isolated latency per request"},
         "loads": loads,
     }
 
