@@ -38,11 +38,18 @@ radix_hist_kernel(const KT* __restrict__ keys, uint64_t n, int shift, uint32_t* 
     hist[threadIdx.x] = 0;
     __syncthreads();
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * TILE;
+    const uint32_t rem = base >= n ? 0u : static_cast<uint32_t>(min(n - base, static_cast<uint64_t>(TILE)));
+    // all loads first (one round trip per thread), then the shared-memory counts
+    KT k[I];
 #pragma unroll
-    for (int k = 0; k < I; ++k) {
-        const uint64_t i = base + static_cast<uint64_t>(k) * kSortThreads + threadIdx.x;
-        if (i < n) atomicAdd(&hist[static_cast<uint32_t>(keys[i] >> shift) & 0xFFu], 1u);
+    for (int r = 0; r < I; ++r) {
+        const uint32_t i = r * kSortThreads + threadIdx.x;
+        k[r] = i < rem ? __ldg(keys + base + i) : KT(0);
     }
+#pragma unroll
+    for (int r = 0; r < I; ++r)
+        if (static_cast<uint32_t>(r * kSortThreads + threadIdx.x) < rem)
+            atomicAdd(&hist[static_cast<uint32_t>(k[r] >> shift) & 0xFFu], 1u);
     __syncthreads();
     counts[static_cast<uint64_t>(threadIdx.x) * num_tiles + blockIdx.x] = hist[threadIdx.x];
 }
