@@ -358,7 +358,8 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
 // ------------------------------------------------------------------- level 1
 // Sorted position k: the sorted neighbour with an equal key is the next point of the
 // same block (stable sort keeps indices increasing within a block).  Each thread takes
-// four consecutive positions and loads them, and the fifth neighbour, before using any.
+// groups of four consecutive positions, two groups at a time, and loads them (16-byte
+// loads) and each group's fifth neighbour before using any.
 template <typename KT>
 __global__ void __launch_bounds__(256)
 k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_t n, const EncState* st,
@@ -368,32 +369,58 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
     const int64_t thr = st->threshold;
     const int64_t c = static_cast<int64_t>(D) * maxb_bits;
     const uint64_t ng = (n + 3) / 4;
-    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < ng;
-         g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        KT key[5];
-        uint32_t idx[5];
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    constexpr int kU = 2;   // groups per thread whose loads are in flight together
+    for (uint64_t g0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g0 < ng; g0 += stride * kU) {
+        KT keys[kU][5];
+        uint32_t idxs[kU][5];
 #pragma unroll
-        for (int j = 0; j < 5; ++j) {
-            const uint64_t k = 4 * g + j;
-            key[j] = k < n ? skey[k] : KT(0);
-            idx[j] = k < n ? sidx[k] : 0u;
+        for (int u = 0; u < kU; ++u) {
+            const uint64_t g = g0 + u * stride;
+            if (4 * g + 4 <= n) {   // four positions by 16-byte loads (the arrays are 256-byte aligned)
+                if constexpr (sizeof(KT) == 4) {
+                    const uint4 kv = __ldg(reinterpret_cast<const uint4*>(skey) + g);
+                    keys[u][0] = kv.x; keys[u][1] = kv.y; keys[u][2] = kv.z; keys[u][3] = kv.w;
+                } else {
+                    const ulonglong2 a = __ldg(reinterpret_cast<const ulonglong2*>(skey) + 2 * g);
+                    const ulonglong2 b = __ldg(reinterpret_cast<const ulonglong2*>(skey) + 2 * g + 1);
+                    keys[u][0] = a.x; keys[u][1] = a.y; keys[u][2] = b.x; keys[u][3] = b.y;
+                }
+                const uint4 iv = __ldg(reinterpret_cast<const uint4*>(sidx) + g);
+                idxs[u][0] = iv.x; idxs[u][1] = iv.y; idxs[u][2] = iv.z; idxs[u][3] = iv.w;
+                const uint64_t k = 4 * g + 4;
+                keys[u][4] = k < n ? __ldg(skey + k) : KT(0);
+                idxs[u][4] = k < n ? __ldg(sidx + k) : 0u;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 5; ++j) {
+                    const uint64_t k = 4 * g + j;
+                    keys[u][j] = k < n ? skey[k] : KT(0);
+                    idxs[u][j] = k < n ? sidx[k] : 0u;
+                }
+            }
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const uint64_t k = 4 * g + j;
-            uint32_t out = 0;
-            if (k + 1 < n && key[j + 1] == key[j]) {
-                const uint32_t dist = idx[j + 1] - idx[j];
-                // bit j of block coordinate d sits at key bit j * D + d, so the widest
-                // coordinate of the block has ceil(bitlen(key) / D) bits
-                const int local_bits = (bitlen64(static_cast<uint64_t>(key[j])) + D - 1) / D;
-                const int tag_bits = bitlen32(static_cast<uint32_t>(local_bits));
-                const int64_t a = static_cast<int64_t>(local_bits) * D + tag_bits;
-                const int64_t smaller = a < c ? a : c;
-                const int dl = bitlen32(dist);
-                if (static_cast<int64_t>(dl + bitlen32(static_cast<uint32_t>(dl))) < smaller - thr) out = dist;
+        for (int u = 0; u < kU; ++u) {
+            const uint64_t g = g0 + u * stride;
+            if (g >= ng) break;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint64_t k = 4 * g + j;
+                uint32_t out = 0;
+                if (k + 1 < n && keys[u][j + 1] == keys[u][j]) {
+                    const uint32_t dist = idxs[u][j + 1] - idxs[u][j];
+                    // bit j of block coordinate d sits at key bit j * D + d, so the widest
+                    // coordinate of the block has ceil(bitlen(key) / D) bits
+                    const int local_bits = (bitlen64(static_cast<uint64_t>(keys[u][j])) + D - 1) / D;
+                    const int tag_bits = bitlen32(static_cast<uint32_t>(local_bits));
+                    const int64_t a = static_cast<int64_t>(local_bits) * D + tag_bits;
+                    const int64_t smaller = a < c ? a : c;
+                    const int dl = bitlen32(dist);
+                    if (static_cast<int64_t>(dl + bitlen32(static_cast<uint32_t>(dl))) < smaller - thr) out = dist;
+                }
+                if (k < n) idrel[idxs[u][j]] = out;
             }
-            if (k < n) idrel[idx[j]] = out;
         }
     }
 }
@@ -429,22 +456,34 @@ __global__ void __launch_bounds__(256) k_l2_stats(const uint32_t* __restrict__ r
     const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     uint64_t first_scalar = 0;
     if (D == 3 && (reinterpret_cast<uintptr_t>(rec) & 15) == 0) {
+        // groups of four 3-D records; kU groups per thread in flight at once
+        constexpr int kU = 4;
         const uint64_t ng = B / 4;
-        for (uint64_t g = tid; g < ng; g += nthreads) {
-            uint32_t v[15];   // the previous record, then four records
-            const uint4* q = reinterpret_cast<const uint4*>(rec + 12 * g);
-            const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
-            v[3] = a.x; v[4] = a.y; v[5] = a.z; v[6] = a.w; v[7] = b.x; v[8] = b.y;
-            v[9] = b.z; v[10] = b.w; v[11] = c.x; v[12] = c.y; v[13] = c.z; v[14] = c.w;
+        for (uint64_t g0 = tid; g0 < ng; g0 += nthreads * kU) {
+            uint32_t v[kU][15];   // per group: the previous record, then four records
 #pragma unroll
-            for (int d = 0; d < 3; ++d) v[d] = g ? __ldg(rec + 12 * g - 3 + d) : v[3 + d];
+            for (int u = 0; u < kU; ++u) {
+                const uint64_t g = g0 + u * nthreads;
+                if (g < ng) {
+                    const uint4* q = reinterpret_cast<const uint4*>(rec + 12 * g);
+                    const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+                    v[u][3] = a.x; v[u][4] = a.y; v[u][5] = a.z; v[u][6] = a.w; v[u][7] = b.x; v[u][8] = b.y;
+                    v[u][9] = b.z; v[u][10] = b.w; v[u][11] = c.x; v[u][12] = c.y; v[u][13] = c.z; v[u][14] = c.w;
 #pragma unroll
-            for (int k = 3; k < 15; ++k) {
-                mn = v[k] < mn ? v[k] : mn;
-                mx = v[k] > mx ? v[k] : mx;
-                const uint32_t u = v[k - 3];
-                const uint32_t df = v[k] >= u ? v[k] - u : u - v[k];
-                md = df > md ? df : md;
+                    for (int d = 0; d < 3; ++d) v[u][d] = g ? __ldg(rec + 12 * g - 3 + d) : v[u][3 + d];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                if (g0 + u * nthreads >= ng) continue;
+#pragma unroll
+                for (int k = 3; k < 15; ++k) {
+                    mn = v[u][k] < mn ? v[u][k] : mn;
+                    mx = v[u][k] > mx ? v[u][k] : mx;
+                    const uint32_t w = v[u][k - 3];
+                    const uint32_t df = v[u][k] >= w ? v[u][k] - w : w - v[u][k];
+                    md = df > md ? df : md;
+                }
             }
         }
         first_scalar = ng * 4;
@@ -958,11 +997,14 @@ __global__ void __launch_bounds__(32 * kPackWarps) k_pack_fixed(const uint32_t* 
             const uint32_t w = fp.width[d];
             if (w == 0) continue;
             const uint32_t mv = fp.minv[d];
-#pragma unroll 8
+            uint32_t x[32];   // all 32 loads in flight together
+#pragma unroll
             for (int j = 0; j < 32; ++j) {
                 const uint64_t k = r0 + 32 * j + lane;
-                sw[33 * j + lane] = k < nrec ? __ldg(data + k * D + d) - mv : 0u;
+                x[j] = k < nrec ? __ldg(data + k * D + d) : mv;
             }
+#pragma unroll
+            for (int j = 0; j < 32; ++j) sw[33 * j + lane] = x[j] - mv;
             __syncwarp();
             uint64_t acc = 0;
             uint32_t nacc = 0, m = 0;
