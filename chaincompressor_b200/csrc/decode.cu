@@ -63,7 +63,10 @@ __global__ void __launch_bounds__(1024) k_section_setup(SectionRefs refs, const 
     const SectionRef R = refs.r[blockIdx.x];
     const SectionPlan& s = *R.sec;
     __shared__ uint64_t red[33];
-    if (!parse_table_block(data + s.table_off, s.table_len, s.alphabet, s.prec, R.prob, R.cum, R.scratch) &&
+    __shared__ uint8_t stage[kParseStage];
+    __shared__ uint32_t stage_scratch[kParseStageScratch];
+    if (!parse_table_block(data + s.table_off, s.table_len, s.alphabet, s.prec, R.prob, R.cum, R.scratch, stage,
+                           stage_scratch) &&
         threadIdx.x == 0)
         set_error(&st->err, kErrCorrupt);
     // chunk offsets: exclusive prefix of the u32 chunk lengths

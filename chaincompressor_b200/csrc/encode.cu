@@ -798,6 +798,7 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
 __global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncState* st, const uint32_t* hist,
                                                            uint64_t hist_stride, uint32_t* prob, uint32_t* cum,
                                                            uint32_t* tag_prob, uint32_t* tag_cum, int s0) {
+    extern __shared__ __align__(16) uint32_t tstage[];   // kTableStageBytes
     const int s = s0 + blockIdx.x, kind = blockIdx.y;
     const StreamRef r = refs.s[s];
     const uint64_t nrec = stream_records(r);
@@ -805,10 +806,11 @@ __global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncSt
         const uint32_t maxall = st->st[s].maxall;
         const bool ok = nrec > 0 && maxall < kRansMaxAlphabet;
         build_rans_table(hist + hist_stride * s, ok ? maxall + 1 : 0, ok ? nrec * r.dims : 0,
-                         prob + hist_stride * s, cum + hist_stride * s, &st->raw_tab[s]);
+                         prob + hist_stride * s, cum + hist_stride * s, &st->raw_tab[s], tstage);
     } else {
         const uint32_t A = nrec ? st->st[s].maxtag + 1 : 0;
-        build_rans_table(st->st[s].tag_hist, A, nrec, tag_prob + 64 * s, tag_cum + 64 * s, &st->tag_tab[s]);
+        build_rans_table(st->st[s].tag_hist, A, nrec, tag_prob + 64 * s, tag_cum + 64 * s, &st->tag_tab[s],
+                         tstage);
     }
 }
 
@@ -1597,8 +1599,11 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     refs.s[kCorrGaps] = StreamRef{corr_gaps, 1, nullptr, 0};
     refs.s[kCorrIds] = StreamRef{corr_ids, 1, nullptr, 0};
     launch_stats(refs, st, hist, hist_stride, dims, n, 0, kStreams, stream);
-    k_tables<<<dim3(kStreams, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob,
-                                                               tag_cum, 0); count_launch();
+    // per device, cheap; set on every call, always to the same value
+    CHAIN_CUDA(cudaFuncSetAttribute(k_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(kTableStageBytes)));
+    k_tables<<<dim3(kStreams, 2), kTableThreads, kTableStageBytes, stream>>>(refs, st, hist, hist_stride, prob, cum,
+                                                                               tag_prob, tag_cum, 0); count_launch();
     k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, 0, kStreams); count_launch();
     CHAIN_LAUNCH_CHECK("plan");
     T.mark("stats+tables+plan", stream);
@@ -1632,8 +1637,8 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         refs.s[kCorrIds].count_const = nc;
         const unsigned g = grid_for(nc, 256, 148u * 4u);
         launch_stats(refs, st, hist, hist_stride, dims, nc, kCorrGaps, 2, stream);
-        k_tables<<<dim3(2, 2), kTableThreads, 0, stream>>>(refs, st, hist, hist_stride, prob, cum, tag_prob, tag_cum,
-                                                          kCorrGaps); count_launch();
+        k_tables<<<dim3(2, 2), kTableThreads, kTableStageBytes, stream>>>(refs, st, hist, hist_stride, prob, cum,
+                                                                         tag_prob, tag_cum, kCorrGaps); count_launch();
         k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, kCorrGaps, 2); count_launch();
         CHAIN_LAUNCH_CHECK("corrections");
         CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));

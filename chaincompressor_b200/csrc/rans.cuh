@@ -67,9 +67,34 @@ __device__ inline void table_block_argmax(const uint32_t* prob, uint32_t A, uint
     __syncthreads();
 }
 
-__device__ inline void build_rans_table(const uint32_t* __restrict__ hist, uint32_t A, uint64_t n,
-                                        uint32_t* __restrict__ prob, uint32_t* __restrict__ cum,
-                                        RansTableDev* desc) {
+// Tables of up to kTableStageSyms symbols are built in shared memory (the builder makes
+// a dozen passes over the histogram and the probabilities).
+constexpr uint32_t kTableStageSyms = 16384;
+constexpr size_t kTableStageBytes = 2ull * kTableStageSyms * 4;
+
+// Copies n u32 global -> shared with the whole CTA, eight loads in flight per thread.
+__device__ __forceinline__ void block_copy32(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src,
+                                             uint32_t n) {
+    constexpr int kDepth = 8;
+    for (uint32_t i0 = threadIdx.x; i0 < n; i0 += blockDim.x * kDepth) {
+        uint32_t v[kDepth];
+#pragma unroll
+        for (int u = 0; u < kDepth; ++u) {
+            const uint32_t i = i0 + u * blockDim.x;
+            if (i < n) v[u] = __ldg(src + i);
+        }
+#pragma unroll
+        for (int u = 0; u < kDepth; ++u) {
+            const uint32_t i = i0 + u * blockDim.x;
+            if (i < n) dst[i] = v[u];
+        }
+    }
+}
+
+// stage: kTableStageBytes of shared memory, or null (work in global memory).
+__device__ inline void build_rans_table(const uint32_t* __restrict__ hist_in, uint32_t A, uint64_t n,
+                                        uint32_t* __restrict__ prob_out, uint32_t* __restrict__ cum,
+                                        RansTableDev* desc, uint32_t* stage) {
     __shared__ uint64_t red[33];
     __shared__ double redd[33];
     __shared__ uint32_t sh_best;
@@ -79,6 +104,15 @@ __device__ inline void build_rans_table(const uint32_t* __restrict__ hist, uint3
             desc->alphabet = 0; desc->prec = 0; desc->n = 0; desc->cost_bits = 0; desc->table_bytes = 0;
         }
         return;
+    }
+    const bool staged = stage && A <= kTableStageSyms;
+    const uint32_t* hist = hist_in;
+    uint32_t* prob = prob_out;
+    if (staged) {
+        block_copy32(stage, hist_in, A);
+        hist = stage;
+        prob = stage + kTableStageSyms;
+        __syncthreads();
     }
     uint64_t uniq = 0;
     for (uint32_t s = threadIdx.x; s < A; s += blockDim.x) uniq += hist[s] != 0;
@@ -203,6 +237,8 @@ __device__ inline void build_rans_table(const uint32_t* __restrict__ hist, uint3
             tbytes += 1;  // start of a zero run (runs longer than 64 are counted below)
         }
     }
+    if (staged)
+        for (uint32_t s = threadIdx.x; s < A; s += blockDim.x) prob_out[s] = prob[s];
     uint64_t zeros = 0;
     for (uint32_t s = threadIdx.x; s < A; s += blockDim.x) zeros += prob[s] == 0;
     zeros = block_reduce_sum(zeros, red);
@@ -329,16 +365,42 @@ __device__ __forceinline__ void token_shape(uint8_t first, uint32_t* bytes, uint
 }
 
 constexpr uint32_t kParseSeg = 64;
+constexpr uint32_t kParseStage = 24576;   // token bytes staged in shared memory up to this length
+constexpr uint32_t kParseStageScratch = 8 * (kParseStage / kParseSeg + 2);   // u32 scratch of a staged parse
 
 // Parses tokens with the whole CTA.  Every 64-byte segment is parsed speculatively
 // from each of its 3 possible entry offsets (a token is at most 3 bytes); one thread
 // then chains the true entries, a scan gives each segment's first symbol, and the
-// segments are parsed again for real.  scratch: 8 * (len / 64 + 2) u32.
+// segments are parsed again for real.  Token walks and the entry chain are chains of
+// dependent reads, so a table of up to kParseStage bytes is first copied to shared
+// memory (`stage`, kParseStage bytes) and its scratch kept there too (`stage_scratch`,
+// kParseStageScratch u32); larger ones use `global_scratch`, 8 * (len / 64 + 2) u32.
 // Returns false (in every thread) on malformed input.
-__device__ inline bool parse_table_block(const uint8_t* in, uint32_t len, uint32_t A, uint32_t prec,
-                                         uint32_t* prob, uint32_t* cum, uint32_t* scratch) {
+__device__ inline bool parse_table_block(const uint8_t* in_global, uint32_t len, uint32_t A, uint32_t prec,
+                                         uint32_t* prob, uint32_t* cum, uint32_t* global_scratch, uint8_t* stage,
+                                         uint32_t* stage_scratch) {
     __shared__ int s_ok;
     __shared__ uint64_t sscratch[33];
+    const uint8_t* in = in_global;
+    uint32_t* scratch = global_scratch;
+    if (len <= kParseStage) {
+        constexpr int kDepth = 8;   // loads in flight per thread
+        for (uint32_t i0 = threadIdx.x; i0 < len; i0 += blockDim.x * kDepth) {
+            uint8_t v[kDepth];
+#pragma unroll
+            for (int u = 0; u < kDepth; ++u) {
+                const uint32_t i = i0 + u * blockDim.x;
+                v[u] = i < len ? in_global[i] : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < kDepth; ++u) {
+                const uint32_t i = i0 + u * blockDim.x;
+                if (i < len) stage[i] = v[u];
+            }
+        }
+        in = stage;   // the __syncthreads below orders the copy before the reads
+        scratch = stage_scratch;
+    }
     const uint32_t nseg = (len + kParseSeg - 1) / kParseSeg;
     uint32_t* ex = scratch;              // [nseg][3] exit offset into the next segment
     uint32_t* cnt = scratch + 3 * nseg;  // [nseg][3] symbols
@@ -412,17 +474,29 @@ __device__ inline bool parse_table_block(const uint8_t* in, uint32_t len, uint32
     }
     __syncthreads();
     if (!s_ok) return false;
-    // cumulative table and total: each thread sums a contiguous run of symbols, one
-    // block scan gives the runs' offsets
+    // cumulative table and total: each thread sums a contiguous run of symbols (read
+    // eight at a time), one block scan gives the runs' offsets
     const uint32_t per = (A + blockDim.x - 1) / blockDim.x;
     const uint32_t s0 = threadIdx.x * per, s1 = min(A, s0 + per);
     uint64_t run = 0;
-    for (uint32_t s = s0; s < s1; ++s) run += prob[s];
+    for (uint32_t b = s0; b < s1; b += 8) {
+        uint32_t v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = b + u < s1 ? prob[b + u] : 0u;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) run += v[u];
+    }
     uint64_t total;
     uint64_t c = block_exclusive_sum(run, sscratch, &total);
-    for (uint32_t s = s0; s < s1; ++s) {
-        cum[s] = static_cast<uint32_t>(c > 0xffffffffull ? 0xffffffffu : c);
-        c += prob[s];
+    for (uint32_t b = s0; b < s1; b += 8) {
+        uint32_t v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = b + u < s1 ? prob[b + u] : 0u;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (b + u < s1) cum[b + u] = static_cast<uint32_t>(c > 0xffffffffull ? 0xffffffffu : c);
+            c += v[u];
+        }
     }
     return total == M;
 }
