@@ -53,6 +53,7 @@ struct SectionRef {
     uint8_t* image;     // the rANS decoder's shared-memory tables (dec_image_bytes), or null
     uint64_t* slots;    // packed slot entries when the section has no image, or null
     uint64_t* chunk_off;
+    uint64_t states_first;   // the section's first entry in the decoder's lane-state array
 };
 struct SectionRefs {
     SectionRef r[kCodeStreams];
@@ -135,19 +136,21 @@ __global__ void __launch_bounds__(256) k_lookup(SectionRefs refs, const DecState
 }
 
 // Unpacks the final lane states of every chunk (prec + 10 bits each, MSB-first).
-__global__ void __launch_bounds__(256) k_states(SectionRefs refs, const uint8_t* data, uint32_t* states_base,
-                                                 const uint64_t* states_first) {
+__global__ void __launch_bounds__(256) k_states(SectionRefs refs, const uint8_t* data, uint32_t* states_base) {
     const SectionRef R = refs.r[blockIdx.y];
     const SectionPlan& s = *R.sec;
-    uint32_t* out = states_base + states_first[blockIdx.y];
+    uint32_t* out = states_base + R.states_first;
     const uint64_t words = static_cast<uint64_t>(s.lanes) * s.chunks;
-    const uint32_t B = state_bits(s.prec);
+    const uint32_t B = state_bits(s.prec);   // <= 32
     const uint8_t* q = data + s.states_off;
     for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < words;
          w += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint64_t bit = w * B, v = 0;
-        for (uint32_t k = 0; k < B; ++k, ++bit) v = (v << 1) | ((q[bit >> 3] >> (7 - (bit & 7))) & 1u);
-        out[w] = static_cast<uint32_t>(v);
+        // the state's B bits lie in the (at most five) bytes from its first bit's byte
+        const uint64_t bit = w * B;
+        const uint32_t off = static_cast<uint32_t>(bit & 7), nb = (off + B + 7) >> 3;
+        uint64_t acc = 0;
+        for (uint32_t i = 0; i < nb; ++i) acc = (acc << 8) | q[(bit >> 3) + i];
+        out[w] = static_cast<uint32_t>((acc >> (8 * nb - off - B)) & ((1ull << B) - 1));
     }
 }
 
@@ -938,7 +941,6 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     // ---- entropy sections
     SectionRefs refs{};
     RansJobs jobs{};
-    uint64_t states_first[kCodeStreams] = {0};
     uint64_t slot_base = 0, image_base = 0, alpha_base = 0, chunk_base = 0, off_base = 0, pscr_base = 0;
     uint32_t first = 0;
     int nsec = 0;
@@ -955,7 +957,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         R.image = img ? image_buf + image_base : nullptr;
         R.slots = img ? nullptr : slots64 + slot_base;
         R.chunk_off = chunk_off + off_base;
-        states_first[nsec] = chunk_base * 32;
+        R.states_first = chunk_base * 32;
         RansJob& jb = jobs.job[jobs.njobs++];
         jb.count = c.sec.count;
         jb.prob = R.prob;
@@ -983,13 +985,10 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     }
     refs.count = nsec;
     jobs.total_blocks = first;
-    uint64_t* d_states_first = misc + 8;   // nsec <= 7 entries -> misc[8..14]
-    CHAIN_CUDA(cudaMemcpyAsync(d_states_first, states_first, sizeof(uint64_t) * kCodeStreams, cudaMemcpyHostToDevice,
-                               stream));
     if (nsec) {
         k_section_setup<<<nsec, 1024, 0, stream>>>(refs, dcont, st); count_launch();
         k_lookup<<<dim3(256, nsec), 256, 0, stream>>>(refs, st); count_launch();
-        k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states, d_states_first); count_launch();
+        k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states); count_launch();
         T.mark("tables", stream);
         rans_plan_smem(jobs, true);
         if (rans_dec_smem(jobs) > kRansDecSmemMax)

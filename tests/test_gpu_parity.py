@@ -142,3 +142,21 @@ def test_gpu_matches_reference_golden(codec, path):
         assert np.array_equal(got[k], g[k]), k
     dec = codec.decompress(data)
     assert np.array_equal(dec.view(np.uint64), g["decoded"].view(np.uint64))
+
+
+@pytest.mark.parametrize("name", ["column", "blobs200k", "traj_f64_e4_p1", "blobs_clipped", "uniform_p64_t25"])
+def test_device_container_decodes_like_host_container(codec, name):
+    """A container already in device memory is parsed on the device (the host copy is
+    parsed on the host); both must give the same points, for device and host outputs."""
+    import torch
+    pts, eb, p, t, kw = case(name)
+    data = codec.compress(_soa(pts), eb, p, t, layout=N.CHAIN_SOA, **kw)
+    want = codec.decompress(data)
+    n, d = want.shape
+    dsrc = torch.frombuffer(bytearray(data), dtype=torch.uint8).cuda()
+    dout = torch.empty((n, d), dtype=torch.float64, device="cuda")
+    assert codec.decompress_ptr(dsrc.data_ptr(), len(data), dout.data_ptr(), dout.numel() * 8) == (n, d)
+    assert np.array_equal(dout.cpu().numpy().view(np.uint64), want.view(np.uint64))
+    hout = np.empty((n, d), np.float64)
+    codec.decompress_ptr(dsrc.data_ptr(), len(data), hout.ctypes.data, hout.nbytes)
+    assert np.array_equal(hout.view(np.uint64), want.view(np.uint64))
