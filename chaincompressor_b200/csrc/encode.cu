@@ -545,50 +545,86 @@ struct Level2In {
         return value_bits >= diff_bits ? 1u : 0u;
     }
 };
-// choice2[j] for every record (1 = difference from the previous record).  Three-
-// dimensional records are read four per thread with 16-byte loads (the rule of
-// Level2In, lcps_cpp.cpp:1305-1454, applied in registers).
-__global__ void __launch_bounds__(256) k_l2_choice(Level2In f, uint32_t* choice2) {
+// choice2[j] for every record (1 = difference from the previous record), one CTA per
+// flag-scan tile of kFlagTile records; each CTA also writes its tile's count of
+// difference records, so the level-2 flag scan needs no counting pass.  Three-
+// dimensional records are read in groups of four with 16-byte loads, four groups per
+// thread, all loads first (the rule of Level2In, lcps_cpp.cpp:1305-1454, applied in
+// registers).
+__global__ void __launch_bounds__(256) k_l2_choice(Level2In f, uint32_t* choice2, uint32_t* tile_counts) {
+    static_assert(kFlagTile == 4 * 4 * 256, "four groups of four records per thread");
+    __shared__ uint32_t wsum[8];
     const EncState* st = f.st;
     const uint32_t B = st->B, D = st->dims;
-    const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    uint64_t first_scalar = 0;
+    const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile;
+    uint32_t cnt = 0;
     if (f.l2 && D == 3 && ((reinterpret_cast<uintptr_t>(f.rec) | reinterpret_cast<uintptr_t>(choice2)) & 15) == 0) {
         const uint64_t fvb = 3ull * bitlen32(st->rec_max);
         const uint64_t fdb = 3ull * bitlen32(st->rec_maxdiff);
-        const uint64_t ng = B / 4;
-        for (uint64_t g = tid; g < ng; g += nthreads) {
-            uint32_t v[15];
-            const uint4* q = reinterpret_cast<const uint4*>(f.rec + 12 * g);
-            const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
-            v[3] = a.x; v[4] = a.y; v[5] = a.z; v[6] = a.w; v[7] = b.x; v[8] = b.y;
-            v[9] = b.z; v[10] = b.w; v[11] = c.x; v[12] = c.y; v[13] = c.z; v[14] = c.w;
+        constexpr int kG = 4;
+        uint32_t v[kG][15];   // per group: the previous record, then four records
 #pragma unroll
-            for (int d = 0; d < 3; ++d) v[d] = g ? __ldg(f.rec + 12 * g - 3 + d) : 0u;
-            uint32_t ch[4];
+        for (int u = 0; u < kG; ++u) {
+            const uint64_t g = tile0 / 4 + u * 256 + threadIdx.x;
+            if (4 * g + 4 <= B) {
+                const uint4* q = reinterpret_cast<const uint4*>(f.rec + 12 * g);
+                const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+                v[u][3] = a.x; v[u][4] = a.y; v[u][5] = a.z; v[u][6] = a.w; v[u][7] = b.x; v[u][8] = b.y;
+                v[u][9] = b.z; v[u][10] = b.w; v[u][11] = c.x; v[u][12] = c.y; v[u][13] = c.z; v[u][14] = c.w;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                uint32_t mv = 0, mdd = 0;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    const uint32_t x = v[3 + 3 * k + d], u = v[3 * k + d];
-                    mv = x > mv ? x : mv;
-                    const uint32_t df = x >= u ? x - u : u - x;
-                    mdd = df > mdd ? df : mdd;
-                }
-                const int tvw = bitlen32(mv), tdw = bitlen32(mdd);
-                const uint64_t tvb = 3ull * tvw + bitlen32(static_cast<uint32_t>(tvw));
-                const uint64_t tdb = 3ull * tdw + bitlen32(static_cast<uint32_t>(tdw));
-                const uint64_t value_bits = tvb < fvb ? tvb : fvb;
-                const uint64_t diff_bits = tdb > fdb ? tdb : fdb;
-                ch[k] = (4 * g + k == 0) ? 0u : (value_bits >= diff_bits ? 1u : 0u);
+                for (int d = 0; d < 3; ++d) v[u][d] = g ? __ldg(f.rec + 12 * g - 3 + d) : 0u;
             }
-            *reinterpret_cast<uint4*>(choice2 + 4 * g) = make_uint4(ch[0], ch[1], ch[2], ch[3]);
         }
-        first_scalar = ng * 4;
+#pragma unroll
+        for (int u = 0; u < kG; ++u) {
+            const uint64_t g = tile0 / 4 + u * 256 + threadIdx.x;
+            if (4 * g + 4 <= B) {
+                uint32_t ch[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    uint32_t mv = 0, mdd = 0;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const uint32_t x = v[u][3 + 3 * k + d], w = v[u][3 * k + d];
+                        mv = x > mv ? x : mv;
+                        const uint32_t df = x >= w ? x - w : w - x;
+                        mdd = df > mdd ? df : mdd;
+                    }
+                    const int tvw = bitlen32(mv), tdw = bitlen32(mdd);
+                    const uint64_t tvb = 3ull * tvw + bitlen32(static_cast<uint32_t>(tvw));
+                    const uint64_t tdb = 3ull * tdw + bitlen32(static_cast<uint32_t>(tdw));
+                    const uint64_t value_bits = tvb < fvb ? tvb : fvb;
+                    const uint64_t diff_bits = tdb > fdb ? tdb : fdb;
+                    ch[k] = (4 * g + k == 0) ? 0u : (value_bits >= diff_bits ? 1u : 0u);
+                    cnt += ch[k];
+                }
+                *reinterpret_cast<uint4*>(choice2 + 4 * g) = make_uint4(ch[0], ch[1], ch[2], ch[3]);
+            } else {
+                for (uint64_t j = 4 * g; j < 4 * g + 4 && j < B; ++j) {
+                    const uint32_t c = f(j);
+                    choice2[j] = c;
+                    cnt += c;
+                }
+            }
+        }
+    } else {
+        for (int k = 0; k < kFlagTile / 256; ++k) {
+            const uint64_t j = tile0 + k * 256 + threadIdx.x;
+            if (j < B) {
+                const uint32_t c = f(j);
+                choice2[j] = c;
+                cnt += c;
+            }
+        }
     }
-    for (uint64_t j = first_scalar + tid; j < B; j += nthreads) choice2[j] = f(j);
+    cnt = warp_sum(cnt);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < 8; ++w) t += wsum[w];
+        tile_counts[blockIdx.x] = t;
+    }
 }
 struct Level2Flag {
     const uint32_t* choice2;
@@ -1582,8 +1618,8 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     T.mark("explicit_records", stream);
     k_l2_stats<<<grid_for(n), 256, 0, stream>>>(rec, st); count_launch();
     k_l2_params<<<1, 1, 0, stream>>>(st); count_launch();
-    k_l2_choice<<<grid_for(n), 256, 0, stream>>>(Level2In{rec, st, l2}, choice2); count_launch();
-    device_flag_scan(Level2Flag{choice2, st}, Level2Out{rec, st, keep, diff}, n, scan32, &st->ndiff, stream);
+    k_l2_choice<<<static_cast<unsigned>(flag_tiles(n)), 256, 0, stream>>>(Level2In{rec, st, l2}, choice2, scan32); count_launch();
+    device_flag_scan_counted(Level2Flag{choice2, st}, Level2Out{rec, st, keep, diff}, n, scan32, &st->ndiff, stream);
     k_l2_counts<<<1, 1, 0, stream>>>(st); count_launch();
     CHAIN_LAUNCH_CHECK("level 2");
     T.mark("level2", stream);

@@ -291,4 +291,18 @@ void device_flag_scan(Pred pred, OutF out, uint64_t n, uint32_t* tile_buf, uint3
     flag_apply_kernel<Pred, OutF><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, out, n, tile_buf); count_launch();
 }
 
+// The same scan when the per-tile counts are already in `tile_buf` (a producer kernel
+// that runs one CTA per kFlagTile elements wrote them).
+template <typename Pred, typename OutF>
+void device_flag_scan_counted(Pred pred, OutF out, uint64_t n, uint32_t* tile_buf, uint32_t* total,
+                              cudaStream_t stream) {
+    const uint64_t tiles = flag_tiles(n);
+    if (tiles == 0) {
+        if (total) cudaMemsetAsync(total, 0, sizeof(uint32_t), stream);
+        return;
+    }
+    scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(tile_buf, tiles, total, SumOp<uint32_t>()); count_launch();
+    flag_apply_kernel<Pred, OutF><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, out, n, tile_buf); count_launch();
+}
+
 }  // namespace chain
