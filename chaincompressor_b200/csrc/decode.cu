@@ -370,6 +370,19 @@ struct L2Geo {
         bad = bad || !ok;
         return ok ? static_cast<uint32_t>(corr <= 0 ? -corr : static_cast<int64_t>(range) - corr) : 0u;
     }
+    // The same two rules on an already loaded value.
+    __device__ __forceinline__ uint32_t diff_value(uint32_t sym, bool& bad) const {
+        const int64_t corr = unzigzag(sym);
+        const bool ok = corr >= minc && corr <= maxc;   // lcps_cpp.cpp:1917-1918
+        bad = bad || !ok;
+        return ok ? static_cast<uint32_t>(corr <= 0 ? -corr : static_cast<int64_t>(range) - corr) : 0u;
+    }
+    __device__ __forceinline__ uint32_t keep_check(uint32_t raw, bool& bad) const {
+        const int64_t v = raw;
+        const bool ok = v >= wrap_min && v <= wrap_max;   // lcps_cpp.cpp:1905-1907
+        bad = bad || !ok;
+        return ok ? static_cast<uint32_t>(v - wrap_min) : 0u;
+    }
     __device__ __forceinline__ uint32_t keep_value(uint64_t row, uint32_t kk, bool& bad) const {
         const int64_t v = keep[row * D + d0 + kk];
         const bool ok = v >= wrap_min && v <= wrap_max;   // lcps_cpp.cpp:1905-1907
@@ -489,6 +502,20 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec
     __syncthreads();
     uint64_t rank = g.tile_diff[blockIdx.x] + incl_cnt - cnt;   // diff records before j0
     for (int w = 0; w < warp; ++w) rank += s_cnt[w];
+    // every record's row first (one memory round trip for the lane), then the terms
+    uint32_t raw[P][3];
+    {
+        uint64_t rk = rank;
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const uint64_t j = j0 + k;
+            const bool is_diff = (dmask >> k) & 1u;
+            const uint32_t* row = is_diff ? g.diff + rk * g.D + g.d0 : g.keep + (j - rk) * g.D + g.d0;
+#pragma unroll
+            for (uint32_t kk = 0; kk < 3; ++kk) raw[k][kk] = (j < g.B && g.d0 + kk < g.D) ? __ldg(row + kk) : 0u;
+            rk += is_diff;
+        }
+    }
     L2Vec t[P];
 #pragma unroll
     for (int k = 0; k < P; ++k) {
@@ -498,13 +525,12 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec
         if ((dmask >> k) & 1u) {
 #pragma unroll
             for (uint32_t kk = 0; kk < 3; ++kk)
-                if (g.d0 + kk < g.D) t[k].v[kk] = g.diff_term(rank, kk, bad);
-            ++rank;
+                if (g.d0 + kk < g.D) t[k].v[kk] = g.diff_value(raw[k][kk], bad);
         } else {
             t[k].restart = 1;
 #pragma unroll
             for (uint32_t kk = 0; kk < 3; ++kk)
-                if (g.d0 + kk < g.D) t[k].v[kk] = g.keep_value(j - rank, kk, bad);
+                if (g.d0 + kk < g.D) t[k].v[kk] = g.keep_check(raw[k][kk], bad);
         }
     }
     L2Vec agg = t[0];
