@@ -689,10 +689,36 @@ struct ReconCtx {
         return fma(__dadd_rn(static_cast<double>(q), 0.5), two_eb, minima[d]);
     }
 };
+// REL0 read straight from its fixed-width packing (three dimensions, widths <= 8) when
+// `on`, instead of from an unpacked array: a dimension's value of point i is minv + the
+// w bits at bit i * w of that dimension's MSB-first stream.
+struct RelBits {
+    const uint8_t* data;
+    uint64_t len;
+    uint64_t off[3];
+    uint32_t minv[3], w[3];
+    int on;
+    // Dimension d of points i0 .. i0 + 3: four w-bit values span at most 39 bits, the
+    // five bytes from the first value's byte.
+    __device__ __forceinline__ void four(uint64_t i0, uint32_t d, uint32_t (&v)[4]) const {
+        const uint32_t wd = w[d];
+        const uint64_t bit0 = i0 * wd;
+        const uint64_t b = off[d] + (bit0 >> 3);
+        uint64_t win = 0;
+#pragma unroll
+        for (int i = 0; i < 5; ++i) win = (win << 8) | (b + i < len ? __ldg(data + b + i) : 0u);
+        const uint32_t top = 40 - static_cast<uint32_t>(bit0 & 7);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            v[k] = minv[d] + (wd ? static_cast<uint32_t>((win >> (top - (k + 1) * wd)) & ((1u << wd) - 1)) : 0u);
+    }
+};
+
 template <typename OT, bool SOA>
 __global__ void __launch_bounds__(256)
 k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ compact,
-              const uint32_t* __restrict__ rel, const DecState* stc, DecState* st, OT* __restrict__ out) {
+              const uint32_t* __restrict__ rel, const DecState* stc, DecState* st, OT* __restrict__ out,
+              RelBits rb) {
     const DecodePlan& P = stc->plan;
     const uint32_t D = P.D;
     const uint64_t n = P.N;
@@ -722,12 +748,23 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
             }
         }
         if (D == 3 && full && vec) {
-            // four whole points: 16-byte loads of rel, 16-byte stores of the output
+            // four whole points: 16-byte loads of rel (or its packed bits), 16-byte stores
+            // of the output
             uint32_t rl[12];
-            const uint4* rp = reinterpret_cast<const uint4*>(rel + g * 12);
-            *reinterpret_cast<uint4*>(rl) = __ldg(rp);
-            *reinterpret_cast<uint4*>(rl + 4) = __ldg(rp + 1);
-            *reinterpret_cast<uint4*>(rl + 8) = __ldg(rp + 2);
+            if (rb.on) {
+#pragma unroll
+                for (uint32_t d = 0; d < 3; ++d) {
+                    uint32_t v[4];
+                    rb.four(g * kReconPer, d, v);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) rl[3 * k + d] = v[k];
+                }
+            } else {
+                const uint4* rp = reinterpret_cast<const uint4*>(rel + g * 12);
+                *reinterpret_cast<uint4*>(rl) = __ldg(rp);
+                *reinterpret_cast<uint4*>(rl + 4) = __ldg(rp + 1);
+                *reinterpret_cast<uint4*>(rl + 8) = __ldg(rp + 2);
+            }
             uint32_t blk[kReconPer][3];
 #pragma unroll
             for (int k = 0; k < kReconPer; ++k) {
@@ -774,6 +811,16 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
                 }
             }
         } else if (D == 3) {
+            uint32_t rl[12];
+            if (rb.on) {
+#pragma unroll
+                for (uint32_t d = 0; d < 3; ++d) {
+                    uint32_t v[4];
+                    rb.four(g * kReconPer, d, v);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) rl[3 * k + d] = v[k];
+                }
+            }
             uint32_t blk[kReconPer][3];
 #pragma unroll
             for (int k = 0; k < kReconPer; ++k) {
@@ -789,7 +836,7 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
                 bool b = (pw[k] & kParentMask) >= R.B;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    const int64_t off = rel[i * 3 + d];
+                    const int64_t off = rb.on ? rl[3 * k + d] : rel[i * 3 + d];
                     if (off >= R.p) b = true;
                     const int64_t bk = b ? 0 : static_cast<int64_t>(blk[k][d]);
                     if (bk > R.safe_blk && bk > (INT64_MAX - off) / R.p) b = true;
@@ -1029,10 +1076,30 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     }
     CHAIN_LAUNCH_CHECK("entropy decode");
     T.mark("rans_decode", stream);
+    // REL0 fixed-width with three narrow dimensions is read by the reconstruction
+    // straight from its packing (no unpacked copy)
+    RelBits relbits{};
+    {
+        const CompPlan& c = plan.comp[4];
+        bool on = c.enc == kEncFixed && c.dims == 3 && D == 3;
+        for (uint32_t d = 0; on && d < 3; ++d)
+            on = c.width[d] <= 8 && c.minv[d] + ((1ull << c.width[d]) - 1) <= 0xffffffffull;
+        if (on) {
+            relbits.data = dcont;
+            relbits.len = len;
+            for (uint32_t d = 0; d < 3; ++d) {
+                relbits.off[d] = c.packed_off[d];
+                relbits.minv[d] = static_cast<uint32_t>(c.minv[d]);
+                relbits.w[d] = c.width[d];
+            }
+            relbits.on = 1;
+        }
+    }
     // ---- tagged and fixed components
     for (int s = 0; s < kCodeStreams; ++s) {
         const CompPlan& c = plan.comp[s];
         const CompPlan* dc = &st->plan.comp[s];
+        if (s == 4 && relbits.on) continue;
         if (c.enc == kEncFixed) {
             uint32_t wsum = 0;
             for (uint32_t d = 0; d < c.dims; ++d) wsum += c.width[d];
@@ -1112,22 +1179,22 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         if (out_dtype == CHAIN_F64) {
             double* o = static_cast<double*>(dout);
             if (soa) {
-                k_reconstruct<double, true><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o); count_launch();
+                k_reconstruct<double, true><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o, relbits); count_launch();
                 if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<double, true>{streams[kCorrIds], dcont, st, st, o},
                                                          ncx, sb, static_cast<uint64_t*>(nullptr), stream);
             } else {
-                k_reconstruct<double, false><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o); count_launch();
+                k_reconstruct<double, false><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o, relbits); count_launch();
                 if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<double, false>{streams[kCorrIds], dcont, st, st, o},
                                                          ncx, sb, static_cast<uint64_t*>(nullptr), stream);
             }
         } else {
             float* o = static_cast<float*>(dout);
             if (soa) {
-                k_reconstruct<float, true><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o); count_launch();
+                k_reconstruct<float, true><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o, relbits); count_launch();
                 if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<float, true>{streams[kCorrIds], dcont, st, st, o},
                                                          ncx, sb, static_cast<uint64_t*>(nullptr), stream);
             } else {
-                k_reconstruct<float, false><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o); count_launch();
+                k_reconstruct<float, false><<<g, 256, 0, stream>>>(parent, compact, streams[4], st, st, o, relbits); count_launch();
                 if (ncx) device_exclusive_scan<uint64_t>(cin, CorrOut<float, false>{streams[kCorrIds], dcont, st, st, o},
                                                          ncx, sb, static_cast<uint64_t*>(nullptr), stream);
             }
