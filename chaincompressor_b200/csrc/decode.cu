@@ -317,6 +317,27 @@ struct ResetAddOp {
     __device__ __forceinline__ static L2Vec identity() { return L2Vec{0, {0, 0, 0}}; }
 };
 
+// Difference records per flag-scan tile from CH20's 1-bit packing: one CTA per tile,
+// one 32-record word per thread.
+__global__ void __launch_bounds__(kFlagTile / 32) k_choice_counts(const uint8_t* cbits, uint64_t len, uint64_t off,
+                                                                  uint64_t B, uint32_t* tile_counts) {
+    __shared__ uint32_t wsum[kFlagTile / 32 / 32];
+    const uint64_t j0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile + 32ull * threadIdx.x;
+    uint32_t c = 0;
+    if (j0 < B) {
+        const uint32_t valid = B - j0 >= 32 ? 0xffffffffu : (1u << (B - j0)) - 1u;
+        c = __popc(__brev(load_be32(cbits, len, off + j0 / 8)) & valid);
+    }
+    c = warp_sum(c);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kFlagTile / 32 / 32; ++w) t += wsum[w];
+        tile_counts[blockIdx.x] = t;
+    }
+}
+
 // Choice values are clamped to {0, 1} for the ranks (so every derived index stays in
 // bounds) and validated separately (lcps_cpp.cpp:1899-1900, 1911-1912).
 struct ChoiceIn {
@@ -337,7 +358,9 @@ constexpr int kL2Warps = 16;
 constexpr int kL2Rounds = kFlagTile / (32 * kL2Warps);
 static_assert(kL2Rounds * 32 * kL2Warps == kFlagTile, "level-2 tiles are flag-scan tiles");
 struct L2Geo {
-    const uint32_t* choice2;
+    const uint32_t* choice2;     // unpacked choices, when cbits is null
+    const uint8_t* cbits;        // else CH20's fixed 1-bit packing (minimum 0): record j = bit j from cbits_off
+    uint64_t cbits_off, cbits_len;
     const uint32_t* keep;
     const uint32_t* diff;
     const uint32_t* tile_diff;   // exclusive count of difference records before each tile
@@ -347,14 +370,25 @@ struct L2Geo {
     int64_t wrap_min, wrap_max, minc, maxc;
     // Difference-record masks of this warp's rounds and the warp's first diff rank.
     // Contains a __syncthreads: every thread of the CTA calls it.
+    // Difference flags of records [j0, j0 + 32) as a lane mask (j0 a multiple of 32).
+    __device__ __forceinline__ uint32_t flags32(uint64_t j0) const {
+        if (cbits) {
+            const uint32_t valid = j0 >= B ? 0u : (B - j0 >= 32 ? 0xffffffffu : (1u << (B - j0)) - 1u);
+            return __brev(load_be32(cbits, cbits_len, cbits_off + j0 / 8)) & valid;
+        }
+        const int lane = threadIdx.x & 31;
+        const uint64_t j = j0 + lane;
+        return __ballot_sync(0xffffffffu, j < B && choice2[j] != 0);
+    }
     __device__ __forceinline__ uint32_t ranks(uint32_t (&m)[kL2Rounds], uint32_t* s_cnt) const {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * kL2Rounds;
         uint32_t c = 0;
+        // packed choices: lane k loads round k's word, then every lane takes them all
+        const uint32_t mine = cbits && lane < kL2Rounds ? flags32(base + 32 * lane) : 0u;
 #pragma unroll
         for (int k = 0; k < kL2Rounds; ++k) {
-            const uint64_t j = base + 32 * k + lane;
-            m[k] = __ballot_sync(0xffffffffu, j < B && choice2[j] != 0);
+            m[k] = cbits ? __shfl_sync(0xffffffffu, mine, k) : flags32(base + 32 * k);
             c += __popc(m[k]);
         }
         if (lane == 0) s_cnt[warp] = c;
@@ -475,7 +509,13 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec
                         static_cast<uint64_t>(lane) * P;
     const ResetAddOp op{static_cast<uint32_t>(g.range), static_cast<uint32_t>(g.range >> 32)};
     uint32_t c[P];
-    if (j0 + P <= g.B && (reinterpret_cast<uintptr_t>(g.choice2 + j0) & 15) == 0) {
+    if (g.cbits) {   // records j0 .. j0 + 7: one byte of the packing (j0 is a multiple of 8)
+        static_assert(P == 8, "one packed byte per lane");
+        const uint64_t at = g.cbits_off + j0 / 8;
+        const uint32_t byte = at < g.cbits_len ? __ldg(g.cbits + at) : 0u;
+#pragma unroll
+        for (int k = 0; k < P; ++k) c[k] = (byte >> (7 - k)) & 1u;
+    } else if (j0 + P <= g.B && (reinterpret_cast<uintptr_t>(g.choice2 + j0) & 15) == 0) {
         const uint4* q = reinterpret_cast<const uint4*>(g.choice2 + j0);
 #pragma unroll
         for (int v = 0; v < P / 4; ++v) {
@@ -1095,11 +1135,15 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
             relbits.on = 1;
         }
     }
+    // CH20 packed one bit per record with minimum 0 (values 0 and 1) is read bitwise by
+    // the level-2 inverse
+    const bool choice_packed =
+        plan.comp[3].enc == kEncFixed && plan.comp[3].dims == 1 && plan.comp[3].width[0] == 1 && plan.comp[3].minv[0] == 0;
     // ---- tagged and fixed components
     for (int s = 0; s < kCodeStreams; ++s) {
         const CompPlan& c = plan.comp[s];
         const CompPlan* dc = &st->plan.comp[s];
-        if (s == 4 && relbits.on) continue;
+        if ((s == 4 && relbits.on) || (s == 3 && choice_packed)) continue;
         if (c.enc == kEncFixed) {
             uint32_t wsum = 0;
             for (uint32_t d = 0; d < c.dims; ++d) wsum += c.width[d];
@@ -1126,13 +1170,21 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     uint32_t* tile_diff = reinterpret_cast<uint32_t*>(scanbuf);
     L2Vec* tile_l2 = reinterpret_cast<L2Vec*>(reinterpret_cast<uint8_t*>(scanbuf) + ((4 * l2tiles + 15) & ~15ull));
     if (l2tiles) {
-        flag_count_kernel<ChoiceIn><<<static_cast<unsigned>(l2tiles), kFlagThreads, 0, stream>>>(ChoiceIn{streams[3]}, B,
-                                                                                                 tile_diff); count_launch();
+        if (choice_packed)
+            k_choice_counts<<<static_cast<unsigned>(l2tiles), kFlagTile / 32, 0, stream>>>(
+                dcont, len, plan.comp[3].packed_off[0], B, tile_diff);
+        else
+            flag_count_kernel<ChoiceIn><<<static_cast<unsigned>(l2tiles), kFlagThreads, 0, stream>>>(
+                ChoiceIn{streams[3]}, B, tile_diff);
+        count_launch();
         scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(tile_diff, l2tiles, ndiff_dev,
                                                                                 SumOp<uint32_t>()); count_launch();
         const ResetAddOp l2op{static_cast<uint32_t>(range), static_cast<uint32_t>(range >> 32)};
         L2Geo g;
         g.choice2 = streams[3];
+        g.cbits = choice_packed ? dcont : nullptr;
+        g.cbits_off = plan.comp[3].packed_off[0];
+        g.cbits_len = len;
         g.keep = streams[2];
         g.diff = streams[1];
         g.tile_diff = tile_diff;
