@@ -928,9 +928,10 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
         c.est[kEncTagged] = 13 + 1 + section_overhead(t.table_bytes, tag_ch, tag_lanes, t.prec) +
                             static_cast<uint64_t>(payload) + 1 + 8 + (g.tag_bits + 7) / 8;
     }
-    // raw.  Tables too large for shared memory cost one L2 round trip per coded symbol on
-    // both sides, so on streams long enough to fill the GPU their lanes get a shorter
-    // serial depth.
+    // raw.  Tables too large for the shared-memory fast paths make every coded symbol
+    // slower on both sides, so from kLargeTableMinSymbols on their lanes get a shorter
+    // serial depth: kLargeTableShortSteps while the frame's chunks still fit one decoder
+    // wave, kLargeTableMaxSteps beyond.
     uint32_t raw_ch = 0, raw_lanes = 0;
     uint64_t raw_S = 0;
     if (g.maxall < kRansMaxAlphabet && st->raw_tab[s].alphabet != 0) {
@@ -938,7 +939,8 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
         const double payload = t.cost_bits / 8.0;
         const bool large = (t.alphabet > kSmemEncSyms || (1u << t.prec) > kSmemLookupSlots) &&
                            nrec * r.dims >= kLargeTableMinSymbols;
-        const uint32_t steps = large ? min(max_steps, kLargeTableMaxSteps) : max_steps;
+        const uint32_t deep = nrec * r.dims >= kLargeTableDeepSymbols ? kLargeTableMaxSteps : kLargeTableShortSteps;
+        const uint32_t steps = large ? min(max_steps, deep) : max_steps;
         plan_chunks(nrec * r.dims, payload, bytes_per_lane, steps, &raw_ch, &raw_S, &raw_lanes);
         c.est[kEncRaw] = 13 + section_overhead(t.table_bytes, raw_ch, raw_lanes, t.prec) + static_cast<uint64_t>(payload) + 1;
     }

@@ -552,8 +552,14 @@ constexpr uint32_t kSmemLookupSlots = 16384;  // u16 decode lookup in shared mem
 constexpr uint32_t kBucketBits = 13;          // bucketed decode: 2^13 buckets of slots ...
 constexpr uint32_t kBucketMaxSyms = 16384;    // ... for M above kSmemLookupSlots and alphabets up to this
 constexpr uint32_t kWindow = 4096;            // decoder byte window per warp
-constexpr uint32_t kLargeTableMaxSteps = 512; // serial depth of lanes whose tables stay in L2
+constexpr uint32_t kLargeTableMaxSteps = 512; // serial depth of lanes whose tables are not in shared memory
 constexpr uint64_t kLargeTableMinSymbols = 1ull << 18;  // ... on streams at least this long
+// Below this many symbols a large-table stream's lanes go to kLargeTableShortSteps: the
+// frame's chunks then still fill less than one wave of the decoder (about 16 chunk warps
+// per SM), so the shorter chain is the shorter kernel; above it, more chunks would add a
+// wave.
+constexpr uint64_t kLargeTableDeepSymbols = 1ull << 23;
+constexpr uint32_t kLargeTableShortSteps = 256;
 
 // Decoder slot entry for tables kept in global memory: one load per step gives the
 // symbol, its frequency and slot - cum[symbol].
