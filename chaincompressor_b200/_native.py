@@ -32,7 +32,7 @@ EXPORTS = ("chain_ctx_create", "chain_ctx_destroy", "chain_last_error_message", 
            "chain_compress", "chain_result_copy", "chain_result_device_ptr", "chain_peek", "chain_decompress",
            "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count",
            "chain_decompress_noalloc", "chain_batch_create", "chain_batch_destroy", "chain_batch_compress",
-           "chain_batch_decompress", "chain_server_create", "chain_server_destroy", "chain_server_submit",
+           "chain_batch_decompress", "chain_batch_tune", "chain_server_create", "chain_server_destroy", "chain_server_submit",
            "chain_server_wait", "chain_transcode_lcp2")
 
 
@@ -46,6 +46,11 @@ class ChainOpts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("bl", ctypes.c_int32), ("l1", ctypes.c_int32),
                 ("l2", ctypes.c_int32), ("rans_bytes_per_lane", ctypes.c_uint32),
                 ("rans_max_steps", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 10)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("rans_max_steps", ctypes.c_uint32), ("workers", ctypes.c_uint32), ("best_ms", ctypes.c_double),
+                ("default_ms", ctypes.c_double), ("best_bytes", ctypes.c_uint64), ("default_bytes", ctypes.c_uint64)]
 
 
 class BatchItem(ctypes.Structure):
@@ -87,6 +92,7 @@ def load() -> ctypes.CDLL:
         L.chain_batch_destroy.restype = None
         L.chain_batch_compress.argtypes = [P, ctypes.POINTER(BatchItem), sz, ctypes.POINTER(ChainOpts)]
         L.chain_batch_decompress.argtypes = [P, ctypes.POINTER(BatchItem), sz]
+        L.chain_batch_tune.argtypes = [P, ctypes.POINTER(BatchItem), sz, ctypes.POINTER(TuneResult)]
         L.chain_server_create.argtypes = [i32, i32, sz, ctypes.POINTER(ChainOpts), ctypes.POINTER(P)]
         L.chain_server_destroy.argtypes = [P]
         L.chain_server_destroy.restype = None
@@ -95,7 +101,8 @@ def load() -> ctypes.CDLL:
         L.chain_transcode_lcp2.argtypes = [P, sz, P, sz, ctypes.POINTER(sz)]
         for f in ("chain_ctx_create", "chain_compress", "chain_result_copy", "chain_peek", "chain_decompress",
                   "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_decompress_noalloc",
-                  "chain_batch_create", "chain_batch_compress", "chain_batch_decompress", "chain_server_create",
+                  "chain_batch_create", "chain_batch_compress", "chain_batch_decompress", "chain_batch_tune",
+                  "chain_server_create",
                   "chain_server_submit", "chain_server_wait", "chain_transcode_lcp2"):
             getattr(L, f).restype = ctypes.c_int
         L.chain_launch_count.restype = ctypes.c_uint64
@@ -268,6 +275,27 @@ class Batch:
         arr = (BatchItem * len(items))(*items)
         _check(self.L.chain_batch_decompress(self.h, arr, len(items)))
         return arr
+
+    def tune_items(self, items) -> dict:
+        """chain_batch_tune on compress items (their outputs are overwritten)."""
+        arr = (BatchItem * len(items))(*items)
+        r = TuneResult()
+        _check(self.L.chain_batch_tune(self.h, arr, len(items), ctypes.byref(r)))
+        return {k: getattr(r, k) for k, _ in TuneResult._fields_}
+
+    def tune(self, frames, layout: int = CHAIN_SOA) -> dict:
+        """chain_batch_tune on a sample of frames (the compress() form)."""
+        keep, items = [], []
+        for pts, eb, p, t in frames:
+            pts = np.ascontiguousarray(pts)
+            n, d = (pts.shape[1], pts.shape[0]) if layout == CHAIN_SOA else pts.shape
+            cap = compress_bound(n, d)
+            out = np.empty(cap, np.uint8)
+            keep.append((pts, out))
+            items.append(BatchItem(input=pts.ctypes.data, dtype=CHAIN_F32 if pts.dtype == np.float32 else CHAIN_F64,
+                                   layout=layout, n=n, dims=d, eb=float(eb), p=int(p), threshold=int(t),
+                                   output=out.ctypes.data, output_capacity=cap))
+        return self.tune_items(items)
 
     def compress(self, frames, layout: int = CHAIN_SOA) -> list[bytes]:
         """frames: list of (points, eb, p, threshold) with numpy points ((D, N) for SoA)."""

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
 #include <string>
 #include <thread>
 #include <vector>
@@ -18,6 +19,9 @@
 struct chain_batch {
     int device = 0;
     std::vector<chain_ctx*> ctx;
+    size_t active = 0;          // contexts a call uses (0 = all)
+    bool tuned = false;
+    chain_opts tuned_opts{};    // used by chain_batch_compress when its opts are null
 };
 
 using namespace chain;
@@ -30,7 +34,7 @@ template <typename Fn>
 chain_status run_batch(chain_batch* b, size_t count, chain_batch_item* items, Fn fn) {
     std::atomic<size_t> next{0};
     std::vector<std::string> msg(count);
-    const size_t nthreads = std::min(b->ctx.size(), count);
+    const size_t nthreads = std::min(b->active ? b->active : b->ctx.size(), count);
     std::vector<std::thread> threads;
     threads.reserve(nthreads);
     for (size_t t = 0; t < nthreads; ++t) {
@@ -83,6 +87,7 @@ void chain_batch_destroy(chain_batch* b) {
 
 chain_status chain_batch_compress(chain_batch* b, chain_batch_item* items, size_t count, const chain_opts* opts) {
     if (!b || (count && !items)) return set_err(CHAIN_ERR_INVALID_ARGUMENT, "null argument");
+    if (!opts && b->tuned) opts = &b->tuned_opts;
     return run_batch(b, count, items, [opts](chain_ctx* c, chain_batch_item& it) -> chain_status {
         it.output_bytes = 0;
         size_t len = 0;
@@ -110,6 +115,67 @@ chain_status chain_batch_decompress(chain_batch* b, chain_batch_item* items, siz
         if (s == CHAIN_OK) it.output_bytes = static_cast<size_t>(n) * d * (it.dtype == CHAIN_F64 ? 8 : 4);
         return s;
     });
+}
+
+chain_status chain_batch_tune(chain_batch* b, chain_batch_item* items, size_t count, chain_tune_result* result) {
+    if (!b || !items || !count || !result) return set_err(CHAIN_ERR_INVALID_ARGUMENT, "null or empty argument");
+    using Clock = std::chrono::steady_clock;
+    struct Cand {
+        uint32_t steps;
+        size_t workers;
+    };
+    const size_t all = b->ctx.size();
+    std::vector<Cand> cands;
+    for (uint32_t steps : {1024u, 512u, 256u})
+        for (size_t w : {all, (all + 1) / 2, (all + 3) / 4})
+            if (w >= 1 && (cands.empty() || cands.back().steps != steps || cands.back().workers != w))
+                cands.push_back({steps, w});
+    b->tuned = false;
+    const size_t saved_active = b->active;
+    double best_ms = 0, default_ms = 0;
+    uint64_t best_bytes = 0, default_bytes = 0;
+    Cand best{1024u, all};
+    chain_status st = CHAIN_OK;
+    for (size_t ci = 0; ci < cands.size() && st == CHAIN_OK; ++ci) {
+        chain_opts o{};
+        o.struct_size = sizeof(chain_opts);
+        o.bl = o.l1 = o.l2 = 1;
+        o.rans_max_steps = cands[ci].steps;
+        b->active = cands[ci].workers;
+        double ms = 0;
+        uint64_t bytes = 0;
+        for (int rep = 0; rep < 3 && st == CHAIN_OK; ++rep) {   // a warm-up, then the best of two
+            const auto t0 = Clock::now();
+            st = chain_batch_compress(b, items, count, &o);
+            const double t = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+            if (rep == 1 || (rep == 2 && t < ms)) ms = t;
+        }
+        if (st != CHAIN_OK) break;
+        for (size_t i = 0; i < count; ++i) bytes += items[i].output_bytes;
+        if (ci == 0) {
+            default_ms = best_ms = ms;
+            default_bytes = best_bytes = bytes;
+        } else if (ms < best_ms && static_cast<double>(bytes) <= 1.003 * static_cast<double>(default_bytes)) {
+            best_ms = ms;
+            best_bytes = bytes;
+            best = cands[ci];
+        }
+    }
+    b->active = saved_active;
+    if (st != CHAIN_OK) return st;
+    b->tuned_opts = chain_opts{};
+    b->tuned_opts.struct_size = sizeof(chain_opts);
+    b->tuned_opts.bl = b->tuned_opts.l1 = b->tuned_opts.l2 = 1;
+    b->tuned_opts.rans_max_steps = best.steps;
+    b->tuned = true;
+    b->active = best.workers;
+    result->rans_max_steps = best.steps;
+    result->workers = static_cast<uint32_t>(best.workers);
+    result->best_ms = best_ms;
+    result->default_ms = default_ms;
+    result->best_bytes = best_bytes;
+    result->default_bytes = default_bytes;
+    return set_err(CHAIN_OK, std::string());
 }
 
 }  // extern "C"

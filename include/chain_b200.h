@@ -68,7 +68,8 @@ typedef struct chain_opts {
     int32_t l1;                     /* level-1 chaining                                   */
     int32_t l2;                     /* level-2 block differencing                         */
     uint32_t rans_bytes_per_lane;   /* entropy stage: target coded bytes per rANS lane
-                                       (each lane adds a 4-byte state); 0 = default 4096  */
+                                       (each lane adds its final state, prec + 10 bits);
+                                       0 = default 4096                                   */
     uint32_t rans_max_steps;        /* entropy stage: most symbols one lane codes
                                        (serial depth); 0 = default 1024                   */
     uint32_t reserved[10];
@@ -156,6 +157,27 @@ CHAIN_API void chain_batch_destroy(chain_batch* batch);
 CHAIN_API chain_status chain_batch_compress(chain_batch* batch, chain_batch_item* items, size_t count,
                                             const chain_opts* opts);
 CHAIN_API chain_status chain_batch_decompress(chain_batch* batch, chain_batch_item* items, size_t count);
+
+/* Autotuner of the batched compress path (no counterpart in the reference, which has
+ * no batched path).  Runs `items` (a sample of the frames to come, in the compress item
+ * form; their outputs are overwritten) through chain_batch_compress once per candidate:
+ * rANS lane depth (chain_opts.rans_max_steps) 1024, 512 or 256, on all, half or a
+ * quarter of the batch's contexts; each candidate is timed on the host clock (the best
+ * of two runs after one warm-up).  It keeps the fastest candidate whose total container
+ * bytes on the sample stay within 0.3% of the default's (1024, all contexts), and from
+ * then on chain_batch_compress uses it whenever its opts argument is null.  Kernel block
+ * sizes and the 8-bit sort digits are fixed by the kernels' resource budgets and are not
+ * tuned. */
+typedef struct chain_tune_result {
+    uint32_t rans_max_steps;   /* chosen lane depth */
+    uint32_t workers;          /* contexts a batch call uses */
+    double best_ms;            /* the chosen candidate's sample time */
+    double default_ms;         /* the default candidate's sample time */
+    uint64_t best_bytes;       /* container bytes of the sample, chosen candidate */
+    uint64_t default_bytes;    /* ... default candidate */
+} chain_tune_result;
+CHAIN_API chain_status chain_batch_tune(chain_batch* batch, chain_batch_item* items, size_t count,
+                                        chain_tune_result* result);
 
 /* Rewrites an LCG2 container as the reference CPU Chain's LCP2 bitstream, which the
  * reference decoder (lcps_cpu_decompress.lcps_decompress_serial, chain_caller.py:23-30)

@@ -113,3 +113,21 @@ def test_many_small_frames_many_workers(codec):
         for g, c in zip(dec, got):
             assert np.array_equal(g.view(np.uint64), codec.decompress(c).view(np.uint64))
     batch.close()
+
+
+def test_tuned_batch_matches_single_calls_with_the_tuned_depth(codec, frames):
+    """chain_batch_tune picks a lane depth and worker count from a sample; later batch
+    calls without options use them, and each container is then byte-identical to a
+    one-frame call with that lane depth."""
+    batch = N.Batch(0, workers=4)
+    r = batch.tune(frames[:6])
+    assert r["rans_max_steps"] in (256, 512, 1024)
+    assert 1 <= r["workers"] <= 4
+    assert r["best_bytes"] <= 1.003 * r["default_bytes"]
+    assert r["best_ms"] <= r["default_ms"]
+    got = batch.compress(frames, layout=N.CHAIN_SOA)
+    for (pts, eb, p, t), g in zip(frames, got):
+        assert g == codec.compress(pts, eb, p, t, layout=N.CHAIN_SOA, rans_max_steps=r["rans_max_steps"])
+    for g, d in zip(got, batch.decompress(got)):
+        assert np.array_equal(d.view(np.uint64), codec.decompress(g).view(np.uint64))
+    batch.close()
