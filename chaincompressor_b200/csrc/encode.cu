@@ -689,28 +689,29 @@ __device__ __forceinline__ void warp_hist_add(uint32_t* bins, uint32_t v, bool v
     if ((peers & lanemask_lt()) == 0) atomicAdd(&bins[v], static_cast<uint32_t>(__popc(peers)));
 }
 
-// Eight 16-bit counters packed into four registers (bins 0..7), for the hot small
-// values of a stream; flushed into shared memory at the end.
+// Eight 16-bit counters packed into two 64-bit registers (bins 0..3 and 4..7), for the
+// hot small values of a stream; flushed into shared memory at the end.
 struct PackedCount8 {
-    uint32_t r0 = 0, r1 = 0, r2 = 0, r3 = 0;
+    uint64_t lo = 0, hi = 0;
     __device__ __forceinline__ void add(uint32_t v) {   // v < 8
-        const uint32_t inc = 1u << ((v & 1u) << 4);
-        const uint32_t h = v >> 1;
-        r0 += h == 0 ? inc : 0u;
-        r1 += h == 1 ? inc : 0u;
-        r2 += h == 2 ? inc : 0u;
-        r3 += h == 3 ? inc : 0u;
+        const uint64_t inc = 1ull << ((v & 3u) << 4);
+        if (v & 4u) hi += inc;
+        else lo += inc;
     }
     // Warp-sums the counters and adds them to bins[0..7] (lane 0).
     __device__ __forceinline__ void flush(uint32_t* bins) {
-        uint32_t c[8] = {r0 & 0xffffu, r0 >> 16, r1 & 0xffffu, r1 >> 16,
-                         r2 & 0xffffu, r2 >> 16, r3 & 0xffffu, r3 >> 16};
+        uint32_t c[8];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            c[k] = static_cast<uint32_t>(lo >> (16 * k)) & 0xffffu;
+            c[4 + k] = static_cast<uint32_t>(hi >> (16 * k)) & 0xffffu;
+        }
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const uint32_t t = warp_sum(c[k]);
             if ((threadIdx.x & 31) == 0 && t) atomicAdd(&bins[k], t);
         }
-        r0 = r1 = r2 = r3 = 0;
+        lo = hi = 0;
     }
 };
 
