@@ -200,8 +200,34 @@ inline uint64_t scan_tiles(uint64_t n) {
 // bytes needs.
 inline uint64_t scan_scratch_bytes(uint64_t n) { return 16 * (n / 2048 + 16); }
 
-// Launches the three scan kernels on `stream`; `tile_buf` holds scan_tiles<T>(n) values.
-// out() runs in striped (coalesced) element order for 4-byte element types.
+// Scans of up to kScanSingleMax elements run as one CTA (one launch instead of three):
+// thread t takes the 16 consecutive elements from 16 t, one block scan joins the runs.
+constexpr uint64_t kScanSingleMax = 16384;
+template <typename T, typename InF, typename OutF, typename Op>
+__global__ void __launch_bounds__(1024) scan_single_kernel(InF in, OutF out, uint64_t n, T* total, Op op) {
+    constexpr int kPer = static_cast<int>(kScanSingleMax / 1024);
+    __shared__ T scratch[33];
+    const uint64_t b = static_cast<uint64_t>(threadIdx.x) * kPer;
+    T v[kPer];
+    T agg = Op::identity();
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        v[k] = b + k < n ? in(b + k) : Op::identity();
+        agg = op(agg, v[k]);
+    }
+    T tot;
+    T ex = block_exclusive_scan_op(agg, op, scratch, &tot);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        if (b + k < n) out(b + k, ex, v[k]);
+        ex = op(ex, v[k]);
+    }
+    if (threadIdx.x == 0 && total) *total = tot;
+}
+
+// Launches the scan kernels on `stream`; `tile_buf` holds scan_tiles<T>(n) values.
+// out() runs in striped (coalesced) element order for 4-byte element types (in thread
+// runs for scans of up to kScanSingleMax elements).
 template <typename T, typename InF, typename OutF, typename Op = SumOp<T>>
 void device_exclusive_scan(InF in, OutF out, uint64_t n, T* tile_buf, T* total, cudaStream_t stream,
                            Op op = Op()) {
@@ -209,6 +235,10 @@ void device_exclusive_scan(InF in, OutF out, uint64_t n, T* tile_buf, T* total, 
     const uint64_t tiles = scan_tiles<T>(n);
     if (tiles == 0) {
         if (total) cudaMemsetAsync(total, 0, sizeof(T), stream);
+        return;
+    }
+    if (n <= kScanSingleMax) {
+        scan_single_kernel<T, InF, OutF, Op><<<1, 1024, 0, stream>>>(in, out, n, total, op); count_launch();
         return;
     }
     scan_reduce_kernel<T, InF, Op><<<static_cast<unsigned>(tiles), kScanThreads, 0, stream>>>(in, n, tile_buf, op); count_launch();
