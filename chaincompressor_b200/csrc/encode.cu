@@ -359,7 +359,8 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
 // Sorted position k: the sorted neighbour with an equal key is the next point of the
 // same block (stable sort keeps indices increasing within a block).  Each thread takes
 // groups of four consecutive positions, two groups at a time, and loads them (16-byte
-// loads) and each group's fifth neighbour before using any.
+// loads) and each group's fifth neighbour before using any.  `idrel` arrives zeroed
+// and only links (idrel != 0, a minority of points) are scattered into it.
 template <typename KT>
 __global__ void __launch_bounds__(256)
 k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_t n, const EncState* st,
@@ -419,7 +420,7 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
                     const int dl = bitlen32(dist);
                     if (static_cast<int64_t>(dl + bitlen32(static_cast<uint32_t>(dl))) < smaller - thr) out = dist;
                 }
-                if (k < n) idrel[idxs[u][j]] = out;
+                if (k < n && out) idrel[idxs[u][j]] = out;   // idrel was zeroed: only links are written
             }
         }
     }
@@ -1589,6 +1590,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     T.mark("quantize", stream);
 
     if (l1) {
+        CHAIN_CUDA(cudaMemsetAsync(idrel, 0, sizeof(uint32_t) * n, stream));   // k_level1 writes the links only
         // stage marks around every scatter pass; the key width is in the name
         const auto sort_marks = [&](bool after) {
             T.mark(after ? (wide ? "sort_scatter_k64" : "sort_scatter_k32") : "sort_hist_scan", stream);
