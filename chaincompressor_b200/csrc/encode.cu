@@ -1443,15 +1443,39 @@ static chain_status status_from_err(uint32_t err) {
     return set_err(CHAIN_ERR_DEVICE, "internal encoder error (flags " + std::to_string(err) + ")");
 }
 
+// Statistics of CH20 without reading it: its values are 0 and 1 (record 0 is 0), B
+// records of which st->ndiff are 1, so every field follows (the same values the
+// counting kernel would accumulate from the stream's reset state).
+__global__ void k_choice_stats(EncState* st, uint32_t* gh) {
+    if (threadIdx.x || blockIdx.x) return;
+    const uint64_t B = st->B, ones = st->ndiff;
+    if (B == 0) return;
+    StreamStats& g = st->st[3];
+    g.minv[0] = ones == B ? 1u : 0u;
+    g.maxv[0] = ones ? 1u : 0u;
+    g.maxall = g.maxv[0];
+    g.tag_hist[1] = static_cast<uint32_t>(B);   // tag max(1, bitlen(v)) = 1 for 0 and 1
+    g.maxtag = 1;
+    g.tag_bits = B;
+    gh[0] = static_cast<uint32_t>(B - ones);
+    gh[1] = static_cast<uint32_t>(ones);
+}
+
 // Statistics of streams s0 .. s0+count-1: one launch for the one-dimensional streams
-// and one for the D-dimensional ones (templated on D when D <= 4).
+// and one for the D-dimensional ones (templated on D when D <= 4); CH20 (stream 3) by
+// k_choice_stats.
 static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, uint64_t hist_stride, uint32_t dims,
                          uint64_t max_records, int s0, int count, cudaStream_t stream) {
     StreamSel one{}, many{};
     int n1 = 0, nd = 0;
     for (int s = s0; s < s0 + count; ++s) {
-        if (refs.s[s].dims == 1) one.s[n1++] = s;
-        else many.s[nd++] = s;
+        if (s == 3) {
+            k_choice_stats<<<1, 1, 0, stream>>>(st, hist + hist_stride * 3); count_launch();
+        } else if (refs.s[s].dims == 1) {
+            one.s[n1++] = s;
+        } else {
+            many.s[nd++] = s;
+        }
     }
     const unsigned g = grid_for((max_records + 3) / 4, 256, 148u * 4u);
     if (n1) { k_stream_stats<1><<<dim3(g, n1), 256, 0, stream>>>(refs, st, hist, hist_stride, one); count_launch(); }
