@@ -1648,7 +1648,8 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     k_l2_stats<<<grid_for(n), 256, 0, stream>>>(rec, st); count_launch();
     k_l2_params<<<1, 1, 0, stream>>>(st); count_launch();
     k_l2_choice<<<static_cast<unsigned>(flag_tiles(n)), 256, 0, stream>>>(Level2In{rec, st, l2}, choice2, scan32); count_launch();
-    device_flag_scan_counted(Level2Flag{choice2, st}, Level2Out{rec, st, keep, diff}, n, scan32, &st->ndiff, stream);
+    device_flag_scan_counted<Level2Flag, Level2Out, kFlagItems>(Level2Flag{choice2, st}, Level2Out{rec, st, keep, diff},
+                                                                 n, scan32, &st->ndiff, stream);
     k_l2_counts<<<1, 1, 0, stream>>>(st); count_launch();
     CHAIN_LAUNCH_CHECK("level 2");
     T.mark("level2", stream);

@@ -278,7 +278,9 @@ __global__ void __launch_bounds__(kFlagThreads) flag_count_kernel(Pred pred, uin
     }
 }
 
-template <typename Pred, typename OutF>
+// kOutUnroll: rounds of out() calls unrolled together (more loads in flight against
+// more registers; the best depth depends on out()).
+template <typename Pred, typename OutF, int kOutUnroll = 4>
 __global__ void __launch_bounds__(kFlagThreads) flag_apply_kernel(Pred pred, OutF out, uint64_t n,
                                                                    const uint32_t* tile_prefix) {
     __shared__ uint32_t wsum[kFlagThreads / 32];
@@ -297,7 +299,7 @@ __global__ void __launch_bounds__(kFlagThreads) flag_apply_kernel(Pred pred, Out
     uint32_t run = tile_prefix[blockIdx.x];
     for (int w = 0; w < warp; ++w) run += wsum[w];
     const uint32_t lt = lanemask_lt();
-#pragma unroll 4
+#pragma unroll kOutUnroll
     for (int k = 0; k < kFlagItems; ++k) {
         const uint64_t i = base + 32 * k + lane;
         if (i < n) out(i, run + __popc(m[k] & lt), (m[k] >> lane) & 1u);
@@ -323,7 +325,7 @@ void device_flag_scan(Pred pred, OutF out, uint64_t n, uint32_t* tile_buf, uint3
 
 // The same scan when the per-tile counts are already in `tile_buf` (a producer kernel
 // that runs one CTA per kFlagTile elements wrote them).
-template <typename Pred, typename OutF>
+template <typename Pred, typename OutF, int kOutUnroll = 4>
 void device_flag_scan_counted(Pred pred, OutF out, uint64_t n, uint32_t* tile_buf, uint32_t* total,
                               cudaStream_t stream) {
     const uint64_t tiles = flag_tiles(n);
@@ -332,7 +334,8 @@ void device_flag_scan_counted(Pred pred, OutF out, uint64_t n, uint32_t* tile_bu
         return;
     }
     scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(tile_buf, tiles, total, SumOp<uint32_t>()); count_launch();
-    flag_apply_kernel<Pred, OutF><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, out, n, tile_buf); count_launch();
+    flag_apply_kernel<Pred, OutF, kOutUnroll><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, out, n,
+                                                                                                    tile_buf); count_launch();
 }
 
 }  // namespace chain
