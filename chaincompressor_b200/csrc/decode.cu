@@ -499,6 +499,7 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_tail(L2Geo g, L2Vec* tile_
 // tile + w * 32 * kL2Rounds + l * kL2Rounds, combines them in order, and one warp scan
 // of the lane aggregates (then the CTA's warp totals and the tile prefix) seeds them.
 // Also checks the choice values (lcps_cpp.cpp:1899-1900, 1911-1912) and the value ranges.
+constexpr size_t kL2ApplySmem = static_cast<size_t>(kL2Warps) * 3 * 32 * kL2Rounds * 4;   // staged rows (3-D)
 __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec* tile_prefix, uint32_t* compact,
                                                              DecState* st) {
     constexpr int P = kL2Rounds;   // records per lane
@@ -544,7 +545,39 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec
     for (int w = 0; w < warp; ++w) rank += s_cnt[w];
     // every record's row first (one memory round trip for the lane), then the terms
     uint32_t raw[P][3];
-    {
+    if (g.D == 3) {
+        // The warp's 256 records use one run of diff rows and one of keep rows; both are
+        // copied into shared memory with coalesced loads (diff rows first), and every
+        // lane takes its records' rows from there.
+        extern __shared__ uint32_t l2rows[];   // kL2Warps * 3 * 32 * P words
+        uint32_t* s = l2rows + warp * (3 * 32 * P);
+        const uint64_t jw = j0 - static_cast<uint64_t>(lane) * P;   // the warp's first record
+        const uint64_t dr0 = __shfl_sync(0xffffffffu, rank, 0);
+        const uint32_t nd = __shfl_sync(0xffffffffu, incl_cnt, 31);
+        const uint32_t nv = jw >= g.B ? 0u : static_cast<uint32_t>(min(g.B - jw, static_cast<uint64_t>(32 * P)));
+        const uint64_t kr0 = jw - dr0;
+        const uint32_t* dsrc = g.diff + 3 * dr0;
+        const uint32_t* ksrc = g.keep + 3 * kr0 - 3 * static_cast<uint64_t>(nd);   // word w >= 3 nd of the run
+        uint32_t v[3 * P];
+#pragma unroll
+        for (int it = 0; it < 3 * P; ++it) {
+            const uint32_t w = lane + 32 * it;
+            v[it] = w < 3 * nd ? __ldg(dsrc + w) : (w < 3 * nv ? __ldg(ksrc + w) : 0u);
+        }
+#pragma unroll
+        for (int it = 0; it < 3 * P; ++it) s[lane + 32 * it] = v[it];
+        __syncwarp();
+        uint32_t rk = static_cast<uint32_t>(rank - dr0);   // diff rows of this warp before the lane's
+        const uint32_t rec0 = static_cast<uint32_t>(lane) * P;
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const bool is_diff = (dmask >> k) & 1u;
+            const uint32_t row = is_diff ? rk : nd + (rec0 + k - rk);
+#pragma unroll
+            for (uint32_t kk = 0; kk < 3; ++kk) raw[k][kk] = j0 + k < g.B ? s[3 * row + kk] : 0u;
+            rk += is_diff;
+        }
+    } else {
         uint64_t rk = rank;
 #pragma unroll
         for (int k = 0; k < P; ++k) {
@@ -1196,12 +1229,15 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         const int64_t r = static_cast<int64_t>(range);
         g.maxc = r / 2 - ((r & 1) == 0 ? 1 : 0);
         g.minc = -(r / 2);
+        // per device, cheap; set on every call, always to the same value
+        CHAIN_CUDA(cudaFuncSetAttribute(k_l2_apply, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(kL2ApplySmem)));
         for (uint32_t d0 = 0; d0 < D; d0 += 3) {
             g.d0 = d0;
             k_l2_tail<<<static_cast<unsigned>(l2tiles), 32 * kL2Warps, 0, stream>>>(g, tile_l2); count_launch();
             scan_tilesums_kernel<L2Vec, ResetAddOp><<<1, 1024, 0, stream>>>(tile_l2, l2tiles, static_cast<L2Vec*>(nullptr),
                                                                            l2op); count_launch();
-            k_l2_apply<<<static_cast<unsigned>(l2tiles), 32 * kL2Warps, 0, stream>>>(g, tile_l2, compact, st); count_launch();
+            k_l2_apply<<<static_cast<unsigned>(l2tiles), 32 * kL2Warps, kL2ApplySmem, stream>>>(g, tile_l2, compact, st); count_launch();
         }
     } else {
         CHAIN_CUDA(cudaMemsetAsync(ndiff_dev, 0, sizeof(uint32_t), stream));
