@@ -474,10 +474,19 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_tail(L2Geo g, L2Vec* tile_
         }
         run += __popc(m[k]);
     }
+    // modular sums (every operand is below range, so one conditional subtraction per
+    // addition keeps them reduced; no division)
+    const unsigned long long r = g.range;
+    auto mod_add = [r](unsigned long long a, unsigned long long b) {
+        const unsigned long long s = a + b;
+        return s >= r ? s - r : s;
+    };
 #pragma unroll
     for (int kk = 0; kk < 3; ++kk) {
-        unsigned long long a = warp_sum(acc[kk]);   // < 32 * 2^32
-        if (lane == 0) s_sum[warp][kk] = a % g.range;
+        unsigned long long a = acc[kk];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a = mod_add(a, __shfl_xor_sync(0xffffffffu, a, o));
+        if (lane == 0) s_sum[warp][kk] = a;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -486,7 +495,7 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_tail(L2Geo g, L2Vec* tile_
 #pragma unroll
         for (int kk = 0; kk < 3; ++kk) {
             unsigned long long t = o.restart ? s_keep[kk] : 0ull;
-            for (int w = 0; w < kL2Warps; ++w) t = (t + s_sum[w][kk]) % g.range;
+            for (int w = 0; w < kL2Warps; ++w) t = mod_add(t, s_sum[w][kk]);
             o.v[kk] = static_cast<uint32_t>(t);
         }
         tile_aggr[blockIdx.x] = o;
