@@ -72,6 +72,9 @@ struct EncState {
     RansTableDev tag_tab[kCodeStreams];
     StreamChoice ch[kCodeStreams];
     uint32_t ndistinct;   // distinct exact-correction values
+    // level-1 links (idrel != 0), accumulated by k_level1 for IDR0's statistics
+    unsigned long long l1_links, l1_link_bits;
+    uint32_t l1_link_min, l1_link_max;
     uint32_t pad3;
     uint64_t total_bytes;
     uint32_t npieces;
@@ -363,8 +366,19 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
 // and only links (idrel != 0, a minority of points) are scattered into it.
 template <typename KT>
 __global__ void __launch_bounds__(256)
-k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_t n, const EncState* st,
-         uint32_t* __restrict__ idrel) {
+k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_t n, EncState* st,
+         uint32_t* __restrict__ idrel, uint32_t* __restrict__ gh) {
+    // IDR0 statistics of the links (the zeros are added by k_idrel_stats)
+    constexpr uint32_t kSmallBins = 256;
+    __shared__ uint32_t sh[kSmallBins], stag[34];
+    __shared__ unsigned long long s_links, s_bits;
+    __shared__ uint32_t s_min, s_max;
+    for (uint32_t t = threadIdx.x; t < kSmallBins; t += blockDim.x) sh[t] = 0;
+    if (threadIdx.x < 34) stag[threadIdx.x] = 0;
+    if (threadIdx.x == 0) { s_links = 0; s_bits = 0; s_min = 0xffffffffu; s_max = 0; }
+    __syncthreads();
+    uint32_t links = 0, lmin = 0xffffffffu, lmax = 0;
+    unsigned long long lbits = 0;
     const int D = static_cast<int>(st->dims);
     const int64_t maxb_bits = st->maxb_bits;
     const int64_t thr = st->threshold;
@@ -420,10 +434,62 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
                     const int dl = bitlen32(dist);
                     if (static_cast<int64_t>(dl + bitlen32(static_cast<uint32_t>(dl))) < smaller - thr) out = dist;
                 }
-                if (k < n && out) idrel[idxs[u][j]] = out;   // idrel was zeroed: only links are written
+                if (k < n && out) {   // idrel was zeroed: only links are written
+                    idrel[idxs[u][j]] = out;
+                    ++links;
+                    lmin = out < lmin ? out : lmin;
+                    lmax = out > lmax ? out : lmax;
+                    const uint32_t tag = bitlen32(out);   // >= 1
+                    lbits += tag;
+                    atomicAdd(&stag[tag], 1u);
+                    if (out < kSmallBins) atomicAdd(&sh[out], 1u);
+                    else if (out < kRansMaxAlphabet) atomicAdd(&gh[out], 1u);
+                }
             }
         }
     }
+    links = warp_sum(links);
+    lbits = warp_sum(lbits);
+    lmin = warp_min(lmin);
+    lmax = warp_max(lmax);
+    if ((threadIdx.x & 31) == 0) {
+        if (links) {
+            atomicAdd(&s_links, static_cast<unsigned long long>(links));
+            atomicAdd(&s_bits, lbits);
+            atomicMin(&s_min, lmin);
+            atomicMax(&s_max, lmax);
+        }
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < kSmallBins; t += blockDim.x)
+        if (sh[t]) atomicAdd(&gh[t], sh[t]);
+    if (threadIdx.x < 34 && stag[threadIdx.x]) {
+        atomicAdd(&st->st[0].tag_hist[threadIdx.x], stag[threadIdx.x]);
+        atomicMax(&st->st[0].maxtag, threadIdx.x);
+    }
+    if (threadIdx.x == 0 && s_links) {
+        atomicAdd(&st->l1_links, s_links);
+        atomicAdd(&st->l1_link_bits, s_bits);
+        atomicMin(&st->l1_link_min, s_min);
+        atomicMax(&st->l1_link_max, s_max);
+    }
+}
+
+// IDR0's statistics completed from the level-1 links: the n - links zeros (tag 1) join
+// them.  The same values the counting kernel would accumulate from the stream.
+__global__ void k_idrel_stats(EncState* st, uint32_t* gh, uint64_t n) {
+    if (threadIdx.x || blockIdx.x || n == 0) return;
+    const unsigned long long links = st->l1_links, zeros = n - links;
+    StreamStats& g = st->st[0];
+    g.minv[0] = zeros ? 0u : st->l1_link_min;
+    g.maxv[0] = links ? st->l1_link_max : 0u;
+    g.maxall = g.maxv[0];
+    if (zeros) {
+        g.tag_hist[1] += static_cast<uint32_t>(zeros);
+        if (g.maxtag < 1) g.maxtag = 1;
+        gh[0] += static_cast<uint32_t>(zeros);
+    }
+    g.tag_bits = st->l1_link_bits + zeros;
 }
 
 // Explicit block records, in index order (lcps_cpp.cpp:2196-2199).
@@ -1410,6 +1476,10 @@ __global__ void k_init_state(EncState* st, uint32_t dims, uint64_t n, double eb,
     st->rec_max = 0;
     st->rec_maxdiff = 0;
     st->ndistinct = 0;
+    st->l1_links = 0;
+    st->l1_link_bits = 0;
+    st->l1_link_min = 0xffffffffu;
+    st->l1_link_max = 0;
     for (int s = 0; s < kCodeStreams; ++s) {
         st->ch[s].enc = kEncEmpty;
         st->ch[s].records = 0;
@@ -1463,7 +1533,7 @@ __global__ void k_choice_stats(EncState* st, uint32_t* gh) {
 
 // Statistics of streams s0 .. s0+count-1: one launch for the one-dimensional streams
 // and one for the D-dimensional ones (templated on D when D <= 4); CH20 (stream 3) by
-// k_choice_stats.
+// k_choice_stats, IDR0 (stream 0) from the links k_level1 counted, by k_idrel_stats.
 static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, uint64_t hist_stride, uint32_t dims,
                          uint64_t max_records, int s0, int count, cudaStream_t stream) {
     StreamSel one{}, many{};
@@ -1471,6 +1541,8 @@ static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, u
     for (int s = s0; s < s0 + count; ++s) {
         if (s == 3) {
             k_choice_stats<<<1, 1, 0, stream>>>(st, hist + hist_stride * 3); count_launch();
+        } else if (s == 0) {
+            k_idrel_stats<<<1, 1, 0, stream>>>(st, hist, refs.s[0].count_const); count_launch();
         } else if (refs.s[s].dims == 1) {
             one.s[n1++] = s;
         } else {
@@ -1622,14 +1694,16 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         if (wide) {
             const bool in_b = radix_sort_pairs<uint64_t>(key_idx, key_a, val_a, key_b, val_b, n, key_bits, counts,
                                                          reinterpret_cast<uint32_t*>(scanbuf), stream, sort_marks);
-            k_level1<uint64_t><<<grid_for(n), 256, 0, stream>>>(in_b ? key_b : key_a, in_b ? val_b : val_a, n, st, idrel); count_launch();
+            k_level1<uint64_t><<<grid_for(n), 256, 0, stream>>>(in_b ? key_b : key_a, in_b ? val_b : val_a, n, st, idrel,
+                                                               hist); count_launch();
         } else {
             uint32_t* k32 = reinterpret_cast<uint32_t*>(key_idx);
             uint32_t* ka = reinterpret_cast<uint32_t*>(key_a);
             uint32_t* kb = reinterpret_cast<uint32_t*>(key_b);
             const bool in_b = radix_sort_pairs<uint32_t>(k32, ka, val_a, kb, val_b, n, key_bits, counts,
                                                          reinterpret_cast<uint32_t*>(scanbuf), stream, sort_marks);
-            k_level1<uint32_t><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel); count_launch();
+            k_level1<uint32_t><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel,
+                                                               hist); count_launch();
         }
     } else {
         CHAIN_CUDA(cudaMemsetAsync(idrel, 0, sizeof(uint32_t) * n, stream));
