@@ -160,3 +160,17 @@ def test_device_container_decodes_like_host_container(codec, name):
     hout = np.empty((n, d), np.float64)
     codec.decompress_ptr(dsrc.data_ptr(), len(data), hout.ctypes.data, hout.nbytes)
     assert np.array_equal(hout.view(np.uint64), want.view(np.uint64))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
+def test_encoder_reproduces_committed_lcg2_fixture(codec, path):
+    """The container of every golden input equals, byte for byte, the LCG2 fixture that
+    tests/golden/make_lcg2.py committed (the CPU transcoder tests decode those files).
+    This pins the whole encoder output (statistics, tables, chunking, layout) against
+    silent changes; a deliberate format change regenerates the fixtures."""
+    g = np.load(path)
+    fixture = path.parent / "lcg2" / (path.stem + ".lcg2")
+    kw = {"bl": bool(g["bl"]), "l1": bool(g["l1"]), "l2": bool(g["l2"])}
+    data = codec.compress(_soa(g["points"]), float(g["eb"]), int(g["p"]), int(g["threshold"]), layout=N.CHAIN_SOA,
+                          **kw)
+    assert data == fixture.read_bytes()
