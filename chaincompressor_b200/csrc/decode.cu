@@ -755,8 +755,21 @@ __global__ void __launch_bounds__(256) k_jump(uint32_t* parent, const uint32_t* 
 // Points whose parent word is not resolved yet are skipped: the caller runs the
 // pointer-jumping rounds and this kernel again (or reports them unresolved).  Each
 // thread takes kReconPer consecutive points and issues their block-record gathers
-// together.
+// together.  Four CTAs of 256 threads per SM (64 registers, a few spilled) stream
+// faster than three without spills.
 constexpr int kReconPer = 4;
+constexpr int kReconThreads = 256;
+// Shared 16-byte word of a warp's staged output word w (0 .. 191 for float64): one word
+// of padding after every 24, so that a quarter warp storing words 6 l + c lands on eight
+// distinct bank groups.
+__device__ __forceinline__ uint32_t kReconPad(uint32_t w) { return w + w / 24; }
+constexpr int kReconStageWords = 192 + 192 / 24;
+// blk * p + off > INT64_MAX, for 0 <= blk, 0 <= off < p, from the exact 128-bit product
+// (the same test as blk > (INT64_MAX - off) / p, without a 64-bit division)
+__device__ __forceinline__ bool q_overflows(int64_t blk, int64_t p, int64_t off) {
+    const uint64_t b = static_cast<uint64_t>(blk), m = static_cast<uint64_t>(p);
+    return __umul64hi(b, m) != 0 || b * m > static_cast<uint64_t>(INT64_MAX) - static_cast<uint64_t>(off);
+}
 struct ReconCtx {
     const uint32_t* compact;
     uint32_t D, B;
@@ -766,7 +779,7 @@ struct ReconCtx {
     __device__ __forceinline__ double coord(uint32_t cr, uint32_t d, int64_t off, bool& bad) const {
         if (off >= p) bad = true;
         const int64_t blk = bad ? 0 : compact[static_cast<uint64_t>(cr) * D + d];
-        if (blk > safe_blk && blk > (INT64_MAX - off) / p) bad = true;
+        if (blk > safe_blk && q_overflows(blk, p, off)) bad = true;
         const int64_t q = bad ? 0 : blk * p + off;
         return fma(__dadd_rn(static_cast<double>(q), 0.5), two_eb, minima[d]);
     }
@@ -797,10 +810,13 @@ struct RelBits {
 };
 
 template <typename OT, bool SOA>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kReconThreads, 4)
 k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ compact,
               const uint32_t* __restrict__ rel, const DecState* stc, DecState* st, OT* __restrict__ out,
               RelBits rb) {
+    // a warp's 128 three-dimensional points pass through shared memory on the way out,
+    // so that each store instruction writes 512 contiguous bytes
+    __shared__ __align__(16) OT stage[kReconThreads / 32][kReconStageWords * 16 / sizeof(OT)];
     const DecodePlan& P = stc->plan;
     const uint32_t D = P.D;
     const uint64_t n = P.N;
@@ -815,23 +831,19 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
     bool bad = false;
     const bool vec = ((reinterpret_cast<uintptr_t>(parent) | reinterpret_cast<uintptr_t>(rel) |
                        reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+    const uint32_t lane = threadIdx.x & 31;
+    OT* sw = stage[threadIdx.x >> 5];
     const uint64_t ng = (n + kReconPer - 1) / kReconPer;
-    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < ng;
-         g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint32_t pw[kReconPer];
-        const bool full = g * kReconPer + kReconPer <= n;
-        if (full && vec) {
+    // the loop runs warp by warp (gw = group of the warp's lane 0), so that every lane of
+    // a warp takes the same iterations
+    for (uint64_t gw = static_cast<uint64_t>(blockIdx.x) * blockDim.x + (threadIdx.x - lane); gw < ng;
+         gw += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t g = gw + lane;
+        if (D == 3 && vec && (gw + 32) * kReconPer <= n) {
+            // the whole warp holds four whole points per lane: 16-byte loads of parent and
+            // rel (or REL0's packed bits), stores staged through shared memory
+            uint32_t pw[kReconPer];
             *reinterpret_cast<uint4*>(pw) = __ldg(reinterpret_cast<const uint4*>(parent + g * kReconPer));
-        } else {
-#pragma unroll
-            for (int k = 0; k < kReconPer; ++k) {
-                const uint64_t i = g * kReconPer + k;
-                pw[k] = i < n ? parent[i] : 0u;
-            }
-        }
-        if (D == 3 && full && vec) {
-            // four whole points: 16-byte loads of rel (or its packed bits), 16-byte stores
-            // of the output
             uint32_t rl[12];
             if (rb.on) {
 #pragma unroll
@@ -855,44 +867,101 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
 #pragma unroll
                 for (int d = 0; d < 3; ++d) blk[k][d] = ok ? compact[static_cast<uint64_t>(cr) * 3 + d] : 0u;
             }
-            OT x[12];
+            const uint64_t i0 = g * kReconPer;
             bool all = true;
 #pragma unroll
-            for (int k = 0; k < kReconPer; ++k) {
-                all = all && (pw[k] & kResolved);
-                bool b = (pw[k] & kParentMask) >= R.B;
+            for (int k = 0; k < kReconPer; ++k) all = all && (pw[k] & kResolved);
+            // coordinate d of point k; marks the point bad on a corrupt block or offset
+            auto coord = [&](int k, int d, bool& b) -> double {
+                const int64_t off = rl[3 * k + d];
+                if (off >= R.p) b = true;
+                const int64_t bk = b ? 0 : static_cast<int64_t>(blk[k][d]);
+                if (bk > R.safe_blk && q_overflows(bk, R.p, off)) b = true;
+                const int64_t q = b ? 0 : bk * R.p + off;
+                return fma(__dadd_rn(static_cast<double>(q), 0.5), R.two_eb, R.minima[d]);
+            };
+            if constexpr (!SOA) {
+                // two points (six values) at a time into shared memory: lane l's values
+                // are the 16-byte words 6 l .. 6 l + 5 of the warp's 3072 bytes (float64)
+                // or 3 l .. 3 l + 2 of its 1536 bytes (float32); float64 words are stored
+                // at word + word / 24, which keeps a quarter warp's stores on distinct banks
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    const int64_t off = rl[3 * k + d];
-                    if (off >= R.p) b = true;
-                    const int64_t bk = b ? 0 : static_cast<int64_t>(blk[k][d]);
-                    if (bk > R.safe_blk && bk > (INT64_MAX - off) / R.p) b = true;
-                    const int64_t q = b ? 0 : bk * R.p + off;
-                    x[3 * k + d] = static_cast<OT>(fma(__dadd_rn(static_cast<double>(q), 0.5), R.two_eb, R.minima[d]));
+                for (int kp = 0; kp < kReconPer / 2; ++kp) {
+                    bool b0 = (pw[2 * kp] & kParentMask) >= R.B, b1 = (pw[2 * kp + 1] & kParentMask) >= R.B;
+                    double v[6];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) v[d] = coord(2 * kp, d, b0);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) v[3 + d] = coord(2 * kp + 1, d, b1);
+                    bad = bad || (b0 && (pw[2 * kp] & kResolved)) || (b1 && (pw[2 * kp + 1] & kResolved));
+                    if constexpr (sizeof(OT) == 8) {
+                        double2* s = reinterpret_cast<double2*>(sw);
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) s[kReconPad(6 * lane + 3 * kp + c)] = make_double2(v[2 * c], v[2 * c + 1]);
+                    } else {
+                        float2* s = reinterpret_cast<float2*>(sw + 12 * lane + 6 * kp);
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            s[c] = make_float2(static_cast<float>(v[2 * c]), static_cast<float>(v[2 * c + 1]));
+                    }
                 }
-                bad = bad || (b && (pw[k] & kResolved));
-            }
-            const uint64_t i0 = g * kReconPer;
-            if (!SOA && all) {
-                if constexpr (sizeof(OT) == 8) {
-                    double2* o = reinterpret_cast<double2*>(out + i0 * 3);
+                __syncwarp();
+                if (__all_sync(0xffffffffu, all)) {
+                    // the warp's 128 points (384 values) leave as 16-byte words,
+                    // consecutive lanes on consecutive words
+                    uint4* o = reinterpret_cast<uint4*>(out + gw * kReconPer * 3);
+                    const uint4* s16 = reinterpret_cast<const uint4*>(sw);
+                    if constexpr (sizeof(OT) == 8) {
 #pragma unroll
-                    for (int v = 0; v < 6; ++v) o[v] = make_double2(x[2 * v], x[2 * v + 1]);
+                        for (int w = 0; w < 6; ++w) o[32 * w + lane] = s16[kReconPad(32 * w + lane)];
+                    } else {
+#pragma unroll
+                        for (int w = 0; w < 3; ++w) o[32 * w + lane] = s16[32 * w + lane];
+                    }
                 } else {
-                    float4* o = reinterpret_cast<float4*>(out + i0 * 3);
 #pragma unroll
-                    for (int v = 0; v < 3; ++v) o[v] = make_float4(x[4 * v], x[4 * v + 1], x[4 * v + 2], x[4 * v + 3]);
+                    for (int k = 0; k < kReconPer; ++k) {
+                        if (!(pw[k] & kResolved)) continue;
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            const int j = 3 * k + d;
+                            OT x;
+                            if constexpr (sizeof(OT) == 8)
+                                x = sw[2 * kReconPad(6 * lane + j / 2) + (j & 1)];
+                            else
+                                x = sw[12 * lane + j];
+                            out[(i0 + k) * 3 + d] = x;
+                        }
+                    }
                 }
+                __syncwarp();
             } else {
 #pragma unroll
                 for (int k = 0; k < kReconPer; ++k) {
-                    if (!(pw[k] & kResolved)) continue;
+                    bool b = (pw[k] & kParentMask) >= R.B;
 #pragma unroll
-                    for (int d = 0; d < 3; ++d)
-                        out[SOA ? static_cast<uint64_t>(d) * n + i0 + k : (i0 + k) * 3 + d] = x[3 * k + d];
+                    for (int d = 0; d < 3; ++d) {
+                        const double x = coord(k, d, b);
+                        if (pw[k] & kResolved) out[static_cast<uint64_t>(d) * n + i0 + k] = static_cast<OT>(x);
+                    }
+                    bad = bad || (b && (pw[k] & kResolved));
                 }
             }
-        } else if (D == 3) {
+            continue;
+        }
+        if (g >= ng) continue;
+        uint32_t pw[kReconPer];
+        const bool full = g * kReconPer + kReconPer <= n;
+        if (full && vec) {
+            *reinterpret_cast<uint4*>(pw) = __ldg(reinterpret_cast<const uint4*>(parent + g * kReconPer));
+        } else {
+#pragma unroll
+            for (int k = 0; k < kReconPer; ++k) {
+                const uint64_t i = g * kReconPer + k;
+                pw[k] = i < n ? parent[i] : 0u;
+            }
+        }
+        if (D == 3) {
             uint32_t rl[12];
             if (rb.on) {
 #pragma unroll
@@ -921,7 +990,7 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
                     const int64_t off = rb.on ? rl[3 * k + d] : rel[i * 3 + d];
                     if (off >= R.p) b = true;
                     const int64_t bk = b ? 0 : static_cast<int64_t>(blk[k][d]);
-                    if (bk > R.safe_blk && bk > (INT64_MAX - off) / R.p) b = true;
+                    if (bk > R.safe_blk && q_overflows(bk, R.p, off)) b = true;
                     const int64_t q = b ? 0 : bk * R.p + off;
                     const double x = fma(__dadd_rn(static_cast<double>(q), 0.5), R.two_eb, R.minima[d]);
                     out[SOA ? static_cast<uint64_t>(d) * n + i : i * 3 + d] = static_cast<OT>(x);
