@@ -428,7 +428,7 @@ struct L2Geo {
 // Tile aggregate of the reset-scan: the value at the tile's end when the tile holds a
 // kept record (restart), else the modular sum of its difference terms.  Only the terms
 // after the tile's last kept record are read.
-__global__ void __launch_bounds__(32 * kL2Warps) k_l2_tail(L2Geo g, L2Vec* tile_aggr) {
+__global__ void __launch_bounds__(32 * kL2Warps, 2) k_l2_tail(L2Geo g, L2Vec* tile_aggr) {
     __shared__ uint32_t s_cnt[kL2Warps];
     __shared__ int s_last[kL2Warps];
     __shared__ unsigned long long s_sum[kL2Warps][3];
@@ -508,7 +508,15 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_tail(L2Geo g, L2Vec* tile_
 // tile + w * 32 * kL2Rounds + l * kL2Rounds, combines them in order, and one warp scan
 // of the lane aggregates (then the CTA's warp totals and the tile prefix) seeds them.
 // Also checks the choice values (lcps_cpp.cpp:1899-1900, 1911-1912) and the value ranges.
-constexpr size_t kL2ApplySmem = static_cast<size_t>(kL2Warps) * 3 * 32 * kL2Rounds * 4;   // staged rows (3-D)
+// Shared-memory slot of 16-byte word w when a warp stages 32 lanes x 6 words (lane l's
+// words 6 l .. 6 l + 5) and reads them back in order: one word of padding after every 24
+// keeps a quarter warp's stores (words 6 l + c, l = 0 .. 7) on eight distinct bank groups.
+__device__ __forceinline__ uint32_t pad24(uint32_t w) { return w + w / 24; }
+constexpr uint32_t kPad24Words = 192 + 192 / 24;   // slots for 192 words
+// per warp: the staged input rows (3 * 32 * kL2Rounds words), reused for the output
+constexpr uint32_t kL2WarpWords = 4 * kPad24Words;
+static_assert(kL2WarpWords >= 3 * 32 * kL2Rounds, "staged rows fit");
+constexpr size_t kL2ApplySmem = static_cast<size_t>(kL2Warps) * kL2WarpWords * 4;
 __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec* tile_prefix, uint32_t* compact,
                                                              DecState* st) {
     constexpr int P = kL2Rounds;   // records per lane
@@ -558,8 +566,8 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec
         // The warp's 256 records use one run of diff rows and one of keep rows; both are
         // copied into shared memory with coalesced loads (diff rows first), and every
         // lane takes its records' rows from there.
-        extern __shared__ uint32_t l2rows[];   // kL2Warps * 3 * 32 * P words
-        uint32_t* s = l2rows + warp * (3 * 32 * P);
+        extern __shared__ uint32_t l2rows[];   // kL2Warps * kL2WarpWords words
+        uint32_t* s = l2rows + warp * kL2WarpWords;
         const uint64_t jw = j0 - static_cast<uint64_t>(lane) * P;   // the warp's first record
         const uint64_t dr0 = __shfl_sync(0xffffffffu, rank, 0);
         const uint32_t nd = __shfl_sync(0xffffffffu, incl_cnt, 31);
@@ -634,7 +642,21 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec
         for (int kk = 0; kk < 3; ++kk) o[3 * k + kk] = static_cast<uint32_t>(g.wrap_min + carry.v[kk]);
     }
     uint32_t* dst = compact + j0 * g.D;
-    if (g.D == 3 && j0 + P <= g.B && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+    const uint64_t jw = j0 - static_cast<uint64_t>(lane) * P;   // the warp's first record
+    if (g.D == 3 && jw + 32 * P <= g.B && (reinterpret_cast<uintptr_t>(compact + jw * 3) & 15) == 0) {
+        // the warp's 256 whole records (3072 bytes) leave through its shared rows as
+        // 16-byte words, consecutive lanes on consecutive words
+        static_assert(3 * P / 4 == 6, "six 16-byte words per lane");
+        extern __shared__ uint32_t l2rows[];
+        uint4* s = reinterpret_cast<uint4*>(l2rows + warp * kL2WarpWords);
+        __syncwarp();   // every lane has read its input rows
+#pragma unroll
+        for (int v = 0; v < 6; ++v) s[pad24(6 * lane + v)] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+        __syncwarp();
+        uint4* q = reinterpret_cast<uint4*>(compact + jw * 3);
+#pragma unroll
+        for (int w = 0; w < 6; ++w) q[32 * w + lane] = s[pad24(32 * w + lane)];
+    } else if (g.D == 3 && j0 + P <= g.B && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
         uint4* q = reinterpret_cast<uint4*>(dst);
 #pragma unroll
         for (int v = 0; v < 3 * P / 4; ++v) q[v] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
@@ -759,11 +781,6 @@ __global__ void __launch_bounds__(256) k_jump(uint32_t* parent, const uint32_t* 
 // faster than three without spills.
 constexpr int kReconPer = 4;
 constexpr int kReconThreads = 256;
-// Shared 16-byte word of a warp's staged output word w (0 .. 191 for float64): one word
-// of padding after every 24, so that a quarter warp storing words 6 l + c lands on eight
-// distinct bank groups.
-__device__ __forceinline__ uint32_t kReconPad(uint32_t w) { return w + w / 24; }
-constexpr int kReconStageWords = 192 + 192 / 24;
 // blk * p + off > INT64_MAX, for 0 <= blk, 0 <= off < p, from the exact 128-bit product
 // (the same test as blk > (INT64_MAX - off) / p, without a 64-bit division)
 __device__ __forceinline__ bool q_overflows(int64_t blk, int64_t p, int64_t off) {
@@ -816,7 +833,7 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
               RelBits rb) {
     // a warp's 128 three-dimensional points pass through shared memory on the way out,
     // so that each store instruction writes 512 contiguous bytes
-    __shared__ __align__(16) OT stage[kReconThreads / 32][kReconStageWords * 16 / sizeof(OT)];
+    __shared__ __align__(16) OT stage[kReconThreads / 32][kPad24Words * 16 / sizeof(OT)];
     const DecodePlan& P = stc->plan;
     const uint32_t D = P.D;
     const uint64_t n = P.N;
@@ -897,7 +914,7 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
                     if constexpr (sizeof(OT) == 8) {
                         double2* s = reinterpret_cast<double2*>(sw);
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) s[kReconPad(6 * lane + 3 * kp + c)] = make_double2(v[2 * c], v[2 * c + 1]);
+                        for (int c = 0; c < 3; ++c) s[pad24(6 * lane + 3 * kp + c)] = make_double2(v[2 * c], v[2 * c + 1]);
                     } else {
                         float2* s = reinterpret_cast<float2*>(sw + 12 * lane + 6 * kp);
 #pragma unroll
@@ -913,7 +930,7 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
                     const uint4* s16 = reinterpret_cast<const uint4*>(sw);
                     if constexpr (sizeof(OT) == 8) {
 #pragma unroll
-                        for (int w = 0; w < 6; ++w) o[32 * w + lane] = s16[kReconPad(32 * w + lane)];
+                        for (int w = 0; w < 6; ++w) o[32 * w + lane] = s16[pad24(32 * w + lane)];
                     } else {
 #pragma unroll
                         for (int w = 0; w < 3; ++w) o[32 * w + lane] = s16[32 * w + lane];
@@ -927,7 +944,7 @@ k_reconstruct(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ 
                             const int j = 3 * k + d;
                             OT x;
                             if constexpr (sizeof(OT) == 8)
-                                x = sw[2 * kReconPad(6 * lane + j / 2) + (j & 1)];
+                                x = sw[2 * pad24(6 * lane + j / 2) + (j & 1)];
                             else
                                 x = sw[12 * lane + j];
                             out[(i0 + k) * 3 + d] = x;

@@ -365,7 +365,7 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
 // loads) and each group's fifth neighbour before using any.  `idrel` arrives zeroed
 // and only links (idrel != 0, a minority of points) are scattered into it.
 template <typename KT>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(KT) == 4 ? 4 : 3)   // 64-bit keys spill at four CTAs per SM
 k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_t n, EncState* st,
          uint32_t* __restrict__ idrel, uint32_t* __restrict__ gh) {
     // IDR0 statistics of the links (the zeros are added by k_idrel_stats)
@@ -1092,7 +1092,7 @@ struct FixedPack {
     uint32_t width[kMaxDims];
 };
 constexpr int kPackWarps = 8;
-__global__ void __launch_bounds__(32 * kPackWarps) k_pack_fixed(const uint32_t* __restrict__ data, uint32_t D,
+__global__ void __launch_bounds__(32 * kPackWarps, 3) k_pack_fixed(const uint32_t* __restrict__ data, uint32_t D,
                                                                  uint64_t nrec, FixedPack fp) {
     __shared__ uint32_t stage[kPackWarps][33 * 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

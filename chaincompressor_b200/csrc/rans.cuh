@@ -981,7 +981,7 @@ static __global__ void __launch_bounds__(32 * kRansDecWarps) rans_decode_kernel(
     const RansJob& jb = J.job[job_of_block(J)];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t prec = jb.prec;
-    const uint32_t M = 1u << prec, L = 4u << prec;
+    const uint32_t L = 4u << prec;
     uint8_t* win = rsm + J.table_bytes + warp * kWindow;
     const bool bucketed = rans_dec_bucketed(prec, jb.alphabet);
     const bool smem_look = rans_dec_smem_look(prec, jb.alphabet);
