@@ -64,8 +64,9 @@ __global__ void __launch_bounds__(1024) k_section_setup(SectionRefs refs, const 
     const SectionRef R = refs.r[blockIdx.x];
     const SectionPlan& s = *R.sec;
     __shared__ uint64_t red[33];
-    __shared__ uint8_t stage[kParseStage];
-    __shared__ uint32_t stage_scratch[kParseStageScratch];
+    extern __shared__ __align__(16) uint8_t setup_smem[];   // kParseSmem bytes
+    uint8_t* stage = setup_smem;
+    uint32_t* stage_scratch = reinterpret_cast<uint32_t*>(setup_smem + kParseStage);
     if (!parse_table_block(data + s.table_off, s.table_len, s.alphabet, s.prec, R.prob, R.cum, R.scratch, stage,
                            stage_scratch) &&
         threadIdx.x == 0)
@@ -1227,7 +1228,9 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     refs.count = nsec;
     jobs.total_blocks = first;
     if (nsec) {
-        k_section_setup<<<nsec, 1024, 0, stream>>>(refs, dcont, st); count_launch();
+        CHAIN_CUDA(cudaFuncSetAttribute(k_section_setup, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(kParseSmem)));
+        k_section_setup<<<nsec, 1024, kParseSmem, stream>>>(refs, dcont, st); count_launch();
         k_lookup<<<dim3(256, nsec), 256, 0, stream>>>(refs, st); count_launch();
         k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states); count_launch();
         T.mark("tables", stream);

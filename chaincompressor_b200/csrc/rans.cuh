@@ -365,13 +365,42 @@ __device__ __forceinline__ void token_shape(uint8_t first, uint32_t* bytes, uint
 }
 
 constexpr uint32_t kParseSeg = 64;
-constexpr uint32_t kParseStage = 24576;   // token bytes staged in shared memory up to this length
+constexpr uint32_t kParseStage = 131072;   // token bytes staged in shared memory up to this length
 constexpr uint32_t kParseStageScratch = 8 * (kParseStage / kParseSeg + 2);   // u32 scratch of a staged parse
+constexpr uint32_t kParseSmem = kParseStage + 4 * kParseStageScratch;         // dynamic shared bytes of a staged parse
+
+// Segment entry maps: where the next segment's first token starts (offset 0, 1 or 2)
+// as a function of where this segment's first token starts, 2 bits per entry offset.
+// (a after b)(e) = a(b(e)).
+constexpr uint32_t kEntryMapId = 0u | (1u << 2) | (2u << 4);
+__device__ __forceinline__ uint32_t entry_map_after(uint32_t a, uint32_t b) {
+    uint32_t h = 0;
+#pragma unroll
+    for (uint32_t e = 0; e < 3; ++e) h |= ((a >> (2 * ((b >> (2 * e)) & 3u))) & 3u) << (2 * e);
+    return h;
+}
+// Exclusive block scan of entry maps in thread order: the composition of the maps of
+// all lower threads (kEntryMapId for thread 0).  Every thread of the CTA calls it.
+__device__ __forceinline__ uint32_t block_entry_map_prefix(uint32_t m, uint32_t* s_warp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = m;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc = entry_map_after(inc, prev);
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    uint32_t pre = kEntryMapId;
+    for (int w = 0; w < warp; ++w) pre = entry_map_after(s_warp[w], pre);
+    const uint32_t exc_lane = __shfl_up_sync(0xffffffffu, inc, 1);
+    return lane ? entry_map_after(exc_lane, pre) : pre;
+}
 
 // Parses tokens with the whole CTA.  Every 64-byte segment is parsed speculatively
-// from each of its 3 possible entry offsets (a token is at most 3 bytes); one thread
-// then chains the true entries, a scan gives each segment's first symbol, and the
-// segments are parsed again for real.  Token walks and the entry chain are chains of
+// from each of its 3 possible entry offsets (a token is at most 3 bytes); a block scan
+// of the segments' entry maps gives the true entries, a scan gives each segment's first
+// symbol, and the segments are parsed again for real.  Token walks are chains of
 // dependent reads, so a table of up to kParseStage bytes is first copied to shared
 // memory (`stage`, kParseStage bytes) and its scratch kept there too (`stage_scratch`,
 // kParseStageScratch u32); larger ones use `global_scratch`, 8 * (len / 64 + 2) u32.
@@ -423,19 +452,26 @@ __device__ inline bool parse_table_block(const uint8_t* in_global, uint32_t len,
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t e = 0;
-        for (uint32_t k = 0; k < nseg; ++k) {
+    {
+        // entry[k] = (F_{k-1} after ... after F_0)(0), F_k(e) = ex[3 k + e]: each thread
+        // composes a contiguous run of segments, a block scan of the runs' maps gives each
+        // run's entry, and the thread walks its run
+        __shared__ uint32_t s_wmap[32];
+        const uint32_t per = (nseg + blockDim.x - 1) / blockDim.x;
+        const uint32_t k0 = min(nseg, threadIdx.x * per), k1 = min(nseg, k0 + per);
+        uint32_t mine = kEntryMapId;
+        for (uint32_t k = k0; k < k1; ++k)
+            mine = entry_map_after(ex[3 * k] | (ex[3 * k + 1] << 2) | (ex[3 * k + 2] << 4), mine);
+        uint32_t e = block_entry_map_prefix(mine, s_wmap) & 3u;
+        for (uint32_t k = k0; k < k1; ++k) {
             entry[k] = e;
-            if (k * kParseSeg + e > len) { s_ok = 0; break; }
             e = ex[3 * k + e];
         }
-        // the last segment must end exactly at len
-        if (s_ok && nseg) {
-            const uint32_t k = nseg - 1;
-            if (ex[3 * k + entry[k]] != 0) s_ok = 0;
-        }
     }
+    __syncthreads();
+    // the last segment, entered at its entry, must end exactly at len (an entry past
+    // the end of a short last segment leaves a nonzero exit too)
+    if (threadIdx.x == 0 && nseg && ex[3 * (nseg - 1) + entry[nseg - 1]] != 0) s_ok = 0;
     __syncthreads();
     if (!s_ok) return false;
     // first symbol of each segment
