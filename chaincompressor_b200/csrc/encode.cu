@@ -506,6 +506,14 @@ struct ExplicitOut {
     __device__ void operator()(uint64_t i, uint32_t pos, uint32_t flag) const {
         if (!flag) return;
         const int D = static_cast<int>(st->dims);
+        if (D == 3 && st->kb <= 21) {   // the three de-interleaved coordinates straight to the record
+            const uint64_t k = static_cast<uint64_t>(key[i]);
+            uint32_t* r = rec + static_cast<uint64_t>(pos) * 3;
+            r[0] = compact3(k);
+            r[1] = compact3(k >> 1);
+            r[2] = compact3(k >> 2);
+            return;
+        }
         uint32_t b[kMaxDims];
         block_unkey(static_cast<uint64_t>(key[i]), D, st->kb, b);
         for (int d = 0; d < D; ++d) rec[static_cast<uint64_t>(pos) * D + d] = b[d];

@@ -311,7 +311,7 @@ inline uint64_t flag_tiles(uint64_t n) { return (n + kFlagTile - 1) / kFlagTile;
 
 // `tile_buf` holds flag_tiles(n) u32 (scan_scratch_bytes(n) bytes suffice); *total
 // (may be null) receives the number of set flags.
-template <typename Pred, typename OutF>
+template <typename Pred, typename OutF, int kOutUnroll = 4>
 void device_flag_scan(Pred pred, OutF out, uint64_t n, uint32_t* tile_buf, uint32_t* total, cudaStream_t stream) {
     const uint64_t tiles = flag_tiles(n);
     if (tiles == 0) {
@@ -320,7 +320,8 @@ void device_flag_scan(Pred pred, OutF out, uint64_t n, uint32_t* tile_buf, uint3
     }
     flag_count_kernel<Pred><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, n, tile_buf); count_launch();
     scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(tile_buf, tiles, total, SumOp<uint32_t>()); count_launch();
-    flag_apply_kernel<Pred, OutF><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, out, n, tile_buf); count_launch();
+    flag_apply_kernel<Pred, OutF, kOutUnroll><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, out, n,
+                                                                                                    tile_buf); count_launch();
 }
 
 // The same scan when the per-tile counts are already in `tile_buf` (a producer kernel
