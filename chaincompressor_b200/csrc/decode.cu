@@ -67,8 +67,9 @@ __global__ void __launch_bounds__(1024) k_section_setup(SectionRefs refs, const 
     extern __shared__ __align__(16) uint8_t setup_smem[];   // kParseSmem bytes
     uint8_t* stage = setup_smem;
     uint32_t* stage_scratch = reinterpret_cast<uint32_t*>(setup_smem + kParseStage);
+    uint32_t* sprob = reinterpret_cast<uint32_t*>(setup_smem + kParseStage + 4 * kParseStageScratch);
     if (!parse_table_block(data + s.table_off, s.table_len, s.alphabet, s.prec, R.prob, R.cum, R.scratch, stage,
-                           stage_scratch) &&
+                           stage_scratch, sprob) &&
         threadIdx.x == 0)
         set_error(&st->err, kErrCorrupt);
     // chunk offsets: exclusive prefix of the u32 chunk lengths

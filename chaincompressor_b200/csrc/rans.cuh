@@ -364,10 +364,11 @@ __device__ __forceinline__ void token_shape(uint8_t first, uint32_t* bytes, uint
     else { *bytes = 1 + t; *syms = 1; }
 }
 
-constexpr uint32_t kParseSeg = 64;
-constexpr uint32_t kParseStage = 131072;   // token bytes staged in shared memory up to this length
+constexpr uint32_t kParseSeg = 16;
+constexpr uint32_t kParseStage = 49152;   // token bytes staged in shared memory up to this length
 constexpr uint32_t kParseStageScratch = 8 * (kParseStage / kParseSeg + 2);   // u32 scratch of a staged parse
-constexpr uint32_t kParseSmem = kParseStage + 4 * kParseStageScratch;         // dynamic shared bytes of a staged parse
+constexpr uint32_t kParseProbSyms = 16384;   // alphabets whose probabilities are built in shared memory
+constexpr uint32_t kParseSmem = kParseStage + 4 * kParseStageScratch + 4 * kParseProbSyms;   // dynamic shared bytes
 
 // Segment entry maps: where the next segment's first token starts (offset 0, 1 or 2)
 // as a function of where this segment's first token starts, 2 bits per entry offset.
@@ -383,6 +384,7 @@ __device__ __forceinline__ uint32_t entry_map_after(uint32_t a, uint32_t b) {
 // all lower threads (kEntryMapId for thread 0).  Every thread of the CTA calls it.
 __device__ __forceinline__ uint32_t block_entry_map_prefix(uint32_t m, uint32_t* s_warp) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
     uint32_t inc = m;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -391,28 +393,52 @@ __device__ __forceinline__ uint32_t block_entry_map_prefix(uint32_t m, uint32_t*
     }
     if (lane == 31) s_warp[warp] = inc;
     __syncthreads();
-    uint32_t pre = kEntryMapId;
-    for (int w = 0; w < warp; ++w) pre = entry_map_after(s_warp[w], pre);
+    if (warp == 0) {   // the warps' maps scanned by one warp
+        uint32_t wi = lane < nwarps ? s_warp[lane] : kEntryMapId;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t prev = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi = entry_map_after(wi, prev);
+        }
+        const uint32_t we = __shfl_up_sync(0xffffffffu, wi, 1);
+        __syncwarp();
+        if (lane < nwarps) s_warp[lane] = lane ? we : kEntryMapId;
+    }
+    __syncthreads();
+    const uint32_t pre = s_warp[warp];
     const uint32_t exc_lane = __shfl_up_sync(0xffffffffu, inc, 1);
     return lane ? entry_map_after(exc_lane, pre) : pre;
 }
 
-// Parses tokens with the whole CTA.  Every 64-byte segment is parsed speculatively
+__device__ __forceinline__ uint32_t clamp_u32(uint64_t v) {
+    return static_cast<uint32_t>(v > 0xffffffffull ? 0xffffffffull : v);
+}
+
+// Parses tokens with the whole CTA.  Every 16-byte segment is parsed speculatively
 // from each of its 3 possible entry offsets (a token is at most 3 bytes); a block scan
 // of the segments' entry maps gives the true entries, a scan gives each segment's first
 // symbol, and the segments are parsed again for real.  Token walks are chains of
 // dependent reads, so a table of up to kParseStage bytes is first copied to shared
 // memory (`stage`, kParseStage bytes) and its scratch kept there too (`stage_scratch`,
-// kParseStageScratch u32); larger ones use `global_scratch`, 8 * (len / 64 + 2) u32.
+// kParseStageScratch u32); larger ones use `global_scratch`, 8 * (len / 16 + 2) u32.
+// A staged table of at most kParseProbSyms symbols builds its probabilities in shared
+// memory (`sprob`, kParseProbSyms u32) and scans them there, four per thread, so that
+// prob and cum leave with coalesced stores (a single CTA streaming them through global
+// memory with per-thread runs was the slowest part of the parse).
 // Returns false (in every thread) on malformed input.
 __device__ inline bool parse_table_block(const uint8_t* in_global, uint32_t len, uint32_t A, uint32_t prec,
                                          uint32_t* prob, uint32_t* cum, uint32_t* global_scratch, uint8_t* stage,
-                                         uint32_t* stage_scratch) {
+                                         uint32_t* stage_scratch, uint32_t* sprob) {
     __shared__ int s_ok;
     __shared__ uint64_t sscratch[33];
+    __shared__ uint32_t s_wmap[32];
     const uint8_t* in = in_global;
     uint32_t* scratch = global_scratch;
-    if (len <= kParseStage) {
+    const bool staged = len <= kParseStage;
+    const bool shared_prob = staged && A <= kParseProbSyms;
+    constexpr uint32_t kScanRound = 4 * 1024;   // symbols per round of the shared scan (blockDim.x = 1024)
+    const uint32_t a_pad = (A + kScanRound - 1) / kScanRound * kScanRound;
+    if (staged) {
         constexpr int kDepth = 8;   // loads in flight per thread
         for (uint32_t i0 = threadIdx.x; i0 < len; i0 += blockDim.x * kDepth) {
             uint8_t v[kDepth];
@@ -430,6 +456,8 @@ __device__ inline bool parse_table_block(const uint8_t* in_global, uint32_t len,
         in = stage;   // the __syncthreads below orders the copy before the reads
         scratch = stage_scratch;
     }
+    if (shared_prob)   // the scan reads whole rounds: symbols A .. a_pad count zero
+        for (uint32_t i = A + threadIdx.x; i < a_pad; i += blockDim.x) sprob[i] = 0;
     const uint32_t nseg = (len + kParseSeg - 1) / kParseSeg;
     uint32_t* ex = scratch;              // [nseg][3] exit offset into the next segment
     uint32_t* cnt = scratch + 3 * nseg;  // [nseg][3] symbols
@@ -456,7 +484,6 @@ __device__ inline bool parse_table_block(const uint8_t* in_global, uint32_t len,
         // entry[k] = (F_{k-1} after ... after F_0)(0), F_k(e) = ex[3 k + e]: each thread
         // composes a contiguous run of segments, a block scan of the runs' maps gives each
         // run's entry, and the thread walks its run
-        __shared__ uint32_t s_wmap[32];
         const uint32_t per = (nseg + blockDim.x - 1) / blockDim.x;
         const uint32_t k0 = min(nseg, threadIdx.x * per), k1 = min(nseg, k0 + per);
         uint32_t mine = kEntryMapId;
@@ -481,11 +508,12 @@ __device__ inline bool parse_table_block(const uint8_t* in_global, uint32_t len,
         const uint64_t c = k < nseg ? cnt[3 * k + entry[k]] : 0;
         uint64_t tot;
         const uint64_t ex_sum = block_exclusive_sum(c, sscratch, &tot);
-        if (k < nseg) first_sym[k] = static_cast<uint32_t>(carry + ex_sum > 0xffffffffull ? 0xffffffffu : carry + ex_sum);
+        if (k < nseg) first_sym[k] = clamp_u32(carry + ex_sum);
         carry += tot;
     }
     if (carry != A) return false;   // uniform: every thread computed the same total
     const uint64_t M = 1ull << prec;
+    uint32_t* dst = shared_prob ? sprob : prob;
     for (uint32_t k = threadIdx.x; k < nseg; k += blockDim.x) {
         const uint32_t end = min((k + 1) * kParseSeg, len);
         uint32_t pos = k * kParseSeg + entry[k], s = first_sym[k];
@@ -496,12 +524,12 @@ __device__ inline bool parse_table_block(const uint8_t* in_global, uint32_t len,
             token_shape(first, &b, &sy);
             if (pos + b > len || s + sy > A) { ok = false; break; }
             if ((first & 3u) == 3u) {
-                for (uint32_t j = 0; j < sy; ++j) prob[s + j] = 0;
+                for (uint32_t j = 0; j < sy; ++j) dst[s + j] = 0;
             } else {
                 uint32_t p = first >> 2;
                 for (uint32_t j = 1; j < b; ++j) p |= static_cast<uint32_t>(in[pos + j]) << (6 + 8 * (j - 1));
                 if (p == 0 || p > M) ok = false;
-                prob[s] = p;
+                dst[s] = p;
             }
             pos += b;
             s += sy;
@@ -510,6 +538,34 @@ __device__ inline bool parse_table_block(const uint8_t* in_global, uint32_t len,
     }
     __syncthreads();
     if (!s_ok) return false;
+    if (shared_prob) {
+        // cumulative table in shared memory (the segment scratch is free now): rounds of
+        // four consecutive symbols per thread and one block scan, then prob and cum out
+        uint32_t* scum = scratch;
+        uint64_t run = 0;
+        for (uint32_t base = 0; base < a_pad; base += 4 * blockDim.x) {
+            const uint32_t i = base + 4 * threadIdx.x;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (i < a_pad) v = *reinterpret_cast<const uint4*>(sprob + i);
+            uint64_t tot;
+            uint64_t c = run + block_exclusive_sum(static_cast<uint64_t>(v.x) + v.y + v.z + v.w, sscratch, &tot);
+            if (i < a_pad) {
+                uint4 o;
+                o.x = clamp_u32(c); c += v.x;
+                o.y = clamp_u32(c); c += v.y;
+                o.z = clamp_u32(c); c += v.z;
+                o.w = clamp_u32(c);
+                *reinterpret_cast<uint4*>(scum + i) = o;
+            }
+            run += tot;
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < A; i += blockDim.x) {
+            prob[i] = sprob[i];
+            cum[i] = scum[i];
+        }
+        return run == M;
+    }
     // cumulative table and total: each thread sums a contiguous run of symbols (read
     // eight at a time), one block scan gives the runs' offsets
     const uint32_t per = (A + blockDim.x - 1) / blockDim.x;
@@ -530,7 +586,7 @@ __device__ inline bool parse_table_block(const uint8_t* in_global, uint32_t len,
         for (int u = 0; u < 8; ++u) v[u] = b + u < s1 ? prob[b + u] : 0u;
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-            if (b + u < s1) cum[b + u] = static_cast<uint32_t>(c > 0xffffffffull ? 0xffffffffu : c);
+            if (b + u < s1) cum[b + u] = clamp_u32(c);
             c += v[u];
         }
     }
