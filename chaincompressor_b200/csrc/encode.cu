@@ -1189,11 +1189,14 @@ __global__ void k_words_to_bytes(uint32_t* words, uint64_t nwords) {
 // Serialises every chosen table (one CTA per stream).
 __global__ void __launch_bounds__(1024) k_serialize_tables(EncState* st, const uint32_t* prob, const uint32_t* tag_prob,
                                                             uint64_t hist_stride, uint8_t* out, uint64_t out_stride) {
+    extern __shared__ __align__(16) uint32_t ser_stage[];   // kSerStageSyms u32
     const int s = blockIdx.x;
     StreamChoice& c = st->ch[s];
     uint32_t len = 0;
-    if (c.enc == kEncRaw) len = serialize_table_block(prob + hist_stride * s, c.sec_alphabet, out + out_stride * s);
-    else if (c.enc == kEncTagged) len = serialize_table_block(tag_prob + 64 * s, c.sec_alphabet, out + out_stride * s);
+    if (c.enc == kEncRaw)
+        len = serialize_table_block(prob + hist_stride * s, c.sec_alphabet, out + out_stride * s, ser_stage);
+    else if (c.enc == kEncTagged)
+        len = serialize_table_block(tag_prob + 64 * s, c.sec_alphabet, out + out_stride * s, ser_stage);
     if (threadIdx.x == 0) c.table_len = len;
 }
 
@@ -1943,7 +1946,10 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     }
     jobs.total_blocks = first;
     T.mark("corrections+packing", stream);
-    k_serialize_tables<<<kCodeStreams, 1024, 0, stream>>>(st, prob, tag_prob, hist_stride, tables, table_stride); count_launch();
+    CHAIN_CUDA(cudaFuncSetAttribute(k_serialize_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(4 * kSerStageSyms)));
+    k_serialize_tables<<<kCodeStreams, 1024, 4 * kSerStageSyms, stream>>>(st, prob, tag_prob, hist_stride, tables,
+                                                                          table_stride); count_launch();
     T.mark("serialize_tables", stream);
     if (jobs.total_blocks) {
         k_enc_symbols<<<dim3(64, jobs.njobs), 256, 0, stream>>>(jobs); count_launch();

@@ -309,9 +309,18 @@ __device__ inline uint32_t block_inclusive_max(uint32_t v, uint32_t* scratch) {
 // Serialises prob[0..A) into tokens with the whole CTA.  Returns the byte count (in
 // every thread).  A zero at s starts a token when (s - run_start) % 64 == 0; the
 // token covers up to 64 zeros of its run.
-__device__ inline uint32_t serialize_table_block(const uint32_t* prob, uint32_t A, uint8_t* out) {
+constexpr uint32_t kSerStageSyms = 16384;   // alphabets serialized from a shared-memory copy
+__device__ inline uint32_t serialize_table_block(const uint32_t* prob_in, uint32_t A, uint8_t* out, uint32_t* stage) {
     __shared__ uint32_t mscratch[33];
     __shared__ uint64_t sscratch[33];
+    // the zero-run lookahead below is a chain of dependent reads: serve it from shared
+    // memory (`stage`, kSerStageSyms u32) when the alphabet fits
+    const uint32_t* prob = prob_in;
+    if (A <= kSerStageSyms) {
+        for (uint32_t i = threadIdx.x; i < A; i += blockDim.x) stage[i] = prob_in[i];
+        __syncthreads();
+        prob = stage;
+    }
     uint32_t carry_last = 0;   // (index of the last nonzero so far) + 1
     uint64_t carry_off = 0;
     for (uint32_t base = 0; base < A; base += blockDim.x) {
