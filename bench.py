@@ -222,8 +222,12 @@ def run_ours(args, rank: int, world: int):
         return ev0.elapsed_time(ev1) / 1e3 / args.steps, launches, {k: v / args.steps for k, v in acc.items()}
 
     clocks = Clocks(dev)
-    t_c, launches_c, stages_c = timed(lambda: comp(soa_dev.data_ptr()), stages=True)
-    t_d, launches_d, stages_d = timed(lambda: decomp(cont_dev.data_ptr(), out_dev.data_ptr()), stages=True)
+    # headline timings without stage events; the per-stage breakdown (and the per-kernel
+    # durations of the roofline) come from a second pass of the same steps with them
+    t_c, launches_c, _ = timed(lambda: comp(soa_dev.data_ptr()))
+    t_d, launches_d, _ = timed(lambda: decomp(cont_dev.data_ptr(), out_dev.data_ptr()))
+    _, _, stages_c = timed(lambda: comp(soa_dev.data_ptr()), stages=True)
+    _, _, stages_d = timed(lambda: decomp(cont_dev.data_ptr(), out_dev.data_ptr()), stages=True)
 
     def e2e_c():
         comp(soa_host.data_ptr())
@@ -238,10 +242,9 @@ def run_ours(args, rank: int, world: int):
     err = float(np.abs(dec - pts.astype(np.float64)).max())
 
     # roofline of the dominant kernels: algorithmic bytes per launch / event-timed duration
-    sys.path.insert(0, str(ROOT / "tests"))
-    import lcg2_inspect
+    from chaincompressor_b200 import lcg2
 
-    info = lcg2_inspect.inspect(bytes(cont_host.numpy()))
+    info = lcg2.inspect(bytes(cont_host.numpy()))
     rans_syms = sum(c["section"]["symbols"] for c in info["components"].values() if "section" in c)
     rans_bytes = sum(c["section"]["payload"] + c["section"]["state_bytes"] + 4 * c["section"]["chunks"]
                      for c in info["components"].values() if "section" in c)
@@ -646,39 +649,79 @@ def main():
                     help="one warm-up and one measured compress + decompress, no timing (for ncu launch lists)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.gpus < 1:
+        raise SystemExit("--gpus must be >= 1")
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        # not started by torchrun: start the N local ranks ourselves
+        return spawn_local_ranks(args.gpus, sys.argv[1:])
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; launch one rank per GPU", file=sys.stderr)
+        return 2
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)))
-        return
+        return 0
     if args.once:
         run_once(args)
-        return
+        return 0
+    if args.config in ("batch", "serve") and world > 1:
+        print(f"bench.py: --config {args.config} runs on one GPU", file=sys.stderr)
+        return 2
     if args.config == "batch":
-        if rank == 0:
-            print(json.dumps(run_batch_bench(args)))
-        return
+        print(json.dumps(run_batch_bench(args)))
+        return 0
     if args.config == "serve":
-        if rank == 0:
-            print(json.dumps(run_serve_bench(args)))
-        return
+        print(json.dumps(run_serve_bench(args)))
+        return 0
+    import torch
+
+    gpu = torch.cuda.is_available()
     if world > 1:
         import datetime
 
-        import torch
         import torch.distributed as tdist
 
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = run_ours(args, rank, world)
+        if gpu:
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)) % torch.cuda.device_count())
+        tdist.init_process_group("nccl" if gpu else "gloo", timeout=datetime.timedelta(seconds=120))
+    line = _rank_work()(args, rank, world)
     if world > 1:
         import torch.distributed as tdist
 
         tdist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+    return 0
+
+
+def _rank_work():
+    """The per-rank step function: run_ours, or -- for tests of the launch path on
+    machines without a GPU -- the callable named by CHAIN_BENCH_RANK_FN
+    ("module:function", same signature)."""
+    spec = os.environ.get("CHAIN_BENCH_RANK_FN")
+    if not spec:
+        return run_ours
+    import importlib
+
+    mod, fn = spec.split(":")
+    return getattr(importlib.import_module(mod), fn)
+
+
+def spawn_local_ranks(nproc: int, argv) -> int:
+    """Starts `nproc` ranks of this script on this node through torch.distributed.run
+    (rendezvous on 127.0.0.1, a free port) and returns its exit status; rank 0 prints
+    the JSON line.  Used when bench.py --gpus N (N > 1) is started without torchrun."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nproc}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *argv]
+    return subprocess.run(cmd).returncode
 
 
 if __name__ == "__main__":
-    main()
+    sys.exit(main())

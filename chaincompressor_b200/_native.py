@@ -31,7 +31,7 @@ CHAIN_SOA, CHAIN_AOS = 0, 1
 EXPORTS = ("chain_ctx_create", "chain_ctx_destroy", "chain_last_error_message", "chain_compress_bound",
            "chain_compress", "chain_result_copy", "chain_result_device_ptr", "chain_peek", "chain_decompress",
            "chain_debug_streams", "chain_set_stage_timing", "chain_stage_times", "chain_launch_count",
-           "chain_decompress_noalloc", "chain_batch_create", "chain_batch_destroy", "chain_batch_compress",
+           "chain_alloc_count", "chain_decompress_noalloc", "chain_batch_create", "chain_batch_destroy", "chain_batch_compress",
            "chain_batch_decompress", "chain_batch_tune", "chain_server_create", "chain_server_destroy", "chain_server_submit",
            "chain_server_wait", "chain_transcode_lcp2")
 
@@ -106,6 +106,7 @@ def load() -> ctypes.CDLL:
                   "chain_server_submit", "chain_server_wait", "chain_transcode_lcp2"):
             getattr(L, f).restype = ctypes.c_int
         L.chain_launch_count.restype = ctypes.c_uint64
+        L.chain_alloc_count.restype = ctypes.c_uint64
         _LIB = L
     return _LIB
 
@@ -385,6 +386,11 @@ def transcode_lcp2(data: bytes) -> bytes:
 def launch_count() -> int:
     """Kernel launches issued by the library in this process so far."""
     return load().chain_launch_count()
+
+
+def alloc_count() -> int:
+    """cudaMalloc / cudaMallocHost calls made by the library in this process so far."""
+    return load().chain_alloc_count()
 
 
 def compress_bound(n: int, dims: int) -> int:

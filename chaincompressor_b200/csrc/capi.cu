@@ -17,6 +17,9 @@ static thread_local std::string g_last_error;
 static std::atomic<uint64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 uint64_t launch_count_total() { return g_launches.load(std::memory_order_relaxed); }
+static std::atomic<uint64_t> g_allocs{0};
+void count_alloc() { g_allocs.fetch_add(1, std::memory_order_relaxed); }
+uint64_t alloc_count_total() { return g_allocs.load(std::memory_order_relaxed); }
 
 chain_status set_err(chain_status st, const std::string& msg) {
     g_last_error = msg;
@@ -46,7 +49,9 @@ chain_status ensure_state(chain_ctx* ctx, size_t bytes) {
     ctx->state_host = nullptr;
     ctx->state_bytes = 0;
     const size_t want = bytes < (64u << 10) ? (64u << 10) : bytes;
+    count_alloc();
     CHAIN_CUDA(cudaMalloc(&ctx->state_dev, want));
+    count_alloc();
     CHAIN_CUDA(cudaMallocHost(&ctx->state_host, want));
     ctx->state_bytes = want;
     return CHAIN_OK;
@@ -223,6 +228,7 @@ chain_status chain_debug_streams(chain_ctx* ctx, int64_t* idrel, int64_t* diff, 
 }
 
 uint64_t chain_launch_count(void) { return launch_count_total(); }
+uint64_t chain_alloc_count(void) { return alloc_count_total(); }
 
 chain_status chain_set_stage_timing(chain_ctx* ctx, int enabled) {
     if (!ctx) return set_err(CHAIN_ERR_INVALID_ARGUMENT, "null context");

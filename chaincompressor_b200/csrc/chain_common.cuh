@@ -36,6 +36,10 @@ enum Encoding : uint8_t { kEncEmpty = 0, kEncTagged = 1, kEncFixed = 2, kEncRaw 
 // site calls count_launch()).
 void count_launch();          // process-wide, thread-safe
 uint64_t launch_count_total();
+// Host-side count of the library's own memory allocations (every cudaMalloc and
+// cudaMallocHost it issues; allocation sites call count_alloc()).
+void count_alloc();           // process-wide, thread-safe
+uint64_t alloc_count_total();
 
 __host__ __device__ inline int bitlen32(uint32_t v) {
 #ifdef __CUDA_ARCH__

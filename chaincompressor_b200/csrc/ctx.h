@@ -11,6 +11,8 @@
 
 namespace chain {
 
+void count_alloc();   // counts the library's own cudaMalloc / cudaMallocHost calls
+
 // Bump allocator over one device allocation.  reserve() grows the allocation between
 // calls (never while kernels of the current call are queued on it).  A `fixed` arena
 // lies over memory it does not own: reserve() never allocates or frees, it only
@@ -32,6 +34,7 @@ struct Arena {
         base = nullptr;
         cap = 0;
         size_t want = bytes + bytes / 8 + (1u << 20);
+        count_alloc();
         cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&base), want);
         if (e != cudaSuccess) { base = nullptr; return e; }
         cap = want;
@@ -61,6 +64,7 @@ struct PinnedBuf {
         if (ptr) cudaFreeHost(ptr);
         ptr = nullptr;
         cap = 0;
+        count_alloc();
         cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&ptr), bytes);
         if (e != cudaSuccess) { ptr = nullptr; return e; }
         cap = bytes;
@@ -133,7 +137,11 @@ struct chain_ctx {
     chain::Arena dec;      // decoder buffers
     chain::PinnedBuf pinned;
     void* state_dev = nullptr;    // device scratch scalars (EncState / DecState)
-    void* state_host = nullptr;   // pinned mirror
+    // Host mirror of state_dev: pinned when the context allocated it (ensure_state).
+    // chain_decompress_noalloc points it at a pageable static array instead; copies to
+    // and from pageable memory are synchronous, which that entry point relies on no more
+    // than decode_frame does (it synchronises the stream before reading the mirror).
+    void* state_host = nullptr;
     size_t state_bytes = 0;
     const uint8_t* result = nullptr;  // device container of the last compress
     size_t result_len = 0;

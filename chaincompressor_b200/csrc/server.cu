@@ -54,6 +54,7 @@ struct chain_server {
     std::unordered_map<uint64_t, Request> reqs;
     size_t inflight = 0;
     int running = 0;
+    int waiters = 0;                // threads inside chain_server_wait
     uint64_t next_ticket = 1;
     bool stop = false;
 };
@@ -79,13 +80,14 @@ void worker(chain_server* s, size_t k) {
         Request* r = nullptr;
         {
             std::unique_lock<std::mutex> lk(s->mu);
+            // after stop, the queue is drained before the worker exits, so that every
+            // submitted request finishes and its waiter is released
             s->cv_work.wait(lk, [&] {
-                if (s->stop) return true;
-                if (s->queue.empty()) return false;
+                if (s->queue.empty()) return s->stop;
                 const size_t mem = s->reqs.find(s->queue.front())->second.mem;
                 return s->running == 0 || s->inflight + mem <= s->budget;
             });
-            if (s->stop) return;
+            if (s->queue.empty()) return;
             ticket = s->queue.front();
             s->queue.pop_front();
             r = &s->reqs.find(ticket)->second;
@@ -162,6 +164,8 @@ chain_status chain_server_create(int device, int workers, size_t memory_budget_b
     return CHAIN_OK;
 }
 
+// Stops admission, lets the workers finish every queued request, then waits until no
+// thread is left inside chain_server_wait before freeing the server.
 void chain_server_destroy(chain_server* s) {
     if (!s) return;
     {
@@ -170,6 +174,11 @@ void chain_server_destroy(chain_server* s) {
     }
     s->cv_work.notify_all();
     for (auto& t : s->threads) t.join();
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->cv_done.notify_all();
+        s->cv_done.wait(lk, [&] { return s->waiters == 0; });
+    }
     for (chain_ctx* c : s->ctx) chain_ctx_destroy(c);
     delete s;
 }
@@ -200,9 +209,12 @@ chain_status chain_server_wait(chain_server* s, uint64_t ticket, double* queue_m
     auto f = s->reqs.find(ticket);
     if (f == s->reqs.end()) return set_err(CHAIN_ERR_INVALID_ARGUMENT, "unknown ticket");
     Request* rp = &f->second;   // element references survive rehashing; iterators do not
+    ++s->waiters;
     s->cv_done.wait(lk, [&] { return rp->done; });
     const Request r = *rp;
     s->reqs.erase(ticket);
+    --s->waiters;
+    if (s->stop) s->cv_done.notify_all();   // chain_server_destroy waits for the last waiter
     lk.unlock();
     if (queue_ms) *queue_ms = ms_between(r.t_submit, r.t_start);
     if (service_ms) *service_ms = ms_between(r.t_start, r.t_end);

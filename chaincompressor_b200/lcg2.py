@@ -1,8 +1,9 @@
-"""Pure-Python reader of the LCG2 v2 container directory (test helper).
+"""Pure-Python reader of the LCG2 v2 container directory.
 
 Walks the layout documented in chaincompressor_b200/csrc/chain_format.h and returns,
-per component, its encoding, record count, byte size and rANS chunking.  It checks
-structure only; decoding is the library's job.
+per component, its encoding, record count, byte size and rANS chunking (used for
+size reports and for the algorithmic byte counts of the benchmark's roofline).  It
+checks structure only; decoding is the library's job.
 """
 import struct
 

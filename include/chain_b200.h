@@ -199,7 +199,9 @@ CHAIN_API chain_status chain_transcode_lcp2(const void* container, size_t len, v
  * runs alone).  Contexts, arenas and streams stay resident between requests.
  * chain_server_wait blocks until the request has finished and returns its status, its
  * queueing time (submit -> start) and its service time (start -> end), in milliseconds.
- * Every submitted ticket must be waited for once.  No counterpart in the reference,
+ * Every submitted ticket must be waited for once.  chain_server_destroy stops admission,
+ * finishes every queued request and returns once no thread is inside chain_server_wait;
+ * no call on the server may start after destroy has begun.  No counterpart in the reference,
  * which compresses one frame per synchronous call (chain_caller.py:33-40). */
 typedef struct chain_server chain_server;
 CHAIN_API chain_status chain_server_create(int device, int workers, size_t memory_budget_bytes,
@@ -248,6 +250,10 @@ CHAIN_API chain_status chain_set_stage_timing(chain_ctx* ctx, int enabled);
 /* Number of CUDA kernels the library has launched in this process so far (all threads,
  * batch workers included). */
 CHAIN_API uint64_t chain_launch_count(void);
+/* Number of memory allocations (cudaMalloc and cudaMallocHost calls) the library has
+ * made in this process so far, all threads included.  Tracing aid: it lets a caller
+ * check that a code path allocated nothing (no counterpart in the reference). */
+CHAIN_API uint64_t chain_alloc_count(void);
 CHAIN_API int chain_stage_times(const chain_ctx* ctx, const char** names, float* ms, int max);
 
 #ifdef __cplusplus

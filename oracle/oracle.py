@@ -28,6 +28,16 @@ REF_DIR = HERE / "_ref"
 _LIB = None
 
 
+def reference_dir() -> Path:
+    """The reference checkout the recipe in oracle/Makefile compiles from:
+    $CHAIN_REFERENCE_DIR when set, else the Makefile's default (``make print-ref``)."""
+    env = os.environ.get("CHAIN_REFERENCE_DIR")
+    if env:
+        return Path(env)
+    r = subprocess.run(["make", "-s", "-C", str(HERE), "print-ref"], capture_output=True, text=True)
+    return Path(r.stdout.strip())
+
+
 def build_own() -> Path:
     so = HERE / "libchain_oracle.so"
     src = [HERE / "chain_oracle.c", HERE / "chain_oracle.h"]

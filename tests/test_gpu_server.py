@@ -76,3 +76,45 @@ def test_failing_request_does_not_disturb_others(codec):
         srv.wait(t)
         _check(op, item, bufs, want)
     srv.close()
+
+
+def test_destroy_finishes_queued_requests(codec):
+    """chain_server_destroy right after the submits, with most requests still queued on
+    the single worker: every request still runs to completion, with the same result as
+    alone (the items carry status and output)."""
+    reqs = _requests(codec)[:12]
+    srv = N.Server(0, workers=1, memory_budget_bytes=40 << 30)
+    for op, item, _, _ in reqs:
+        srv.submit(op, item)
+    srv.close()
+    for op, item, bufs, want in reqs:
+        assert item.status == N.CHAIN_OK
+        _check(op, item, bufs, want)
+
+
+def test_destroy_releases_a_blocked_waiter(codec):
+    """A thread blocked in chain_server_wait when destroy begins is released with its
+    request's status, and destroy returns only after it has left the call."""
+    import ctypes
+    import threading
+    import time
+
+    reqs = _requests(codec)[:4]
+    srv = N.Server(0, workers=1, memory_budget_bytes=40 << 30)
+    tickets = [srv.submit(op, item) for op, item, _, _ in reqs]
+    h = srv.h
+    got = []
+
+    def waiter():
+        got.append(srv.L.chain_server_wait(h, ctypes.c_uint64(tickets[-1]), None, None))
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    time.sleep(0.5)            # the waiter is inside chain_server_wait by now
+    srv.h = None
+    srv.L.chain_server_destroy(h)
+    th.join(timeout=120)
+    assert not th.is_alive()
+    assert got == [N.CHAIN_OK]
+    op, item, bufs, want = reqs[-1]
+    _check(op, item, bufs, want)

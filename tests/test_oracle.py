@@ -99,7 +99,7 @@ def test_dambreak_frame_if_present():
     """The reference's bundled DamBreak frame (only where the reference checkout exists)."""
     import xml.etree.ElementTree as ET
 
-    files = sorted(Path("/root/reference/data/DamBreak").glob("0654*.vtp"))
+    files = sorted((oracle.reference_dir() / "data" / "DamBreak").glob("0654*.vtp"))
     if not files:
         pytest.skip("reference data not present")
     root = ET.parse(files[0]).getroot()
@@ -112,3 +112,31 @@ def test_dambreak_frame_if_present():
     s = oracle.streams(arr, eb, 4, 25)
     for k in STREAMS:
         assert np.array_equal(np.asarray(rs[k]), s[k]), k
+
+
+def _dambreak():
+    import json
+
+    g = np.load(Path(__file__).parent / "golden" / "dambreak" / "frame0654.npz")
+    return g["points"], json.loads(str(g["cases"]))
+
+
+_DB_POINTS, _DB_CASES = _dambreak()
+
+
+@pytest.mark.parametrize("case", _DB_CASES, ids=[f"{c['table']}_qb{c['qb']}" for c in _DB_CASES])
+def test_oracle_matches_dambreak_fixture(case):
+    """The reference's DamBreak frame at the reader.py (p, threshold) tables: the
+    restatement's streams, corrections and decoded output hash to what the reference
+    encoder and decoder produced (tests/golden/make_dambreak.py)."""
+    import hashlib
+
+    def digest(a, dt="<i8"):
+        return hashlib.sha256(np.ascontiguousarray(np.asarray(a, dtype=dt)).tobytes()).hexdigest()
+
+    s = oracle.streams(_DB_POINTS, case["eb"], case["p"], case["threshold"])
+    for k in STREAMS:
+        assert list(s[k].shape) == case[k + "_shape"], k
+        assert digest(s[k]) == case[k], k
+    assert digest(s["exact_index"].astype(np.int64)) == case["exact_index"]
+    assert digest(oracle.decode(s), "<f8") == case["decoded"]

@@ -41,12 +41,25 @@ def frames(torch_cuda):
 
 
 def _noalloc(src_ptr, length, out_ptr, capacity, dtype, layout, stream=0):
-    """One call through the C ABI; returns (status, n, dims)."""
+    """One call through the C ABI; returns (status, n, dims).  Every call, failing ones
+    included, must leave the library's count of its own cudaMalloc / cudaMallocHost
+    calls unchanged: the entry point's defining property."""
     L = N.load()
     n, d = ctypes.c_uint64(), ctypes.c_uint32()
+    before = N.alloc_count()
     st = L.chain_decompress_noalloc(ctypes.c_void_p(src_ptr), length, dtype, layout, ctypes.c_void_p(out_ptr),
                                     capacity, ctypes.byref(n), ctypes.byref(d), ctypes.c_void_p(stream))
+    assert N.alloc_count() == before, "chain_decompress_noalloc allocated memory"
     return st, n.value, d.value
+
+
+def test_allocation_counter_sees_context_allocations(torch_cuda, frames):
+    """The counter the no-allocation checks rely on does move when the library
+    allocates (a fresh context's arenas and state on its first decode)."""
+    data, n, d = frames[0]
+    before = N.alloc_count()
+    _existing(data, n, d, np.float64, N.CHAIN_AOS)
+    assert N.alloc_count() > before
 
 
 def _existing(data, n, d, dtype, layout):
