@@ -210,20 +210,33 @@ chain_status chain_debug_streams(chain_ctx* ctx, int64_t* idrel, int64_t* diff, 
     if (ndiff) *ndiff = d.ndiff;
     if (nkeep) *nkeep = d.nkeep;
     if (nblocks) *nblocks = d.nblocks;
-    auto fetch = [&](const uint32_t* src, uint64_t count, int64_t* dst) -> chain_status {
+    // streams are stored with esz bytes per value (1, 2 or 4)
+    auto fetch = [&](const void* src, uint32_t esz, uint64_t count, int64_t* dst) -> chain_status {
         if (!dst || count == 0) return CHAIN_OK;
-        std::vector<uint32_t> tmp(count);
-        CHAIN_CUDA(cudaMemcpyAsync(tmp.data(), src, count * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        std::vector<uint8_t> tmp(count * esz);
+        CHAIN_CUDA(cudaMemcpyAsync(tmp.data(), src, count * esz, cudaMemcpyDeviceToHost, ctx->stream));
         CHAIN_CUDA(cudaStreamSynchronize(ctx->stream));
-        for (uint64_t i = 0; i < count; ++i) dst[i] = tmp[i];
+        for (uint64_t i = 0; i < count; ++i) {
+            if (esz == 1) {
+                dst[i] = tmp[i];
+            } else if (esz == 2) {
+                uint16_t v;
+                std::memcpy(&v, tmp.data() + 2 * i, 2);
+                dst[i] = v;
+            } else {
+                uint32_t v;
+                std::memcpy(&v, tmp.data() + 4 * i, 4);
+                dst[i] = v;
+            }
+        }
         return CHAIN_OK;
     };
     chain_status s;
-    if ((s = fetch(d.idrel, d.n, idrel)) != CHAIN_OK) return s;
-    if ((s = fetch(d.diff, d.ndiff * d.dims, diff)) != CHAIN_OK) return s;
-    if ((s = fetch(d.keep, d.nkeep * d.dims, keep)) != CHAIN_OK) return s;
-    if ((s = fetch(d.choice2, d.nblocks, choice2)) != CHAIN_OK) return s;
-    if ((s = fetch(d.rel, d.n * d.dims, rel)) != CHAIN_OK) return s;
+    if ((s = fetch(d.idrel, 4, d.n, idrel)) != CHAIN_OK) return s;
+    if ((s = fetch(d.diff, d.kd_esz, d.ndiff * d.dims, diff)) != CHAIN_OK) return s;
+    if ((s = fetch(d.keep, d.kd_esz, d.nkeep * d.dims, keep)) != CHAIN_OK) return s;
+    if ((s = fetch(d.choice2, 1, d.nblocks, choice2)) != CHAIN_OK) return s;
+    if ((s = fetch(d.rel, d.rel_esz, d.n * d.dims, rel)) != CHAIN_OK) return s;
     return CHAIN_OK;
 }
 

@@ -76,6 +76,13 @@ __host__ __device__ inline double from_ordered_bits(uint64_t o) {
 
 __device__ inline void set_error(uint32_t* err, uint32_t bits) { atomicOr(err, bits); }
 
+// Element i of an integer stream stored with esz bytes per value (1, 2 or 4).
+__device__ __forceinline__ uint32_t load_elem(const void* p, uint64_t i, uint32_t esz) {
+    if (esz == 1) return static_cast<const uint8_t*>(p)[i];
+    if (esz == 2) return static_cast<const uint16_t*>(p)[i];
+    return static_cast<const uint32_t*>(p)[i];
+}
+
 __device__ inline uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -116,12 +116,17 @@ struct StageTimer {
     }
 };
 
+// The encoder's integer streams of the last compress (device memory).  idrel is stored
+// with four bytes per value, choice2 with one, diff and keep with kd_esz (1, 2 or 4),
+// rel with rel_esz (1 when p <= 256, else 4).
 struct EncodeDebug {
     const uint32_t* idrel = nullptr;
-    const uint32_t* diff = nullptr;
-    const uint32_t* keep = nullptr;
-    const uint32_t* choice2 = nullptr;
-    const uint32_t* rel = nullptr;
+    const void* diff = nullptr;
+    const void* keep = nullptr;
+    uint32_t kd_esz = 4;
+    const uint8_t* choice2 = nullptr;
+    const void* rel = nullptr;
+    uint32_t rel_esz = 4;
     uint64_t n = 0, ndiff = 0, nkeep = 0, nblocks = 0;
     uint32_t dims = 0;
 };

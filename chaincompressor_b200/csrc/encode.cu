@@ -245,8 +245,12 @@ struct BlockDiv {
 // IEEE double, the reconstruction fma(q + 0.5, 2 eb, min) checked against eb (values
 // outside go to the exact-correction list), the block index and the offset inside the
 // block, and the point's Z-order block key.  DIM is the dimension count (0 = run time).
-// Three-dimensional SoA input is processed four points per thread with 16-byte loads and
-// stores (the rest of the points, and every other shape, one point per thread).
+// One CTA per sort tile (SortShape<KT>::kTile consecutive points), so that the CTA can
+// also count its tile's first radix digits (key & (2^hist_bits - 1)) into the sort's
+// count table (digit-major, `tiles` columns) when hist_counts is set: the first sort
+// pass then needs no histogram launch.  The offsets go out as RT (one byte each when
+// p <= 256).  Three-dimensional SoA input is processed four points per thread with
+// 16-byte loads (the rest of the points, and every other shape, one point per thread).
 struct QuantCtx {
     const double* mins;
     double eb, denom, two_eb;
@@ -256,8 +260,8 @@ struct QuantCtx {
     double* corr_val;
     uint64_t corr_cap;
     // Quantizes coordinate x (flat index fi = i*D + d); returns the block index and
-    // stores the offset inside the block in *rel.
-    __device__ __forceinline__ uint32_t coord(double x, uint32_t d, uint64_t fi, uint32_t* rel) const {
+    // stores the offset inside the block in rel.
+    __device__ __forceinline__ uint32_t coord(double x, uint32_t d, uint64_t fi, uint32_t& rel) const {
         const double qv = floor(__ddiv_rn(__dsub_rn(x, mins[d]), denom));
         const uint32_t q = static_cast<uint32_t>(qv);
         const double restored = fma(__dadd_rn(static_cast<double>(q), 0.5), two_eb, mins[d]);
@@ -269,24 +273,30 @@ struct QuantCtx {
             }
         }
         const uint32_t bb = bd.div(q);
-        *rel = static_cast<uint32_t>(q - static_cast<uint64_t>(bb) * bd.p);
+        rel = static_cast<uint32_t>(q - static_cast<uint64_t>(bb) * bd.p);
         return bb;
     }
 };
 
-template <typename FT, bool SOA, typename KT, int DIM>
+template <typename FT, bool SOA, typename KT, int DIM, typename RT>
 __global__ void __launch_bounds__(256)
 k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT* __restrict__ key_out,
-           uint32_t* __restrict__ rel_out, uint64_t* __restrict__ corr_idx, double* __restrict__ corr_val,
-           uint64_t corr_cap) {
+           RT* __restrict__ rel_out, uint64_t* __restrict__ corr_idx, double* __restrict__ corr_val,
+           uint64_t corr_cap, uint32_t* __restrict__ hist_counts, int hist_bits, uint32_t tiles) {
+    static_assert(SortShape<KT>::kTile % 1024 == 0, "tiles hold whole groups of four points per thread");
+    constexpr uint64_t TILE = SortShape<KT>::kTile;
     __shared__ double s_min[kMaxDims];
     __shared__ double s_eb;
     __shared__ uint64_t s_p;
     __shared__ int s_kb;
+    __shared__ uint32_t s_hist[kSortBins];
     const uint32_t D = DIM ? DIM : D_rt;
     if (threadIdx.x < D) s_min[threadIdx.x] = st->mins[threadIdx.x];
     if (threadIdx.x == 0) { s_eb = st->eb; s_p = st->p; s_kb = st->kb; }
+    s_hist[threadIdx.x] = 0;
     __syncthreads();
+    const uint32_t hmask = (1u << hist_bits) - 1;
+    const bool hist = hist_counts != nullptr;
     QuantCtx Q;
     Q.mins = s_min;
     Q.eb = s_eb;
@@ -300,16 +310,16 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
     Q.corr_val = corr_val;
     Q.corr_cap = corr_cap;
     const int kb = s_kb;
-    const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    uint64_t first_scalar = 0;
+    const uint64_t tile_begin = static_cast<uint64_t>(blockIdx.x) * TILE;
+    const uint64_t tile_end = min(n, tile_begin + TILE);
+    uint64_t first_scalar = tile_begin;
     if constexpr (SOA && DIM == 3) {
         const bool vec = ((reinterpret_cast<uintptr_t>(p) | (n * sizeof(FT))) & 15) == 0 &&
                          (reinterpret_cast<uintptr_t>(rel_out) & 15) == 0 &&
                          (reinterpret_cast<uintptr_t>(key_out) & 15) == 0;
         if (vec) {
-            const uint64_t ng = n / 4;
-            for (uint64_t g = tid; g < ng; g += nthreads) {
+            const uint64_t ng = tile_end / 4;   // whole groups of four points below tile_end
+            for (uint64_t g = tile_begin / 4 + threadIdx.x; g < ng; g += blockDim.x) {
                 FT x[3][4];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
@@ -328,13 +338,21 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
                     uint32_t b[3];
 #pragma unroll
                     for (int d = 0; d < 3; ++d)
-                        b[d] = Q.coord(static_cast<double>(x[d][k]), d, (4 * g + k) * 3 + d, &rel[3 * k + d]);
+                        b[d] = Q.coord(static_cast<double>(x[d][k]), d, (4 * g + k) * 3 + d, rel[3 * k + d]);
                     keys[k] = static_cast<KT>(block_key(b, 3, kb));
+                    if (hist) atomicAdd(&s_hist[static_cast<uint32_t>(keys[k]) & hmask], 1u);
                 }
-                uint4* ro = reinterpret_cast<uint4*>(rel_out + 12 * g);
-                ro[0] = make_uint4(rel[0], rel[1], rel[2], rel[3]);
-                ro[1] = make_uint4(rel[4], rel[5], rel[6], rel[7]);
-                ro[2] = make_uint4(rel[8], rel[9], rel[10], rel[11]);
+                if constexpr (sizeof(RT) == 4) {
+                    uint4* ro = reinterpret_cast<uint4*>(rel_out + 12 * g);
+                    ro[0] = make_uint4(rel[0], rel[1], rel[2], rel[3]);
+                    ro[1] = make_uint4(rel[4], rel[5], rel[6], rel[7]);
+                    ro[2] = make_uint4(rel[8], rel[9], rel[10], rel[11]);
+                } else {   // twelve bytes as three little-endian words
+                    uint32_t* ro = reinterpret_cast<uint32_t*>(rel_out + 12 * g);
+#pragma unroll
+                    for (int w = 0; w < 3; ++w)
+                        ro[w] = rel[4 * w] | (rel[4 * w + 1] << 8) | (rel[4 * w + 2] << 16) | (rel[4 * w + 3] << 24);
+                }
                 if constexpr (sizeof(KT) == 4) {
                     *reinterpret_cast<uint4*>(key_out + 4 * g) = make_uint4(keys[0], keys[1], keys[2], keys[3]);
                 } else {
@@ -343,18 +361,27 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
                     ko[1] = make_ulonglong2(keys[2], keys[3]);
                 }
             }
-            first_scalar = ng * 4;
+            first_scalar = max(ng * 4, tile_begin);
         }
     }
     constexpr int KD = DIM ? DIM : kMaxDims;
-    for (uint64_t i = first_scalar + tid; i < n; i += nthreads) {
+    for (uint64_t i = first_scalar + threadIdx.x; i < tile_end; i += blockDim.x) {
         uint32_t b[KD];
 #pragma unroll
         for (int d = 0; d < KD; ++d) {
             if (!DIM && d >= static_cast<int>(D)) break;
-            b[d] = Q.coord(load_coord<FT, SOA>(p, n, D, i, d), d, i * D + d, &rel_out[i * D + d]);
+            uint32_t r;
+            b[d] = Q.coord(load_coord<FT, SOA>(p, n, D, i, d), d, i * D + d, r);
+            rel_out[i * D + d] = static_cast<RT>(r);
         }
-        key_out[i] = static_cast<KT>(block_key(b, static_cast<int>(D), kb));
+        const KT key = static_cast<KT>(block_key(b, static_cast<int>(D), kb));
+        key_out[i] = key;
+        if (hist) atomicAdd(&s_hist[static_cast<uint32_t>(key) & hmask], 1u);
+    }
+    if (hist) {
+        __syncthreads();
+        if (threadIdx.x <= hmask)
+            hist_counts[static_cast<uint64_t>(threadIdx.x) * tiles + blockIdx.x] = s_hist[threadIdx.x];
     }
 }
 
@@ -498,80 +525,88 @@ struct ExplicitIn {
     const uint32_t* idrel;
     __device__ uint32_t operator()(uint64_t i) const { return idrel[i] == 0 ? 1u : 0u; }
 };
+// An explicit record is kept as its point's block key (the block coordinates are
+// decoded from it where they are used), which moves D times fewer bytes than the
+// coordinates themselves through the level-2 passes.
 template <typename KT>
 struct ExplicitOut {
     const KT* key;
-    const EncState* st;
-    uint32_t* rec;
+    KT* rec;
     __device__ void operator()(uint64_t i, uint32_t pos, uint32_t flag) const {
-        if (!flag) return;
-        const int D = static_cast<int>(st->dims);
-        if (D == 3 && st->kb <= 21) {   // the three de-interleaved coordinates straight to the record
-            const uint64_t k = static_cast<uint64_t>(key[i]);
-            uint32_t* r = rec + static_cast<uint64_t>(pos) * 3;
-            r[0] = compact3(k);
-            r[1] = compact3(k >> 1);
-            r[2] = compact3(k >> 2);
-            return;
-        }
-        uint32_t b[kMaxDims];
-        block_unkey(static_cast<uint64_t>(key[i]), D, st->kb, b);
-        for (int d = 0; d < D; ++d) rec[static_cast<uint64_t>(pos) * D + d] = b[d];
+        if (flag) rec[pos] = key[i];
     }
 };
 
+// Block coordinates of a record key (D dimensions of kb bits each).
+template <int DIM>
+__device__ __forceinline__ void rec_coords(uint64_t k, int D, int kb, uint32_t* b) {
+    if constexpr (DIM == 3) {
+        b[0] = compact3(k);
+        b[1] = compact3(k >> 1);
+        b[2] = compact3(k >> 2);
+    } else {
+        block_unkey(k, D, kb, b);
+    }
+}
+
+// Level-2 work runs with DIM = 3 (three dimensions, kb <= 21) or DIM = 0 (any shape).
+__device__ __forceinline__ bool l2_dim3(const EncState* st) { return st->dims == 3 && st->kb <= 21; }
+
 // ------------------------------------------------------------------- level 2
 // Record minimum, maximum and largest per-dimension difference between consecutive
-// records.  Three-dimensional records are read four per thread with 16-byte loads.
-__global__ void __launch_bounds__(256) k_l2_stats(const uint32_t* __restrict__ rec, EncState* st) {
+// records.  Each thread takes groups of four consecutive record keys (16-byte loads for
+// 32-bit keys), kU groups in flight at once.
+template <typename KT, int DIM>
+__global__ void __launch_bounds__(256) k_l2_stats(const KT* __restrict__ rec, EncState* st) {
     const uint32_t B = st->B;
-    const uint32_t D = st->dims;
+    const int D = DIM ? DIM : static_cast<int>(st->dims);
+    const int kb = st->kb;
+    if (DIM == 3 && !l2_dim3(st)) return;
+    if (DIM == 0 && l2_dim3(st)) return;
     uint32_t mn = 0xffffffffu, mx = 0, md = 0;
     const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const uint64_t nthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    uint64_t first_scalar = 0;
-    if (D == 3 && (reinterpret_cast<uintptr_t>(rec) & 15) == 0) {
-        // groups of four 3-D records; kU groups per thread in flight at once
-        constexpr int kU = 4;
-        const uint64_t ng = B / 4;
-        for (uint64_t g0 = tid; g0 < ng; g0 += nthreads * kU) {
-            uint32_t v[kU][15];   // per group: the previous record, then four records
+    constexpr int KD = DIM ? DIM : kMaxDims;
+    constexpr int kU = 2;
+    const uint64_t ng = (B + 3) / 4;
+    for (uint64_t g0 = tid; g0 < ng; g0 += nthreads * kU) {
+        KT k[kU][5];   // per group: the previous key, then four keys
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                const uint64_t g = g0 + u * nthreads;
-                if (g < ng) {
-                    const uint4* q = reinterpret_cast<const uint4*>(rec + 12 * g);
-                    const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
-                    v[u][3] = a.x; v[u][4] = a.y; v[u][5] = a.z; v[u][6] = a.w; v[u][7] = b.x; v[u][8] = b.y;
-                    v[u][9] = b.z; v[u][10] = b.w; v[u][11] = c.x; v[u][12] = c.y; v[u][13] = c.z; v[u][14] = c.w;
+        for (int u = 0; u < kU; ++u) {
+            const uint64_t g = g0 + u * nthreads;
+            const uint64_t j0 = 4 * g;
+            if (g < ng && j0 + 4 <= B && sizeof(KT) == 4) {
+                const uint4 v = __ldg(reinterpret_cast<const uint4*>(rec) + g);
+                k[u][1] = static_cast<KT>(v.x); k[u][2] = static_cast<KT>(v.y);
+                k[u][3] = static_cast<KT>(v.z); k[u][4] = static_cast<KT>(v.w);
+            } else {
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) v[u][d] = g ? __ldg(rec + 12 * g - 3 + d) : v[u][3 + d];
-                }
+                for (int q = 0; q < 4; ++q) k[u][1 + q] = g < ng && j0 + q < B ? __ldg(rec + j0 + q) : KT(0);
             }
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                if (g0 + u * nthreads >= ng) continue;
-#pragma unroll
-                for (int k = 3; k < 15; ++k) {
-                    mn = v[u][k] < mn ? v[u][k] : mn;
-                    mx = v[u][k] > mx ? v[u][k] : mx;
-                    const uint32_t w = v[u][k - 3];
-                    const uint32_t df = v[u][k] >= w ? v[u][k] - w : w - v[u][k];
-                    md = df > md ? df : md;
-                }
-            }
+            k[u][0] = g < ng && j0 ? __ldg(rec + j0 - 1) : KT(0);
         }
-        first_scalar = ng * 4;
-    }
-    for (uint64_t j = first_scalar + tid; j < B; j += nthreads) {
-        for (uint32_t d = 0; d < D; ++d) {
-            const uint32_t v = rec[j * D + d];
-            mn = v < mn ? v : mn;
-            mx = v > mx ? v : mx;
-            if (j) {
-                const uint32_t u = rec[(j - 1) * D + d];
-                const uint32_t a = v >= u ? v - u : u - v;
-                md = a > md ? a : md;
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint64_t g = g0 + u * nthreads;
+            if (g >= ng) continue;
+            uint32_t prev[KD], cur[KD];
+            rec_coords<DIM>(static_cast<uint64_t>(k[u][0]), D, kb, prev);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint64_t j = 4 * g + q;
+                if (j >= B) break;
+                rec_coords<DIM>(static_cast<uint64_t>(k[u][1 + q]), D, kb, cur);
+#pragma unroll
+                for (int d = 0; d < KD; ++d) {
+                    if (!DIM && d >= D) break;
+                    mn = cur[d] < mn ? cur[d] : mn;
+                    mx = cur[d] > mx ? cur[d] : mx;
+                    if (j) {
+                        const uint32_t df = cur[d] >= prev[d] ? cur[d] - prev[d] : prev[d] - cur[d];
+                        md = df > md ? df : md;
+                    }
+                    prev[d] = cur[d];
+                }
             }
         }
     }
@@ -596,100 +631,84 @@ __global__ void k_l2_params(EncState* st) {
     st->wrap_min_corr = -(range / 2);
 }
 
-struct Level2In {
-    const uint32_t* rec;
-    const EncState* st;
-    int l2;
-    __device__ uint32_t operator()(uint64_t j) const {
-        if (!l2 || j == 0 || j >= st->B) return 0u;
-        const uint32_t D = st->dims;
-        const uint64_t fvb = static_cast<uint64_t>(D) * bitlen32(st->rec_max);
-        const uint64_t fdb = static_cast<uint64_t>(D) * bitlen32(st->rec_maxdiff);
-        uint32_t mv = 0, md = 0;
-        for (uint32_t d = 0; d < D; ++d) {
-            const uint32_t v = rec[j * D + d], u = rec[(j - 1) * D + d];
-            mv = v > mv ? v : mv;
-            const uint32_t a = v >= u ? v - u : u - v;
-            md = a > md ? a : md;
-        }
-        const int tvw = bitlen32(mv), tdw = bitlen32(md);
-        const uint64_t tvb = static_cast<uint64_t>(D) * tvw + bitlen32(static_cast<uint32_t>(tvw));
-        const uint64_t tdb = static_cast<uint64_t>(D) * tdw + bitlen32(static_cast<uint32_t>(tdw));
-        const uint64_t value_bits = tvb < fvb ? tvb : fvb;
-        const uint64_t diff_bits = tdb > fdb ? tdb : fdb;
-        return value_bits >= diff_bits ? 1u : 0u;
+// The level-2 rule (lcps_cpp.cpp:1305-1454) for record j given its and its
+// predecessor's coordinates: 1 = code it as the difference from the previous record.
+__device__ __forceinline__ uint32_t l2_rule(const uint32_t* cur, const uint32_t* prev, int D, uint64_t fvb,
+                                           uint64_t fdb) {
+    uint32_t mv = 0, md = 0;
+    for (int d = 0; d < D; ++d) {
+        mv = cur[d] > mv ? cur[d] : mv;
+        const uint32_t a = cur[d] >= prev[d] ? cur[d] - prev[d] : prev[d] - cur[d];
+        md = a > md ? a : md;
     }
-};
+    const int tvw = bitlen32(mv), tdw = bitlen32(md);
+    const uint64_t tvb = static_cast<uint64_t>(D) * tvw + bitlen32(static_cast<uint32_t>(tvw));
+    const uint64_t tdb = static_cast<uint64_t>(D) * tdw + bitlen32(static_cast<uint32_t>(tdw));
+    const uint64_t value_bits = tvb < fvb ? tvb : fvb;
+    const uint64_t diff_bits = tdb > fdb ? tdb : fdb;
+    return value_bits >= diff_bits ? 1u : 0u;
+}
+
 // choice2[j] for every record (1 = difference from the previous record), one CTA per
 // flag-scan tile of kFlagTile records; each CTA also writes its tile's count of
-// difference records, so the level-2 flag scan needs no counting pass.  Three-
-// dimensional records are read in groups of four with 16-byte loads, four groups per
-// thread, all loads first (the rule of Level2In, lcps_cpp.cpp:1305-1454, applied in
-// registers).
-__global__ void __launch_bounds__(256) k_l2_choice(Level2In f, uint32_t* choice2, uint32_t* tile_counts) {
+// difference records, so the level-2 flag scan needs no counting pass.  Each thread
+// takes four groups of four consecutive record keys, all loads first.
+template <typename KT, int DIM>
+__global__ void __launch_bounds__(256) k_l2_choice(const KT* __restrict__ rec, const EncState* st, int l2,
+                                                   uint8_t* choice2, uint32_t* tile_counts) {
     static_assert(kFlagTile == 4 * 4 * 256, "four groups of four records per thread");
     __shared__ uint32_t wsum[8];
-    const EncState* st = f.st;
-    const uint32_t B = st->B, D = st->dims;
+    if (DIM == 3 && !l2_dim3(st)) return;
+    if (DIM == 0 && l2_dim3(st)) return;
+    const uint32_t B = st->B;
+    const int D = DIM ? DIM : static_cast<int>(st->dims);
+    const int kb = st->kb;
     const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile;
+    const uint64_t fvb = static_cast<uint64_t>(D) * bitlen32(st->rec_max);
+    const uint64_t fdb = static_cast<uint64_t>(D) * bitlen32(st->rec_maxdiff);
+    constexpr int KD = DIM ? DIM : kMaxDims;
+    constexpr int kG = 4;
     uint32_t cnt = 0;
-    if (f.l2 && D == 3 && ((reinterpret_cast<uintptr_t>(f.rec) | reinterpret_cast<uintptr_t>(choice2)) & 15) == 0) {
-        const uint64_t fvb = 3ull * bitlen32(st->rec_max);
-        const uint64_t fdb = 3ull * bitlen32(st->rec_maxdiff);
-        constexpr int kG = 4;
-        uint32_t v[kG][15];   // per group: the previous record, then four records
+    KT k[kG][5];   // per group: the previous key, then four keys
 #pragma unroll
-        for (int u = 0; u < kG; ++u) {
-            const uint64_t g = tile0 / 4 + u * 256 + threadIdx.x;
-            if (4 * g + 4 <= B) {
-                const uint4* q = reinterpret_cast<const uint4*>(f.rec + 12 * g);
-                const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
-                v[u][3] = a.x; v[u][4] = a.y; v[u][5] = a.z; v[u][6] = a.w; v[u][7] = b.x; v[u][8] = b.y;
-                v[u][9] = b.z; v[u][10] = b.w; v[u][11] = c.x; v[u][12] = c.y; v[u][13] = c.z; v[u][14] = c.w;
+    for (int u = 0; u < kG; ++u) {
+        const uint64_t g = tile0 / 4 + u * 256 + threadIdx.x;
+        const uint64_t j0 = 4 * g;
+        if (j0 + 4 <= B && sizeof(KT) == 4) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4*>(rec) + g);
+            k[u][1] = static_cast<KT>(v.x); k[u][2] = static_cast<KT>(v.y);
+            k[u][3] = static_cast<KT>(v.z); k[u][4] = static_cast<KT>(v.w);
+        } else {
 #pragma unroll
-                for (int d = 0; d < 3; ++d) v[u][d] = g ? __ldg(f.rec + 12 * g - 3 + d) : 0u;
+            for (int q = 0; q < 4; ++q) k[u][1 + q] = j0 + q < B ? __ldg(rec + j0 + q) : KT(0);
+        }
+        k[u][0] = j0 && j0 - 1 < B ? __ldg(rec + j0 - 1) : KT(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kG; ++u) {
+        const uint64_t g = tile0 / 4 + u * 256 + threadIdx.x;
+        const uint64_t j0 = 4 * g;
+        if (j0 >= B) continue;
+        uint32_t prev[KD], cur[KD];
+        rec_coords<DIM>(static_cast<uint64_t>(k[u][0]), D, kb, prev);
+        uint32_t ch[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint64_t j = j0 + q;
+            if (j >= B) break;
+            rec_coords<DIM>(static_cast<uint64_t>(k[u][1 + q]), D, kb, cur);
+            ch[q] = (l2 && j > 0) ? l2_rule(cur, prev, D, fvb, fdb) : 0u;
+            cnt += ch[q];
+#pragma unroll
+            for (int d = 0; d < KD; ++d) {
+                if (!DIM && d >= D) break;
+                prev[d] = cur[d];
             }
         }
-#pragma unroll
-        for (int u = 0; u < kG; ++u) {
-            const uint64_t g = tile0 / 4 + u * 256 + threadIdx.x;
-            if (4 * g + 4 <= B) {
-                uint32_t ch[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    uint32_t mv = 0, mdd = 0;
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        const uint32_t x = v[u][3 + 3 * k + d], w = v[u][3 * k + d];
-                        mv = x > mv ? x : mv;
-                        const uint32_t df = x >= w ? x - w : w - x;
-                        mdd = df > mdd ? df : mdd;
-                    }
-                    const int tvw = bitlen32(mv), tdw = bitlen32(mdd);
-                    const uint64_t tvb = 3ull * tvw + bitlen32(static_cast<uint32_t>(tvw));
-                    const uint64_t tdb = 3ull * tdw + bitlen32(static_cast<uint32_t>(tdw));
-                    const uint64_t value_bits = tvb < fvb ? tvb : fvb;
-                    const uint64_t diff_bits = tdb > fdb ? tdb : fdb;
-                    ch[k] = (4 * g + k == 0) ? 0u : (value_bits >= diff_bits ? 1u : 0u);
-                    cnt += ch[k];
-                }
-                *reinterpret_cast<uint4*>(choice2 + 4 * g) = make_uint4(ch[0], ch[1], ch[2], ch[3]);
-            } else {
-                for (uint64_t j = 4 * g; j < 4 * g + 4 && j < B; ++j) {
-                    const uint32_t c = f(j);
-                    choice2[j] = c;
-                    cnt += c;
-                }
-            }
-        }
-    } else {
-        for (int k = 0; k < kFlagTile / 256; ++k) {
-            const uint64_t j = tile0 + k * 256 + threadIdx.x;
-            if (j < B) {
-                const uint32_t c = f(j);
-                choice2[j] = c;
-                cnt += c;
-            }
+        if (j0 + 4 <= B && (reinterpret_cast<uintptr_t>(choice2) & 3) == 0) {
+            *reinterpret_cast<uint32_t*>(choice2 + j0) = ch[0] | (ch[1] << 8) | (ch[2] << 16) | (ch[3] << 24);
+        } else {
+            for (int q = 0; q < 4 && j0 + q < B; ++q) choice2[j0 + q] = static_cast<uint8_t>(ch[q]);
         }
     }
     cnt = warp_sum(cnt);
@@ -702,31 +721,44 @@ __global__ void __launch_bounds__(256) k_l2_choice(Level2In f, uint32_t* choice2
     }
 }
 struct Level2Flag {
-    const uint32_t* choice2;
+    const uint8_t* choice2;
     const EncState* st;
     __device__ bool operator()(uint64_t j) const { return j < st->B && choice2[j] != 0; }
 };
+// Writes record j as a kept row or as its ZigZag'd wrapped difference from the previous
+// record (lcps_cpp.cpp:1305-1454), ET bytes per value; DIM as for k_l2_choice.
+template <typename KT, typename ET, int DIM>
 struct Level2Out {
-    const uint32_t* rec;
+    const KT* rec;
     const EncState* st;
-    uint32_t* keep;
-    uint32_t* diff;
+    ET* keep;
+    ET* diff;
     __device__ void operator()(uint64_t j, uint32_t drank, uint32_t use_diff) const {
         if (j >= st->B) return;
-        const uint32_t D = st->dims;
+        const int D = DIM ? DIM : static_cast<int>(st->dims);
+        const int kb = st->kb;
+        constexpr int KD = DIM ? DIM : kMaxDims;
+        uint32_t cur[KD];
+        rec_coords<DIM>(static_cast<uint64_t>(rec[j]), D, kb, cur);
         if (!use_diff) {
             const uint64_t k = j - drank;
-            for (uint32_t d = 0; d < D; ++d) keep[k * D + d] = rec[j * D + d];
+#pragma unroll
+            for (int d = 0; d < KD; ++d)
+                if (DIM || d < D) keep[k * D + d] = static_cast<ET>(cur[d]);
             return;
         }
-        for (uint32_t d = 0; d < D; ++d) {
+        uint32_t prev[KD];
+        rec_coords<DIM>(static_cast<uint64_t>(rec[j - 1]), D, kb, prev);
+#pragma unroll
+        for (int d = 0; d < KD; ++d) {
+            if (!DIM && d >= D) break;
             // prediction = previous record (already inside [wrap_min, wrap_max])
-            int64_t corr = static_cast<int64_t>(rec[(j - 1) * D + d]) - static_cast<int64_t>(rec[j * D + d]);
+            int64_t corr = static_cast<int64_t>(prev[d]) - static_cast<int64_t>(cur[d]);
             if (corr < st->wrap_min_corr) corr += st->wrap_range;
             else if (corr > st->wrap_max_corr) corr -= st->wrap_range;
             const uint64_t zz = corr >= 0 ? static_cast<uint64_t>(corr) << 1
                                           : (static_cast<uint64_t>(-(corr + 1)) << 1) | 1u;
-            diff[static_cast<uint64_t>(drank) * D + d] = static_cast<uint32_t>(zz);
+            diff[static_cast<uint64_t>(drank) * D + d] = static_cast<ET>(zz);
         }
     }
 };
@@ -738,8 +770,9 @@ __global__ void k_l2_counts(EncState* st) {
 
 // ------------------------------------------------------------- stream stats
 struct StreamRef {
-    const uint32_t* data;   // record-major
+    const void* data;       // record-major, esz bytes per value
     uint32_t dims;
+    uint32_t esz;           // 1, 2 or 4
     const uint32_t* count_dev;  // records (device) or null -> count_const
     uint64_t count_const;
 };
@@ -844,17 +877,36 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     const uint64_t rounds = (ngroups + stride - 1) / stride;
     const bool vec_ok = (reinterpret_cast<uintptr_t>(r.data) & 15) == 0;
+    const uint32_t esz = r.esz;
     for (uint64_t rr = 0; rr < rounds; ++rr) {
         const uint64_t g = rr * stride + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
         if (g < ngroups) {
             const uint64_t rec0 = 4 * g;
             if (DIM && vec_ok && rec0 + 4 <= nrec) {
                 uint32_t v[4 * KD];
-                const uint4* p = reinterpret_cast<const uint4*>(r.data + rec0 * D);
+                if (esz == 4) {
+                    const uint4* p = reinterpret_cast<const uint4*>(static_cast<const uint32_t*>(r.data) + rec0 * D);
 #pragma unroll
-                for (int q = 0; q < KD; ++q) {
-                    const uint4 t = __ldg(p + q);
-                    v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+                    for (int q = 0; q < KD; ++q) {
+                        const uint4 t = __ldg(p + q);
+                        v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+                    }
+                } else if (esz == 2) {   // 8 KD bytes = 2 KD aligned words
+                    const uint32_t* p = reinterpret_cast<const uint32_t*>(static_cast<const uint16_t*>(r.data) + rec0 * D);
+#pragma unroll
+                    for (int q = 0; q < 2 * KD; ++q) {
+                        const uint32_t t = __ldg(p + q);
+                        v[2 * q] = t & 0xFFFFu;
+                        v[2 * q + 1] = t >> 16;
+                    }
+                } else {   // 4 KD bytes = KD aligned words
+                    const uint32_t* p = reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(r.data) + rec0 * D);
+#pragma unroll
+                    for (int q = 0; q < KD; ++q) {
+                        const uint32_t t = __ldg(p + q);
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) v[4 * q + b] = (t >> (8 * b)) & 0xFFu;
+                    }
                 }
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
@@ -868,7 +920,7 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
                     uint32_t tag = 1;
 #pragma unroll
                     for (int d = 0; d < KD; ++d)
-                        if (DIM || d < static_cast<int>(D)) value(r.data[rec * D + d], d, tag);
+                        if (DIM || d < static_cast<int>(D)) value(load_elem(r.data, rec * D + d, esz), d, tag);
                     record_done(tag);
                 }
             }
@@ -1047,7 +1099,8 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
 
 // ------------------------------------------------------------------ packing
 // Tags of a tagged component: max(1, max_d bitlen(v)) per record (lcps_cpp.cpp:1032-1046).
-__global__ void __launch_bounds__(256) k_tags(const uint32_t* __restrict__ data, uint32_t D, uint64_t nrec,
+template <typename ET>
+__global__ void __launch_bounds__(256) k_tags(const ET* __restrict__ data, uint32_t D, uint64_t nrec,
                                                uint32_t* __restrict__ tags) {
     for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nrec;
          j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
@@ -1077,8 +1130,9 @@ struct TagBitsIn {
     uint32_t D;
     __device__ uint64_t operator()(uint64_t j) const { return static_cast<uint64_t>(tags[j]) * D; }
 };
+template <typename ET>
 struct TagPackOut {
-    const uint32_t* data;
+    const ET* data;
     const uint32_t* tags;
     uint32_t D;
     uint32_t* words;
@@ -1100,7 +1154,8 @@ struct FixedPack {
     uint32_t width[kMaxDims];
 };
 constexpr int kPackWarps = 8;
-__global__ void __launch_bounds__(32 * kPackWarps, 3) k_pack_fixed(const uint32_t* __restrict__ data, uint32_t D,
+template <typename ET>
+__global__ void __launch_bounds__(32 * kPackWarps, 3) k_pack_fixed(const ET* __restrict__ data, uint32_t D,
                                                                  uint64_t nrec, FixedPack fp) {
     __shared__ uint32_t stage[kPackWarps][33 * 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1117,7 +1172,7 @@ __global__ void __launch_bounds__(32 * kPackWarps, 3) k_pack_fixed(const uint32_
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
                 const uint64_t k = r0 + 32 * j + lane;
-                x[j] = k < nrec ? __ldg(data + k * D + d) : mv;
+                x[j] = k < nrec ? static_cast<uint32_t>(__ldg(data + k * D + d)) : mv;
             }
 #pragma unroll
             for (int j = 0; j < 32; ++j) sw[33 * j + lane] = x[j] - mv;
@@ -1574,16 +1629,75 @@ static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, u
     }
 }
 
-template <typename FT, bool SOA, typename KT>
-static void launch_quantize(const void* pts, uint64_t n, uint32_t D, EncState* st, void* key, uint32_t* rel,
-                            uint64_t* cidx, double* cval, uint64_t cap, cudaStream_t s) {
+// hist: the first sort pass's count table (nullptr: no sort follows).
+template <typename FT, bool SOA, typename KT, typename RT>
+static void launch_quantize(const void* pts, uint64_t n, uint32_t D, EncState* st, void* key, void* rel,
+                            uint64_t* cidx, double* cval, uint64_t cap, uint32_t* hist, int hist_bits,
+                            cudaStream_t s) {
+    const uint32_t tiles = radix_tiles<KT>(n);
+    const unsigned grid = std::max(1u, tiles);
     if (D == 3)
-        k_quantize<FT, SOA, KT, 3><<<grid_for(n), 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st,
-                                                                static_cast<KT*>(key), rel, cidx, cval, cap);
+        k_quantize<FT, SOA, KT, 3, RT><<<grid, 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st,
+                                                            static_cast<KT*>(key), static_cast<RT*>(rel), cidx, cval,
+                                                            cap, hist, hist_bits, tiles);
     else
-        k_quantize<FT, SOA, KT, 0><<<grid_for(n), 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st,
-                                                                static_cast<KT*>(key), rel, cidx, cval, cap);
+        k_quantize<FT, SOA, KT, 0, RT><<<grid, 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st,
+                                                            static_cast<KT*>(key), static_cast<RT*>(rel), cidx, cval,
+                                                            cap, hist, hist_bits, tiles);
     count_launch();
+}
+
+// The quantizer for a run-time input type, layout, key width and offset width.
+template <typename FT, bool SOA>
+static void launch_quantize_rt(bool wide, uint32_t rel_esz, const void* pts, uint64_t n, uint32_t D, EncState* st,
+                               void* key, void* rel, uint64_t* cidx, double* cval, uint64_t cap, uint32_t* hist,
+                               int hist_bits, cudaStream_t s) {
+    if (wide) {
+        if (rel_esz == 1) launch_quantize<FT, SOA, uint64_t, uint8_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, s);
+        else launch_quantize<FT, SOA, uint64_t, uint32_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, s);
+    } else {
+        if (rel_esz == 1) launch_quantize<FT, SOA, uint32_t, uint8_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, s);
+        else launch_quantize<FT, SOA, uint32_t, uint32_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, s);
+    }
+}
+
+// Explicit records (keys of the points with idrel == 0, index order) and level 2: record
+// statistics, wrap parameters, choice2 with per-tile difference counts, and the keep /
+// diff rows (kd_esz bytes per value).
+template <typename KT>
+static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, uint64_t n, EncState* st, int l2, bool d3,
+                       uint32_t kd_esz, uint8_t* choice2, void* keep, void* diff, uint32_t* scan32, StageTimer& T,
+                       cudaStream_t stream) {
+    KT* rec = static_cast<KT*>(rec_v);
+    device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT>{key_idx, rec}, n, scan32, &st->B, stream);
+    T.mark("explicit_records", stream);
+    if (d3) {
+        k_l2_stats<KT, 3><<<grid_for((n + 3) / 4), 256, 0, stream>>>(rec, st); count_launch();
+    } else {
+        k_l2_stats<KT, 0><<<grid_for((n + 3) / 4), 256, 0, stream>>>(rec, st); count_launch();
+    }
+    k_l2_params<<<1, 1, 0, stream>>>(st); count_launch();
+    const unsigned tiles = static_cast<unsigned>(flag_tiles(n));
+    if (d3) {
+        k_l2_choice<KT, 3><<<tiles, 256, 0, stream>>>(rec, st, l2, choice2, scan32); count_launch();
+    } else {
+        k_l2_choice<KT, 0><<<tiles, 256, 0, stream>>>(rec, st, l2, choice2, scan32); count_launch();
+    }
+#define CHAIN_L2OUT(ET, DIM)                                                                            \
+    device_flag_scan_counted<Level2Flag, Level2Out<KT, ET, DIM>, kFlagItems>(                          \
+        Level2Flag{choice2, st}, Level2Out<KT, ET, DIM>{rec, st, static_cast<ET*>(keep), static_cast<ET*>(diff)}, \
+        n, scan32, &st->ndiff, stream)
+    if (d3) {
+        if (kd_esz == 1) CHAIN_L2OUT(uint8_t, 3);
+        else if (kd_esz == 2) CHAIN_L2OUT(uint16_t, 3);
+        else CHAIN_L2OUT(uint32_t, 3);
+    } else {
+        if (kd_esz == 1) CHAIN_L2OUT(uint8_t, 0);
+        else if (kd_esz == 2) CHAIN_L2OUT(uint16_t, 0);
+        else CHAIN_L2OUT(uint32_t, 0);
+    }
+#undef CHAIN_L2OUT
+    k_l2_counts<<<1, 1, 0, stream>>>(st); count_launch();
 }
 
 template <typename FT, bool SOA>
@@ -1592,13 +1706,19 @@ static void launch_minmax(const void* pts, uint64_t n, uint32_t D, EncState* st,
     k_minmax<FT, SOA><<<g, 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st); count_launch();
 }
 
-chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype, chain_layout layout, uint64_t n,
-                          uint32_t dims, double eb, int64_t p, int64_t threshold, int bl, int l1, int l2,
-                          uint32_t bytes_per_lane, uint32_t max_steps, size_t* out_len) {
+// One attempt at a frame with room for corr_cap exact corrections.  When the frame has
+// more, it returns CHAIN_ERR_OUT_OF_MEMORY with *corr_needed set to their count (the
+// caller retries with that capacity).
+static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_dtype dtype, chain_layout layout,
+                                     uint64_t n, uint32_t dims, double eb, int64_t p, int64_t threshold, int bl, int l1,
+                                     int l2, uint32_t bytes_per_lane, uint32_t max_steps, uint64_t corr_cap,
+                                     uint64_t* corr_needed, size_t* out_len) {
     cudaStream_t stream = ctx->stream;
     const size_t esz = dtype == CHAIN_F64 ? 8 : 4;
     const uint64_t nd = n * dims;
     const int64_t p_eff = bl ? p : 1;
+    // block offsets are < p: one byte each when p <= 256
+    const uint32_t rel_esz = p_eff <= 256 ? 1u : 4u;
     if (bytes_per_lane == 0) bytes_per_lane = 4096;
     if (max_steps == 0) max_steps = 1024;
 
@@ -1607,8 +1727,7 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     EncState* st = static_cast<EncState*>(ctx->state_dev);
     EncState* hs = static_cast<EncState*>(ctx->state_host);
 
-    // ---- frame arena (sizes known from n and dims)
-    const uint64_t corr_cap = std::min<uint64_t>(nd, 1ull << 20);
+    // ---- frame arena (sizes known from n, dims and the correction capacity)
     const uint64_t sort_counts = radix_counts_elems(std::max<uint64_t>(n, corr_cap));
     const uint64_t hist_stride = kRansMaxAlphabet;
     size_t need = 0;
@@ -1619,7 +1738,8 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     need += Arena::need(nsort, 4) * 2;                      // sort values ping-pong
     need += Arena::need(sort_counts, 4);
     need += Arena::need(scan_scratch_bytes(std::max<uint64_t>(sort_counts, nd)), 1);
-    need += Arena::need(nd, 4) * 4;           // rel, rec, keep, diff
+    need += Arena::need(nd, 4) * 3;           // rel, keep, diff
+    need += Arena::need(std::max<uint64_t>(nd * 4, n * 8), 1);   // record keys
     need += Arena::need(n, 4) * 2;            // idrel, choice2
     need += Arena::need(corr_cap, 8) * 4;     // corrections idx/val + sorted copies
     need += Arena::need(hist_stride * kCodeStreams, 4) * 3;  // hist, prob, cum
@@ -1644,12 +1764,12 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     uint32_t* val_b = A.take<uint32_t>(nsort);
     uint32_t* counts = A.take<uint32_t>(sort_counts);
     uint64_t* scanbuf = reinterpret_cast<uint64_t*>(A.take<uint8_t>(scan_scratch_bytes(std::max<uint64_t>(sort_counts, nd))));
-    uint32_t* rel = A.take<uint32_t>(nd);
-    uint32_t* rec = A.take<uint32_t>(nd);
-    uint32_t* keep = A.take<uint32_t>(nd);
-    uint32_t* diff = A.take<uint32_t>(nd);
+    void* rel = A.take<uint8_t>(nd * rel_esz);
+    void* rec = A.take<uint8_t>(std::max<uint64_t>(nd * 4, n * 8));   // record keys (KT each)
+    void* keep = A.take<uint32_t>(nd);
+    void* diff = A.take<uint32_t>(nd);
     uint32_t* idrel = A.take<uint32_t>(n);
-    uint32_t* choice2 = A.take<uint32_t>(n);
+    uint8_t* choice2 = A.take<uint8_t>(n);
     uint64_t* corr_idx = A.take<uint64_t>(corr_cap);
     double* corr_val = A.take<double>(corr_cap);
     uint64_t* corr_idx_s = A.take<uint64_t>(corr_cap);
@@ -1682,15 +1802,19 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     if (hs->err) return status_from_err(hs->err);
     const int key_bits = hs->key_bits;
     const bool wide = key_bits > 32;
+    // keep rows hold block coordinates (< 2^kb), diff rows ZigZag'd wrapped differences
+    // (<= the record range <= 2^kb): the narrowest width that holds kb + 1 bits
+    const uint32_t kd_esz = hs->kb + 1 <= 8 ? 1u : (hs->kb + 1 <= 16 ? 2u : 4u);
 
     // ---- phase 2: quantize, sort, level 1, level 2, statistics, plan
-#define CHAIN_Q(FT, SOA_, KT) launch_quantize<FT, SOA_, KT>(pts, n, dims, st, key_idx, rel, corr_idx, corr_val, corr_cap, stream)
+    // the quantizer counts the first sort pass's digits (when a sort follows)
+    const RadixPlan plan = radix_plan(key_bits);
+    uint32_t* hist0 = l1 ? counts : nullptr;
+#define CHAIN_Q(FT, SOA_) launch_quantize_rt<FT, SOA_>(wide, rel_esz, pts, n, dims, st, key_idx, rel, corr_idx, corr_val, corr_cap, hist0, plan.bits, stream)
     if (dtype == CHAIN_F32) {
-        if (soa) { if (wide) CHAIN_Q(float, true, uint64_t); else CHAIN_Q(float, true, uint32_t); }
-        else { if (wide) CHAIN_Q(float, false, uint64_t); else CHAIN_Q(float, false, uint32_t); }
+        if (soa) CHAIN_Q(float, true); else CHAIN_Q(float, false);
     } else {
-        if (soa) { if (wide) CHAIN_Q(double, true, uint64_t); else CHAIN_Q(double, true, uint32_t); }
-        else { if (wide) CHAIN_Q(double, false, uint64_t); else CHAIN_Q(double, false, uint32_t); }
+        if (soa) CHAIN_Q(double, true); else CHAIN_Q(double, false);
     }
 #undef CHAIN_Q
     CHAIN_LAUNCH_CHECK("quantize");
@@ -1704,15 +1828,15 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         };
         if (wide) {
             const bool in_b = radix_sort_pairs<uint64_t>(key_idx, key_a, val_a, key_b, val_b, n, key_bits, counts,
-                                                         reinterpret_cast<uint32_t*>(scanbuf), stream, sort_marks);
+                                                         stream, sort_marks, true);
             k_level1<uint64_t><<<grid_for(n), 256, 0, stream>>>(in_b ? key_b : key_a, in_b ? val_b : val_a, n, st, idrel,
                                                                hist); count_launch();
         } else {
             uint32_t* k32 = reinterpret_cast<uint32_t*>(key_idx);
             uint32_t* ka = reinterpret_cast<uint32_t*>(key_a);
             uint32_t* kb = reinterpret_cast<uint32_t*>(key_b);
-            const bool in_b = radix_sort_pairs<uint32_t>(k32, ka, val_a, kb, val_b, n, key_bits, counts,
-                                                         reinterpret_cast<uint32_t*>(scanbuf), stream, sort_marks);
+            const bool in_b = radix_sort_pairs<uint32_t>(k32, ka, val_a, kb, val_b, n, key_bits, counts, stream,
+                                                         sort_marks, true);
             k_level1<uint32_t><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel,
                                                                hist); count_launch();
         }
@@ -1722,33 +1846,25 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     CHAIN_LAUNCH_CHECK("level 1");
     T.mark("level1", stream);
     uint32_t* scan32 = reinterpret_cast<uint32_t*>(scanbuf);
+    const bool d3 = dims == 3 && hs->kb <= 21;
     if (wide)
-        device_flag_scan(ExplicitIn<uint64_t>{idrel}, ExplicitOut<uint64_t>{key_idx, st, rec}, n, scan32, &st->B,
-                         stream);
+        run_level2<uint64_t>(key_idx, idrel, rec, n, st, l2, d3, kd_esz, choice2, keep, diff, scan32, T, stream);
     else
-        device_flag_scan(ExplicitIn<uint32_t>{idrel},
-                         ExplicitOut<uint32_t>{reinterpret_cast<uint32_t*>(key_idx), st, rec}, n, scan32, &st->B,
-                         stream);
-    T.mark("explicit_records", stream);
-    k_l2_stats<<<grid_for(n), 256, 0, stream>>>(rec, st); count_launch();
-    k_l2_params<<<1, 1, 0, stream>>>(st); count_launch();
-    k_l2_choice<<<static_cast<unsigned>(flag_tiles(n)), 256, 0, stream>>>(Level2In{rec, st, l2}, choice2, scan32); count_launch();
-    device_flag_scan_counted<Level2Flag, Level2Out, kFlagItems>(Level2Flag{choice2, st}, Level2Out{rec, st, keep, diff},
-                                                                 n, scan32, &st->ndiff, stream);
-    k_l2_counts<<<1, 1, 0, stream>>>(st); count_launch();
+        run_level2<uint32_t>(reinterpret_cast<const uint32_t*>(key_idx), idrel, rec, n, st, l2, d3, kd_esz, choice2, keep,
+                             diff, scan32, T, stream);
     CHAIN_LAUNCH_CHECK("level 2");
     T.mark("level2", stream);
     // The level-2 scan covers n >= B entries; its functors ignore entries j >= B (read
     // from the device), so no host round trip is needed for B.
 
     StreamRefs refs;
-    refs.s[0] = StreamRef{idrel, 1, nullptr, n};
-    refs.s[1] = StreamRef{diff, dims, &st->ndiff, 0};
-    refs.s[2] = StreamRef{keep, dims, &st->nkeep, 0};
-    refs.s[3] = StreamRef{choice2, 1, &st->B, 0};
-    refs.s[4] = StreamRef{rel, dims, nullptr, n};
-    refs.s[kCorrGaps] = StreamRef{corr_gaps, 1, nullptr, 0};
-    refs.s[kCorrIds] = StreamRef{corr_ids, 1, nullptr, 0};
+    refs.s[0] = StreamRef{idrel, 1, 4, nullptr, n};
+    refs.s[1] = StreamRef{diff, dims, kd_esz, &st->ndiff, 0};
+    refs.s[2] = StreamRef{keep, dims, kd_esz, &st->nkeep, 0};
+    refs.s[3] = StreamRef{choice2, 1, 1, &st->B, 0};
+    refs.s[4] = StreamRef{rel, dims, rel_esz, nullptr, n};
+    refs.s[kCorrGaps] = StreamRef{corr_gaps, 1, 4, nullptr, 0};
+    refs.s[kCorrIds] = StreamRef{corr_ids, 1, 4, nullptr, 0};
     launch_stats(refs, st, hist, hist_stride, dims, n, 0, kStreams, stream);
     // per device, cheap; set on every call, always to the same value
     CHAIN_CUDA(cudaFuncSetAttribute(k_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1762,9 +1878,10 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     CHAIN_CUDA(cudaStreamSynchronize(stream));
     T.mark("sync2", stream);
     if (hs->err) return status_from_err(hs->err);
-    if (hs->ncorr > corr_cap)
-        return set_err(CHAIN_ERR_UNSUPPORTED, "more exact corrections than this build buffers (" +
-                                                  std::to_string(hs->ncorr) + ")");
+    if (hs->ncorr > corr_cap) {
+        *corr_needed = hs->ncorr;
+        return set_err(CHAIN_ERR_OUT_OF_MEMORY, "more exact corrections than buffered");
+    }
 
     // ---- exact corrections: increasing index order, then gaps + value-id streams
     if (hs->ncorr) {
@@ -1775,12 +1892,12 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
         uint32_t* scan32b = reinterpret_cast<uint32_t*>(scanbuf);
         // flat indices are unique, and equal values need no order for the dictionary,
         // so the small unstable sort serves both sorts here
-        bool in_b = sort_pairs<uint64_t>(corr_idx, key_a, val_a, key_b, val_b, nc, bits, counts, scan32b, stream);
+        bool in_b = sort_pairs<uint64_t>(corr_idx, key_a, val_a, key_b, val_b, nc, bits, counts, stream);
         k_gather_corrections<<<grid_for(nc), 256, 0, stream>>>(in_b ? val_b : val_a, in_b ? key_b : key_a, corr_val,
                                                                corr_idx_s, corr_val_s, nc); count_launch();
         k_corr_gaps<<<grid_for(nc), 256, 0, stream>>>(corr_idx_s, nc, corr_gaps); count_launch();
         const uint64_t* vbits = reinterpret_cast<const uint64_t*>(corr_val_s);
-        in_b = sort_pairs<uint64_t>(vbits, key_a, val_a, key_b, val_b, nc, 64, counts, scan32b, stream);
+        in_b = sort_pairs<uint64_t>(vbits, key_a, val_a, key_b, val_b, nc, 64, counts, stream);
         device_exclusive_scan<uint32_t>(DictIn{in_b ? key_b : key_a},
                                         DictOut{in_b ? key_b : key_a, in_b ? val_b : val_a, corr_dict, corr_ids}, nc,
                                         scan32b, &st->ndistinct, stream);
@@ -1886,26 +2003,51 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
                 fp.width[d] = c.width[d];
             }
             const uint64_t tiles = (c.records + 1023) / 1024;
-            k_pack_fixed<<<grid_for(tiles, kPackWarps, 148u * 16u), 32 * kPackWarps, 0, stream>>>(r.data, c.dims,
-                                                                                                 c.records, fp); count_launch();
+            const unsigned pg = grid_for(tiles, kPackWarps, 148u * 16u);
+            if (r.esz == 1)
+                k_pack_fixed<uint8_t><<<pg, 32 * kPackWarps, 0, stream>>>(static_cast<const uint8_t*>(r.data), c.dims,
+                                                                         c.records, fp);
+            else if (r.esz == 2)
+                k_pack_fixed<uint16_t><<<pg, 32 * kPackWarps, 0, stream>>>(static_cast<const uint16_t*>(r.data),
+                                                                          c.dims, c.records, fp);
+            else
+                k_pack_fixed<uint32_t><<<pg, 32 * kPackWarps, 0, stream>>>(static_cast<const uint32_t*>(r.data),
+                                                                          c.dims, c.records, fp);
+            count_launch();
             ain.packed[s] = packed + packed_off[s];
             ain.packed_dim_stride[s] = packed_stride[s];
         }
-        const uint32_t* symbols = r.data;
+        const void* symbols = r.data;
+        uint32_t sym_esz = r.esz;
         if (c.enc == kEncTagged) {
             uint32_t* tg = tags + tags_off[s];
-            k_tags<<<grid_for(c.records), 256, 0, stream>>>(r.data, c.dims, c.records, tg); count_launch();
             uint32_t* words = reinterpret_cast<uint32_t*>(packed + packed_off[s]);
-            device_exclusive_scan<uint64_t>(TagBitsIn{tg, c.dims}, TagPackOut{r.data, tg, c.dims, words}, c.records,
-                                            scanbuf, static_cast<uint64_t*>(nullptr), stream);
+            if (r.esz == 1) {
+                const uint8_t* d8 = static_cast<const uint8_t*>(r.data);
+                k_tags<uint8_t><<<grid_for(c.records), 256, 0, stream>>>(d8, c.dims, c.records, tg); count_launch();
+                device_exclusive_scan<uint64_t>(TagBitsIn{tg, c.dims}, TagPackOut<uint8_t>{d8, tg, c.dims, words},
+                                                c.records, scanbuf, static_cast<uint64_t*>(nullptr), stream);
+            } else if (r.esz == 2) {
+                const uint16_t* d16 = static_cast<const uint16_t*>(r.data);
+                k_tags<uint16_t><<<grid_for(c.records), 256, 0, stream>>>(d16, c.dims, c.records, tg); count_launch();
+                device_exclusive_scan<uint64_t>(TagBitsIn{tg, c.dims}, TagPackOut<uint16_t>{d16, tg, c.dims, words},
+                                                c.records, scanbuf, static_cast<uint64_t*>(nullptr), stream);
+            } else {
+                const uint32_t* d32 = static_cast<const uint32_t*>(r.data);
+                k_tags<uint32_t><<<grid_for(c.records), 256, 0, stream>>>(d32, c.dims, c.records, tg); count_launch();
+                device_exclusive_scan<uint64_t>(TagBitsIn{tg, c.dims}, TagPackOut<uint32_t>{d32, tg, c.dims, words},
+                                                c.records, scanbuf, static_cast<uint64_t*>(nullptr), stream);
+            }
             const uint64_t nwords = (c.packed_bits + 31) / 32;
             k_words_to_bytes<<<grid_for(nwords), 256, 0, stream>>>(words, nwords); count_launch();
             ain.packed[s] = packed + packed_off[s];
             symbols = tg;
+            sym_esz = 4;
         }
         if (c.enc == kEncRaw || c.enc == kEncTagged) {
             RansJob& jb = jobs.job[jobs.njobs++];
             jb.sym = symbols;
+            jb.sym_esz = sym_esz;
             jb.count = c.sec_count;
             jb.prob = c.enc == kEncRaw ? prob + hist_stride * s : tag_prob + 64 * s;
             jb.cum = c.enc == kEncRaw ? cum + hist_stride * s : tag_cum + 64 * s;
@@ -1983,9 +2125,30 @@ chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype,
     if (hs->total_bytes > bound) return set_err(CHAIN_ERR_DEVICE, "container exceeds its bound");
     ctx->result = container;
     ctx->result_len = hs->total_bytes;
-    ctx->dbg = EncodeDebug{idrel, diff, keep, choice2, rel, n, hs->ndiff, hs->nkeep, hs->B, dims};
+    ctx->dbg = EncodeDebug{idrel, diff, keep, kd_esz, choice2, rel, rel_esz, n, hs->ndiff, hs->nkeep, hs->B, dims};
     *out_len = hs->total_bytes;
     return CHAIN_OK;
+}
+
+// Encodes a frame.  Exact corrections are buffered for up to min(n * dims, 2^20) values
+// on the first attempt; a frame with more (clipped or tightly bounded data) is encoded
+// again with room for exactly as many as the first attempt counted.
+chain_status encode_frame(chain_ctx* ctx, const void* points, chain_dtype dtype, chain_layout layout, uint64_t n,
+                          uint32_t dims, double eb, int64_t p, int64_t threshold, int bl, int l1, int l2,
+                          uint32_t bytes_per_lane, uint32_t max_steps, size_t* out_len) {
+    uint64_t cap = std::min<uint64_t>(n * dims, 1ull << 20);
+    uint64_t needed = 0;
+    chain_status s = encode_frame_cap(ctx, points, dtype, layout, n, dims, eb, p, threshold, bl, l1, l2, bytes_per_lane,
+                                      max_steps, cap, &needed, out_len);
+    if (s == CHAIN_ERR_OUT_OF_MEMORY && needed > cap) {
+        cap = needed;
+        needed = 0;
+        s = encode_frame_cap(ctx, points, dtype, layout, n, dims, eb, p, threshold, bl, l1, l2, bytes_per_lane,
+                             max_steps, cap, &needed, out_len);
+        if (s == CHAIN_ERR_OUT_OF_MEMORY && needed > cap)
+            return set_err(CHAIN_ERR_DEVICE, "internal: exact-correction count changed between two passes");
+    }
+    return s;
 }
 
 }  // namespace chain

@@ -5,13 +5,16 @@
 // "the next point of the same block" is the sorted neighbour (lcps_cpp.cpp:2116-2138
 // computes the same relation with a hash map).
 //
-// Each 8-bit pass is three launches: a per-tile digit histogram, a device-wide
-// exclusive scan of the digit-major count table, and a stable scatter.  The scatter
-// loads its whole tile at once (indices wait in shared memory in input order), ranks
-// keys with 8 ballots per 32 keys (each warp owns a contiguous slice, processed 32 keys
-// per round in order, so equal digits keep their input order), reorders the tile by
-// digit in shared memory, and writes each digit's run to its global position with
-// consecutive threads on consecutive addresses.
+// The key bits are split into ceil(key_bits / 8) passes of equal digit width (at most 8
+// bits: a 21-bit key takes three 7-bit passes).  Each pass is three launches: a per-tile
+// digit histogram (for the first pass the caller may have produced it already, as the
+// quantizer does), a per-digit scan of that digit's row of tile counts (one CTA per
+// digit; the rows' totals are scanned by each scatter CTA itself), and a stable scatter.
+// The scatter loads its whole tile at once (indices wait in shared memory in input
+// order), ranks keys with one ballot per digit bit per 32 keys (each warp owns a
+// contiguous slice, processed 32 keys per round in order, so equal digits keep their
+// input order), reorders the tile by digit in shared memory, and writes each digit's run
+// to its global position with consecutive threads on consecutive addresses.
 #pragma once
 
 #include "chain_common.cuh"
@@ -21,7 +24,8 @@ namespace chain {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortBins = 256;
+constexpr int kSortBins = 256;      // bins of the widest (8-bit) digit
+constexpr int kSortMaxBits = 8;
 
 template <typename KT>
 struct SortShape {
@@ -29,12 +33,27 @@ struct SortShape {
     static constexpr int kTile = kSortThreads * kItems;
 };
 
+// Passes and digit width for a key of key_bits bits: as few passes of at most 8 bits
+// as cover it, all of the same width (at least one pass: it yields the identity).
+struct RadixPlan {
+    int passes;
+    int bits;
+};
+inline RadixPlan radix_plan(int key_bits) {
+    RadixPlan r;
+    r.passes = key_bits <= 0 ? 1 : (key_bits + kSortMaxBits - 1) / kSortMaxBits;
+    r.bits = key_bits <= 0 ? 1 : (key_bits + r.passes - 1) / r.passes;
+    return r;
+}
+
+// Per-tile histogram of digit (key >> shift) & (2^bits - 1) into counts[d * tiles + t].
 template <typename KT>
 __global__ void __launch_bounds__(kSortThreads)
-radix_hist_kernel(const KT* __restrict__ keys, uint64_t n, int shift, uint32_t* __restrict__ counts,
+radix_hist_kernel(const KT* __restrict__ keys, uint64_t n, int shift, int bits, uint32_t* __restrict__ counts,
                   uint32_t num_tiles) {
     constexpr int I = SortShape<KT>::kItems, TILE = SortShape<KT>::kTile;
     __shared__ uint32_t hist[kSortBins];
+    const uint32_t bins = 1u << bits, mask = bins - 1;
     hist[threadIdx.x] = 0;
     __syncthreads();
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * TILE;
@@ -49,9 +68,38 @@ radix_hist_kernel(const KT* __restrict__ keys, uint64_t n, int shift, uint32_t* 
 #pragma unroll
     for (int r = 0; r < I; ++r)
         if (static_cast<uint32_t>(r * kSortThreads + threadIdx.x) < rem)
-            atomicAdd(&hist[static_cast<uint32_t>(k[r] >> shift) & 0xFFu], 1u);
+            atomicAdd(&hist[static_cast<uint32_t>(k[r] >> shift) & mask], 1u);
     __syncthreads();
-    counts[static_cast<uint64_t>(threadIdx.x) * num_tiles + blockIdx.x] = hist[threadIdx.x];
+    if (threadIdx.x < bins) counts[static_cast<uint64_t>(threadIdx.x) * num_tiles + blockIdx.x] = hist[threadIdx.x];
+}
+
+// One CTA per digit: exclusive scan, in place, of the digit's row of tile counts
+// (counts[d * tiles .. d * tiles + tiles)); the row's total goes to row_total[d].
+__global__ void __launch_bounds__(kSortThreads)
+radix_rowscan_kernel(uint32_t* __restrict__ counts, uint32_t num_tiles, uint32_t* __restrict__ row_total) {
+    constexpr int kPer = 8;   // consecutive tiles per thread per round
+    __shared__ uint32_t scratch[33];
+    uint32_t* row = counts + static_cast<uint64_t>(blockIdx.x) * num_tiles;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < num_tiles; base += kSortThreads * kPer) {
+        const uint32_t t0 = base + threadIdx.x * kPer;
+        uint32_t v[kPer];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            v[k] = t0 + k < num_tiles ? row[t0 + k] : 0u;
+            sum += v[k];
+        }
+        uint32_t tot;
+        uint32_t ex = carry + block_exclusive_sum(sum, scratch, &tot);
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            if (t0 + k < num_tiles) row[t0 + k] = ex;
+            ex += v[k];
+        }
+        carry += tot;
+    }
+    if (threadIdx.x == 0) row_total[blockIdx.x] = carry;
 }
 
 // Shared-memory staging of a tile's reordered pairs: one 8-byte word per pair for
@@ -76,17 +124,22 @@ struct ScatterStage<uint32_t> {
 
 // Four CTAs per SM (63 registers, <= 46 KB of shared memory): the ranking loop is
 // latency-bound, so resident warps matter more than registers.
-template <typename KT>
+// offsets: the tile's row-exclusive prefix per digit (counts[d * tiles + t] after
+// radix_rowscan_kernel); row_total: each digit's count over all tiles.
+template <typename KT, int BITS>
 __global__ void __launch_bounds__(kSortThreads, 4)
 radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                      KT* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint64_t n, int shift,
-                     const uint32_t* __restrict__ offsets, uint32_t num_tiles) {
+                     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ row_total,
+                     uint32_t num_tiles) {
     constexpr int I = SortShape<KT>::kItems;
+    constexpr int bits = BITS;
     __shared__ uint32_t whist[kSortWarps][kSortBins];
     __shared__ int32_t delta[kSortBins];         // global position - tile-local position, per digit
-    __shared__ uint32_t scratch[33];
+    __shared__ uint64_t scratch[33];
     __shared__ ScatterStage<KT> stage;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t bins = 1u << bits, mask = bins - 1;
     for (int t = threadIdx.x; t < kSortWarps * kSortBins; t += kSortThreads) (&whist[0][0])[t] = 0;
     __syncthreads();
     const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * SortShape<KT>::kTile;
@@ -118,10 +171,10 @@ radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict_
 #pragma unroll
     for (int r = 0; r < I; ++r) {
         const bool valid = static_cast<uint32_t>(r * 32 + lane) < rem;
-        const uint32_t digit = static_cast<uint32_t>(key[r] >> shift) & 0xFFu;
+        const uint32_t digit = static_cast<uint32_t>(key[r] >> shift) & mask;
         uint32_t peers = __ballot_sync(0xffffffffu, valid);
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
+        for (int b = 0; b < BITS; ++b) {
             const bool bit = (digit >> b) & 1u;
             const uint32_t bal = __ballot_sync(0xffffffffu, bit);
             peers &= bit ? bal : ~bal;
@@ -134,14 +187,20 @@ radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict_
     }
     __syncthreads();
     {
-        // per digit: tile count, then per-warp offsets inside the tile
+        // per digit: tile count, then per-warp offsets inside the tile; one scan gives
+        // both the digit's start inside the tile (low word: the tile's counts) and its
+        // start in the output (high word: the digits' totals over all tiles)
         const int d = threadIdx.x;
         uint32_t cnt = 0;
 #pragma unroll
         for (int w = 0; w < kSortWarps; ++w) cnt += whist[w][d];
-        uint32_t tot;
-        const uint32_t start = block_exclusive_sum(cnt, scratch, &tot);
-        delta[d] = static_cast<int32_t>(offsets[static_cast<uint64_t>(d) * num_tiles + blockIdx.x] - start);
+        const uint64_t total = static_cast<uint32_t>(d) < bins ? __ldg(row_total + d) : 0u;
+        const uint64_t ex = block_exclusive_sum((total << 32) | cnt, scratch, static_cast<uint64_t*>(nullptr));
+        const uint32_t start = static_cast<uint32_t>(ex);
+        const uint32_t digit_base = static_cast<uint32_t>(ex >> 32);
+        if (static_cast<uint32_t>(d) < bins)
+            delta[d] = static_cast<int32_t>(digit_base + offsets[static_cast<uint64_t>(d) * num_tiles + blockIdx.x] -
+                                            start);
         uint32_t run = start;
 #pragma unroll
         for (int w = 0; w < kSortWarps; ++w) {
@@ -162,29 +221,46 @@ radix_scatter_kernel(const KT* __restrict__ keys_in, const uint32_t* __restrict_
         KT k;
         uint32_t v;
         stage.get(j, k, v);
-        const uint32_t digit = static_cast<uint32_t>(k >> shift) & 0xFFu;
+        const uint32_t digit = static_cast<uint32_t>(k >> shift) & mask;
         const uint32_t pos = static_cast<uint32_t>(delta[digit] + static_cast<int32_t>(j));
         keys_out[pos] = k;
         vals_out[pos] = v;
     }
 }
 
-struct CountIn {
-    const uint32_t* c;
-    __device__ uint32_t operator()(uint64_t i) const { return c[i]; }
-};
-struct CountOut {
-    uint32_t* c;
-    __device__ void operator()(uint64_t i, uint32_t prefix, uint32_t) const { c[i] = prefix; }
-};
-
 template <typename KT>
 inline uint32_t radix_tiles(uint64_t n) {
     return static_cast<uint32_t>((n + SortShape<KT>::kTile - 1) / SortShape<KT>::kTile);
 }
 
-// Count-table entries radix_sort_pairs needs for n keys of either key width.
-inline size_t radix_counts_elems(uint64_t n) { return static_cast<size_t>(radix_tiles<uint64_t>(n)) * kSortBins; }
+// Count-table entries radix_sort_pairs needs for n keys of either key width (the digit
+// rows, then the rows' totals).
+inline size_t radix_counts_elems(uint64_t n) {
+    return static_cast<size_t>(radix_tiles<uint32_t>(n) + radix_tiles<uint64_t>(n)) * kSortBins + kSortBins;
+}
+
+// The scatter for a run-time digit width (instantiated per width, so that the ranking
+// loop is fully unrolled).
+template <typename KT>
+inline void launch_radix_scatter(int bits, uint32_t tiles, cudaStream_t stream, const KT* kin, const uint32_t* vin,
+                                 KT* kout, uint32_t* vout, uint64_t n, int shift, const uint32_t* counts,
+                                 const uint32_t* row_total) {
+#define CHAIN_SCATTER(B)                                                                                          \
+    radix_scatter_kernel<KT, B><<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, shift, counts, row_total, \
+                                                                    tiles)
+    switch (bits) {
+        case 1: CHAIN_SCATTER(1); break;
+        case 2: CHAIN_SCATTER(2); break;
+        case 3: CHAIN_SCATTER(3); break;
+        case 4: CHAIN_SCATTER(4); break;
+        case 5: CHAIN_SCATTER(5); break;
+        case 6: CHAIN_SCATTER(6); break;
+        case 7: CHAIN_SCATTER(7); break;
+        default: CHAIN_SCATTER(8); break;
+    }
+#undef CHAIN_SCATTER
+    count_launch();
+}
 
 struct NoSortHook {
     void operator()(bool /*after_scatter*/) const {}
@@ -192,31 +268,32 @@ struct NoSortHook {
 
 // Sorts keys_in (values implicitly 0..n-1) by bits [0, key_bits), stably.  Ping-pongs
 // between (keys_a, vals_a) and (keys_b, vals_b); keys_in is only read.  Returns true
-// when the result is in the *_b buffers.  counts: radix_counts_elems(n) u32;
-// scan_buf: scan_scratch_bytes(counts) bytes.  hook(false) runs before each pass's
-// scatter launch and hook(true) after it (stage timing).
+// when the result is in the *_b buffers.  counts: radix_counts_elems(n) u32.  When
+// first_counts_ready, counts already holds the first pass's per-tile histogram (digit
+// rows of radix_tiles<KT>(n) tiles, digit width radix_plan(key_bits).bits).  hook(false)
+// runs before each pass's scatter launch and hook(true) after it (stage timing).
 template <typename KT, typename Hook = NoSortHook>
 bool radix_sort_pairs(const KT* keys_in, KT* keys_a, uint32_t* vals_a, KT* keys_b, uint32_t* vals_b, uint64_t n,
-                      int key_bits, uint32_t* counts, uint32_t* scan_buf, cudaStream_t stream,
-                      const Hook& hook = Hook()) {
+                      int key_bits, uint32_t* counts, cudaStream_t stream, const Hook& hook = Hook(),
+                      bool first_counts_ready = false) {
     const uint32_t tiles = radix_tiles<KT>(n);
-    int passes = (key_bits + 7) / 8;
-    if (passes == 0) passes = 1;  // one pass produces the identity permutation
-    for (int p = 0; p < passes; ++p) {
-        const int shift = 8 * p;
+    const RadixPlan plan = radix_plan(key_bits);
+    uint32_t* row_total = counts + static_cast<size_t>(tiles) * kSortBins;
+    for (int p = 0; p < plan.passes; ++p) {
+        const int shift = plan.bits * p;
         const KT* kin = p == 0 ? keys_in : (p % 2 == 1 ? keys_a : keys_b);
         const uint32_t* vin = p == 0 ? nullptr : (p % 2 == 1 ? vals_a : vals_b);
         KT* kout = p % 2 == 0 ? keys_a : keys_b;
         uint32_t* vout = p % 2 == 0 ? vals_a : vals_b;
-        radix_hist_kernel<KT><<<tiles, kSortThreads, 0, stream>>>(kin, n, shift, counts, tiles); count_launch();
-        const uint64_t ncounts = static_cast<uint64_t>(tiles) * kSortBins;
-        device_exclusive_scan<uint32_t>(CountIn{counts}, CountOut{counts}, ncounts, scan_buf,
-                                        static_cast<uint32_t*>(nullptr), stream);
+        if (p > 0 || !first_counts_ready) {
+            radix_hist_kernel<KT><<<tiles, kSortThreads, 0, stream>>>(kin, n, shift, plan.bits, counts, tiles); count_launch();
+        }
+        radix_rowscan_kernel<<<1u << plan.bits, kSortThreads, 0, stream>>>(counts, tiles, row_total); count_launch();
         hook(false);
-        radix_scatter_kernel<KT><<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, shift, counts, tiles); count_launch();
+        launch_radix_scatter<KT>(plan.bits, tiles, stream, kin, vin, kout, vout, n, shift, counts, row_total);
         hook(true);
     }
-    return passes % 2 == 0;
+    return plan.passes % 2 == 0;
 }
 
 // ------------------------------------------------------------- small sorts
@@ -265,12 +342,12 @@ __global__ void __launch_bounds__(1024) small_sort_kernel(const KT* __restrict__
 // (not stable; the result is then in the *_a buffers).
 template <typename KT>
 bool sort_pairs(const KT* keys_in, KT* keys_a, uint32_t* vals_a, KT* keys_b, uint32_t* vals_b, uint64_t n,
-                int key_bits, uint32_t* counts, uint32_t* scan_buf, cudaStream_t stream) {
+                int key_bits, uint32_t* counts, cudaStream_t stream) {
     if (n <= kSmallSort) {
         small_sort_kernel<KT><<<1, 1024, 0, stream>>>(keys_in, keys_a, vals_a, static_cast<uint32_t>(n)); count_launch();
         return false;
     }
-    return radix_sort_pairs<KT>(keys_in, keys_a, vals_a, keys_b, vals_b, n, key_bits, counts, scan_buf, stream);
+    return radix_sort_pairs<KT>(keys_in, keys_a, vals_a, keys_b, vals_b, n, key_bits, counts, stream);
 }
 
 }  // namespace chain

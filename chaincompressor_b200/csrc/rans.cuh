@@ -621,7 +621,7 @@ __device__ __forceinline__ uint4 make_enc_symbol(uint32_t freq, uint32_t cum, ui
 
 struct RansJob {
     const uint4* etab;        // encode: symbol entries [A] (make_enc_symbol)
-    const uint32_t* sym;      // encode: symbols
+    const void* sym;          // encode: symbols, sym_esz bytes each (1, 2 or 4)
     uint32_t* out;            // decode: symbol output
     uint64_t count;           // symbols
     const uint32_t* prob;     // [A]
@@ -633,7 +633,7 @@ struct RansJob {
     uint32_t chunks;
     uint32_t lanes;           // interleaved states per chunk (1..32)
     uint32_t first_block;     // first CTA of this job (kRansEncWarps / kRansDecWarps chunks per CTA)
-    uint32_t pad;
+    uint32_t sym_esz;         // encode: bytes per symbol (1, 2 or 4)
     uint64_t S;               // symbols per chunk (multiple of 32)
     uint8_t* bytes;           // encode: chunk slots (slot_cap each); decode: container
     uint64_t bytes_len;       // decode: container length (staged loads stay inside it)
@@ -766,12 +766,67 @@ __device__ __forceinline__ int job_of_block(const RansJobs& J) {
     return j;
 }
 
-// Loads symbols [tb, te) (a tile of up to 1024) into regs; full tiles use 16-byte loads.
-__device__ __forceinline__ void tile_load(const uint32_t* sym, uint64_t tb, uint64_t te, uint32_t (&r)[32],
-                                          bool& vec) {
+// Register layouts of a loaded symbol tile (tile_load -> tile_store).
+enum TileLayout : int {
+    kTileScalar = 0,   // r[i]      = symbol tb + lane + 32 i
+    kTileVec4 = 1,     // r[4i + k] = symbol tb + 4 (lane + 32 i) + k
+    kTileVec16 = 2,    // r[16i + k] = symbol tb + 16 (lane + 32 i) + k
+    kTileVec8 = 3,     // r[8i + k]  = symbol tb + 8 (lane + 32 i) + k
+};
+
+// Loads symbols [tb, te) (a tile of up to 1024) of esz bytes each into regs; full,
+// aligned tiles use 16-byte loads.
+__device__ __forceinline__ void tile_load(const void* sym_v, uint32_t esz, uint64_t tb, uint64_t te,
+                                          uint32_t (&r)[32], int& layout) {
     const int lane = threadIdx.x & 31;
-    vec = (te - tb == 1024) && ((reinterpret_cast<uintptr_t>(sym + tb) & 15) == 0);
-    if (vec) {
+    const bool full = te - tb == 1024;
+    if (esz == 1) {
+        const uint8_t* sym = static_cast<const uint8_t*>(sym_v);
+        if (full && (reinterpret_cast<uintptr_t>(sym + tb) & 15) == 0) {
+            layout = kTileVec16;
+            const uint4* p = reinterpret_cast<const uint4*>(sym + tb);
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const uint4 v = __ldg(p + lane + 32 * i);
+                const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int k = 0; k < 16; ++k) r[16 * i + k] = (w[k >> 2] >> (8 * (k & 3))) & 0xFFu;
+            }
+        } else {
+            layout = kTileScalar;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const uint64_t k = tb + lane + 32 * i;
+                r[i] = k < te ? static_cast<uint32_t>(__ldg(sym + k)) : 0u;
+            }
+        }
+        return;
+    }
+    if (esz == 2) {
+        const uint16_t* sym = static_cast<const uint16_t*>(sym_v);
+        if (full && (reinterpret_cast<uintptr_t>(sym + tb) & 15) == 0) {
+            layout = kTileVec8;
+            const uint4* p = reinterpret_cast<const uint4*>(sym + tb);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const uint4 v = __ldg(p + lane + 32 * i);
+                const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int k = 0; k < 8; ++k) r[8 * i + k] = (w[k >> 1] >> (16 * (k & 1))) & 0xFFFFu;
+            }
+        } else {
+            layout = kTileScalar;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const uint64_t k = tb + lane + 32 * i;
+                r[i] = k < te ? static_cast<uint32_t>(__ldg(sym + k)) : 0u;
+            }
+        }
+        return;
+    }
+    const uint32_t* sym = static_cast<const uint32_t*>(sym_v);
+    if (full && (reinterpret_cast<uintptr_t>(sym + tb) & 15) == 0) {
+        layout = kTileVec4;
         const uint4* p = reinterpret_cast<const uint4*>(sym + tb);
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -779,6 +834,7 @@ __device__ __forceinline__ void tile_load(const uint32_t* sym, uint64_t tb, uint
             r[4 * i] = v.x; r[4 * i + 1] = v.y; r[4 * i + 2] = v.z; r[4 * i + 3] = v.w;
         }
     } else {
+        layout = kTileScalar;
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
             const uint64_t k = tb + lane + 32 * i;
@@ -786,12 +842,29 @@ __device__ __forceinline__ void tile_load(const uint32_t* sym, uint64_t tb, uint
         }
     }
 }
-__device__ __forceinline__ void tile_store(uint32_t* buf, const uint32_t (&r)[32], bool vec) {
+// Stores a loaded tile to buf in symbol order (buf[j] = symbol tb + j).
+__device__ __forceinline__ void tile_store(uint32_t* buf, const uint32_t (&r)[32], int layout) {
     const int lane = threadIdx.x & 31;
-    if (vec) {
+    if (layout == kTileVec4) {
         uint4* p = reinterpret_cast<uint4*>(buf);
 #pragma unroll
         for (int i = 0; i < 8; ++i) p[lane + 32 * i] = make_uint4(r[4 * i], r[4 * i + 1], r[4 * i + 2], r[4 * i + 3]);
+    } else if (layout == kTileVec8) {
+        uint4* p = reinterpret_cast<uint4*>(buf);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+                p[2 * (lane + 32 * i) + q] =
+                    make_uint4(r[8 * i + 4 * q], r[8 * i + 4 * q + 1], r[8 * i + 4 * q + 2], r[8 * i + 4 * q + 3]);
+    } else if (layout == kTileVec16) {
+        uint4* p = reinterpret_cast<uint4*>(buf);
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                p[4 * (lane + 32 * i) + q] =
+                    make_uint4(r[16 * i + 4 * q], r[16 * i + 4 * q + 1], r[16 * i + 4 * q + 2], r[16 * i + 4 * q + 3]);
     } else {
 #pragma unroll
         for (int i = 0; i < 32; ++i) buf[lane + 32 * i] = r[i];
@@ -886,17 +959,17 @@ static __global__ void __launch_bounds__(32 * kRansEncWarps) rans_encode_kernel(
     uint32_t rel = kWindow;                               // window index of the lowest byte written
     bool overflow = false;
     uint32_t r[32];
-    bool vec;
+    int layout;
     {
         const uint64_t tb = cbeg + tile_syms * (ntiles - 1);
-        tile_load(jb.sym, tb, min(tb + tile_syms, cend), r, vec);
-        tile_store(buf + ((ntiles - 1) & 1) * 1024, r, vec);
+        tile_load(jb.sym, jb.sym_esz, tb, min(tb + tile_syms, cend), r, layout);
+        tile_store(buf + ((ntiles - 1) & 1) * 1024, r, layout);
         __syncwarp();
     }
     for (int k = static_cast<int>(ntiles) - 1; k >= 0; --k) {
         if (k > 0) {
             const uint64_t tb = cbeg + tile_syms * (k - 1);
-            tile_load(jb.sym, tb, min(tb + tile_syms, cend), r, vec);
+            tile_load(jb.sym, jb.sym_esz, tb, min(tb + tile_syms, cend), r, layout);
         }
         if (rel < kGroupBytes) {   // flush the aligned part of the window
             const uint32_t a = (rel + 15) & ~15u;
@@ -935,7 +1008,7 @@ static __global__ void __launch_bounds__(32 * kRansEncWarps) rans_encode_kernel(
         }
         if (k > 0) {
             __syncwarp();
-            tile_store(buf + ((k - 1) & 1) * 1024, r, vec);
+            tile_store(buf + ((k - 1) & 1) * 1024, r, layout);
             __syncwarp();
         }
     }
