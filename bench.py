@@ -55,12 +55,16 @@ def _peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def _frame(config: str, rank: int):
+def _frame(config: str, rank: int, n: int = 0):
+    """(points, eb, p, threshold, workload name); n > 0 overrides the blobs frame's size
+    (smaller profiling cases of the same distribution)."""
     from chaincompressor_b200 import workloads as W
 
     if config == "blobs":
-        pts = W.blobs(W.BLOBS_N, seed=1 + rank)
-        return pts, W.eb_for(pts, 1e-3), 4, 2, "blobs-16M-f32 (64 Gaussian blobs + 20% uniform, random order)"
+        size = n or W.BLOBS_N
+        pts = W.blobs(size, seed=1 + rank)
+        name = "blobs-16M-f32" if size == W.BLOBS_N else f"blobs-{size}-f32"
+        return pts, W.eb_for(pts, 1e-3), 4, 2, name + " (64 Gaussian blobs + 20% uniform, random order)"
     if config == "column":
         pts = W.column(seed=rank)
         return pts, W.eb_for(pts, 1e-3), 4, 2, "column-80703-f32 (dam-break-like lattice, random order)"
@@ -159,7 +163,7 @@ def run_ours(args, rank: int, world: int):
     ndev = max(1, torch.cuda.device_count())
     dev = int(os.environ.get("LOCAL_RANK", rank)) % ndev
     torch.cuda.set_device(dev)
-    pts, eb, p, t, wl = _frame(args.config, rank)
+    pts, eb, p, t, wl = _frame(args.config, rank, args.n)
     n, d = pts.shape
     esz = pts.dtype.itemsize
     raw = n * d * esz
@@ -618,7 +622,7 @@ def run_once(args):
 
     from chaincompressor_b200 import _native as N
 
-    pts, eb, p, t, wl = _frame(args.config, 0)
+    pts, eb, p, t, wl = _frame(args.config, 0, args.n)
     n, d = pts.shape
     soa = torch.from_numpy(np.ascontiguousarray(pts.T)).cuda()
     codec = N.Codec(0)
@@ -645,6 +649,8 @@ def main():
     ap.add_argument("--requests", type=int, default=20000, help="requests of the serving run (--config serve)")
     ap.add_argument("--workers", type=int, default=8, help="contexts of the batch path (--config batch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--n", type=int, default=0,
+                    help="particles of the blobs frame (default 16,777,216); smaller sizes are profiling cases")
     ap.add_argument("--once", action="store_true",
                     help="one warm-up and one measured compress + decompress, no timing (for ncu launch lists)")
     args = ap.parse_args()

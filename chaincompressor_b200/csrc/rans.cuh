@@ -644,7 +644,7 @@ struct RansJob {
 };
 
 constexpr int kMaxRansJobs = 16;
-constexpr int kRansEncWarps = 4;              // chunks (warps) per encoder CTA
+constexpr int kRansEncWarps = 8;              // chunks (warps) per encoder CTA
 constexpr int kRansDecWarps = 8;              // chunks (warps) per decoder CTA (shares its table image)
 constexpr int kRansTile = 32;                 // steps per staged tile
 constexpr uint32_t kSmemTableSyms = 4096;     // decoder prob/cum in shared memory up to this alphabet
@@ -740,7 +740,7 @@ inline void rans_plan_smem(RansJobs& J, bool decode) {
     J.table_bytes = image;
 }
 inline size_t rans_enc_smem(const RansJobs& J) {
-    return J.tab_cap * 16ull + kRansEncWarps * (2 * kRansTile * 32 * 4 + kWindow);
+    return J.tab_cap * 16ull + kRansEncWarps * (kRansTile * 32 * 4 + kWindow);
 }
 inline size_t rans_dec_smem(const RansJobs& J) {
     return J.table_bytes + kRansDecWarps * kWindow + 16;   // +16: 3-byte renorm reads
@@ -753,7 +753,7 @@ inline size_t rans_dec_smem(const RansJobs& J) {
 // that launch fail).
 // Two decoder CTAs of the largest size still fit one SM (228 KB less 1 KB per CTA).
 constexpr size_t kRansEncSmemMax =
-    kSmemEncSyms * 16ull + kRansEncWarps * 2 * kRansTile * 32 * 4 + kRansEncWarps * kWindow;
+    kSmemEncSyms * 16ull + kRansEncWarps * kRansTile * 32 * 4 + kRansEncWarps * kWindow;
 constexpr size_t kDecDirectBytes = kSmemTableSyms * 8ull + kSmemLookupSlots * 2ull;
 constexpr size_t kDecBucketBytes = (((kBucketMaxSyms + 1 + 3) & ~3ull) * 4 + (kBucketCount + 1) * 2 + 15) & ~15ull;
 constexpr size_t kRansDecSmemMax =
@@ -919,8 +919,10 @@ __device__ __forceinline__ uint32_t rans_encode_full_tile(uint32_t x, const uint
 }
 
 // Encoder: one warp per chunk, kRansEncWarps chunks of one job per CTA.  The job's table
-// sits in shared memory when small; symbols are prefetched one 32-step tile ahead
-// into shared memory; the warp's byte counts are prefix-summed with two ballots
+// sits in shared memory when small; the next 32-step tile of symbols is loaded into
+// registers while the current one is coded from the warp's shared-memory tile buffer,
+// then stored there (one buffer per warp; eight warps per CTA, two CTAs per SM); the
+// warp's byte counts are prefix-summed with two ballots
 // (0..3 bytes per lane).  Bytes are written backwards into a kWindow-byte shared-memory
 // window; before each group of kRansTile steps, if fewer than a group's worst case
 // (kRansTile * 96 bytes) are free, the window's 16-byte-aligned written part goes to
@@ -938,8 +940,8 @@ static __global__ void __launch_bounds__(32 * kRansEncWarps) rans_encode_kernel(
     __syncthreads();
     const uint32_t c = (blockIdx.x - jb.first_block) * kRansEncWarps + warp;
     if (c >= jb.chunks) return;
-    uint32_t* buf = reinterpret_cast<uint32_t*>(rsm + J.tab_cap * 16ull) + warp * 2 * 1024;
-    uint8_t* ow = rsm + J.tab_cap * 16ull + kRansEncWarps * 2 * kRansTile * 32 * 4 + warp * kWindow;
+    uint32_t* buf = reinterpret_cast<uint32_t*>(rsm + J.tab_cap * 16ull) + warp * 1024;
+    uint8_t* ow = rsm + J.tab_cap * 16ull + kRansEncWarps * kRansTile * 32 * 4 + warp * kWindow;
     const uint64_t cbeg = static_cast<uint64_t>(c) * jb.S;
     const uint64_t cend = min(cbeg + jb.S, jb.count);
     const uint32_t W = jb.lanes;
@@ -963,7 +965,7 @@ static __global__ void __launch_bounds__(32 * kRansEncWarps) rans_encode_kernel(
     {
         const uint64_t tb = cbeg + tile_syms * (ntiles - 1);
         tile_load(jb.sym, jb.sym_esz, tb, min(tb + tile_syms, cend), r, layout);
-        tile_store(buf + ((ntiles - 1) & 1) * 1024, r, layout);
+        tile_store(buf, r, layout);
         __syncwarp();
     }
     for (int k = static_cast<int>(ntiles) - 1; k >= 0; --k) {
@@ -988,7 +990,7 @@ static __global__ void __launch_bounds__(32 * kRansEncWarps) rans_encode_kernel(
             wtop -= kWindow - a;
             rel = kWindow - h;
         }
-        const uint32_t* cur = buf + (k & 1) * 1024;
+        const uint32_t* cur = buf;
         if (static_cast<uint32_t>(32 * k + 32) <= full_steps) {
             x = smem_tab ? rans_encode_full_tile<true>(x, cur, tab, jb.etab, ow, rel, lt)
                          : rans_encode_full_tile<false>(x, cur, tab, jb.etab, ow, rel, lt);
@@ -1008,7 +1010,7 @@ static __global__ void __launch_bounds__(32 * kRansEncWarps) rans_encode_kernel(
         }
         if (k > 0) {
             __syncwarp();
-            tile_store(buf + ((k - 1) & 1) * 1024, r, layout);
+            tile_store(buf, r, layout);   // the tile just coded is no longer needed
             __syncwarp();
         }
     }

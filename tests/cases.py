@@ -78,6 +78,14 @@ def case(name):
         pts = np.arange(n, dtype=np.float64).reshape(n, 1)
         pts[-1, 0] = 1.0
         return pts, 0.5, 1, -30, {}
+    if name == "many_corrections":
+        # half the points on the far corner of the box, where the float64 reconstruction
+        # of every coordinate misses the bound: more than 2^20 exact corrections
+        rng = np.random.default_rng(15)
+        pts = rng.uniform(0, 1, size=(1 << 20, 3))
+        pts[: 1 << 19] = 1.0
+        pts[-1] = 0.0
+        return pts, 0.1, 4, 2, {}
     if name == "negative_zero":
         pts = np.array([[0.0, -0.0], [-0.0, 0.0], [1.0, 2.0], [0.5, -0.0]], np.float64)
         return pts, 0.05, 2, 0, {}
@@ -86,4 +94,4 @@ def case(name):
 
 GPU_CASES = ["column", "column_qb11", "blobs200k", "blobs_clipped", "traj_f64_e4_p1", "traj_f64_e2",
              "uniform_p64_t25", "single_point", "one_block", "long_chain", "p1_big_threshold", "neg_threshold", "dims1", "dims2",
-             "dims4", "no_l1", "no_l2", "no_bl", "big_values_tagged", "wide_jump", "negative_zero"]
+             "dims4", "no_l1", "no_l2", "no_bl", "big_values_tagged", "wide_jump", "negative_zero", "many_corrections"]
