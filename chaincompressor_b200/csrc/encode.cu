@@ -75,10 +75,10 @@ struct EncState {
     // level-1 links (idrel != 0), accumulated by k_level1 for IDR0's statistics
     unsigned long long l1_links, l1_link_bits;
     uint32_t l1_link_min, l1_link_max;
-    uint32_t pad3;
+    uint32_t done_a;          // CTAs finished (last-CTA hand-offs; zero between them)
     uint64_t total_bytes;
     uint32_t npieces;
-    uint32_t pad2;
+    uint32_t done_b;          // second hand-off counter
     uint64_t nsegs;
 };
 
@@ -118,6 +118,8 @@ template <typename FT, bool SOA>
 __device__ __forceinline__ double load_coord(const FT* p, uint64_t n, uint32_t D, uint64_t i, uint32_t d) {
     return static_cast<double>(SOA ? p[static_cast<uint64_t>(d) * n + i] : p[i * D + d]);
 }
+
+__device__ void qparams(EncState* st);
 
 // Per-axis extrema (as ordered bits of the double value), the first index of -0.0 and
 // of +0.0, and a non-finite flag.  blockIdx.y is the axis.  Values are compared in their
@@ -179,22 +181,33 @@ __global__ void __launch_bounds__(256) k_minmax(const FT* __restrict__ p, uint64
         if (zneg != ~0ull) atomicMin(reinterpret_cast<unsigned long long*>(&st->zero_first[d][0]), zneg);
         if (zpos != ~0ull) atomicMin(reinterpret_cast<unsigned long long*>(&st->zero_first[d][1]), zpos);
     }
-    if (__syncthreads_or(bad) && threadIdx.x == 0) set_error(&st->err, kErrNonFinite);
+    const bool any_bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) {
+        if (any_bad) set_error(&st->err, kErrNonFinite);
+        // the CTA that finishes last derives the quantization parameters from the
+        // completed extrema (no separate launch)
+        __threadfence();
+        if (atomicAdd(&st->done_a, 1u) == gridDim.x * gridDim.y - 1) {
+            __threadfence();
+            qparams(st);
+            st->done_a = 0;
+        }
+    }
 }
 
 // Per-axis minimum exactly as std::min keeps it (first of equal values, which only
 // matters for +0.0 vs -0.0), the largest quantized value and the block-key width.
-__global__ void k_qparams(EncState* st) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (st->err & kErrNonFinite) return;
+__device__ void qparams(EncState* st) {
+    if (__ldcg(&st->err) & kErrNonFinite) return;
     const double denom = 2.0 * st->eb;
     uint32_t bmax = 0;
     int kb = 0;
     for (uint32_t d = 0; d < st->dims; ++d) {
-        double mn = from_ordered_bits(st->minbits[d]);
-        if (mn == 0.0) mn = st->zero_first[d][0] < st->zero_first[d][1] ? -0.0 : 0.0;
+        // the extrema were combined by other CTAs' atomics: read them from L2
+        double mn = from_ordered_bits(__ldcg(&st->minbits[d]));
+        if (mn == 0.0) mn = __ldcg(&st->zero_first[d][0]) < __ldcg(&st->zero_first[d][1]) ? -0.0 : 0.0;
         st->mins[d] = mn;
-        const double mx = from_ordered_bits(st->maxbits[d]);
+        const double mx = from_ordered_bits(__ldcg(&st->maxbits[d]));
         const double qv = floor((mx - mn) / denom);
         if (!(qv >= 0.0 && qv < 0x1p63)) { set_error(&st->err, kErrQuantOverflow); return; }
         if (qv >= 2147483648.0) { set_error(&st->err, kErrUnsupported); return; }
@@ -282,7 +295,8 @@ template <typename FT, bool SOA, typename KT, int DIM, typename RT>
 __global__ void __launch_bounds__(256)
 k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT* __restrict__ key_out,
            RT* __restrict__ rel_out, uint64_t* __restrict__ corr_idx, double* __restrict__ corr_val,
-           uint64_t corr_cap, uint32_t* __restrict__ hist_counts, int hist_bits, uint32_t tiles) {
+           uint64_t corr_cap, uint32_t* __restrict__ hist_counts, int hist_bits, uint32_t tiles,
+           uint32_t* __restrict__ idrel_zero) {
     static_assert(SortShape<KT>::kTile % 1024 == 0, "tiles hold whole groups of four points per thread");
     constexpr uint64_t TILE = SortShape<KT>::kTile;
     __shared__ double s_min[kMaxDims];
@@ -353,6 +367,8 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
                     for (int w = 0; w < 3; ++w)
                         ro[w] = rel[4 * w] | (rel[4 * w + 1] << 8) | (rel[4 * w + 2] << 16) | (rel[4 * w + 3] << 24);
                 }
+                // idrel starts at zero (level 1 writes only the links)
+                reinterpret_cast<uint4*>(idrel_zero)[g] = make_uint4(0, 0, 0, 0);
                 if constexpr (sizeof(KT) == 4) {
                     *reinterpret_cast<uint4*>(key_out + 4 * g) = make_uint4(keys[0], keys[1], keys[2], keys[3]);
                 } else {
@@ -376,6 +392,7 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
         }
         const KT key = static_cast<KT>(block_key(b, static_cast<int>(D), kb));
         key_out[i] = key;
+        idrel_zero[i] = 0;
         if (hist) atomicAdd(&s_hist[static_cast<uint32_t>(key) & hmask], 1u);
     }
     if (hist) {
@@ -504,8 +521,8 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
 
 // IDR0's statistics completed from the level-1 links: the n - links zeros (tag 1) join
 // them.  The same values the counting kernel would accumulate from the stream.
-__global__ void k_idrel_stats(EncState* st, uint32_t* gh, uint64_t n) {
-    if (threadIdx.x || blockIdx.x || n == 0) return;
+__device__ void idrel_stats(EncState* st, uint32_t* gh, uint64_t n) {
+    if (n == 0) return;
     const unsigned long long links = st->l1_links, zeros = n - links;
     StreamStats& g = st->st[0];
     g.minv[0] = zeros ? 0u : st->l1_link_min;
@@ -619,8 +636,7 @@ __global__ void __launch_bounds__(256) k_l2_stats(const KT* __restrict__ rec, En
 }
 
 // lcps_cpp.cpp:1221-1253 wrap parameters; also the !l2 keep-all variant (:1456-1478).
-__global__ void k_l2_params(EncState* st) {
-    if (threadIdx.x || blockIdx.x) return;
+__device__ void l2_params(EncState* st) {
     const int64_t mn = st->B ? st->rec_min : 0;
     const int64_t mx = st->rec_max;
     const int64_t range = mx - mn + 1;
@@ -654,12 +670,13 @@ __device__ __forceinline__ uint32_t l2_rule(const uint32_t* cur, const uint32_t*
 // difference records, so the level-2 flag scan needs no counting pass.  Each thread
 // takes four groups of four consecutive record keys, all loads first.
 template <typename KT, int DIM>
-__global__ void __launch_bounds__(256) k_l2_choice(const KT* __restrict__ rec, const EncState* st, int l2,
+__global__ void __launch_bounds__(256) k_l2_choice(const KT* __restrict__ rec, EncState* st, int l2,
                                                    uint8_t* choice2, uint32_t* tile_counts) {
     static_assert(kFlagTile == 4 * 4 * 256, "four groups of four records per thread");
     __shared__ uint32_t wsum[8];
     if (DIM == 3 && !l2_dim3(st)) return;
     if (DIM == 0 && l2_dim3(st)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) l2_params(st);   // read by the level-2 output and the layout
     const uint32_t B = st->B;
     const int D = DIM ? DIM : static_cast<int>(st->dims);
     const int kb = st->kb;
@@ -763,10 +780,6 @@ struct Level2Out {
     }
 };
 
-__global__ void k_l2_counts(EncState* st) {
-    if (threadIdx.x || blockIdx.x) return;
-    st->nkeep = st->B - st->ndiff;
-}
 
 // ------------------------------------------------------------- stream stats
 struct StreamRef {
@@ -774,6 +787,7 @@ struct StreamRef {
     uint32_t dims;
     uint32_t esz;           // 1, 2 or 4
     const uint32_t* count_dev;  // records (device) or null -> count_const
+    const uint32_t* count_sub;  // when set, subtracted from *count_dev
     uint64_t count_const;
 };
 struct StreamRefs {
@@ -786,7 +800,8 @@ struct StreamSel {
 };
 
 __device__ __forceinline__ uint64_t stream_records(const StreamRef& r) {
-    return r.count_dev ? static_cast<uint64_t>(*r.count_dev) : r.count_const;
+    if (!r.count_dev) return r.count_const;
+    return static_cast<uint64_t>(*r.count_dev) - (r.count_sub ? *r.count_sub : 0u);
 }
 
 // Warp-aggregated histogram increment: lanes holding equal values add once.
@@ -825,6 +840,9 @@ struct PackedCount8 {
 
 constexpr int kSmemHistBins = 4096;
 
+__device__ void idrel_stats(EncState* st, uint32_t* gh, uint64_t n);
+__device__ void choice_stats(EncState* st, uint32_t* gh);
+
 // Per-stream statistics in one pass: per-dimension min/max, overall max, the record
 // tags (max(1, max_d bitlen v)) histogram and bit total, and the value histogram of
 // the raw candidate (values < 2^18; a larger max makes the candidate ineligible).
@@ -833,9 +851,15 @@ constexpr int kSmemHistBins = 4096;
 // below kSmemHistBins in shared memory, the rest in global memory.  Register
 // counters flush before they could overflow.  blockIdx.y selects the stream from
 // sel[] (the streams of one launch share DIM).
+// derive: bit 0 = complete IDR0's statistics from the level-1 links, bit 1 = CH20's from
+// the level-2 counts (done once, by block (0, 0), before its own stream).
 template <int DIM>
 __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState* st, uint32_t* hist,
-                                                       uint64_t hist_stride, StreamSel sel) {
+                                                       uint64_t hist_stride, StreamSel sel, int derive) {
+    if (derive && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+        if (derive & 1) idrel_stats(st, hist, refs.s[0].count_const);
+        if (derive & 2) choice_stats(st, hist + hist_stride * 3);
+    }
     const int s = sel.s[blockIdx.y];
     const StreamRef r = refs.s[s];
     const uint32_t D = DIM ? DIM : r.dims;
@@ -959,9 +983,14 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
 }
 
 // One CTA per (stream, kind): kind 0 = raw value table, kind 1 = tag table.
+__device__ void plan_stream(const StreamRefs& refs, EncState* st, uint32_t bytes_per_lane, uint32_t max_steps, int s);
+
+// The CTA that finishes last plans the launch's streams (plan_stream), so that the plan
+// needs no launch of its own.
 __global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncState* st, const uint32_t* hist,
                                                            uint64_t hist_stride, uint32_t* prob, uint32_t* cum,
-                                                           uint32_t* tag_prob, uint32_t* tag_cum, int s0) {
+                                                           uint32_t* tag_prob, uint32_t* tag_cum, int s0,
+                                                           uint32_t bytes_per_lane, uint32_t max_steps) {
     extern __shared__ __align__(16) uint32_t tstage[];   // kTableStageBytes
     const int s = s0 + blockIdx.x, kind = blockIdx.y;
     const StreamRef r = refs.s[s];
@@ -976,6 +1005,17 @@ __global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncSt
         build_rans_table(st->st[s].tag_hist, A, nrec, tag_prob + 64 * s, tag_cum + 64 * s, &st->tag_tab[s],
                          tstage);
     }
+    __shared__ bool s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&st->done_b, 1u) == gridDim.x * gridDim.y - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x < gridDim.x) plan_stream(refs, st, bytes_per_lane, max_steps, s0 + threadIdx.x);
+    if (threadIdx.x == 0) st->done_b = 0;
 }
 
 __device__ inline uint64_t section_overhead(uint32_t table_bytes, uint32_t chunks, uint32_t lanes, uint32_t prec) {
@@ -1012,12 +1052,24 @@ __device__ inline void plan_chunks(uint64_t count, double est_payload, uint32_t 
     *chunks = static_cast<uint32_t>((count + s - 1) / s);
 }
 
-// Chooses each component's encoding: the smallest estimated size among tagged, fixed
-// and raw (ties in that order, as lcps_cpp.cpp:1150-1170), empty when no records.
-__global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, uint32_t max_steps, int s0,
-                       int count) {
-    const int s = s0 + threadIdx.x;
-    if (static_cast<int>(threadIdx.x) >= count || blockIdx.x) return;
+// A table descriptor written by another CTA of the same launch, read from L2.
+__device__ __forceinline__ RansTableDev load_table_cg(const RansTableDev* t) {
+    RansTableDev v;
+    v.alphabet = __ldcg(&t->alphabet);
+    v.prec = __ldcg(&t->prec);
+    v.n = __ldcg(&t->n);
+    v.cost_bits = __ldcg(&t->cost_bits);
+    v.table_bytes = __ldcg(&t->table_bytes);
+    v.pad = 0;
+    return v;
+}
+
+// Chooses component s's encoding: the smallest estimated size among tagged, fixed and
+// raw (ties in that order, as lcps_cpp.cpp:1150-1170), empty when no records.  Runs in
+// the table launch's last CTA, once every table of the launch is built.
+__device__ void plan_stream(const StreamRefs& refs, EncState* st, uint32_t bytes_per_lane, uint32_t max_steps, int s) {
+    const RansTableDev tag_t = load_table_cg(&st->tag_tab[s]);
+    const RansTableDev raw_t = load_table_cg(&st->raw_tab[s]);
     const StreamRef r = refs.s[s];
     const uint64_t nrec = stream_records(r);
     StreamChoice& c = st->ch[s];
@@ -1035,7 +1087,7 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
         c.est[kEncEmpty] = 13;
         return;
     }
-    if (st->tag_tab[s].alphabet == 0xFFFFFFFFu || st->raw_tab[s].alphabet == 0xFFFFFFFFu)
+    if (tag_t.alphabet == 0xFFFFFFFFu || raw_t.alphabet == 0xFFFFFFFFu)
         set_error(&st->err, kErrInternal);
     // fixed (width 0 = constant component)
     uint64_t fixed = 13 + 9ull * r.dims;
@@ -1050,7 +1102,7 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
     uint32_t tag_ch = 0, tag_lanes = 0;
     uint64_t tag_S = 0;
     {
-        const RansTableDev& t = st->tag_tab[s];
+        const RansTableDev& t = tag_t;
         const double payload = t.cost_bits / 8.0;
         plan_chunks(nrec, payload, bytes_per_lane, max_steps, &tag_ch, &tag_S, &tag_lanes);
         c.est[kEncTagged] = 13 + 1 + section_overhead(t.table_bytes, tag_ch, tag_lanes, t.prec) +
@@ -1062,8 +1114,8 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
     // wave, kLargeTableMaxSteps beyond.
     uint32_t raw_ch = 0, raw_lanes = 0;
     uint64_t raw_S = 0;
-    if (g.maxall < kRansMaxAlphabet && st->raw_tab[s].alphabet != 0) {
-        const RansTableDev& t = st->raw_tab[s];
+    if (g.maxall < kRansMaxAlphabet && raw_t.alphabet != 0) {
+        const RansTableDev& t = raw_t;
         const double payload = t.cost_bits / 8.0;
         const bool large = (t.alphabet > kSmemEncSyms || (1u << t.prec) > kSmemLookupSlots) &&
                            nrec * r.dims >= kLargeTableMinSymbols;
@@ -1077,7 +1129,7 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
     if (c.est[kEncRaw] < c.est[best]) best = kEncRaw;
     c.enc = best;
     if (best == kEncTagged) {
-        const RansTableDev& t = st->tag_tab[s];
+        const RansTableDev& t = tag_t;
         c.sec_chunks = tag_ch;
         c.sec_S = tag_S;
         c.sec_lanes = tag_lanes;
@@ -1087,7 +1139,7 @@ __global__ void k_plan(StreamRefs refs, EncState* st, uint32_t bytes_per_lane, u
         c.packed_bits = g.tag_bits;
         c.max_width = static_cast<uint8_t>(g.maxtag);
     } else if (best == kEncRaw) {
-        const RansTableDev& t = st->raw_tab[s];
+        const RansTableDev& t = raw_t;
         c.sec_chunks = raw_ch;
         c.sec_S = raw_S;
         c.sec_lanes = raw_lanes;
@@ -1155,11 +1207,9 @@ struct FixedPack {
 };
 constexpr int kPackWarps = 8;
 template <typename ET>
-__global__ void __launch_bounds__(32 * kPackWarps, 3) k_pack_fixed(const ET* __restrict__ data, uint32_t D,
-                                                                 uint64_t nrec, FixedPack fp) {
-    __shared__ uint32_t stage[kPackWarps][33 * 32];
+__device__ __forceinline__ void pack_fixed_tiles(const ET* __restrict__ data, uint32_t D, uint64_t nrec,
+                                                 const FixedPack& fp, uint32_t* sw) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t* sw = stage[warp];
     const uint64_t ntiles = (nrec + 1023) / 1024;
     for (uint64_t tile = static_cast<uint64_t>(blockIdx.x) * kPackWarps + warp; tile < ntiles;
          tile += static_cast<uint64_t>(gridDim.x) * kPackWarps) {
@@ -1197,42 +1247,30 @@ __global__ void __launch_bounds__(32 * kPackWarps, 3) k_pack_fixed(const ET* __r
     }
 }
 
-// Final lane states of every rANS section (blockIdx.y = section) packed MSB-first at
-// prec + 10 bits each, as big-endian 32-bit words (so byte 0 holds the first bits).
-struct StatePacks {
-    const uint32_t* in[kCodeStreams];
-    uint32_t* out[kCodeStreams];   // 4-byte aligned; room for whole words
-    uint32_t count[kCodeStreams];
-    uint32_t bits[kCodeStreams];
+// Every fixed-coded component of a frame in one launch (blockIdx.y = component).
+struct FixedJob {
+    FixedPack fp;
+    const void* data;
+    uint64_t nrec;
+    uint32_t dims;
+    uint32_t esz;
 };
-__global__ void __launch_bounds__(256) k_pack_states(StatePacks sp) {
-    const int k = blockIdx.y;
-    const uint32_t B = sp.bits[k];
-    const uint64_t count = sp.count[k];
-    const uint64_t nwords = (count * B + 31) / 32;
-    const uint32_t* in = sp.in[k];
-    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < nwords;
-         w += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t b0 = w * 32;
-        uint32_t acc = 0;
-        for (uint64_t i = b0 / B; i < count && i * B < b0 + 32; ++i) {
-            // the state's most significant bit sits `start` bits after the word's
-            const int64_t start = static_cast<int64_t>(i * B) - static_cast<int64_t>(b0);
-            const int64_t shift = 32 - (start + static_cast<int64_t>(B));
-            const uint64_t v = in[i];
-            acc |= shift >= 0 ? static_cast<uint32_t>(v << shift) : static_cast<uint32_t>(v >> (-shift));
-        }
-        sp.out[k][w] = __byte_perm(acc, 0, 0x0123);
-    }
+struct FixedJobs {
+    FixedJob job[kCodeStreams];
+};
+__global__ void __launch_bounds__(32 * kPackWarps, 3) k_pack_fixed(FixedJobs J) {
+    __shared__ uint32_t stage[kPackWarps][33 * 32];
+    const FixedJob& j = J.job[blockIdx.y];
+    uint32_t* sw = stage[threadIdx.x >> 5];
+    if (j.esz == 1) pack_fixed_tiles(static_cast<const uint8_t*>(j.data), j.dims, j.nrec, j.fp, sw);
+    else if (j.esz == 2) pack_fixed_tiles(static_cast<const uint16_t*>(j.data), j.dims, j.nrec, j.fp, sw);
+    else pack_fixed_tiles(static_cast<const uint32_t*>(j.data), j.dims, j.nrec, j.fp, sw);
 }
 
-// Encoder symbol entries of every rANS section (blockIdx.y = job).
-__global__ void __launch_bounds__(256) k_enc_symbols(RansJobs J) {
-    const RansJob& jb = J.job[blockIdx.y];
-    uint4* out = const_cast<uint4*>(jb.etab);
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < jb.alphabet; s += gridDim.x * blockDim.x)
-        out[s] = make_enc_symbol(jb.prob[s], jb.cum[s], jb.prec);
-}
+// rANS section of each coded stream (index into RansJobs, -1 = none).
+struct StreamJobs {
+    int job[kCodeStreams];
+};
 
 // Big-endian words -> bytes in place (so that byte 0 holds the first 8 bits).
 __global__ void k_words_to_bytes(uint32_t* words, uint64_t nwords) {
@@ -1241,9 +1279,11 @@ __global__ void k_words_to_bytes(uint32_t* words, uint64_t nwords) {
         words[w] = __byte_perm(words[w], 0, 0x0123);
 }
 
-// Serialises every chosen table (one CTA per stream).
+// Serialises every chosen table (one CTA per stream) and writes the stream's encoder
+// symbol entries (make_enc_symbol) for its rANS section.
 __global__ void __launch_bounds__(1024) k_serialize_tables(EncState* st, const uint32_t* prob, const uint32_t* tag_prob,
-                                                            uint64_t hist_stride, uint8_t* out, uint64_t out_stride) {
+                                                            uint64_t hist_stride, uint8_t* out, uint64_t out_stride,
+                                                            RansJobs J, StreamJobs sj) {
     extern __shared__ __align__(16) uint32_t ser_stage[];   // kSerStageSyms u32
     const int s = blockIdx.x;
     StreamChoice& c = st->ch[s];
@@ -1253,6 +1293,12 @@ __global__ void __launch_bounds__(1024) k_serialize_tables(EncState* st, const u
     else if (c.enc == kEncTagged)
         len = serialize_table_block(tag_prob + 64 * s, c.sec_alphabet, out + out_stride * s, ser_stage);
     if (threadIdx.x == 0) c.table_len = len;
+    if (sj.job[s] >= 0) {
+        const RansJob& jb = J.job[sj.job[s]];
+        uint4* et = const_cast<uint4*>(jb.etab);
+        for (uint32_t a = threadIdx.x; a < jb.alphabet; a += blockDim.x)
+            et[a] = make_enc_symbol(jb.prob[a], jb.cum[a], jb.prec);
+    }
 }
 
 // --------------------------------------------------------------- assembly
@@ -1288,10 +1334,17 @@ struct Writer {
 };
 
 // One CTA per rANS section: payload offsets and copy-segment prefix of its chunks.
-__global__ void __launch_bounds__(1024) k_chunk_prefix(ChunkMaps maps, EncState* st) {
+__device__ void layout(EncState* st, const AssemblyIn& in, uint8_t* out, Piece* pieces, uint32_t max_pieces);
+
+// The CTA that finishes last lays out the container (layout), so that the layout needs
+// no launch of its own; with no rANS section the launch is that one CTA.
+__global__ void __launch_bounds__(1024) k_chunk_prefix(ChunkMaps maps, EncState* st, AssemblyIn ain, uint8_t* out,
+                                                       Piece* pieces, uint32_t max_pieces) {
+    __shared__ uint64_t red[33];
+    __shared__ bool s_last;
+    if (static_cast<int>(blockIdx.x) < maps.nsec) {
     const int s = maps.sec_stream[blockIdx.x];
     const ChunkMap M = maps.m[s];
-    __shared__ uint64_t red[33];
     uint64_t carry_b = 0, carry_s = 0;
     for (uint32_t base = 0; base < M.chunks; base += blockDim.x) {
         const uint32_t k = base + threadIdx.x;
@@ -1311,11 +1364,22 @@ __global__ void __launch_bounds__(1024) k_chunk_prefix(ChunkMaps maps, EncState*
         M.seg[M.chunks] = static_cast<uint32_t>(carry_s);
         st->ch[s].payload_bytes = carry_b;
     }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&st->done_a, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    layout(st, ain, out, pieces, max_pieces);
+    st->done_a = 0;
 }
 
-// Single thread: writes every header field and emits the list of payload pieces.
-__global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* pieces, uint32_t max_pieces) {
-    if (threadIdx.x || blockIdx.x) return;
+// One thread: writes every header field and emits the list of payload pieces (payload
+// sizes and copy-segment counts come from other CTAs of the same launch: read from L2).
+__device__ void layout(EncState* st, const AssemblyIn& in, uint8_t* out, Piece* pieces, uint32_t max_pieces) {
     Writer w{out, 0};
     uint32_t np = 0;
     uint64_t segs = 0;
@@ -1368,10 +1432,11 @@ __global__ void k_layout(EncState* st, AssemblyIn in, uint8_t* out, Piece* piece
             w.uint(c.sec_S, 8);
             w.u8(static_cast<uint8_t>(c.sec_lanes));
             w.uint(c.sec_chunks, 4);
-            w.uint(c.payload_bytes, 8);
+            const uint64_t payload = __ldcg(&c.payload_bytes);
+            w.uint(payload, 8);
             piece(reinterpret_cast<const uint8_t*>(in.chunk_len[s]), 4ull * c.sec_chunks);
             piece(in.states[s], state_bytes(c.sec_lanes, c.sec_chunks, c.sec_prec));
-            chunked(s, c.payload_bytes, in.chunk_segs[s][c.sec_chunks]);
+            chunked(s, payload, __ldcg(&in.chunk_segs[s][c.sec_chunks]));
             if (c.enc == kEncTagged) {
                 w.uint(c.packed_bits, 8);
                 piece(in.packed[s], (c.packed_bits + 7) / 8);
@@ -1523,9 +1588,17 @@ __global__ void k_gather_corrections(const uint32_t* perm, const uint64_t* idx_s
     }
 }
 
-__global__ void k_init_state(EncState* st, uint32_t dims, uint64_t n, double eb, uint64_t p, int64_t threshold) {
+// Resets the frame state and zeroes the value histograms (hist_words u32, grid-stride).
+__global__ void __launch_bounds__(256) k_init_state(EncState* st, uint32_t dims, uint64_t n, double eb, uint64_t p,
+                                                    int64_t threshold, uint32_t* hist, uint64_t hist_words) {
+    uint4* h4 = reinterpret_cast<uint4*>(hist);   // 256-byte aligned, hist_words a multiple of 4
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < hist_words / 4;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        h4[i] = make_uint4(0, 0, 0, 0);
     if (threadIdx.x || blockIdx.x) return;
     st->err = 0;
+    st->done_a = 0;
+    st->done_b = 0;
     st->dims = dims;
     st->n = n;
     st->eb = eb;
@@ -1582,8 +1655,7 @@ static chain_status status_from_err(uint32_t err) {
 // Statistics of CH20 without reading it: its values are 0 and 1 (record 0 is 0), B
 // records of which st->ndiff are 1, so every field follows (the same values the
 // counting kernel would accumulate from the stream's reset state).
-__global__ void k_choice_stats(EncState* st, uint32_t* gh) {
-    if (threadIdx.x || blockIdx.x) return;
+__device__ void choice_stats(EncState* st, uint32_t* gh) {
     const uint64_t B = st->B, ones = st->ndiff;
     if (B == 0) return;
     StreamStats& g = st->st[3];
@@ -1603,12 +1675,12 @@ __global__ void k_choice_stats(EncState* st, uint32_t* gh) {
 static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, uint64_t hist_stride, uint32_t dims,
                          uint64_t max_records, int s0, int count, cudaStream_t stream) {
     StreamSel one{}, many{};
-    int n1 = 0, nd = 0;
+    int n1 = 0, nd = 0, derive = 0;
     for (int s = s0; s < s0 + count; ++s) {
         if (s == 3) {
-            k_choice_stats<<<1, 1, 0, stream>>>(st, hist + hist_stride * 3); count_launch();
+            derive |= 2;
         } else if (s == 0) {
-            k_idrel_stats<<<1, 1, 0, stream>>>(st, hist, refs.s[0].count_const); count_launch();
+            derive |= 1;
         } else if (refs.s[s].dims == 1) {
             one.s[n1++] = s;
         } else {
@@ -1616,14 +1688,17 @@ static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, u
         }
     }
     const unsigned g = grid_for((max_records + 3) / 4, 256, 148u * 4u);
-    if (n1) { k_stream_stats<1><<<dim3(g, n1), 256, 0, stream>>>(refs, st, hist, hist_stride, one); count_launch(); }
+    if (n1) {
+        k_stream_stats<1><<<dim3(g, n1), 256, 0, stream>>>(refs, st, hist, hist_stride, one, derive); count_launch();
+        derive = 0;
+    }
     if (nd) {
         constexpr size_t smem = 0;
         switch (dims) {
-            case 2: k_stream_stats<2><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many); break;
-            case 3: k_stream_stats<3><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many); break;
-            case 4: k_stream_stats<4><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many); break;
-            default: k_stream_stats<0><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many); break;
+            case 2: k_stream_stats<2><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many, derive); break;
+            case 3: k_stream_stats<3><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many, derive); break;
+            case 4: k_stream_stats<4><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many, derive); break;
+            default: k_stream_stats<0><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many, derive); break;
         }
         count_launch();
     }
@@ -1633,17 +1708,17 @@ static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, u
 template <typename FT, bool SOA, typename KT, typename RT>
 static void launch_quantize(const void* pts, uint64_t n, uint32_t D, EncState* st, void* key, void* rel,
                             uint64_t* cidx, double* cval, uint64_t cap, uint32_t* hist, int hist_bits,
-                            cudaStream_t s) {
+                            uint32_t* idrel, cudaStream_t s) {
     const uint32_t tiles = radix_tiles<KT>(n);
     const unsigned grid = std::max(1u, tiles);
     if (D == 3)
         k_quantize<FT, SOA, KT, 3, RT><<<grid, 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st,
                                                             static_cast<KT*>(key), static_cast<RT*>(rel), cidx, cval,
-                                                            cap, hist, hist_bits, tiles);
+                                                            cap, hist, hist_bits, tiles, idrel);
     else
         k_quantize<FT, SOA, KT, 0, RT><<<grid, 256, 0, s>>>(static_cast<const FT*>(pts), n, D, st,
                                                             static_cast<KT*>(key), static_cast<RT*>(rel), cidx, cval,
-                                                            cap, hist, hist_bits, tiles);
+                                                            cap, hist, hist_bits, tiles, idrel);
     count_launch();
 }
 
@@ -1651,13 +1726,13 @@ static void launch_quantize(const void* pts, uint64_t n, uint32_t D, EncState* s
 template <typename FT, bool SOA>
 static void launch_quantize_rt(bool wide, uint32_t rel_esz, const void* pts, uint64_t n, uint32_t D, EncState* st,
                                void* key, void* rel, uint64_t* cidx, double* cval, uint64_t cap, uint32_t* hist,
-                               int hist_bits, cudaStream_t s) {
+                               int hist_bits, uint32_t* idrel, cudaStream_t s) {
     if (wide) {
-        if (rel_esz == 1) launch_quantize<FT, SOA, uint64_t, uint8_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, s);
-        else launch_quantize<FT, SOA, uint64_t, uint32_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, s);
+        if (rel_esz == 1) launch_quantize<FT, SOA, uint64_t, uint8_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, idrel, s);
+        else launch_quantize<FT, SOA, uint64_t, uint32_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, idrel, s);
     } else {
-        if (rel_esz == 1) launch_quantize<FT, SOA, uint32_t, uint8_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, s);
-        else launch_quantize<FT, SOA, uint32_t, uint32_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, s);
+        if (rel_esz == 1) launch_quantize<FT, SOA, uint32_t, uint8_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, idrel, s);
+        else launch_quantize<FT, SOA, uint32_t, uint32_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, idrel, s);
     }
 }
 
@@ -1676,7 +1751,6 @@ static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, ui
     } else {
         k_l2_stats<KT, 0><<<grid_for((n + 3) / 4), 256, 0, stream>>>(rec, st); count_launch();
     }
-    k_l2_params<<<1, 1, 0, stream>>>(st); count_launch();
     const unsigned tiles = static_cast<unsigned>(flag_tiles(n));
     if (d3) {
         k_l2_choice<KT, 3><<<tiles, 256, 0, stream>>>(rec, st, l2, choice2, scan32); count_launch();
@@ -1697,7 +1771,6 @@ static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, ui
         else CHAIN_L2OUT(uint32_t, 0);
     }
 #undef CHAIN_L2OUT
-    k_l2_counts<<<1, 1, 0, stream>>>(st); count_launch();
 }
 
 template <typename FT, bool SOA>
@@ -1784,8 +1857,9 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     uint64_t* corr_dict = A.take<uint64_t>(corr_cap);
     if (!tag_cum) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder frame arena too small");
 
-    k_init_state<<<1, 1, 0, stream>>>(st, dims, n, eb, static_cast<uint64_t>(p_eff), threshold); count_launch();
-    CHAIN_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * hist_stride * kCodeStreams, stream));
+    static_assert((kRansMaxAlphabet * kCodeStreams) % 4 == 0, "histograms zeroed in 16-byte words");
+    k_init_state<<<148, 256, 0, stream>>>(st, dims, n, eb, static_cast<uint64_t>(p_eff), threshold, hist,
+                                          hist_stride * kCodeStreams); count_launch();
 
     // ---- phase 1: extrema and quantization parameters
     const bool soa = layout == CHAIN_SOA;
@@ -1793,7 +1867,6 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
                             : launch_minmax<float, false>(pts, n, dims, st, stream);
     else soa ? launch_minmax<double, true>(pts, n, dims, st, stream)
              : launch_minmax<double, false>(pts, n, dims, st, stream);
-    k_qparams<<<1, 1, 0, stream>>>(st); count_launch();
     CHAIN_LAUNCH_CHECK("encoder phase 1");
     T.mark("extrema", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
@@ -1810,7 +1883,7 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     // the quantizer counts the first sort pass's digits (when a sort follows)
     const RadixPlan plan = radix_plan(key_bits);
     uint32_t* hist0 = l1 ? counts : nullptr;
-#define CHAIN_Q(FT, SOA_) launch_quantize_rt<FT, SOA_>(wide, rel_esz, pts, n, dims, st, key_idx, rel, corr_idx, corr_val, corr_cap, hist0, plan.bits, stream)
+#define CHAIN_Q(FT, SOA_) launch_quantize_rt<FT, SOA_>(wide, rel_esz, pts, n, dims, st, key_idx, rel, corr_idx, corr_val, corr_cap, hist0, plan.bits, idrel, stream)
     if (dtype == CHAIN_F32) {
         if (soa) CHAIN_Q(float, true); else CHAIN_Q(float, false);
     } else {
@@ -1820,8 +1893,7 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     CHAIN_LAUNCH_CHECK("quantize");
     T.mark("quantize", stream);
 
-    if (l1) {
-        CHAIN_CUDA(cudaMemsetAsync(idrel, 0, sizeof(uint32_t) * n, stream));   // k_level1 writes the links only
+    if (l1) {   // idrel was zeroed by the quantizer; k_level1 writes the links only
         // stage marks around every scatter pass; the key width is in the name
         const auto sort_marks = [&](bool after) {
             T.mark(after ? (wide ? "sort_scatter_k64" : "sort_scatter_k32") : "sort_hist_scan", stream);
@@ -1840,8 +1912,6 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
             k_level1<uint32_t><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel,
                                                                hist); count_launch();
         }
-    } else {
-        CHAIN_CUDA(cudaMemsetAsync(idrel, 0, sizeof(uint32_t) * n, stream));
     }
     CHAIN_LAUNCH_CHECK("level 1");
     T.mark("level1", stream);
@@ -1858,20 +1928,20 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     // from the device), so no host round trip is needed for B.
 
     StreamRefs refs;
-    refs.s[0] = StreamRef{idrel, 1, 4, nullptr, n};
-    refs.s[1] = StreamRef{diff, dims, kd_esz, &st->ndiff, 0};
-    refs.s[2] = StreamRef{keep, dims, kd_esz, &st->nkeep, 0};
-    refs.s[3] = StreamRef{choice2, 1, 1, &st->B, 0};
-    refs.s[4] = StreamRef{rel, dims, rel_esz, nullptr, n};
-    refs.s[kCorrGaps] = StreamRef{corr_gaps, 1, 4, nullptr, 0};
-    refs.s[kCorrIds] = StreamRef{corr_ids, 1, 4, nullptr, 0};
+    refs.s[0] = StreamRef{idrel, 1, 4, nullptr, nullptr, n};
+    refs.s[1] = StreamRef{diff, dims, kd_esz, &st->ndiff, nullptr, 0};
+    refs.s[2] = StreamRef{keep, dims, kd_esz, &st->B, &st->ndiff, 0};   // B - ndiff kept records
+    refs.s[3] = StreamRef{choice2, 1, 1, &st->B, nullptr, 0};
+    refs.s[4] = StreamRef{rel, dims, rel_esz, nullptr, nullptr, n};
+    refs.s[kCorrGaps] = StreamRef{corr_gaps, 1, 4, nullptr, nullptr, 0};
+    refs.s[kCorrIds] = StreamRef{corr_ids, 1, 4, nullptr, nullptr, 0};
     launch_stats(refs, st, hist, hist_stride, dims, n, 0, kStreams, stream);
     // per device, cheap; set on every call, always to the same value
     CHAIN_CUDA(cudaFuncSetAttribute(k_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kTableStageBytes)));
     k_tables<<<dim3(kStreams, 2), kTableThreads, kTableStageBytes, stream>>>(refs, st, hist, hist_stride, prob, cum,
-                                                                               tag_prob, tag_cum, 0); count_launch();
-    k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, 0, kStreams); count_launch();
+                                                                               tag_prob, tag_cum, 0, bytes_per_lane,
+                                                                               max_steps); count_launch();
     CHAIN_LAUNCH_CHECK("plan");
     T.mark("stats+tables+plan", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
@@ -1906,8 +1976,8 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
         const unsigned g = grid_for(nc, 256, 148u * 4u);
         launch_stats(refs, st, hist, hist_stride, dims, nc, kCorrGaps, 2, stream);
         k_tables<<<dim3(2, 2), kTableThreads, kTableStageBytes, stream>>>(refs, st, hist, hist_stride, prob, cum,
-                                                                         tag_prob, tag_cum, kCorrGaps); count_launch();
-        k_plan<<<1, 32, 0, stream>>>(refs, st, bytes_per_lane, max_steps, kCorrGaps, 2); count_launch();
+                                                                         tag_prob, tag_cum, kCorrGaps, bytes_per_lane,
+                                                                         max_steps); count_launch();
         CHAIN_LAUNCH_CHECK("corrections");
         CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
         CHAIN_CUDA(cudaStreamSynchronize(stream));
@@ -1963,11 +2033,12 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     CHAIN_CUDA(ctx->coded.reserve(need2));
     Arena& C = ctx->coded;
     uint8_t* slots = C.take<uint8_t>(slots_total + 1);
+    // the packed bit streams and the packed final lane states (128 bytes per chunk) are
+    // OR-ed into: one zeroing covers both
     uint8_t* packed = C.take<uint8_t>(packed_total + 1);
+    uint32_t* packed_states = C.take<uint32_t>(total_chunks * 32 + 1);
     uint32_t* tags = C.take<uint32_t>(tags_total + 1);
     uint32_t* chunk_len = C.take<uint32_t>(total_chunks + 1);
-    uint32_t* states = C.take<uint32_t>(total_chunks * 32 + 1);
-    uint32_t* packed_states = C.take<uint32_t>(total_chunks * 32 + 1);   // 128 bytes per chunk
     uint8_t* tables = C.take<uint8_t>(table_stride * kCodeStreams);
     Piece* pieces = C.take<Piece>(max_pieces);
     uint8_t* container = C.take<uint8_t>(bound);
@@ -1978,10 +2049,16 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     ChunkMaps maps{};
     uint64_t seg_base = 0;
     uint64_t etab_used = 0;
-    if (packed_total) CHAIN_CUDA(cudaMemsetAsync(packed, 0, packed_total, stream));
+    if (packed_states) {
+        const size_t zero_bytes = reinterpret_cast<uint8_t*>(packed_states + total_chunks * 32 + 1) - packed;
+        CHAIN_CUDA(cudaMemsetAsync(packed, 0, zero_bytes, stream));
+    }
 
-    StatePacks sp{};
-    int sp_n = 0;
+    FixedJobs fixed;
+    StreamJobs stream_jobs;
+    for (int s = 0; s < kCodeStreams; ++s) stream_jobs.job[s] = -1;
+    unsigned nfixed = 0;
+    uint64_t fixed_tiles = 0;
     RansJobs jobs{};
     jobs.njobs = 0;
     uint32_t first = 0;
@@ -1995,25 +2072,19 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
         const StreamChoice& c = hs->ch[s];
         const StreamRef& r = refs.s[s];
         if (c.enc == kEncFixed) {
-            FixedPack fp{};
+            FixedJob& fj = fixed.job[nfixed++];
+            fj.fp = FixedPack{};
             for (uint32_t d = 0; d < c.dims; ++d) {
-                fp.words[d] = reinterpret_cast<uint32_t*>(packed + packed_off[s] + packed_stride[s] * d);
-                fp.nwords[d] = (c.records * c.width[d] + 31) / 32;
-                fp.minv[d] = hs->st[s].minv[d];
-                fp.width[d] = c.width[d];
+                fj.fp.words[d] = reinterpret_cast<uint32_t*>(packed + packed_off[s] + packed_stride[s] * d);
+                fj.fp.nwords[d] = (c.records * c.width[d] + 31) / 32;
+                fj.fp.minv[d] = hs->st[s].minv[d];
+                fj.fp.width[d] = c.width[d];
             }
-            const uint64_t tiles = (c.records + 1023) / 1024;
-            const unsigned pg = grid_for(tiles, kPackWarps, 148u * 16u);
-            if (r.esz == 1)
-                k_pack_fixed<uint8_t><<<pg, 32 * kPackWarps, 0, stream>>>(static_cast<const uint8_t*>(r.data), c.dims,
-                                                                         c.records, fp);
-            else if (r.esz == 2)
-                k_pack_fixed<uint16_t><<<pg, 32 * kPackWarps, 0, stream>>>(static_cast<const uint16_t*>(r.data),
-                                                                          c.dims, c.records, fp);
-            else
-                k_pack_fixed<uint32_t><<<pg, 32 * kPackWarps, 0, stream>>>(static_cast<const uint32_t*>(r.data),
-                                                                          c.dims, c.records, fp);
-            count_launch();
+            fj.data = r.data;
+            fj.nrec = c.records;
+            fj.dims = c.dims;
+            fj.esz = r.esz;
+            fixed_tiles = std::max<uint64_t>(fixed_tiles, (c.records + 1023) / 1024);
             ain.packed[s] = packed + packed_off[s];
             ain.packed_dim_stride[s] = packed_stride[s];
         }
@@ -2045,6 +2116,7 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
             sym_esz = 4;
         }
         if (c.enc == kEncRaw || c.enc == kEncTagged) {
+            stream_jobs.job[s] = static_cast<int>(jobs.njobs);
             RansJob& jb = jobs.job[jobs.njobs++];
             jb.sym = symbols;
             jb.sym_esz = sym_esz;
@@ -2061,16 +2133,11 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
             jb.bytes = slots + slot_off[s];
             jb.slot_cap = slot_cap[s];
             jb.chunk_len = chunk_len + chunk_base;
-            jb.states = states + chunk_base * 32;
+            jb.states = packed_states + chunk_base * 32;
             jb.first_block = first;
             first += (c.sec_chunks + kRansEncWarps - 1) / kRansEncWarps;
             ain.chunk_len[s] = jb.chunk_len;
             ain.states[s] = reinterpret_cast<const uint8_t*>(packed_states + chunk_base * 32);
-            sp.in[sp_n] = jb.states;
-            sp.out[sp_n] = packed_states + chunk_base * 32;
-            sp.count[sp_n] = c.sec_lanes * c.sec_chunks;
-            sp.bits[sp_n] = state_bits(c.sec_prec);
-            ++sp_n;
             ain.slots[s] = jb.bytes;
             ain.slot_cap[s] = slot_cap[s];
             ChunkMap& cm = maps.m[s];
@@ -2087,14 +2154,17 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
         }
     }
     jobs.total_blocks = first;
+    if (nfixed) {
+        k_pack_fixed<<<dim3(grid_for(fixed_tiles, kPackWarps, 148u * 16u), nfixed), 32 * kPackWarps, 0, stream>>>(fixed);
+        count_launch();
+    }
     T.mark("corrections+packing", stream);
     CHAIN_CUDA(cudaFuncSetAttribute(k_serialize_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(4 * kSerStageSyms)));
     k_serialize_tables<<<kCodeStreams, 1024, 4 * kSerStageSyms, stream>>>(st, prob, tag_prob, hist_stride, tables,
-                                                                          table_stride); count_launch();
+                                                                          table_stride, jobs, stream_jobs); count_launch();
     T.mark("serialize_tables", stream);
     if (jobs.total_blocks) {
-        k_enc_symbols<<<dim3(64, jobs.njobs), 256, 0, stream>>>(jobs); count_launch();
         rans_plan_smem(jobs, false);
         if (rans_enc_smem(jobs) > kRansEncSmemMax)
             return set_err(CHAIN_ERR_DEVICE, "internal: rANS encoder shared memory above its fixed maximum");
@@ -2105,14 +2175,11 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
                                             static_cast<int>(kRansEncSmemMax)));
         }
         rans_encode_kernel<<<jobs.total_blocks, 32 * kRansEncWarps, rans_enc_smem(jobs), stream>>>(jobs, &st->err); count_launch();
-        k_pack_states<<<dim3(16, sp_n), 256, 0, stream>>>(sp); count_launch();
     }
     CHAIN_LAUNCH_CHECK("entropy coding");
     T.mark("rans_encode", stream);
-    if (maps.nsec) {
-        k_chunk_prefix<<<maps.nsec, 1024, 0, stream>>>(maps, st); count_launch();
-    }
-    k_layout<<<1, 1, 0, stream>>>(st, ain, container, pieces, static_cast<uint32_t>(max_pieces)); count_launch();
+    k_chunk_prefix<<<std::max(1, maps.nsec), 1024, 0, stream>>>(maps, st, ain, container, pieces,
+                                                             static_cast<uint32_t>(max_pieces)); count_launch();
     k_copy_pieces<<<148u * 16u, 256, 0, stream>>>(pieces, maps, st, container); count_launch();
     CHAIN_LAUNCH_CHECK("assembly");
     T.mark("assemble", stream);
@@ -2125,7 +2192,7 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     if (hs->total_bytes > bound) return set_err(CHAIN_ERR_DEVICE, "container exceeds its bound");
     ctx->result = container;
     ctx->result_len = hs->total_bytes;
-    ctx->dbg = EncodeDebug{idrel, diff, keep, kd_esz, choice2, rel, rel_esz, n, hs->ndiff, hs->nkeep, hs->B, dims};
+    ctx->dbg = EncodeDebug{idrel, diff, keep, kd_esz, choice2, rel, rel_esz, n, hs->ndiff, hs->B - hs->ndiff, hs->B, dims};
     *out_len = hs->total_bytes;
     return CHAIN_OK;
 }

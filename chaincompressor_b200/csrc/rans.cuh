@@ -22,6 +22,7 @@
 #pragma once
 
 #include "chain_common.cuh"
+#include "chain_format.h"
 
 namespace chain {
 
@@ -640,7 +641,9 @@ struct RansJob {
     uint64_t slot_cap;        // encode only
     const uint64_t* chunk_off;  // decode: absolute byte offset of each chunk (chunks + 1)
     uint32_t* chunk_len;      // encode: bytes per chunk
-    uint32_t* states;         // encode: out [chunks * lanes]; decode: in
+    uint32_t* states;         // encode: the section's final lane states, packed at state_bits(prec)
+                              // each (MSB first, big-endian 32-bit words, zeroed beforehand);
+                              // decode: unpacked states in
 };
 
 constexpr int kMaxRansJobs = 16;
@@ -1021,7 +1024,21 @@ static __global__ void __launch_bounds__(32 * kRansEncWarps) rans_encode_kernel(
     __syncwarp();
     const int64_t gb = static_cast<int64_t>(wtop) - kWindow;
     for (uint32_t i = rel + lane; i < kWindow; i += 32) out[gb + i] = ow[i];
-    if (static_cast<uint32_t>(lane) < W) jb.states[static_cast<uint64_t>(c) * W + lane] = x;
+    if (static_cast<uint32_t>(lane) < W) {
+        // final state of lane (c, lane) at bits [i B, i B + B) of the section's packed states;
+        // neighbouring chunks share boundary words, so the bits are OR-ed in (byte order
+        // swapped: OR commutes with the swap)
+        const uint32_t B = state_bits(prec);
+        const uint64_t o = (static_cast<uint64_t>(c) * W + lane) * B;
+        uint32_t* words = jb.states + (o >> 5);
+        const int shift = 32 - static_cast<int>(o & 31) - static_cast<int>(B);
+        if (shift >= 0) {
+            atomicOr(words, __byte_perm(x << shift, 0, 0x0123));
+        } else {
+            atomicOr(words, __byte_perm(x >> -shift, 0, 0x0123));
+            atomicOr(words + 1, __byte_perm(x << (32 + shift), 0, 0x0123));
+        }
+    }
     if (lane == 0) jb.chunk_len[c] = static_cast<uint32_t>(jb.slot_cap - (gb + rel));
 }
 
