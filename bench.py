@@ -13,9 +13,13 @@ is timed the same way and reported beside it.
           D2H of the container inside the timed region
   decompress : the same two numbers for the decoder (container -> float64 points)
   roofline   : the dominant kernel of the compress step (radix_scatter_kernel, one
-          launch per 8-bit sort pass) against the measured HBM copy bandwidth;
+          launch per sort pass) against the measured HBM copy bandwidth;
           roofline_rans_encode for the encoder's entropy kernel; decompress.roofline
           for rans_decode_kernel; path_roofline: (input + container bytes) / step time
+
+On one GPU the line also carries `batch` (the uneven 256-frame collection through
+chain_batch_compress against one call per frame, as --config batch) and `serve` (the
+request server's capacity and p50/p99 at 0.5/0.8/0.95 of it, as --config serve).
 
 Multi-GPU: frames are independent, so N ranks compress N independent frames
 (replicas, weak scaling, no collective on the data path; only the timing max-reduce).
@@ -351,7 +355,7 @@ def run_batch_bench(args):
     items = [N.BatchItem(input=x.data_ptr(), dtype=N.CHAIN_F32, layout=N.CHAIN_SOA, n=n, dims=3, eb=eb, p=4,
                          threshold=2, output=outbuf.data_ptr() + int(off), output_capacity=cap)
              for (x, n, eb), off, cap in zip(frames, offs, caps)]
-    batch = N.Batch(0, workers=args.workers)
+    batch = N.Batch(0, workers=args.workers or 8)
 
     def bat_compress():
         arr = batch.compress_items(items)
@@ -404,12 +408,12 @@ def run_batch_bench(args):
         "dtype": "f64 quantize, u32 codes, u8 rANS", "data": "synthetic (seeded)",
         "config": {"workload": "uneven-256 (N log-uniform 1e4..2e6; column/blobs/uniform; eb 1e-2/1e-3/1e-4 x range;"
                                " f32)", "frames": len(frames), "points": sum(n for _, n, _ in frames),
-                   "workers": args.workers, "timing": "host wall clock per pass, device synchronised on both sides",
+                   "workers": args.workers or 8, "timing": "host wall clock per pass, device synchronised on both sides",
                    "l2_flush": "inputs larger than L2 (whole collection > 1 GB)"},
         "sequential": {"value": round(gbs(t_seq), 3), "ms_per_step": round(t_seq * 1e3, 3), "gpu_launches": l_seq},
         "speedup_vs_sequential": round(t_seq / t_tun, 3), "gpu_launches": l_tun,
         "untuned": {"value": round(gbs(t_bat), 3), "ms_per_step": round(t_bat * 1e3, 3),
-                    "speedup_vs_sequential": round(t_seq / t_bat, 3), "workers": args.workers, "rans_max_steps": 1024,
+                    "speedup_vs_sequential": round(t_seq / t_bat, 3), "workers": args.workers or 8, "rans_max_steps": 1024,
                     "compressed_bytes": int(sum(lens_bat))},
         "tuned": {"rans_max_steps": tune["rans_max_steps"], "workers": tune["workers"],
                   "sample_frames": len(items[::8]), "sample_ms": round(tune["best_ms"], 3),
@@ -429,8 +433,10 @@ def run_serve_bench(args):
     30% float64; device-resident) through chain_server with `--workers` contexts and a
     40 GB admission budget.  First the capacity (all requests queued at once), then
     Poisson arrivals at 0.5, 0.8 and 0.95 of it; latency = queueing + service time as
-    stamped by the server.  Requests on the same pool frame share its output buffers
-    (the bench reads no results; tests/test_gpu_server.py checks them)."""
+    stamped by the server.  Every request writes its own output region: regions are cut
+    in submission order from a device ring large enough that a region is reused only
+    long after its previous user finished, and each run checks from the server's time
+    stamps that no two requests whose regions overlap were ever in service at once."""
     import threading
 
     import torch
@@ -455,33 +461,54 @@ def run_serve_bench(args):
         cont = torch.empty(ln, dtype=torch.uint8, device="cuda")
         codec.result_copy_to(cont.data_ptr(), ln)
         cap = N.compress_bound(n, 3)
-        cout = torch.empty(cap, dtype=torch.uint8, device="cuda")
-        dout = torch.empty(n * 3, dtype=torch.float64, device="cuda")
-        pool.append(dict(x=x, n=n, eb=eb, code=code, cont=cont, ln=ln, cout=cout, cap=cap, dout=dout,
-                         raw=n * 3 * pts.dtype.itemsize))
+        pool.append(dict(x=x, n=n, eb=eb, code=code, cont=cont, ln=ln, cap=cap, raw=n * 3 * pts.dtype.itemsize))
     codec.close()
     torch.cuda.synchronize()
     R = args.requests
     picks = rng.integers(0, len(pool), size=R)
     ops = rng.integers(0, 2, size=R)
-    items = []
-    for f, op in zip(picks, ops):
+    # output regions: consecutive, 256-byte aligned slices of one device ring
+    ring_bytes = 6 << 30
+    ring = torch.empty(ring_bytes, dtype=torch.uint8, device="cuda")
+    region = np.zeros((R, 2), np.int64)   # [offset, bytes]
+    lap = np.zeros(R, np.int64)            # how often the ring had wrapped before the request
+    off, laps = 0, 0
+    for i, (f, op) in enumerate(zip(picks, ops)):
         P = pool[int(f)]
+        need = (P["ln"] if op == 0 else P["n"] * 24) + 255 & ~255
+        if off + need > ring_bytes:
+            off, laps = 0, laps + 1
+        region[i] = (off, need)
+        lap[i] = laps
+        off += need
+    items = []
+    for i, (f, op) in enumerate(zip(picks, ops)):
+        P = pool[int(f)]
+        out_ptr = ring.data_ptr() + int(region[i, 0])
         if op == 0:
             items.append(N.BatchItem(input=P["x"].data_ptr(), dtype=P["code"], layout=N.CHAIN_SOA, n=P["n"], dims=3,
-                                     eb=P["eb"], p=4, threshold=2, output=P["cout"].data_ptr(),
-                                     output_capacity=P["cap"]))
+                                     eb=P["eb"], p=4, threshold=2, output=out_ptr, output_capacity=P["ln"]))
         else:
             items.append(N.BatchItem(input=P["cont"].data_ptr(), input_bytes=P["ln"], dtype=N.CHAIN_F64,
-                                     layout=N.CHAIN_AOS, output=P["dout"].data_ptr(), output_capacity=P["n"] * 24))
+                                     layout=N.CHAIN_AOS, output=out_ptr, output_capacity=P["n"] * 24))
+    # requests whose regions overlap, as (earlier, later) pairs: a region overlaps only
+    # regions of the previous lap of the ring (no region exceeds the ring)
+    overlaps = []
+    starts, ends = region[:, 0], region[:, 0] + region[:, 1]
+    by_lap = {int(k): np.nonzero(lap == k)[0] for k in np.unique(lap)}
+    for j in np.nonzero(lap > 0)[0]:
+        prev = by_lap[int(lap[j]) - 1]
+        hit = prev[(starts[prev] < ends[j]) & (starts[j] < ends[prev])]
+        overlaps.extend((int(i), int(j)) for i in hit)
     raw_total = sum(pool[int(f)]["raw"] for f in picks)
-    srv = N.Server(0, workers=args.workers, memory_budget_bytes=40 << 30)
+    srv = N.Server(0, workers=args.workers or 4, memory_budget_bytes=40 << 30)
 
     def run(arrivals):
         """Submit item i at t0 + arrivals[i] (seconds); returns (latencies ms, wall s)."""
         tickets = [None] * R
         lat = np.zeros(R)
         qs = np.zeros(R)
+        sub = np.zeros(R)
         failed = [0]
 
         def waiter():
@@ -503,11 +530,19 @@ def run_serve_bench(args):
                 if d <= 0:
                     break
                 time.sleep(min(d, 5e-4) if d > 1e-3 else 0)
+            sub[i] = time.perf_counter()
             tickets[i] = srv.submit(int(ops[i]), items[i])
         th.join()
         torch.cuda.synchronize()
         if failed[0]:
             raise RuntimeError(f"{failed[0]} of {R} requests failed")
+        # no two requests with overlapping output regions were in service together
+        # (start = submit + queueing, end = start + service; 50 us of stamp slack)
+        for i, j in overlaps:
+            end_i = sub[i] + lat[i] / 1e3
+            start_j = sub[j] + qs[j] / 1e3
+            if start_j < end_i + 5e-5:
+                raise RuntimeError(f"requests {i} and {j} shared output memory while both ran")
         run.queue = qs
         return lat, time.perf_counter() - t0
 
@@ -551,7 +586,7 @@ def run_serve_bench(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 quantize, u32 codes, u8 rANS", "data": "synthetic (seeded)",
         "config": {"workload": "serving mix: 48-frame pool, N log-uniform 1e3..8e6, 70% f32 / 30% f64, "
-                               "50% compress / 50% decompress", "requests": R, "workers": args.workers,
+                               "50% compress / 50% decompress", "requests": R, "workers": args.workers or 4,
                    "memory_budget_gb": 40, "timing": "server-stamped queueing + service time per request; "
                                                      "capacity = requests / wall time with all queued at once"},
         "capacity_gbs": round(raw_total / wall0 / 1e9, 3),
@@ -647,8 +682,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="blobs", choices=["blobs", "column", "trajectory", "batch", "serve"])
     ap.add_argument("--requests", type=int, default=20000, help="requests of the serving run (--config serve)")
-    ap.add_argument("--workers", type=int, default=8, help="contexts of the batch path (--config batch)")
+    ap.add_argument("--workers", type=int, default=0,
+                    help="contexts of the batch path (default 8) or of the request server (default 4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-system-forms", action="store_true",
+                    help="skip the batched and served runs that the default line reports beside the frame")
     ap.add_argument("--n", type=int, default=0,
                     help="particles of the blobs frame (default 16,777,216); smaller sizes are profiling cases")
     ap.add_argument("--once", action="store_true",
@@ -697,9 +735,29 @@ def main():
         import torch.distributed as tdist
 
         tdist.destroy_process_group()
+    if rank == 0 and world == 1 and args.config == "blobs" and not args.n and not args.no_system_forms \
+            and "CHAIN_BENCH_RANK_FN" not in os.environ:
+        line.update(_system_forms(args))
     if rank == 0:
         print(json.dumps(line))
     return 0
+
+
+def _system_forms(args):
+    """The batched and the served forms of the path (the same runs as --config batch and
+    --config serve), summarised beside the single-frame line."""
+    import copy
+
+    b_args = copy.copy(args)
+    b_args.steps, b_args.warmup = 5, 3
+    b = run_batch_bench(b_args)
+    s_args = copy.copy(args)
+    s = run_serve_bench(s_args)
+    return {
+        "batch": {k: b[k] for k in ("metric", "value", "unit", "ms_per_step", "speedup_vs_sequential", "sequential",
+                                    "untuned", "tuned", "decompress", "compressed_bytes", "config")},
+        "serve": {k: s[k] for k in ("metric", "value", "unit", "capacity_gbs", "isolated", "loads", "config")},
+    }
 
 
 def _rank_work():

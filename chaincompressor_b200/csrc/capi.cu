@@ -112,6 +112,7 @@ void chain_ctx_destroy(chain_ctx* ctx) {
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     ctx->frame.release();
+    ctx->keys.release();
     ctx->coded.release();
     ctx->dec.release();
     ctx->pinned.release();

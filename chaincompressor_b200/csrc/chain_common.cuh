@@ -218,4 +218,53 @@ __host__ __device__ inline void block_unkey(uint64_t k, int dims, int kb, uint32
         for (int d = 0; d < dims; ++d, ++pos) b[d] |= static_cast<uint32_t>((k >> pos) & 1u) << bit;
 }
 
+// Block keys of more than 64 bits (D * kb <= 128: for instance three dimensions of 22 to
+// 31 block-coordinate bits).  The same interleave: key bit (bit * D + d) = bit `bit` of
+// coordinate d.
+using u128 = unsigned __int128;
+__host__ __device__ inline int bitlen128(u128 v) {
+    const uint64_t hi = static_cast<uint64_t>(v >> 64);
+    return hi ? 64 + bitlen64(hi) : bitlen64(static_cast<uint64_t>(v));
+}
+__host__ __device__ inline u128 block_key128(const uint32_t* b, int dims, int kb) {
+    u128 k = 0;
+    for (int bit = kb - 1; bit >= 0; --bit)
+        for (int d = dims - 1; d >= 0; --d) k = (k << 1) | ((b[d] >> bit) & 1u);
+    return k;
+}
+__host__ __device__ inline void block_unkey128(u128 k, int dims, int kb, uint32_t* b) {
+    for (int d = 0; d < dims; ++d) b[d] = 0;
+    int pos = 0;
+    for (int bit = 0; bit < kb; ++bit)
+        for (int d = 0; d < dims; ++d, ++pos) b[d] |= static_cast<uint32_t>((k >> pos) & 1u) << bit;
+}
+
+// Key of block coordinates b and its inverse, for a key type of 32, 64 or 128 bits.
+template <typename KT>
+__host__ __device__ inline KT make_block_key(const uint32_t* b, int dims, int kb) {
+    if constexpr (sizeof(KT) == 16) return block_key128(b, dims, kb);
+    else return static_cast<KT>(block_key(b, dims, kb));
+}
+template <typename KT>
+__host__ __device__ inline void block_coords(KT k, int dims, int kb, uint32_t* b) {
+    if constexpr (sizeof(KT) == 16) block_unkey128(k, dims, kb, b);
+    else block_unkey(static_cast<uint64_t>(k), dims, kb, b);
+}
+template <typename KT>
+__host__ __device__ inline int key_bitlen(KT k) {
+    if constexpr (sizeof(KT) == 16) return bitlen128(k);
+    else return bitlen64(static_cast<uint64_t>(k));
+}
+
+// Read-only load of a key (the 128-bit type has no __ldg overload).
+template <typename KT>
+__device__ __forceinline__ KT ldg_key(const KT* p) {
+    if constexpr (sizeof(KT) == 16) {
+        const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p));
+        return (static_cast<u128>(v.y) << 64) | v.x;
+    } else {
+        return __ldg(p);
+    }
+}
+
 }  // namespace chain

@@ -138,6 +138,7 @@ struct chain_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     chain::Arena frame;    // per-frame working buffers (encoder)
+    chain::Arena keys;     // encoder block keys, sort buffers and record keys (sized once the key width is known)
     chain::Arena coded;    // encoder entropy/output buffers
     chain::Arena dec;      // decoder buffers
     chain::PinnedBuf pinned;

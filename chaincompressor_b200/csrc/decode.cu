@@ -31,16 +31,22 @@ struct DecState {
     DecodePlan plan;
 };
 
-__global__ void k_dec_init(DecState* st) {
-    if (threadIdx.x || blockIdx.x) return;
+__device__ void dec_init(DecState* st) {
     st->err = 0;
     st->zeros = 0;
     st->ndiff_seen = 0;
     for (int s = 0; s < kCodeStreams; ++s) { st->tag_bits[s] = 0; st->maxtag[s] = 0; }
 }
 
+__global__ void k_dec_init(DecState* st) {
+    if (threadIdx.x || blockIdx.x) return;
+    dec_init(st);
+}
+
+// Resets the state and parses a device-resident container (one thread).
 __global__ void k_parse(const uint8_t* data, uint64_t len, DecState* st) {
     if (threadIdx.x || blockIdx.x) return;
+    dec_init(st);
     parse_container(data, len, &st->plan);
 }
 
@@ -93,17 +99,15 @@ __global__ void __launch_bounds__(1024) k_section_setup(SectionRefs refs, const 
     }
 }
 
-// The rANS decoder's tables of every section (any grid; blockIdx.y = section): its
-// shared-memory image (layout at dec_image_bytes), or the packed global slot entries.
-// A slot's owner is found by binary search of the cumulative table.
-__global__ void __launch_bounds__(256) k_lookup(SectionRefs refs, const DecState* st) {
-    if (st->err) return;
-    const SectionRef R = refs.r[blockIdx.y];
+// The rANS decoder's tables of section R: its shared-memory image (layout at
+// dec_image_bytes), or the packed global slot entries.  A slot's owner is found by
+// binary search of the cumulative table.  Blocks bx of nbx cover the section.
+__device__ void section_lookup(const SectionRef& R, uint32_t bx, uint32_t nbx) {
     const SectionPlan& s = *R.sec;
     const uint32_t M = 1u << s.prec, A = s.alphabet;
     const bool bucketed = rans_dec_bucketed(s.prec, A);
     const bool smem_look = rans_dec_smem_look(s.prec, A);
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+    const uint32_t tid = bx * blockDim.x + threadIdx.x, nthreads = nbx * blockDim.x;
     uint16_t* owners = nullptr;
     if (bucketed) {
         uint32_t* cum = reinterpret_cast<uint32_t*>(R.image);
@@ -137,16 +141,17 @@ __global__ void __launch_bounds__(256) k_lookup(SectionRefs refs, const DecState
     }
 }
 
-// Unpacks the final lane states of every chunk (prec + 10 bits each, MSB-first).
-__global__ void __launch_bounds__(256) k_states(SectionRefs refs, const uint8_t* data, uint32_t* states_base) {
-    const SectionRef R = refs.r[blockIdx.y];
+// Unpacks the final lane states of section R's chunks (prec + 10 bits each, MSB-first);
+// blocks bx of nbx cover the section.
+__device__ void section_states(const SectionRef& R, const uint8_t* data, uint32_t* states_base, uint32_t bx,
+                               uint32_t nbx) {
     const SectionPlan& s = *R.sec;
     uint32_t* out = states_base + R.states_first;
     const uint64_t words = static_cast<uint64_t>(s.lanes) * s.chunks;
     const uint32_t B = state_bits(s.prec);   // <= 32
     const uint8_t* q = data + s.states_off;
-    for (uint64_t w = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < words;
-         w += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    for (uint64_t w = static_cast<uint64_t>(bx) * blockDim.x + threadIdx.x; w < words;
+         w += static_cast<uint64_t>(nbx) * blockDim.x) {
         // the state's B bits lie in the (at most five) bytes from its first bit's byte
         const uint64_t bit = w * B;
         const uint32_t off = static_cast<uint32_t>(bit & 7), nb = (off + B + 7) >> 3;
@@ -154,6 +159,20 @@ __global__ void __launch_bounds__(256) k_states(SectionRefs refs, const uint8_t*
         for (uint32_t i = 0; i < nb; ++i) acc = (acc << 8) | q[(bit >> 3) + i];
         out[w] = static_cast<uint32_t>((acc >> (8 * nb - off - B)) & ((1ull << B) - 1));
     }
+}
+
+// Tables (blockIdx.x < kLookupBlocks) and final lane states (the rest) of every section
+// (blockIdx.y = section), in one launch.
+constexpr uint32_t kLookupBlocks = 256, kStateBlocks = 64;
+__global__ void __launch_bounds__(256) k_lookup_states(SectionRefs refs, const DecState* st, const uint8_t* data,
+                                                        uint32_t* states_base) {
+    const SectionRef R = refs.r[blockIdx.y];
+    if (blockIdx.x >= kLookupBlocks) {
+        section_states(R, data, states_base, blockIdx.x - kLookupBlocks, kStateBlocks);
+        return;
+    }
+    if (st->err) return;
+    section_lookup(R, blockIdx.x, kLookupBlocks);
 }
 
 __device__ __forceinline__ uint64_t read_bits_msb(const uint8_t* bytes, uint64_t bit, int width) {
@@ -1093,7 +1112,6 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     const uint8_t* dcont = static_cast<const uint8_t*>(container);
     size_t base_need = host_in ? Arena::need(len + 16, 1) : 0;
     if (!host_in) {
-        k_dec_init<<<1, 1, 0, stream>>>(st); count_launch();
         k_parse<<<1, 1, 0, stream>>>(dcont, len, st); count_launch();
         CHAIN_LAUNCH_CHECK("parse");
         CHAIN_CUDA(cudaMemcpyAsync(&hs->plan, &st->plan, sizeof(DecodePlan), cudaMemcpyDeviceToHost, stream));
@@ -1232,8 +1250,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         CHAIN_CUDA(cudaFuncSetAttribute(k_section_setup, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(kParseSmem)));
         k_section_setup<<<nsec, 1024, kParseSmem, stream>>>(refs, dcont, st); count_launch();
-        k_lookup<<<dim3(256, nsec), 256, 0, stream>>>(refs, st); count_launch();
-        k_states<<<dim3(64, nsec), 256, 0, stream>>>(refs, dcont, states); count_launch();
+        k_lookup_states<<<dim3(kLookupBlocks + kStateBlocks, nsec), 256, 0, stream>>>(refs, st, dcont, states); count_launch();
         T.mark("tables", stream);
         rans_plan_smem(jobs, true);
         if (rans_dec_smem(jobs) > kRansDecSmemMax)

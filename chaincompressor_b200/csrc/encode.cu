@@ -220,7 +220,7 @@ __device__ void qparams(EncState* st) {
     st->kb = kb;
     st->key_bits = kb * static_cast<int>(st->dims);
     st->maxb_bits = bitlen32(bmax);
-    if (st->key_bits > 64) set_error(&st->err, kErrUnsupported);
+    if (st->key_bits > 128) set_error(&st->err, kErrUnsupported);
 }
 
 // lcps_cpp.cpp:1502-1523
@@ -353,7 +353,7 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
 #pragma unroll
                     for (int d = 0; d < 3; ++d)
                         b[d] = Q.coord(static_cast<double>(x[d][k]), d, (4 * g + k) * 3 + d, rel[3 * k + d]);
-                    keys[k] = static_cast<KT>(block_key(b, 3, kb));
+                    keys[k] = make_block_key<KT>(b, 3, kb);
                     if (hist) atomicAdd(&s_hist[static_cast<uint32_t>(keys[k]) & hmask], 1u);
                 }
                 if constexpr (sizeof(RT) == 4) {
@@ -371,6 +371,9 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
                 reinterpret_cast<uint4*>(idrel_zero)[g] = make_uint4(0, 0, 0, 0);
                 if constexpr (sizeof(KT) == 4) {
                     *reinterpret_cast<uint4*>(key_out + 4 * g) = make_uint4(keys[0], keys[1], keys[2], keys[3]);
+                } else if constexpr (sizeof(KT) == 16) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) key_out[4 * g + k] = keys[k];
                 } else {
                     ulonglong2* ko = reinterpret_cast<ulonglong2*>(key_out + 4 * g);
                     ko[0] = make_ulonglong2(keys[0], keys[1]);
@@ -390,7 +393,7 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
             b[d] = Q.coord(load_coord<FT, SOA>(p, n, D, i, d), d, i * D + d, r);
             rel_out[i * D + d] = static_cast<RT>(r);
         }
-        const KT key = static_cast<KT>(block_key(b, static_cast<int>(D), kb));
+        const KT key = make_block_key<KT>(b, static_cast<int>(D), kb);
         key_out[i] = key;
         idrel_zero[i] = 0;
         if (hist) atomicAdd(&s_hist[static_cast<uint32_t>(key) & hmask], 1u);
@@ -437,7 +440,10 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
         for (int u = 0; u < kU; ++u) {
             const uint64_t g = g0 + u * stride;
             if (4 * g + 4 <= n) {   // four positions by 16-byte loads (the arrays are 256-byte aligned)
-                if constexpr (sizeof(KT) == 4) {
+                if constexpr (sizeof(KT) == 16) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) keys[u][j] = ldg_key(skey + 4 * g + j);
+                } else if constexpr (sizeof(KT) == 4) {
                     const uint4 kv = __ldg(reinterpret_cast<const uint4*>(skey) + g);
                     keys[u][0] = kv.x; keys[u][1] = kv.y; keys[u][2] = kv.z; keys[u][3] = kv.w;
                 } else {
@@ -448,7 +454,7 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
                 const uint4 iv = __ldg(reinterpret_cast<const uint4*>(sidx) + g);
                 idxs[u][0] = iv.x; idxs[u][1] = iv.y; idxs[u][2] = iv.z; idxs[u][3] = iv.w;
                 const uint64_t k = 4 * g + 4;
-                keys[u][4] = k < n ? __ldg(skey + k) : KT(0);
+                keys[u][4] = k < n ? ldg_key(skey + k) : KT(0);
                 idxs[u][4] = k < n ? __ldg(sidx + k) : 0u;
             } else {
 #pragma unroll
@@ -471,7 +477,7 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
                     const uint32_t dist = idxs[u][j + 1] - idxs[u][j];
                     // bit j of block coordinate d sits at key bit j * D + d, so the widest
                     // coordinate of the block has ceil(bitlen(key) / D) bits
-                    const int local_bits = (bitlen64(static_cast<uint64_t>(keys[u][j])) + D - 1) / D;
+                    const int local_bits = (key_bitlen(keys[u][j]) + D - 1) / D;
                     const int tag_bits = bitlen32(static_cast<uint32_t>(local_bits));
                     const int64_t a = static_cast<int64_t>(local_bits) * D + tag_bits;
                     const int64_t smaller = a < c ? a : c;
@@ -555,14 +561,15 @@ struct ExplicitOut {
 };
 
 // Block coordinates of a record key (D dimensions of kb bits each).
-template <int DIM>
-__device__ __forceinline__ void rec_coords(uint64_t k, int D, int kb, uint32_t* b) {
-    if constexpr (DIM == 3) {
-        b[0] = compact3(k);
-        b[1] = compact3(k >> 1);
-        b[2] = compact3(k >> 2);
+template <int DIM, typename KT>
+__device__ __forceinline__ void rec_coords(KT k, int D, int kb, uint32_t* b) {
+    if constexpr (DIM == 3 && sizeof(KT) <= 8) {   // kb <= 21: the 3-D Morton compaction
+        const uint64_t k64 = static_cast<uint64_t>(k);
+        b[0] = compact3(k64);
+        b[1] = compact3(k64 >> 1);
+        b[2] = compact3(k64 >> 2);
     } else {
-        block_unkey(k, D, kb, b);
+        block_coords<KT>(k, D, kb, b);
     }
 }
 
@@ -598,21 +605,21 @@ __global__ void __launch_bounds__(256) k_l2_stats(const KT* __restrict__ rec, En
                 k[u][3] = static_cast<KT>(v.z); k[u][4] = static_cast<KT>(v.w);
             } else {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) k[u][1 + q] = g < ng && j0 + q < B ? __ldg(rec + j0 + q) : KT(0);
+                for (int q = 0; q < 4; ++q) k[u][1 + q] = g < ng && j0 + q < B ? ldg_key(rec + j0 + q) : KT(0);
             }
-            k[u][0] = g < ng && j0 ? __ldg(rec + j0 - 1) : KT(0);
+            k[u][0] = g < ng && j0 ? ldg_key(rec + j0 - 1) : KT(0);
         }
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
             const uint64_t g = g0 + u * nthreads;
             if (g >= ng) continue;
             uint32_t prev[KD], cur[KD];
-            rec_coords<DIM>(static_cast<uint64_t>(k[u][0]), D, kb, prev);
+            rec_coords<DIM>(k[u][0], D, kb, prev);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const uint64_t j = 4 * g + q;
                 if (j >= B) break;
-                rec_coords<DIM>(static_cast<uint64_t>(k[u][1 + q]), D, kb, cur);
+                rec_coords<DIM>(k[u][1 + q], D, kb, cur);
 #pragma unroll
                 for (int d = 0; d < KD; ++d) {
                     if (!DIM && d >= D) break;
@@ -697,9 +704,9 @@ __global__ void __launch_bounds__(256) k_l2_choice(const KT* __restrict__ rec, E
             k[u][3] = static_cast<KT>(v.z); k[u][4] = static_cast<KT>(v.w);
         } else {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) k[u][1 + q] = j0 + q < B ? __ldg(rec + j0 + q) : KT(0);
+            for (int q = 0; q < 4; ++q) k[u][1 + q] = j0 + q < B ? ldg_key(rec + j0 + q) : KT(0);
         }
-        k[u][0] = j0 && j0 - 1 < B ? __ldg(rec + j0 - 1) : KT(0);
+        k[u][0] = j0 && j0 - 1 < B ? ldg_key(rec + j0 - 1) : KT(0);
     }
 #pragma unroll
     for (int u = 0; u < kG; ++u) {
@@ -707,13 +714,13 @@ __global__ void __launch_bounds__(256) k_l2_choice(const KT* __restrict__ rec, E
         const uint64_t j0 = 4 * g;
         if (j0 >= B) continue;
         uint32_t prev[KD], cur[KD];
-        rec_coords<DIM>(static_cast<uint64_t>(k[u][0]), D, kb, prev);
+        rec_coords<DIM>(k[u][0], D, kb, prev);
         uint32_t ch[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const uint64_t j = j0 + q;
             if (j >= B) break;
-            rec_coords<DIM>(static_cast<uint64_t>(k[u][1 + q]), D, kb, cur);
+            rec_coords<DIM>(k[u][1 + q], D, kb, cur);
             ch[q] = (l2 && j > 0) ? l2_rule(cur, prev, D, fvb, fdb) : 0u;
             cnt += ch[q];
 #pragma unroll
@@ -756,7 +763,7 @@ struct Level2Out {
         const int kb = st->kb;
         constexpr int KD = DIM ? DIM : kMaxDims;
         uint32_t cur[KD];
-        rec_coords<DIM>(static_cast<uint64_t>(rec[j]), D, kb, cur);
+        rec_coords<DIM>(rec[j], D, kb, cur);
         if (!use_diff) {
             const uint64_t k = j - drank;
 #pragma unroll
@@ -765,7 +772,7 @@ struct Level2Out {
             return;
         }
         uint32_t prev[KD];
-        rec_coords<DIM>(static_cast<uint64_t>(rec[j - 1]), D, kb, prev);
+        rec_coords<DIM>(rec[j - 1], D, kb, prev);
 #pragma unroll
         for (int d = 0; d < KD; ++d) {
             if (!DIM && d >= D) break;
@@ -1646,7 +1653,7 @@ static chain_status status_from_err(uint32_t err) {
     if (err & kErrQuantOverflow) return set_err(CHAIN_ERR_QUANT_OVERFLOW, "quantized coordinate does not fit int64");
     if (err & kErrUnsupported)
         return set_err(CHAIN_ERR_UNSUPPORTED,
-                       "quantized coordinates need more than 31 bits or block keys more than 64 bits "
+                       "quantized coordinates need more than 31 bits or block keys more than 128 bits "
                        "(eb too small relative to the coordinate range for this build)");
     if (err & kErrCapacity) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "device buffer capacity exceeded");
     return set_err(CHAIN_ERR_DEVICE, "internal encoder error (flags " + std::to_string(err) + ")");
@@ -1724,16 +1731,32 @@ static void launch_quantize(const void* pts, uint64_t n, uint32_t D, EncState* s
 
 // The quantizer for a run-time input type, layout, key width and offset width.
 template <typename FT, bool SOA>
-static void launch_quantize_rt(bool wide, uint32_t rel_esz, const void* pts, uint64_t n, uint32_t D, EncState* st,
+static void launch_quantize_rt(size_t ksz, uint32_t rel_esz, const void* pts, uint64_t n, uint32_t D, EncState* st,
                                void* key, void* rel, uint64_t* cidx, double* cval, uint64_t cap, uint32_t* hist,
                                int hist_bits, uint32_t* idrel, cudaStream_t s) {
-    if (wide) {
+    if (ksz == 16) {
+        if (rel_esz == 1) launch_quantize<FT, SOA, u128, uint8_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, idrel, s);
+        else launch_quantize<FT, SOA, u128, uint32_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, idrel, s);
+    } else if (ksz == 8) {
         if (rel_esz == 1) launch_quantize<FT, SOA, uint64_t, uint8_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, idrel, s);
         else launch_quantize<FT, SOA, uint64_t, uint32_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, idrel, s);
     } else {
         if (rel_esz == 1) launch_quantize<FT, SOA, uint32_t, uint8_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, idrel, s);
         else launch_quantize<FT, SOA, uint32_t, uint32_t>(pts, n, D, st, key, rel, cidx, cval, cap, hist, hist_bits, idrel, s);
     }
+}
+
+// Stable sort of the block keys (KT each, index order) and the level-1 links from the
+// sorted neighbours.
+template <typename KT, typename Hook>
+static void sort_and_link(void* key_idx, void* key_a, void* key_b, uint32_t* val_a, uint32_t* val_b, uint64_t n,
+                          int key_bits, uint32_t* counts, EncState* st, uint32_t* idrel, uint32_t* hist,
+                          cudaStream_t stream, const Hook& marks) {
+    KT* ka = static_cast<KT*>(key_a);
+    KT* kb = static_cast<KT*>(key_b);
+    const bool in_b = radix_sort_pairs<KT>(static_cast<const KT*>(key_idx), ka, val_a, kb, val_b, n, key_bits, counts,
+                                           stream, marks, true);
+    k_level1<KT><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel, hist); count_launch();
 }
 
 // Explicit records (keys of the points with idrel == 0, index order) and level 2: record
@@ -1807,12 +1830,10 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     const bool host_input = !is_device_ptr(points);
     if (host_input) need += Arena::need(nd, esz);
     const uint64_t nsort = std::max<uint64_t>(n, corr_cap);
-    need += Arena::need(n, 8) + Arena::need(nsort, 8) * 2;  // keys (index order), sort ping-pong
-    need += Arena::need(nsort, 4) * 2;                      // sort values ping-pong
+    need += Arena::need(nsort, 4) * 2;                      // sort values ping-pong (keys: ctx->keys)
     need += Arena::need(sort_counts, 4);
     need += Arena::need(scan_scratch_bytes(std::max<uint64_t>(sort_counts, nd)), 1);
     need += Arena::need(nd, 4) * 3;           // rel, keep, diff
-    need += Arena::need(std::max<uint64_t>(nd * 4, n * 8), 1);   // record keys
     need += Arena::need(n, 4) * 2;            // idrel, choice2
     need += Arena::need(corr_cap, 8) * 4;     // corrections idx/val + sorted copies
     need += Arena::need(hist_stride * kCodeStreams, 4) * 3;  // hist, prob, cum
@@ -1830,15 +1851,11 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
         pts = d;
         T.mark("h2d_points", stream);
     }
-    uint64_t* key_idx = A.take<uint64_t>(n);
-    uint64_t* key_a = A.take<uint64_t>(nsort);
-    uint64_t* key_b = A.take<uint64_t>(nsort);
     uint32_t* val_a = A.take<uint32_t>(nsort);
     uint32_t* val_b = A.take<uint32_t>(nsort);
     uint32_t* counts = A.take<uint32_t>(sort_counts);
     uint64_t* scanbuf = reinterpret_cast<uint64_t*>(A.take<uint8_t>(scan_scratch_bytes(std::max<uint64_t>(sort_counts, nd))));
     void* rel = A.take<uint8_t>(nd * rel_esz);
-    void* rec = A.take<uint8_t>(std::max<uint64_t>(nd * 4, n * 8));   // record keys (KT each)
     void* keep = A.take<uint32_t>(nd);
     void* diff = A.take<uint32_t>(nd);
     uint32_t* idrel = A.take<uint32_t>(n);
@@ -1875,15 +1892,25 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     if (hs->err) return status_from_err(hs->err);
     const int key_bits = hs->key_bits;
     const bool wide = key_bits > 32;
+    // block keys of 4, 8 or 16 bytes: the index-order keys, the sort's ping-pong keys
+    // (which the exact-correction sort reuses with 8-byte keys) and the record keys
+    const size_t ksz = key_bits > 64 ? 16 : (key_bits > 32 ? 8 : 4);
+    const uint64_t kab = std::max<uint64_t>(n * ksz, corr_cap * 8);
+    CHAIN_CUDA(ctx->keys.reserve(Arena::need(n * ksz, 1) * 2 + Arena::need(kab, 1) * 2));
+    uint8_t* key_idx = ctx->keys.take<uint8_t>(n * ksz);
+    uint8_t* key_a = ctx->keys.take<uint8_t>(kab);
+    uint8_t* key_b = ctx->keys.take<uint8_t>(kab);
+    uint8_t* rec = ctx->keys.take<uint8_t>(n * ksz);
+    if (!rec) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder key arena too small");
     // keep rows hold block coordinates (< 2^kb), diff rows ZigZag'd wrapped differences
     // (<= the record range <= 2^kb): the narrowest width that holds kb + 1 bits
     const uint32_t kd_esz = hs->kb + 1 <= 8 ? 1u : (hs->kb + 1 <= 16 ? 2u : 4u);
 
     // ---- phase 2: quantize, sort, level 1, level 2, statistics, plan
     // the quantizer counts the first sort pass's digits (when a sort follows)
-    const RadixPlan plan = radix_plan(key_bits);
+    const RadixPlan plan = radix_plan(key_bits, static_cast<int>(ksz));
     uint32_t* hist0 = l1 ? counts : nullptr;
-#define CHAIN_Q(FT, SOA_) launch_quantize_rt<FT, SOA_>(wide, rel_esz, pts, n, dims, st, key_idx, rel, corr_idx, corr_val, corr_cap, hist0, plan.bits, idrel, stream)
+#define CHAIN_Q(FT, SOA_) launch_quantize_rt<FT, SOA_>(ksz, rel_esz, pts, n, dims, st, key_idx, rel, corr_idx, corr_val, corr_cap, hist0, plan.bits, idrel, stream)
     if (dtype == CHAIN_F32) {
         if (soa) CHAIN_Q(float, true); else CHAIN_Q(float, false);
     } else {
@@ -1896,29 +1923,29 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     if (l1) {   // idrel was zeroed by the quantizer; k_level1 writes the links only
         // stage marks around every scatter pass; the key width is in the name
         const auto sort_marks = [&](bool after) {
-            T.mark(after ? (wide ? "sort_scatter_k64" : "sort_scatter_k32") : "sort_hist_scan", stream);
+            T.mark(after ? (ksz == 16 ? "sort_scatter_k128" : (wide ? "sort_scatter_k64" : "sort_scatter_k32"))
+                         : "sort_hist_scan",
+                   stream);
         };
-        if (wide) {
-            const bool in_b = radix_sort_pairs<uint64_t>(key_idx, key_a, val_a, key_b, val_b, n, key_bits, counts,
-                                                         stream, sort_marks, true);
-            k_level1<uint64_t><<<grid_for(n), 256, 0, stream>>>(in_b ? key_b : key_a, in_b ? val_b : val_a, n, st, idrel,
-                                                               hist); count_launch();
-        } else {
-            uint32_t* k32 = reinterpret_cast<uint32_t*>(key_idx);
-            uint32_t* ka = reinterpret_cast<uint32_t*>(key_a);
-            uint32_t* kb = reinterpret_cast<uint32_t*>(key_b);
-            const bool in_b = radix_sort_pairs<uint32_t>(k32, ka, val_a, kb, val_b, n, key_bits, counts, stream,
-                                                         sort_marks, true);
-            k_level1<uint32_t><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel,
-                                                               hist); count_launch();
-        }
+        if (ksz == 16)
+            sort_and_link<u128>(key_idx, key_a, key_b, val_a, val_b, n, key_bits, counts, st, idrel, hist, stream, sort_marks);
+        else if (ksz == 8)
+            sort_and_link<uint64_t>(key_idx, key_a, key_b, val_a, val_b, n, key_bits, counts, st, idrel, hist, stream,
+                                    sort_marks);
+        else
+            sort_and_link<uint32_t>(key_idx, key_a, key_b, val_a, val_b, n, key_bits, counts, st, idrel, hist, stream,
+                                    sort_marks);
     }
     CHAIN_LAUNCH_CHECK("level 1");
     T.mark("level1", stream);
     uint32_t* scan32 = reinterpret_cast<uint32_t*>(scanbuf);
     const bool d3 = dims == 3 && hs->kb <= 21;
-    if (wide)
-        run_level2<uint64_t>(key_idx, idrel, rec, n, st, l2, d3, kd_esz, choice2, keep, diff, scan32, T, stream);
+    if (ksz == 16)
+        run_level2<u128>(reinterpret_cast<const u128*>(key_idx), idrel, rec, n, st, l2, d3, kd_esz, choice2, keep, diff,
+                         scan32, T, stream);
+    else if (ksz == 8)
+        run_level2<uint64_t>(reinterpret_cast<const uint64_t*>(key_idx), idrel, rec, n, st, l2, d3, kd_esz, choice2, keep,
+                             diff, scan32, T, stream);
     else
         run_level2<uint32_t>(reinterpret_cast<const uint32_t*>(key_idx), idrel, rec, n, st, l2, d3, kd_esz, choice2, keep,
                              diff, scan32, T, stream);
@@ -1960,16 +1987,18 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
         const uint64_t nc = hs->ncorr;
         const int bits = std::max(1, bitlen64(nd - 1));
         uint32_t* scan32b = reinterpret_cast<uint32_t*>(scanbuf);
+        uint64_t* ca = reinterpret_cast<uint64_t*>(key_a);   // room for corr_cap 8-byte keys
+        uint64_t* cb = reinterpret_cast<uint64_t*>(key_b);
         // flat indices are unique, and equal values need no order for the dictionary,
         // so the small unstable sort serves both sorts here
-        bool in_b = sort_pairs<uint64_t>(corr_idx, key_a, val_a, key_b, val_b, nc, bits, counts, stream);
-        k_gather_corrections<<<grid_for(nc), 256, 0, stream>>>(in_b ? val_b : val_a, in_b ? key_b : key_a, corr_val,
+        bool in_b = sort_pairs<uint64_t>(corr_idx, ca, val_a, cb, val_b, nc, bits, counts, stream);
+        k_gather_corrections<<<grid_for(nc), 256, 0, stream>>>(in_b ? val_b : val_a, in_b ? cb : ca, corr_val,
                                                                corr_idx_s, corr_val_s, nc); count_launch();
         k_corr_gaps<<<grid_for(nc), 256, 0, stream>>>(corr_idx_s, nc, corr_gaps); count_launch();
         const uint64_t* vbits = reinterpret_cast<const uint64_t*>(corr_val_s);
-        in_b = sort_pairs<uint64_t>(vbits, key_a, val_a, key_b, val_b, nc, 64, counts, stream);
-        device_exclusive_scan<uint32_t>(DictIn{in_b ? key_b : key_a},
-                                        DictOut{in_b ? key_b : key_a, in_b ? val_b : val_a, corr_dict, corr_ids}, nc,
+        in_b = sort_pairs<uint64_t>(vbits, ca, val_a, cb, val_b, nc, 64, counts, stream);
+        device_exclusive_scan<uint32_t>(DictIn{in_b ? cb : ca},
+                                        DictOut{in_b ? cb : ca, in_b ? val_b : val_a, corr_dict, corr_ids}, nc,
                                         scan32b, &st->ndistinct, stream);
         refs.s[kCorrGaps].count_const = nc;
         refs.s[kCorrIds].count_const = nc;

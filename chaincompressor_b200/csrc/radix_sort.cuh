@@ -29,20 +29,22 @@ constexpr int kSortMaxBits = 8;
 
 template <typename KT>
 struct SortShape {
-    static constexpr int kItems = sizeof(KT) > 4 ? 8 : 12;
+    static constexpr int kItems = sizeof(KT) == 4 ? 12 : (sizeof(KT) == 8 ? 8 : 4);   // 16-byte keys: 4
     static constexpr int kTile = kSortThreads * kItems;
 };
 
 // Passes and digit width for a key of key_bits bits: as few passes of at most 8 bits
-// as cover it, all of the same width (at least one pass: it yields the identity).
+// as cover it, all of the same width (at least one pass: it yields the identity).  Keys
+// stored in 8 or 16 bytes (key_sz) always take 8-bit digits.
 struct RadixPlan {
     int passes;
     int bits;
 };
-inline RadixPlan radix_plan(int key_bits) {
+inline RadixPlan radix_plan(int key_bits, int key_sz = 4) {
     RadixPlan r;
     r.passes = key_bits <= 0 ? 1 : (key_bits + kSortMaxBits - 1) / kSortMaxBits;
     r.bits = key_bits <= 0 ? 1 : (key_bits + r.passes - 1) / r.passes;
+    if (key_sz > 4) r.bits = kSortMaxBits;
     return r;
 }
 
@@ -63,7 +65,7 @@ radix_hist_kernel(const KT* __restrict__ keys, uint64_t n, int shift, int bits, 
 #pragma unroll
     for (int r = 0; r < I; ++r) {
         const uint32_t i = r * kSortThreads + threadIdx.x;
-        k[r] = i < rem ? __ldg(keys + base + i) : KT(0);
+        k[r] = i < rem ? ldg_key(keys + base + i) : KT(0);
     }
 #pragma unroll
     for (int r = 0; r < I; ++r)
@@ -233,10 +235,10 @@ inline uint32_t radix_tiles(uint64_t n) {
     return static_cast<uint32_t>((n + SortShape<KT>::kTile - 1) / SortShape<KT>::kTile);
 }
 
-// Count-table entries radix_sort_pairs needs for n keys of either key width (the digit
-// rows, then the rows' totals).
+// Count-table entries radix_sort_pairs needs for n keys of any key width (the digit
+// rows, then the rows' totals; 16-byte keys have the smallest tiles).
 inline size_t radix_counts_elems(uint64_t n) {
-    return static_cast<size_t>(radix_tiles<uint32_t>(n) + radix_tiles<uint64_t>(n)) * kSortBins + kSortBins;
+    return static_cast<size_t>(radix_tiles<u128>(n)) * kSortBins + kSortBins;
 }
 
 // The scatter for a run-time digit width (instantiated per width, so that the ranking
@@ -248,15 +250,19 @@ inline void launch_radix_scatter(int bits, uint32_t tiles, cudaStream_t stream, 
 #define CHAIN_SCATTER(B)                                                                                          \
     radix_scatter_kernel<KT, B><<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, shift, counts, row_total, \
                                                                     tiles)
-    switch (bits) {
-        case 1: CHAIN_SCATTER(1); break;
-        case 2: CHAIN_SCATTER(2); break;
-        case 3: CHAIN_SCATTER(3); break;
-        case 4: CHAIN_SCATTER(4); break;
-        case 5: CHAIN_SCATTER(5); break;
-        case 6: CHAIN_SCATTER(6); break;
-        case 7: CHAIN_SCATTER(7); break;
-        default: CHAIN_SCATTER(8); break;
+    if constexpr (sizeof(KT) > 4) {   // always 8-bit digits (radix_plan)
+        CHAIN_SCATTER(8);
+    } else {
+        switch (bits) {
+            case 1: CHAIN_SCATTER(1); break;
+            case 2: CHAIN_SCATTER(2); break;
+            case 3: CHAIN_SCATTER(3); break;
+            case 4: CHAIN_SCATTER(4); break;
+            case 5: CHAIN_SCATTER(5); break;
+            case 6: CHAIN_SCATTER(6); break;
+            case 7: CHAIN_SCATTER(7); break;
+            default: CHAIN_SCATTER(8); break;
+        }
     }
 #undef CHAIN_SCATTER
     count_launch();
@@ -277,7 +283,7 @@ bool radix_sort_pairs(const KT* keys_in, KT* keys_a, uint32_t* vals_a, KT* keys_
                       int key_bits, uint32_t* counts, cudaStream_t stream, const Hook& hook = Hook(),
                       bool first_counts_ready = false) {
     const uint32_t tiles = radix_tiles<KT>(n);
-    const RadixPlan plan = radix_plan(key_bits);
+    const RadixPlan plan = radix_plan(key_bits, sizeof(KT));
     uint32_t* row_total = counts + static_cast<size_t>(tiles) * kSortBins;
     for (int p = 0; p < plan.passes; ++p) {
         const int shift = plan.bits * p;

@@ -86,6 +86,14 @@ def case(name):
         pts[: 1 << 19] = 1.0
         pts[-1] = 0.0
         return pts, 0.1, 4, 2, {}
+    if name == "wide_key":
+        # three dimensions of 25 block-coordinate bits (p = 1): 75-bit block keys; 2,000
+        # distinct blocks of about 30 points each, shuffled, so level 1 still chains
+        rng = np.random.default_rng(16)
+        blocks = rng.integers(0, 1 << 25, size=(2000, 3)).astype(np.float64)
+        pts = blocks[rng.integers(0, 2000, size=60_000)] + 0.5
+        pts[0] = 0.5
+        return pts, 0.5, 1, 2, {}
     if name == "negative_zero":
         pts = np.array([[0.0, -0.0], [-0.0, 0.0], [1.0, 2.0], [0.5, -0.0]], np.float64)
         return pts, 0.05, 2, 0, {}
@@ -94,4 +102,4 @@ def case(name):
 
 GPU_CASES = ["column", "column_qb11", "blobs200k", "blobs_clipped", "traj_f64_e4_p1", "traj_f64_e2",
              "uniform_p64_t25", "single_point", "one_block", "long_chain", "p1_big_threshold", "neg_threshold", "dims1", "dims2",
-             "dims4", "no_l1", "no_l2", "no_bl", "big_values_tagged", "wide_jump", "negative_zero", "many_corrections"]
+             "dims4", "no_l1", "no_l2", "no_bl", "big_values_tagged", "wide_jump", "negative_zero", "many_corrections", "wide_key"]
