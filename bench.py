@@ -256,6 +256,15 @@ def run_ours(args, rank: int, world: int):
     rans_syms = sum(c["section"]["symbols"] for c in info["components"].values() if "section" in c)
     rans_bytes = sum(c["section"]["payload"] + c["section"]["state_bytes"] + 4 * c["section"]["chunks"]
                      for c in info["components"].values() if "section" in c)
+    # bytes of the symbols the encoder reads: the library stores each stream no wider than
+    # its values (rel: one byte when p <= 256; choice2: one; keep / diff: the narrowest of
+    # 1, 2, 4 bytes holding kb + 1 bits, kb = bits of the largest block coordinate, which
+    # the container's wrap maximum equals); tags and idrel are four bytes
+    kb = int(info["wrap"][1]).bit_length()
+    kd = 1 if kb + 1 <= 8 else (2 if kb + 1 <= 16 else 4)
+    width = {"IDR0": 4, "DIF0": kd, "KEP0": kd, "CH20": 1, "REL0": 1 if info["p"] <= 256 else 4}
+    rans_sym_bytes = sum(c["section"]["symbols"] * (4 if c["enc"] == "tagged" else width[name])
+                         for name, c in info["components"].items() if "section" in c)
     peaks, src = _peaks()
     peak = float(peaks["hbm_gbs"])
 
@@ -294,7 +303,7 @@ def run_ours(args, rank: int, world: int):
         "e2e": {"value": round(gbs(t_ce), 3), "unit": UNIT, "h2d_bytes_per_step": raw, "d2h_bytes_per_step": clen},
         "gpu_launches": launches_c, "gpu_launches_per_step": launches_c // max(1, args.steps),
         "roofline": scatter_roof,
-        "roofline_rans_encode": roof("rans_encode_kernel", stages_c.get("rans_encode"), 4 * rans_syms + rans_bytes),
+        "roofline_rans_encode": roof("rans_encode_kernel", stages_c.get("rans_encode"), rans_sym_bytes + rans_bytes),
         "decompress": {"value": round(gbs(t_d), 3), "unit": UNIT, "ms_per_step": round(t_d * 1e3, 4),
                        "gpu_launches": launches_d,
                        "e2e": {"value": round(gbs(t_de), 3), "unit": UNIT, "h2d_bytes_per_step": clen,
@@ -548,14 +557,14 @@ def run_serve_bench(args):
 
     run(np.zeros(R))   # warm-up: the resident arenas reach their sizes
     # isolated latency of every (pool frame, operation): the request served alone on the
-    # idle server, median of three
+    # idle server, median of five
     iso_tab = np.zeros((len(pool), 2))
     first = {}
     for i, (f, op) in enumerate(zip(picks, ops)):
         first.setdefault((int(f), int(op)), i)
     for (f, op), i in first.items():
         ts = []
-        for _ in range(3):
+        for _ in range(5):
             st, q, s, _ = srv.wait(srv.submit(op, items[i]), check=True)
             ts.append(q + s)
         iso_tab[f, op] = float(np.median(ts))
@@ -593,7 +602,7 @@ def run_serve_bench(args):
         "saturated": {"p50_ms": round(float(np.percentile(lat0, 50)), 3),
                       "p99_ms": round(float(np.percentile(lat0, 99)), 3)},
         "isolated": {"p50_ms": round(float(np.percentile(iso, 50)), 3), "p99_ms": round(float(np.percentile(iso, 99)), 3),
-                     "note": "each request's latency served alone on the idle server (median of 3), over the "
+                     "note": "each request's latency served alone on the idle server (median of 5), over the "
                              "same request mix; slowdown = served latency / isolated latency per request"},
         "loads": loads,
     }

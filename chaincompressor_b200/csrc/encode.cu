@@ -405,6 +405,32 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
     }
 }
 
+// Eight 16-bit counters packed into two 64-bit registers (bins 0..3 and 4..7), for the
+// hot small values of a stream; flushed into shared memory at the end.
+struct PackedCount8 {
+    uint64_t lo = 0, hi = 0;
+    __device__ __forceinline__ void add(uint32_t v) {   // v < 8
+        const uint64_t inc = 1ull << ((v & 3u) << 4);
+        if (v & 4u) hi += inc;
+        else lo += inc;
+    }
+    // Warp-sums the counters and adds them to bins[0..7] (lane 0).
+    __device__ __forceinline__ void flush(uint32_t* bins) {
+        uint32_t c[8];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            c[k] = static_cast<uint32_t>(lo >> (16 * k)) & 0xffffu;
+            c[4 + k] = static_cast<uint32_t>(hi >> (16 * k)) & 0xffffu;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t t = warp_sum(c[k]);
+            if ((threadIdx.x & 31) == 0 && t) atomicAdd(&bins[k], t);
+        }
+        lo = hi = 0;
+    }
+};
+
 // ------------------------------------------------------------------- level 1
 // Sorted position k: the sorted neighbour with an equal key is the next point of the
 // same block (stable sort keeps indices increasing within a block).  Each thread takes
@@ -426,6 +452,9 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
     __syncthreads();
     uint32_t links = 0, lmin = 0xffffffffu, lmax = 0;
     unsigned long long lbits = 0;
+    // the common short links (distance < 8, tag < 8) count in registers, not in
+    // contended shared-memory bins
+    PackedCount8 vc, tc;
     const int D = static_cast<int>(st->dims);
     const int64_t maxb_bits = st->maxb_bits;
     const int64_t thr = st->threshold;
@@ -491,13 +520,19 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
                     lmax = out > lmax ? out : lmax;
                     const uint32_t tag = bitlen32(out);   // >= 1
                     lbits += tag;
-                    atomicAdd(&stag[tag], 1u);
-                    if (out < kSmallBins) atomicAdd(&sh[out], 1u);
+                    if (tag < 8) tc.add(tag);
+                    else atomicAdd(&stag[tag], 1u);
+                    if (out < 8) vc.add(out);
+                    else if (out < kSmallBins) atomicAdd(&sh[out], 1u);
                     else if (out < kRansMaxAlphabet) atomicAdd(&gh[out], 1u);
                 }
             }
         }
     }
+    // 16-bit counters: a thread handles at most ceil(n / 4 / threads) groups of four
+    // positions, far below 65536 links per thread for any launch of this kernel
+    vc.flush(sh);
+    tc.flush(stag);
     links = warp_sum(links);
     lbits = warp_sum(lbits);
     lmin = warp_min(lmin);
@@ -818,32 +853,6 @@ __device__ __forceinline__ void warp_hist_add(uint32_t* bins, uint32_t v, bool v
     const uint32_t peers = __match_any_sync(active, v);
     if ((peers & lanemask_lt()) == 0) atomicAdd(&bins[v], static_cast<uint32_t>(__popc(peers)));
 }
-
-// Eight 16-bit counters packed into two 64-bit registers (bins 0..3 and 4..7), for the
-// hot small values of a stream; flushed into shared memory at the end.
-struct PackedCount8 {
-    uint64_t lo = 0, hi = 0;
-    __device__ __forceinline__ void add(uint32_t v) {   // v < 8
-        const uint64_t inc = 1ull << ((v & 3u) << 4);
-        if (v & 4u) hi += inc;
-        else lo += inc;
-    }
-    // Warp-sums the counters and adds them to bins[0..7] (lane 0).
-    __device__ __forceinline__ void flush(uint32_t* bins) {
-        uint32_t c[8];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            c[k] = static_cast<uint32_t>(lo >> (16 * k)) & 0xffffu;
-            c[4 + k] = static_cast<uint32_t>(hi >> (16 * k)) & 0xffffu;
-        }
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const uint32_t t = warp_sum(c[k]);
-            if ((threadIdx.x & 31) == 0 && t) atomicAdd(&bins[k], t);
-        }
-        lo = hi = 0;
-    }
-};
 
 constexpr int kSmemHistBins = 4096;
 
@@ -1286,13 +1295,23 @@ __global__ void k_words_to_bytes(uint32_t* words, uint64_t nwords) {
         words[w] = __byte_perm(words[w], 0, 0x0123);
 }
 
-// Serialises every chosen table (one CTA per stream) and writes the stream's encoder
-// symbol entries (make_enc_symbol) for its rANS section.
+// Serialises every chosen table (blockIdx.y == 0, one CTA per stream) and writes the
+// streams' encoder symbol entries (make_enc_symbol) for their rANS sections (blockIdx.y
+// > 0: kEtabSlices CTAs per stream, each a slice of the alphabet).
 __global__ void __launch_bounds__(1024) k_serialize_tables(EncState* st, const uint32_t* prob, const uint32_t* tag_prob,
                                                             uint64_t hist_stride, uint8_t* out, uint64_t out_stride,
                                                             RansJobs J, StreamJobs sj) {
     extern __shared__ __align__(16) uint32_t ser_stage[];   // kSerStageSyms u32
     const int s = blockIdx.x;
+    if (blockIdx.y > 0) {
+        if (sj.job[s] < 0) return;
+        const RansJob& jb = J.job[sj.job[s]];
+        uint4* et = const_cast<uint4*>(jb.etab);
+        for (uint32_t a = (blockIdx.y - 1) * blockDim.x + threadIdx.x; a < jb.alphabet;
+             a += (gridDim.y - 1) * blockDim.x)
+            et[a] = make_enc_symbol(jb.prob[a], jb.cum[a], jb.prec);
+        return;
+    }
     StreamChoice& c = st->ch[s];
     uint32_t len = 0;
     if (c.enc == kEncRaw)
@@ -1300,13 +1319,8 @@ __global__ void __launch_bounds__(1024) k_serialize_tables(EncState* st, const u
     else if (c.enc == kEncTagged)
         len = serialize_table_block(tag_prob + 64 * s, c.sec_alphabet, out + out_stride * s, ser_stage);
     if (threadIdx.x == 0) c.table_len = len;
-    if (sj.job[s] >= 0) {
-        const RansJob& jb = J.job[sj.job[s]];
-        uint4* et = const_cast<uint4*>(jb.etab);
-        for (uint32_t a = threadIdx.x; a < jb.alphabet; a += blockDim.x)
-            et[a] = make_enc_symbol(jb.prob[a], jb.cum[a], jb.prec);
-    }
 }
+constexpr unsigned kEtabSlices = 8;
 
 // --------------------------------------------------------------- assembly
 struct AssemblyIn {
@@ -2190,7 +2204,7 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     T.mark("corrections+packing", stream);
     CHAIN_CUDA(cudaFuncSetAttribute(k_serialize_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(4 * kSerStageSyms)));
-    k_serialize_tables<<<kCodeStreams, 1024, 4 * kSerStageSyms, stream>>>(st, prob, tag_prob, hist_stride, tables,
+    k_serialize_tables<<<dim3(kCodeStreams, 1 + kEtabSlices), 1024, 4 * kSerStageSyms, stream>>>(st, prob, tag_prob, hist_stride, tables,
                                                                           table_stride, jobs, stream_jobs); count_launch();
     T.mark("serialize_tables", stream);
     if (jobs.total_blocks) {
