@@ -441,7 +441,7 @@ template <typename KT>
 __global__ void __launch_bounds__(256, sizeof(KT) == 4 ? 4 : 3)   // 64-bit keys spill at four CTAs per SM
 k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_t n, EncState* st,
          uint32_t* __restrict__ idrel, uint32_t* __restrict__ gh) {
-    // IDR0 statistics of the links (the zeros are added by k_idrel_stats)
+    // IDR0 statistics of the links (idrel_stats adds the zeros)
     constexpr uint32_t kSmallBins = 256;
     __shared__ uint32_t sh[kSmallBins], stag[34];
     __shared__ unsigned long long s_links, s_bits;
@@ -862,7 +862,8 @@ __device__ void choice_stats(EncState* st, uint32_t* gh);
 // Per-stream statistics in one pass: per-dimension min/max, overall max, the record
 // tags (max(1, max_d bitlen v)) histogram and bit total, and the value histogram of
 // the raw candidate (values < 2^18; a larger max makes the candidate ineligible).
-// Template DIM is the records' dimension count (0 = read it at run time).  Each thread
+// Template DIM is the records' dimension count (0 = read it at run time; the encoder
+// launches it for streams of more than four dimensions).  Each thread
 // takes groups of 4 records with 16-byte loads; values below 8 count in registers,
 // below kSmemHistBins in shared memory, the rest in global memory.  Register
 // counters flush before they could overflow.  blockIdx.y selects the stream from
@@ -996,6 +997,187 @@ __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState*
     if (threadIdx.x == 0 && sbits) atomicAdd(reinterpret_cast<unsigned long long*>(&gs.tag_bits), sbits);
     for (int t = threadIdx.x; t < HB; t += blockDim.x)
         if (sh[t]) atomicAdd(&gh[t], sh[t]);
+}
+
+// ------------------------------------------ stream stats, lane-column counting
+// The statistics of k_stream_stats for streams of 1..4 dimensions, counted with one
+// conflict-free shared-memory atomic per value: values below kLaneBins and the record
+// tags land in a [bin][lane] table (word bin * 32 + lane, so the 32 lanes of a warp
+// always hit 32 distinct banks; the warps of a CTA share the table).  A group is DIM
+// 16-byte loads (16 / esz records).  The launch's groups, over all selected streams,
+// split evenly across the CTAs; a CTA whose range crosses a stream boundary flushes its
+// tables at the boundary.  The tag bit total is derived from the tag counts.
+constexpr int kLaneBins = 256;
+constexpr int kStatsTagBins = 34;
+constexpr uint32_t kStatsThreads = 256;
+constexpr size_t kStatsLaneBytes = (kLaneBins + kStatsTagBins) * 32 * sizeof(uint32_t);
+constexpr size_t kStatsWideBytes = kStatsLaneBytes + kSmemHistBins * sizeof(uint32_t);
+
+__device__ __forceinline__ uint32_t uint4_word(const uint4& a, int i) {
+    switch (i & 3) {
+        case 0: return a.x;
+        case 1: return a.y;
+        case 2: return a.z;
+        default: return a.w;
+    }
+}
+
+// Value j of a group held as 16-byte words w[], ESZ bytes per value (j is a constant
+// once the callers' loops are unrolled).
+template <int ESZ>
+__device__ __forceinline__ uint32_t group_value(const uint4* w, int j) {
+    if constexpr (ESZ == 1) return (uint4_word(w[j >> 4], j >> 2) >> (8 * (j & 3))) & 0xFFu;
+    else if constexpr (ESZ == 2) return (uint4_word(w[j >> 3], j >> 1) >> (16 * (j & 1))) & 0xFFFFu;
+    else return uint4_word(w[j >> 2], j);
+}
+
+// Groups [u0, u1) of one stream, strided over the CTA's threads.
+template <int DIM, int ESZ>
+__device__ __forceinline__ void lane_stats_segment(const StreamRef& r, uint64_t nrec, uint64_t u0, uint64_t u1,
+                                                   uint32_t* lp, uint32_t* tl, uint32_t* sh, uint32_t* gh,
+                                                   uint32_t (&mn)[DIM], uint32_t (&mx)[DIM]) {
+    constexpr int GR = 16 / ESZ;   // records per group
+    uint32_t* lpl = lp + (threadIdx.x & 31);
+    uint32_t* tll = tl + (threadIdx.x & 31);
+    const auto record = [&](const uint32_t (&v)[DIM]) {
+        uint32_t o = 1;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const uint32_t x = v[d];
+            mn[d] = x < mn[d] ? x : mn[d];
+            mx[d] = x > mx[d] ? x : mx[d];
+            o |= x;
+            if (ESZ == 1 || x < static_cast<uint32_t>(kLaneBins)) atomicAdd(lpl + (x << 5), 1u);
+            else if (x < static_cast<uint32_t>(kSmemHistBins)) atomicAdd(&sh[x], 1u);
+            else if (x < kRansMaxAlphabet) atomicAdd(&gh[x], 1u);
+        }
+        atomicAdd(tll + (static_cast<uint32_t>(32 - __clz(o)) << 5), 1u);   // tag = max(1, bitlen)
+    };
+    const bool vec_ok = (reinterpret_cast<uintptr_t>(r.data) & 15) == 0;
+    for (uint64_t u = u0 + threadIdx.x; u < u1; u += kStatsThreads) {
+        const uint64_t rec0 = u * GR;
+        if (vec_ok && rec0 + GR <= nrec) {
+            uint4 w[DIM];
+            const uint4* p = static_cast<const uint4*>(r.data) + u * DIM;
+#pragma unroll
+            for (int q = 0; q < DIM; ++q) w[q] = __ldg(p + q);
+#pragma unroll
+            for (int k = 0; k < GR; ++k) {
+                uint32_t v[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) v[d] = group_value<ESZ>(w, k * DIM + d);
+                record(v);
+            }
+        } else {
+            for (uint64_t rec = rec0; rec < rec0 + GR && rec < nrec; ++rec) {
+                uint32_t v[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) v[d] = load_elem(r.data, rec * DIM + d, ESZ);
+                record(v);
+            }
+        }
+    }
+}
+
+// streams: bit s selects refs.s[s].  wide: some selected stream stores 2- or 4-byte values (the table of values
+// kLaneBins..kSmemHistBins-1 follows the lane tables in dynamic shared memory).
+template <int DIM>
+__global__ void __launch_bounds__(kStatsThreads, 4) k_stream_stats_lanes(StreamRefs refs, EncState* st,
+                                                                         uint32_t* hist, uint64_t hist_stride,
+                                                                         uint32_t streams, int derive, int wide) {
+    if (derive && blockIdx.x == 0 && threadIdx.x == 0) {
+        if (derive & 1) idrel_stats(st, hist, refs.s[0].count_const);
+        if (derive & 2) choice_stats(st, hist + hist_stride * 3);
+    }
+    extern __shared__ __align__(16) uint32_t sdyn[];
+    uint32_t* lp = sdyn;                      // [kLaneBins][32]
+    uint32_t* tl = lp + kLaneBins * 32;       // [kStatsTagBins][32]
+    uint32_t* sh = tl + kStatsTagBins * 32;   // [kSmemHistBins], wide launches
+    __shared__ uint32_t smin[DIM], smax[DIM];
+    const uint32_t words = static_cast<uint32_t>((wide ? kStatsWideBytes : kStatsLaneBytes) / 16);
+    for (uint32_t t = threadIdx.x; t < words; t += kStatsThreads)
+        reinterpret_cast<uint4*>(sdyn)[t] = make_uint4(0, 0, 0, 0);
+    uint64_t total = 0;
+#pragma unroll 1
+    for (int s = 0; s < kCodeStreams; ++s) {
+        if (!((streams >> s) & 1u)) continue;
+        const StreamRef r = refs.s[s];
+        total += (stream_records(r) + 16 / r.esz - 1) / (16 / r.esz);
+    }
+    const uint64_t lo = total * blockIdx.x / gridDim.x, hi = total * (blockIdx.x + 1) / gridDim.x;
+    uint64_t off = 0;
+#pragma unroll 1
+    for (int s = 0; s < kCodeStreams; ++s) {
+        if (!((streams >> s) & 1u)) continue;
+        const StreamRef r = refs.s[s];
+        const uint64_t nrec = stream_records(r);
+        const uint64_t base = off, ng = (nrec + 16 / r.esz - 1) / (16 / r.esz);
+        off += ng;
+        const uint64_t a = lo > base ? lo : base, b = hi < base + ng ? hi : base + ng;
+        if (a >= b) continue;   // uniform over the CTA
+        uint32_t* gh = hist + hist_stride * s;
+        if (threadIdx.x < DIM) { smin[threadIdx.x] = 0xffffffffu; smax[threadIdx.x] = 0; }
+        __syncthreads();
+        uint32_t mn[DIM], mx[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) { mn[d] = 0xffffffffu; mx[d] = 0; }
+        if (r.esz == 1)
+            lane_stats_segment<DIM, 1>(r, nrec, a - base, b - base, lp, tl, sh, gh, mn, mx);
+        else if (r.esz == 2)
+            lane_stats_segment<DIM, 2>(r, nrec, a - base, b - base, lp, tl, sh, gh, mn, mx);
+        else
+            lane_stats_segment<DIM, 4>(r, nrec, a - base, b - base, lp, tl, sh, gh, mn, mx);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const uint32_t x = warp_min(mn[d]), y = warp_max(mx[d]);
+            if ((threadIdx.x & 31) == 0) { atomicMin(&smin[d], x); atomicMax(&smax[d], y); }
+        }
+        __syncthreads();
+        StreamStats& gs = st->st[s];
+        uint32_t vmax = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) vmax = smax[d] > vmax ? smax[d] : vmax;
+        if (threadIdx.x < DIM) {
+            atomicMin(&gs.minv[threadIdx.x], smin[threadIdx.x]);
+            atomicMax(&gs.maxv[threadIdx.x], smax[threadIdx.x]);
+            atomicMax(&gs.maxall, smax[threadIdx.x]);
+        }
+        // column sums, read along a diagonal (lane l of a warp reads bank (l + i) & 31),
+        // leaving the tables zeroed for the next segment
+        const uint32_t nb = vmax < static_cast<uint32_t>(kLaneBins) ? vmax + 1 : static_cast<uint32_t>(kLaneBins);
+        for (uint32_t t = threadIdx.x; t < nb; t += kStatsThreads) {
+            uint32_t c = 0;
+#pragma unroll 8
+            for (uint32_t i = 0; i < 32; ++i) {
+                uint32_t* q = lp + t * 32 + ((i + t) & 31);
+                c += *q;
+                *q = 0;
+            }
+            if (c) atomicAdd(&gh[t], c);
+        }
+        if (threadIdx.x < static_cast<uint32_t>(kStatsTagBins)) {
+            const uint32_t t = threadIdx.x;
+            uint32_t c = 0;
+#pragma unroll 8
+            for (uint32_t i = 0; i < 32; ++i) {
+                uint32_t* q = tl + t * 32 + ((i + t) & 31);
+                c += *q;
+                *q = 0;
+            }
+            if (c) {
+                atomicAdd(&gs.tag_hist[t], c);
+                atomicMax(&gs.maxtag, t);
+                atomicAdd(reinterpret_cast<unsigned long long*>(&gs.tag_bits),
+                          static_cast<unsigned long long>(c) * t * DIM);
+            }
+        }
+        if (r.esz > 1) {
+            const uint32_t ne = vmax < static_cast<uint32_t>(kSmemHistBins) ? vmax + 1 : static_cast<uint32_t>(kSmemHistBins);
+            for (uint32_t t = kLaneBins + threadIdx.x; t < ne; t += kStatsThreads)
+                if (sh[t]) { atomicAdd(&gh[t], sh[t]); sh[t] = 0; }
+        }
+        __syncthreads();
+    }
 }
 
 // One CTA per (stream, kind): kind 0 = raw value table, kind 1 = tag table.
@@ -1691,8 +1873,9 @@ __device__ void choice_stats(EncState* st, uint32_t* gh) {
 }
 
 // Statistics of streams s0 .. s0+count-1: one launch for the one-dimensional streams
-// and one for the D-dimensional ones (templated on D when D <= 4); CH20 (stream 3) by
-// k_choice_stats, IDR0 (stream 0) from the links k_level1 counted, by k_idrel_stats.
+// and one for the D-dimensional ones (k_stream_stats_lanes for D <= 4, k_stream_stats
+// above); CH20 (stream 3) and IDR0 (stream 0, from the links k_level1 counted) are
+// derived inside the first of them.
 static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, uint64_t hist_stride, uint32_t dims,
                          uint64_t max_records, int s0, int count, cudaStream_t stream) {
     StreamSel one{}, many{};
@@ -1708,20 +1891,45 @@ static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, u
             many.s[nd++] = s;
         }
     }
-    const unsigned g = grid_for((max_records + 3) / 4, 256, 148u * 4u);
-    if (n1) {
-        k_stream_stats<1><<<dim3(g, n1), 256, 0, stream>>>(refs, st, hist, hist_stride, one, derive); count_launch();
-        derive = 0;
-    }
-    if (nd) {
-        constexpr size_t smem = 0;
-        switch (dims) {
-            case 2: k_stream_stats<2><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many, derive); break;
-            case 3: k_stream_stats<3><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many, derive); break;
-            case 4: k_stream_stats<4><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many, derive); break;
-            default: k_stream_stats<0><<<dim3(g, nd), 256, smem, stream>>>(refs, st, hist, hist_stride, many, derive); break;
+    // streams of 1..4 dimensions: the lane-column kernel, its grid sized to the groups
+    // the selected streams could hold (each CTA takes an even share of the actual ones)
+    const auto lanes = [&](const StreamSel& sel, int ns, uint32_t dm) {
+        bool wide = false;
+        uint32_t mask = 0;
+        for (int i = 0; i < ns; ++i) {
+            wide |= refs.s[sel.s[i]].esz > 1;
+            mask |= 1u << sel.s[i];
         }
+        const uint64_t groups = static_cast<uint64_t>(ns) * ((max_records + 15) / 16);
+        const unsigned g = static_cast<unsigned>(
+            std::max<uint64_t>(1, std::min<uint64_t>(148ull * 4, (groups + kStatsThreads - 1) / kStatsThreads)));
+        const size_t smem = wide ? kStatsWideBytes : kStatsLaneBytes;
+        const int w = wide ? 1 : 0;
+        // more than the default 48 KB of dynamic shared memory: a failed attribute call
+        // fails the launch, which the caller's launch check reports
+#define CHAIN_LANES(DM)                                                                                          \
+    do {                                                                                                         \
+        if (wide)                                                                                                \
+            (void)cudaFuncSetAttribute(k_stream_stats_lanes<DM>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                       static_cast<int>(kStatsWideBytes));                                      \
+        k_stream_stats_lanes<DM><<<g, kStatsThreads, smem, stream>>>(refs, st, hist, hist_stride, mask, derive, w); \
+    } while (0)
+        switch (dm) {
+            case 1: CHAIN_LANES(1); break;
+            case 2: CHAIN_LANES(2); break;
+            case 3: CHAIN_LANES(3); break;
+            default: CHAIN_LANES(4); break;
+        }
+#undef CHAIN_LANES
         count_launch();
+        derive = 0;
+    };
+    if (n1) lanes(one, n1, 1);
+    if (nd && dims <= 4) {
+        lanes(many, nd, dims);
+    } else if (nd) {   // more than four dimensions
+        const unsigned g = grid_for((max_records + 3) / 4, 256, 148u * 4u);
+        k_stream_stats<0><<<dim3(g, nd), 256, 0, stream>>>(refs, st, hist, hist_stride, many, derive); count_launch();
     }
 }
 
@@ -1977,6 +2185,7 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     refs.s[kCorrGaps] = StreamRef{corr_gaps, 1, 4, nullptr, nullptr, 0};
     refs.s[kCorrIds] = StreamRef{corr_ids, 1, 4, nullptr, nullptr, 0};
     launch_stats(refs, st, hist, hist_stride, dims, n, 0, kStreams, stream);
+    T.mark("stats", stream);
     // per device, cheap; set on every call, always to the same value
     CHAIN_CUDA(cudaFuncSetAttribute(k_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(kTableStageBytes)));
@@ -1984,7 +2193,7 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
                                                                                tag_prob, tag_cum, 0, bytes_per_lane,
                                                                                max_steps); count_launch();
     CHAIN_LAUNCH_CHECK("plan");
-    T.mark("stats+tables+plan", stream);
+    T.mark("tables+plan", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
     CHAIN_CUDA(cudaStreamSynchronize(stream));
     T.mark("sync2", stream);

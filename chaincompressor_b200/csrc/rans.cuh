@@ -92,11 +92,34 @@ __device__ __forceinline__ void block_copy32(uint32_t* __restrict__ dst, const u
     }
 }
 
+// Sums of a, b and c over the CTA with one pass of barriers; scratch holds 99 values.
+__device__ inline void block_sum3(uint64_t& a, uint64_t& b, uint64_t& c, uint64_t* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    c = warp_sum(c);
+    if (lane == 0) { scratch[warp] = a; scratch[33 + warp] = b; scratch[66 + warp] = c; }
+    __syncthreads();
+    if (warp == 0) {
+        uint64_t x = lane < nw ? scratch[lane] : 0, y = lane < nw ? scratch[33 + lane] : 0,
+                 z = lane < nw ? scratch[66 + lane] : 0;
+        x = warp_sum(x);
+        y = warp_sum(y);
+        z = warp_sum(z);
+        if (lane == 0) { scratch[32] = x; scratch[65] = y; scratch[98] = z; }
+    }
+    __syncthreads();
+    a = scratch[32];
+    b = scratch[65];
+    c = scratch[98];
+    __syncthreads();
+}
+
 // stage: kTableStageBytes of shared memory, or null (work in global memory).
 __device__ inline void build_rans_table(const uint32_t* __restrict__ hist_in, uint32_t A, uint64_t n,
                                         uint32_t* __restrict__ prob_out, uint32_t* __restrict__ cum,
                                         RansTableDev* desc, uint32_t* stage) {
-    __shared__ uint64_t red[33];
+    __shared__ uint64_t red[99];
     __shared__ double redd[33];
     __shared__ uint32_t sh_best;
     __shared__ uint64_t sh_sum;
@@ -132,8 +155,8 @@ __device__ inline void build_rans_table(const uint32_t* __restrict__ hist_in, ui
         pinned_f += pin ? f : 0;
         prob[s] = pin ? (kPin | 1u) : 0u;
     }
-    pinned = block_reduce_sum(pinned, red);
-    pinned_f = block_reduce_sum(pinned_f, red);
+    uint64_t unused = 0;
+    block_sum3(pinned, pinned_f, unused, red);
     uint64_t sum = 0;
     for (int round = 0; round < 16; ++round) {
         const uint64_t budget = M - pinned, rest = n - pinned_f;
@@ -151,9 +174,7 @@ __device__ inline void build_rans_table(const uint32_t* __restrict__ hist_in, ui
                 free_sum += p;
             }
         }
-        newly = block_reduce_sum(newly, red);
-        newly_f = block_reduce_sum(newly_f, red);
-        free_sum = block_reduce_sum(free_sum, red);
+        block_sum3(newly, newly_f, free_sum, red);
         pinned += newly;
         pinned_f += newly_f;
         sum = pinned + free_sum;
@@ -217,33 +238,56 @@ __device__ inline void build_rans_table(const uint32_t* __restrict__ hist_in, ui
         }
     }
     __syncthreads();
-    // cumulative frequencies (exclusive prefix) and the cost estimate: each thread takes
-    // a contiguous run of symbols, one block scan gives the runs' offsets
+    // cumulative frequencies (exclusive prefix), the cost estimate and the token bytes
     double cost = 0.0;
     uint64_t tbytes = 0;
-    const uint32_t per = (A + blockDim.x - 1) / blockDim.x;
-    const uint32_t s0 = threadIdx.x * per, s1 = min(A, s0 + per);
-    uint64_t run = 0;
-    for (uint32_t s = s0; s < s1; ++s) run += prob[s];
     uint64_t carry;
-    uint64_t c = block_exclusive_sum(run, red, &carry);
-    for (uint32_t s = s0; s < s1; ++s) {
-        const uint64_t p = prob[s];
-        cum[s] = static_cast<uint32_t>(c);
-        c += p;
+    const auto symbol = [&](uint32_t s, uint64_t p) {
         if (p) {
-            cost += static_cast<double>(hist[s]) * (static_cast<double>(prec) - log2(static_cast<double>(p)));
+            // log2(1) = 0 exactly: probability-1 symbols need no logarithm
+            const double lg = p == 1 ? 0.0 : log2(static_cast<double>(p));
+            cost += static_cast<double>(hist[s]) * (static_cast<double>(prec) - lg);
             tbytes += rans_token_bytes(static_cast<uint32_t>(p));
         } else if (s == 0 || prob[s - 1] != 0) {
             tbytes += 1;  // start of a zero run (runs longer than 64 are counted below)
+        }
+    };
+    if (A <= blockDim.x) {   // one symbol per thread
+        const uint32_t s = threadIdx.x;
+        const uint64_t p = s < A ? prob[s] : 0;
+        const uint64_t c = block_exclusive_sum(p, red, &carry);
+        if (s < A) {
+            cum[s] = static_cast<uint32_t>(c);
+            symbol(s, p);
+        }
+    } else {
+        // warp w owns a contiguous range of the symbols and walks it 32 consecutive
+        // symbols at a time (bank-conflict-free in shared memory, coalesced in global);
+        // one block scan of the warps' totals gives the ranges' offsets
+        const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        const uint32_t span = ((A + nw - 1) / nw + 31) & ~31u;
+        const uint32_t c0 = min(A, warp * span), c1 = min(A, c0 + span);
+        uint64_t wsum = 0;
+        for (uint32_t b = c0; b < c1; b += 32) wsum += b + lane < c1 ? prob[b + lane] : 0u;
+        wsum = warp_sum(wsum);
+        uint64_t c = block_exclusive_sum<uint64_t>(lane == 0 ? wsum : 0, red, &carry);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        for (uint32_t b = c0; b < c1; b += 32) {
+            const uint32_t s = b + lane;
+            const uint64_t p = s < c1 ? prob[s] : 0u;
+            const uint64_t inc = warp_inclusive_sum(p);
+            if (s < c1) {
+                cum[s] = static_cast<uint32_t>(c + inc - p);
+                symbol(s, p);
+            }
+            c += __shfl_sync(0xffffffffu, inc, 31);
         }
     }
     if (staged)
         for (uint32_t s = threadIdx.x; s < A; s += blockDim.x) prob_out[s] = prob[s];
     uint64_t zeros = 0;
     for (uint32_t s = threadIdx.x; s < A; s += blockDim.x) zeros += prob[s] == 0;
-    zeros = block_reduce_sum(zeros, red);
-    tbytes = block_reduce_sum(tbytes, red);
+    block_sum3(zeros, tbytes, unused, red);
     // deterministic FP sum: fixed per-thread order, then a fixed tree
     {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
