@@ -119,6 +119,12 @@ void chain_ctx_destroy(chain_ctx* ctx) {
     ctx->timer.release();
     if (ctx->state_dev) cudaFree(ctx->state_dev);
     if (ctx->state_host) cudaFreeHost(ctx->state_host);
+    if (ctx->side) {
+        cudaStreamSynchronize(ctx->side);
+        cudaStreamDestroy(ctx->side);
+    }
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

@@ -137,6 +137,10 @@ struct chain_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // The encoder's side stream (highest priority; created by the first compress) and the
+    // events that fork work onto it after level 1 and join it back before planning.
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     chain::Arena frame;    // per-frame working buffers (encoder)
     chain::Arena keys;     // encoder block keys, sort buffers and record keys (sized once the key width is known)
     chain::Arena coded;    // encoder entropy/output buffers

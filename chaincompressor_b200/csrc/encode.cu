@@ -79,6 +79,7 @@ struct EncState {
     uint64_t total_bytes;
     uint32_t npieces;
     uint32_t done_b;          // second hand-off counter
+    uint32_t done_c;          // hand-off counter of the side stream's IDR0 tables
     uint64_t nsegs;
 };
 
@@ -561,20 +562,25 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
 }
 
 // IDR0's statistics completed from the level-1 links: the n - links zeros (tag 1) join
-// them.  The same values the counting kernel would accumulate from the stream.
-__device__ void idrel_stats(EncState* st, uint32_t* gh, uint64_t n) {
+// them.  The same values the counting kernel would accumulate from the stream.  part 0
+// completes what the value table reads (extrema, value histogram), part 1 what the tag
+// table reads (tag histogram, tag bits), so that the two table CTAs each finish their own.
+__device__ void idrel_stats(EncState* st, uint32_t* gh, uint64_t n, int part) {
     if (n == 0) return;
     const unsigned long long links = st->l1_links, zeros = n - links;
     StreamStats& g = st->st[0];
-    g.minv[0] = zeros ? 0u : st->l1_link_min;
-    g.maxv[0] = links ? st->l1_link_max : 0u;
-    g.maxall = g.maxv[0];
-    if (zeros) {
-        g.tag_hist[1] += static_cast<uint32_t>(zeros);
-        if (g.maxtag < 1) g.maxtag = 1;
-        gh[0] += static_cast<uint32_t>(zeros);
+    if (part == 0) {
+        g.minv[0] = zeros ? 0u : st->l1_link_min;
+        g.maxv[0] = links ? st->l1_link_max : 0u;
+        g.maxall = g.maxv[0];
+        if (zeros) gh[0] += static_cast<uint32_t>(zeros);
+    } else {
+        if (zeros) {
+            g.tag_hist[1] += static_cast<uint32_t>(zeros);
+            if (g.maxtag < 1) g.maxtag = 1;
+        }
+        g.tag_bits = st->l1_link_bits + zeros;
     }
-    g.tag_bits = st->l1_link_bits + zeros;
 }
 
 // Explicit block records, in index order (lcps_cpp.cpp:2196-2199).
@@ -856,7 +862,6 @@ __device__ __forceinline__ void warp_hist_add(uint32_t* bins, uint32_t v, bool v
 
 constexpr int kSmemHistBins = 4096;
 
-__device__ void idrel_stats(EncState* st, uint32_t* gh, uint64_t n);
 __device__ void choice_stats(EncState* st, uint32_t* gh);
 
 // Per-stream statistics in one pass: per-dimension min/max, overall max, the record
@@ -868,15 +873,11 @@ __device__ void choice_stats(EncState* st, uint32_t* gh);
 // below kSmemHistBins in shared memory, the rest in global memory.  Register
 // counters flush before they could overflow.  blockIdx.y selects the stream from
 // sel[] (the streams of one launch share DIM).
-// derive: bit 0 = complete IDR0's statistics from the level-1 links, bit 1 = CH20's from
-// the level-2 counts (done once, by block (0, 0), before its own stream).
+// derive: complete CH20's statistics from the level-2 counts (done once, by block (0, 0)).
 template <int DIM>
 __global__ void __launch_bounds__(256) k_stream_stats(StreamRefs refs, EncState* st, uint32_t* hist,
                                                        uint64_t hist_stride, StreamSel sel, int derive) {
-    if (derive && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
-        if (derive & 1) idrel_stats(st, hist, refs.s[0].count_const);
-        if (derive & 2) choice_stats(st, hist + hist_stride * 3);
-    }
+    if (derive && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) choice_stats(st, hist + hist_stride * 3);
     const int s = sel.s[blockIdx.y];
     const StreamRef r = refs.s[s];
     const uint32_t D = DIM ? DIM : r.dims;
@@ -1079,16 +1080,14 @@ __device__ __forceinline__ void lane_stats_segment(const StreamRef& r, uint64_t 
     }
 }
 
-// streams: bit s selects refs.s[s].  wide: some selected stream stores 2- or 4-byte values (the table of values
-// kLaneBins..kSmemHistBins-1 follows the lane tables in dynamic shared memory).
+// streams: bit s selects refs.s[s].  derive: as for k_stream_stats.  wide: some selected
+// stream stores 2- or 4-byte values (the table of values kLaneBins..kSmemHistBins-1
+// follows the lane tables in dynamic shared memory).
 template <int DIM>
 __global__ void __launch_bounds__(kStatsThreads, 4) k_stream_stats_lanes(StreamRefs refs, EncState* st,
                                                                          uint32_t* hist, uint64_t hist_stride,
                                                                          uint32_t streams, int derive, int wide) {
-    if (derive && blockIdx.x == 0 && threadIdx.x == 0) {
-        if (derive & 1) idrel_stats(st, hist, refs.s[0].count_const);
-        if (derive & 2) choice_stats(st, hist + hist_stride * 3);
-    }
+    if (derive && blockIdx.x == 0 && threadIdx.x == 0) choice_stats(st, hist + hist_stride * 3);
     extern __shared__ __align__(16) uint32_t sdyn[];
     uint32_t* lp = sdyn;                      // [kLaneBins][32]
     uint32_t* tl = lp + kLaneBins * 32;       // [kStatsTagBins][32]
@@ -1184,15 +1183,21 @@ __global__ void __launch_bounds__(kStatsThreads, 4) k_stream_stats_lanes(StreamR
 __device__ void plan_stream(const StreamRefs& refs, EncState* st, uint32_t bytes_per_lane, uint32_t max_steps, int s);
 
 // The CTA that finishes last plans the launch's streams (plan_stream), so that the plan
-// needs no launch of its own.
-__global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncState* st, const uint32_t* hist,
+// needs no launch of its own; done is the launch's hand-off counter.  For IDR0 (s0 = 0)
+// each CTA first completes the statistics its table reads from the level-1 counts.
+__global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncState* st, uint32_t* hist,
                                                            uint64_t hist_stride, uint32_t* prob, uint32_t* cum,
                                                            uint32_t* tag_prob, uint32_t* tag_cum, int s0,
-                                                           uint32_t bytes_per_lane, uint32_t max_steps) {
+                                                           uint32_t bytes_per_lane, uint32_t max_steps,
+                                                           uint32_t* done) {
     extern __shared__ __align__(16) uint32_t tstage[];   // kTableStageBytes
     const int s = s0 + blockIdx.x, kind = blockIdx.y;
     const StreamRef r = refs.s[s];
     const uint64_t nrec = stream_records(r);
+    if (s == 0) {
+        if (threadIdx.x == 0) idrel_stats(st, hist, r.count_const, kind);
+        __syncthreads();
+    }
     if (kind == 0) {
         const uint32_t maxall = st->st[s].maxall;
         const bool ok = nrec > 0 && maxall < kRansMaxAlphabet;
@@ -1207,13 +1212,13 @@ __global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncSt
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        s_last = atomicAdd(&st->done_b, 1u) == gridDim.x * gridDim.y - 1;
+        s_last = atomicAdd(done, 1u) == gridDim.x * gridDim.y - 1;
     }
     __syncthreads();
     if (!s_last) return;
     __threadfence();
     if (threadIdx.x < gridDim.x) plan_stream(refs, st, bytes_per_lane, max_steps, s0 + threadIdx.x);
-    if (threadIdx.x == 0) st->done_b = 0;
+    if (threadIdx.x == 0) *done = 0;
 }
 
 __device__ inline uint64_t section_overhead(uint32_t table_bytes, uint32_t chunks, uint32_t lanes, uint32_t prec) {
@@ -1802,6 +1807,7 @@ __global__ void __launch_bounds__(256) k_init_state(EncState* st, uint32_t dims,
     st->err = 0;
     st->done_a = 0;
     st->done_b = 0;
+    st->done_c = 0;
     st->dims = dims;
     st->n = n;
     st->eb = eb;
@@ -1872,19 +1878,17 @@ __device__ void choice_stats(EncState* st, uint32_t* gh) {
     gh[1] = static_cast<uint32_t>(ones);
 }
 
-// Statistics of streams s0 .. s0+count-1: one launch for the one-dimensional streams
-// and one for the D-dimensional ones (k_stream_stats_lanes for D <= 4, k_stream_stats
-// above); CH20 (stream 3) and IDR0 (stream 0, from the links k_level1 counted) are
-// derived inside the first of them.
+// Statistics of streams s0 .. s0+count-1 (not IDR0, stream 0, whose statistics k_level1
+// counts and k_tables completes): one launch for the one-dimensional streams and one for
+// the D-dimensional ones (k_stream_stats_lanes for D <= 4, k_stream_stats above); CH20
+// (stream 3) is derived from the level-2 counts inside the first of them.
 static void launch_stats(const StreamRefs& refs, EncState* st, uint32_t* hist, uint64_t hist_stride, uint32_t dims,
                          uint64_t max_records, int s0, int count, cudaStream_t stream) {
     StreamSel one{}, many{};
     int n1 = 0, nd = 0, derive = 0;
     for (int s = s0; s < s0 + count; ++s) {
         if (s == 3) {
-            derive |= 2;
-        } else if (s == 0) {
-            derive |= 1;
+            derive = 1;
         } else if (refs.s[s].dims == 1) {
             one.s[n1++] = s;
         } else {
@@ -2027,6 +2031,28 @@ static void launch_minmax(const void* pts, uint64_t n, uint32_t D, EncState* st,
 // One attempt at a frame with room for corr_cap exact corrections.  When the frame has
 // more, it returns CHAIN_ERR_OUT_OF_MEMORY with *corr_needed set to their count (the
 // caller retries with that capacity).
+// Creates the context's side stream (highest priority) and its fork/join events on first use.
+static chain_status ensure_side_stream(chain_ctx* ctx) {
+    if (!ctx->fork_ev) CHAIN_CUDA(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+    if (!ctx->join_ev) CHAIN_CUDA(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
+    if (!ctx->side) {
+        int least = 0, greatest = 0;
+        CHAIN_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CHAIN_CUDA(cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, greatest));
+    }
+    return CHAIN_OK;
+}
+
+// Orders the context's stream after the side stream's work when the encoder returns
+// between the fork and the join (an error), so that nothing later on the context races
+// with it.
+struct SideJoin {
+    chain_ctx* ctx = nullptr;
+    ~SideJoin() {
+        if (ctx) cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0);
+    }
+};
+
 static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_dtype dtype, chain_layout layout,
                                      uint64_t n, uint32_t dims, double eb, int64_t p, int64_t threshold, int bl, int l1,
                                      int l2, uint32_t bytes_per_lane, uint32_t max_steps, uint64_t corr_cap,
@@ -2160,6 +2186,23 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     }
     CHAIN_LAUNCH_CHECK("level 1");
     T.mark("level1", stream);
+    // IDR0's statistics are complete after level 1, so its tables and plan are built on
+    // the side stream while level 2 and the other streams' statistics run on this one
+    st_ = ensure_side_stream(ctx);
+    if (st_ != CHAIN_OK) return st_;
+    // per device, cheap; set on every call, always to the same value
+    CHAIN_CUDA(cudaFuncSetAttribute(k_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(kTableStageBytes)));
+    StreamRefs idr{};
+    idr.s[0] = StreamRef{idrel, 1, 4, nullptr, nullptr, n};
+    CHAIN_CUDA(cudaEventRecord(ctx->fork_ev, stream));
+    CHAIN_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
+    k_tables<<<dim3(1, 2), kTableThreads, kTableStageBytes, ctx->side>>>(idr, st, hist, hist_stride, prob, cum, tag_prob,
+                                                                         tag_cum, 0, bytes_per_lane, max_steps,
+                                                                         &st->done_c); count_launch();
+    CHAIN_CUDA(cudaEventRecord(ctx->join_ev, ctx->side));
+    SideJoin join{ctx};
+    CHAIN_LAUNCH_CHECK("IDR0 tables");
     uint32_t* scan32 = reinterpret_cast<uint32_t*>(scanbuf);
     const bool d3 = dims == 3 && hs->kb <= 21;
     if (ksz == 16)
@@ -2184,14 +2227,13 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     refs.s[4] = StreamRef{rel, dims, rel_esz, nullptr, nullptr, n};
     refs.s[kCorrGaps] = StreamRef{corr_gaps, 1, 4, nullptr, nullptr, 0};
     refs.s[kCorrIds] = StreamRef{corr_ids, 1, 4, nullptr, nullptr, 0};
-    launch_stats(refs, st, hist, hist_stride, dims, n, 0, kStreams, stream);
+    launch_stats(refs, st, hist, hist_stride, dims, n, 1, kStreams - 1, stream);
     T.mark("stats", stream);
-    // per device, cheap; set on every call, always to the same value
-    CHAIN_CUDA(cudaFuncSetAttribute(k_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(kTableStageBytes)));
-    k_tables<<<dim3(kStreams, 2), kTableThreads, kTableStageBytes, stream>>>(refs, st, hist, hist_stride, prob, cum,
-                                                                               tag_prob, tag_cum, 0, bytes_per_lane,
-                                                                               max_steps); count_launch();
+    CHAIN_CUDA(cudaStreamWaitEvent(stream, ctx->join_ev, 0));   // IDR0's tables and plan
+    join.ctx = nullptr;
+    k_tables<<<dim3(kStreams - 1, 2), kTableThreads, kTableStageBytes, stream>>>(refs, st, hist, hist_stride, prob, cum,
+                                                                                   tag_prob, tag_cum, 1, bytes_per_lane,
+                                                                                   max_steps, &st->done_b); count_launch();
     CHAIN_LAUNCH_CHECK("plan");
     T.mark("tables+plan", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
@@ -2229,7 +2271,7 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
         launch_stats(refs, st, hist, hist_stride, dims, nc, kCorrGaps, 2, stream);
         k_tables<<<dim3(2, 2), kTableThreads, kTableStageBytes, stream>>>(refs, st, hist, hist_stride, prob, cum,
                                                                          tag_prob, tag_cum, kCorrGaps, bytes_per_lane,
-                                                                         max_steps); count_launch();
+                                                                         max_steps, &st->done_b); count_launch();
         CHAIN_LAUNCH_CHECK("corrections");
         CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
         CHAIN_CUDA(cudaStreamSynchronize(stream));
