@@ -268,6 +268,7 @@ struct BlockDiv {
 struct QuantCtx {
     const double* mins;
     double eb, denom, two_eb;
+    double inv_denom;   // RN(1 / denom)
     BlockDiv bd;
     EncState* st;
     uint64_t* corr_idx;
@@ -275,8 +276,21 @@ struct QuantCtx {
     uint64_t corr_cap;
     // Quantizes coordinate x (flat index fi = i*D + d); returns the block index and
     // stores the offset inside the block in rel.
+    //
+    // floor(RN(a / denom)) without a division for almost every coordinate: t = RN(a *
+    // RN(1 / denom)) differs from a / denom by at most 2u|t| and RN(a / denom) by at most
+    // 3u|t| (u = 2^-53, to first order), so when t lies farther than m = 2^-49 t from the
+    // nearest integer, both have the same floor.  Closer (or not finite) coordinates
+    // take the IEEE division.  t - floor(t) is exact (Sterbenz), as is m.
+    __device__ __forceinline__ double quotient_floor(double a) const {
+        const double t = __dmul_rn(a, inv_denom);
+        const double ft = floor(t);
+        const double f = __dsub_rn(t, ft), m = __dmul_rn(t, 0x1p-49);
+        if (f > m && __dsub_rn(1.0, f) > m) return ft;
+        return floor(__ddiv_rn(a, denom));
+    }
     __device__ __forceinline__ uint32_t coord(double x, uint32_t d, uint64_t fi, uint32_t& rel) const {
-        const double qv = floor(__ddiv_rn(__dsub_rn(x, mins[d]), denom));
+        const double qv = quotient_floor(__dsub_rn(x, mins[d]));
         const uint32_t q = static_cast<uint32_t>(qv);
         const double restored = fma(__dadd_rn(static_cast<double>(q), 0.5), two_eb, mins[d]);
         if (!within_error_bound(restored, x, eb)) {
@@ -316,6 +330,7 @@ k_quantize(const FT* __restrict__ p, uint64_t n, uint32_t D_rt, EncState* st, KT
     Q.mins = s_min;
     Q.eb = s_eb;
     Q.denom = 2.0 * s_eb;
+    Q.inv_denom = 1.0 / Q.denom;
     Q.two_eb = 2.0 * s_eb;
     Q.bd.p = s_p;
     Q.bd.inv = 1.0 / static_cast<double>(s_p);
