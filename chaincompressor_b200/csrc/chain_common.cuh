@@ -165,6 +165,15 @@ __host__ __device__ inline uint64_t spread3(uint64_t n) {
     n = (n | (n << 2)) & 0x1249249249249249ull;
     return n;
 }
+// The same for the 10 bits a 30-bit key holds per dimension, in 32-bit arithmetic.
+__host__ __device__ inline uint32_t compact3_32(uint32_t x) {
+    x &= 0x09249249u;
+    x = (x ^ (x >> 2)) & 0x030C30C3u;
+    x = (x ^ (x >> 4)) & 0x0300F00Fu;
+    x = (x ^ (x >> 8)) & 0xFF0000FFu;
+    x = (x ^ (x >> 16)) & 0x000003FFu;
+    return x;
+}
 __host__ __device__ inline uint32_t compact3(uint64_t n) {
     n &= 0x1249249249249249ull;
     n = (n ^ (n >> 2)) & 0x10C30C30C30C30C3ull;

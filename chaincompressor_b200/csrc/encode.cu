@@ -619,7 +619,12 @@ struct ExplicitOut {
 // Block coordinates of a record key (D dimensions of kb bits each).
 template <int DIM, typename KT>
 __device__ __forceinline__ void rec_coords(KT k, int D, int kb, uint32_t* b) {
-    if constexpr (DIM == 3 && sizeof(KT) <= 8) {   // kb <= 21: the 3-D Morton compaction
+    if constexpr (DIM == 3 && sizeof(KT) == 4) {   // kb <= 10
+        const uint32_t k32 = static_cast<uint32_t>(k);
+        b[0] = compact3_32(k32);
+        b[1] = compact3_32(k32 >> 1);
+        b[2] = compact3_32(k32 >> 2);
+    } else if constexpr (DIM == 3 && sizeof(KT) <= 8) {   // kb <= 21: the 3-D Morton compaction
         const uint64_t k64 = static_cast<uint64_t>(k);
         b[0] = compact3(k64);
         b[1] = compact3(k64 >> 1);
@@ -690,11 +695,21 @@ __global__ void __launch_bounds__(256) k_l2_stats(const KT* __restrict__ rec, En
             }
         }
     }
+    // one update of each global value per CTA (the CTAs all update the same three words)
+    __shared__ uint32_t s_mn, s_mx, s_md;
+    if (threadIdx.x == 0) { s_mn = 0xffffffffu; s_mx = 0; s_md = 0; }
+    __syncthreads();
     mn = warp_min(mn); mx = warp_max(mx); md = warp_max(md);
     if ((threadIdx.x & 31) == 0) {
-        atomicMin(&st->rec_min, mn);
-        atomicMax(&st->rec_max, mx);
-        atomicMax(&st->rec_maxdiff, md);
+        atomicMin(&s_mn, mn);
+        atomicMax(&s_mx, mx);
+        atomicMax(&s_md, md);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_mn != 0xffffffffu) atomicMin(&st->rec_min, s_mn);
+        if (s_mx) atomicMax(&st->rec_max, s_mx);
+        if (s_md) atomicMax(&st->rec_maxdiff, s_md);
     }
 }
 
@@ -800,49 +815,86 @@ __global__ void __launch_bounds__(256) k_l2_choice(const KT* __restrict__ rec, E
         tile_counts[blockIdx.x] = t;
     }
 }
-struct Level2Flag {
-    const uint8_t* choice2;
-    const EncState* st;
-    __device__ bool operator()(uint64_t j) const { return j < st->B && choice2[j] != 0; }
-};
-// Writes record j as a kept row or as its ZigZag'd wrapped difference from the previous
-// record (lcps_cpp.cpp:1305-1454), ET bytes per value; DIM as for k_l2_choice.
+// Writes record j < B as a kept row or as its ZigZag'd wrapped difference from the
+// previous record (lcps_cpp.cpp:1305-1454), ET bytes per value: the ranked pass of the
+// flag scan of choice2, with the tiles and ranks of flag_apply_kernel (tile_prefix from
+// scan_tilesums_kernel).  Each record's coordinates are decoded once (a difference
+// record takes its predecessor's from the neighbouring lane, or from the previous
+// round's last lane) and the state's parameters are read once per thread.  DIM as for
+// k_l2_choice.
 template <typename KT, typename ET, int DIM>
-struct Level2Out {
-    const KT* rec;
-    const EncState* st;
-    ET* keep;
-    ET* diff;
-    __device__ void operator()(uint64_t j, uint32_t drank, uint32_t use_diff) const {
-        if (j >= st->B) return;
-        const int D = DIM ? DIM : static_cast<int>(st->dims);
-        const int kb = st->kb;
-        constexpr int KD = DIM ? DIM : kMaxDims;
-        uint32_t cur[KD];
-        rec_coords<DIM>(rec[j], D, kb, cur);
-        if (!use_diff) {
-            const uint64_t k = j - drank;
+__global__ void __launch_bounds__(kFlagThreads) k_l2_rows(const KT* __restrict__ rec, const EncState* st,
+                                                          const uint8_t* __restrict__ choice2, ET* __restrict__ keep,
+                                                          ET* __restrict__ diff, const uint32_t* __restrict__ tile_prefix) {
+    if (DIM == 3 && !l2_dim3(st)) return;
+    if (DIM == 0 && l2_dim3(st)) return;
+    __shared__ uint32_t wsum[kFlagThreads / 32];
+    const uint32_t B = st->B;
+    const int D = DIM ? DIM : static_cast<int>(st->dims);
+    const int kb = st->kb;
+    const int64_t wmin = st->wrap_min_corr, wmax = st->wrap_max_corr, wrange = st->wrap_range;
+    constexpr int KD = DIM ? DIM : kMaxDims;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * kFlagItems;
+    uint32_t m[kFlagItems];
+    uint32_t c = 0;
 #pragma unroll
-            for (int d = 0; d < KD; ++d)
-                if (DIM || d < D) keep[k * D + d] = static_cast<ET>(cur[d]);
-            return;
-        }
-        uint32_t prev[KD];
-        rec_coords<DIM>(rec[j - 1], D, kb, prev);
+    for (int k = 0; k < kFlagItems; ++k) {
+        const uint64_t i = base + 32 * k + lane;
+        m[k] = __ballot_sync(0xffffffffu, i < B && choice2[i] != 0);
+        c += __popc(m[k]);
+    }
+    if (lane == 0) wsum[warp] = c;
+    __syncthreads();
+    uint32_t run = tile_prefix[blockIdx.x];
+    for (int w = 0; w < warp; ++w) run += wsum[w];
+    const uint32_t lt = lanemask_lt();
+    // coordinates of the record before this warp's slice (lane 0 of the first round)
+    uint32_t carry[KD];
+#pragma unroll
+    for (int d = 0; d < KD; ++d) carry[d] = 0;
+    if (base > 0 && base - 1 < B) rec_coords<DIM>(ldg_key(rec + base - 1), D, kb, carry);
+#pragma unroll   // constant indices keep m[] in registers
+    for (int k = 0; k < kFlagItems; ++k) {
+        const uint64_t i = base + 32 * k + lane;
+        const bool valid = i < B;
+        uint32_t cur[KD], prev[KD];
+#pragma unroll
+        for (int d = 0; d < KD; ++d) cur[d] = 0;
+        if (valid) rec_coords<DIM>(ldg_key(rec + i), D, kb, cur);
 #pragma unroll
         for (int d = 0; d < KD; ++d) {
             if (!DIM && d >= D) break;
-            // prediction = previous record (already inside [wrap_min, wrap_max])
-            int64_t corr = static_cast<int64_t>(prev[d]) - static_cast<int64_t>(cur[d]);
-            if (corr < st->wrap_min_corr) corr += st->wrap_range;
-            else if (corr > st->wrap_max_corr) corr -= st->wrap_range;
-            const uint64_t zz = corr >= 0 ? static_cast<uint64_t>(corr) << 1
-                                          : (static_cast<uint64_t>(-(corr + 1)) << 1) | 1u;
-            diff[static_cast<uint64_t>(drank) * D + d] = static_cast<ET>(zz);
+            const uint32_t up = __shfl_up_sync(0xffffffffu, cur[d], 1);
+            prev[d] = lane == 0 ? carry[d] : up;
+            carry[d] = __shfl_sync(0xffffffffu, cur[d], 31);
         }
+        const uint32_t mk = m[k];
+        if (valid) {
+            const uint32_t rank = run + __popc(mk & lt);
+            if (!((mk >> lane) & 1u)) {
+                const uint64_t row = (i - rank) * static_cast<uint64_t>(D);
+#pragma unroll
+                for (int d = 0; d < KD; ++d)
+                    if (DIM || d < D) keep[row + d] = static_cast<ET>(cur[d]);
+            } else {
+                const uint64_t row = static_cast<uint64_t>(rank) * D;
+#pragma unroll
+                for (int d = 0; d < KD; ++d) {
+                    if (!DIM && d >= D) break;
+                    // prediction = previous record (already inside [wrap_min, wrap_max])
+                    int64_t corr = static_cast<int64_t>(prev[d]) - static_cast<int64_t>(cur[d]);
+                    if (corr < wmin) corr += wrange;
+                    else if (corr > wmax) corr -= wrange;
+                    const uint64_t zz = corr >= 0 ? static_cast<uint64_t>(corr) << 1
+                                                  : (static_cast<uint64_t>(-(corr + 1)) << 1) | 1u;
+                    diff[row + d] = static_cast<ET>(zz);
+                }
+            }
+        }
+        run += __popc(mk);
     }
-};
-
+}
 
 // ------------------------------------------------------------- stream stats
 struct StreamRef {
@@ -2011,9 +2063,9 @@ static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, ui
     device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT>{key_idx, rec}, n, scan32, &st->B, stream);
     T.mark("explicit_records", stream);
     if (d3) {
-        k_l2_stats<KT, 3><<<grid_for((n + 3) / 4), 256, 0, stream>>>(rec, st); count_launch();
+        k_l2_stats<KT, 3><<<grid_for((n + 3) / 4, 256, 148u * 4u), 256, 0, stream>>>(rec, st); count_launch();
     } else {
-        k_l2_stats<KT, 0><<<grid_for((n + 3) / 4), 256, 0, stream>>>(rec, st); count_launch();
+        k_l2_stats<KT, 0><<<grid_for((n + 3) / 4, 256, 148u * 4u), 256, 0, stream>>>(rec, st); count_launch();
     }
     const unsigned tiles = static_cast<unsigned>(flag_tiles(n));
     if (d3) {
@@ -2021,10 +2073,13 @@ static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, ui
     } else {
         k_l2_choice<KT, 0><<<tiles, 256, 0, stream>>>(rec, st, l2, choice2, scan32); count_launch();
     }
-#define CHAIN_L2OUT(ET, DIM)                                                                            \
-    device_flag_scan_counted<Level2Flag, Level2Out<KT, ET, DIM>, kFlagItems>(                          \
-        Level2Flag{choice2, st}, Level2Out<KT, ET, DIM>{rec, st, static_cast<ET*>(keep), static_cast<ET*>(diff)}, \
-        n, scan32, &st->ndiff, stream)
+    // the flag scan of choice2 over tiles of n entries (entries j >= B are not records):
+    // k_l2_choice wrote the tile counts
+    scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(scan32, tiles, &st->ndiff,
+                                                                          SumOp<uint32_t>()); count_launch();
+#define CHAIN_L2OUT(ET, DIM)                                                                                   \
+    k_l2_rows<KT, ET, DIM><<<tiles, kFlagThreads, 0, stream>>>(rec, st, choice2, static_cast<ET*>(keep),       \
+                                                               static_cast<ET*>(diff), scan32)
     if (d3) {
         if (kd_esz == 1) CHAIN_L2OUT(uint8_t, 3);
         else if (kd_esz == 2) CHAIN_L2OUT(uint16_t, 3);
@@ -2035,6 +2090,7 @@ static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, ui
         else CHAIN_L2OUT(uint32_t, 0);
     }
 #undef CHAIN_L2OUT
+    count_launch();
 }
 
 template <typename FT, bool SOA>
