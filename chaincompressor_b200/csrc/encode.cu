@@ -452,8 +452,9 @@ struct PackedCount8 {
 // same block (stable sort keeps indices increasing within a block).  Each thread takes
 // groups of four consecutive positions, two groups at a time, and loads them (16-byte
 // loads) and each group's fifth neighbour before using any.  `idrel` arrives zeroed
-// and only links (idrel != 0, a minority of points) are scattered into it.
-template <typename KT>
+// and only links (idrel != 0, a minority of points) are scattered into it.  DIM: 3, or 0
+// for a dimension count read at run time.
+template <typename KT, int DIM>
 __global__ void __launch_bounds__(256, sizeof(KT) == 4 ? 4 : 3)   // 64-bit keys spill at four CTAs per SM
 k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_t n, EncState* st,
          uint32_t* __restrict__ idrel, uint32_t* __restrict__ gh) {
@@ -471,7 +472,7 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
     // the common short links (distance < 8, tag < 8) count in registers, not in
     // contended shared-memory bins
     PackedCount8 vc, tc;
-    const int D = static_cast<int>(st->dims);
+    const int D = DIM ? DIM : static_cast<int>(st->dims);
     const int64_t maxb_bits = st->maxb_bits;
     const int64_t thr = st->threshold;
     const int64_t c = static_cast<int64_t>(D) * maxb_bits;
@@ -604,16 +605,16 @@ struct ExplicitIn {
     const uint32_t* idrel;
     __device__ uint32_t operator()(uint64_t i) const { return idrel[i] == 0 ? 1u : 0u; }
 };
-// An explicit record is kept as its point's block key (the block coordinates are
-// decoded from it where they are used), which moves D times fewer bytes than the
-// coordinates themselves through the level-2 passes.
-template <typename KT>
+// An explicit record is kept in one key-sized word, which moves D times fewer bytes
+// than separate coordinates through the level-2 passes: for three dimensions with kb <=
+// 21 (kPack3) the block coordinates packed at a fixed field width (rec3_pack; the level-2
+// passes then unpack them with shifts), otherwise the point's block key (decoded where
+// it is used).
+template <typename KT, bool kPack3>
 struct ExplicitOut {
     const KT* key;
     KT* rec;
-    __device__ void operator()(uint64_t i, uint32_t pos, uint32_t flag) const {
-        if (flag) rec[pos] = key[i];
-    }
+    __device__ void operator()(uint64_t i, uint32_t pos, uint32_t flag) const;
 };
 
 // Block coordinates of a record key (D dimensions of kb bits each).
@@ -636,6 +637,41 @@ __device__ __forceinline__ void rec_coords(KT k, int D, int kb, uint32_t* b) {
 
 // Level-2 work runs with DIM = 3 (three dimensions, kb <= 21) or DIM = 0 (any shape).
 __device__ __forceinline__ bool l2_dim3(const EncState* st) { return st->dims == 3 && st->kb <= 21; }
+
+// Three block coordinates of kb <= 21 bits packed into a key-sized word: fields of 10 bits
+// in a 32-bit word (3 kb <= 32 there, so kb <= 10), of 21 bits in a 64-bit one.
+// (16-byte keys have kb > 21 in three dimensions: their records stay keys.)
+template <typename KT>
+struct Rec3 {
+    static constexpr int kField = sizeof(KT) == 4 ? 10 : 21;
+    static constexpr KT kMask = (KT(1) << kField) - 1;
+};
+template <typename KT>
+__device__ __forceinline__ KT rec3_pack(KT key) {
+    uint32_t b[3];
+    rec_coords<3, KT>(key, 3, 0, b);
+    constexpr int F = Rec3<KT>::kField;
+    return static_cast<KT>(b[0]) | (static_cast<KT>(b[1]) << F) | (static_cast<KT>(b[2]) << (2 * F));
+}
+template <typename KT, bool kPack3>
+__device__ void ExplicitOut<KT, kPack3>::operator()(uint64_t i, uint32_t pos, uint32_t flag) const {
+    if (!flag) return;
+    if constexpr (kPack3) rec[pos] = rec3_pack<KT>(key[i]);
+    else rec[pos] = key[i];
+}
+
+// Block coordinates of an explicit record (as ExplicitOut stored it).
+template <int DIM, typename KT>
+__device__ __forceinline__ void rec_read(KT r, int D, int kb, uint32_t* b) {
+    if constexpr (DIM == 3 && sizeof(KT) <= 8) {
+        constexpr int F = Rec3<KT>::kField;
+        b[0] = static_cast<uint32_t>(r & Rec3<KT>::kMask);
+        b[1] = static_cast<uint32_t>((r >> F) & Rec3<KT>::kMask);
+        b[2] = static_cast<uint32_t>((r >> (2 * F)) & Rec3<KT>::kMask);
+    } else {
+        block_coords<KT>(r, D, kb, b);
+    }
+}
 
 // ------------------------------------------------------------------- level 2
 // Record minimum, maximum and largest per-dimension difference between consecutive
@@ -675,12 +711,12 @@ __global__ void __launch_bounds__(256) k_l2_stats(const KT* __restrict__ rec, En
             const uint64_t g = g0 + u * nthreads;
             if (g >= ng) continue;
             uint32_t prev[KD], cur[KD];
-            rec_coords<DIM>(k[u][0], D, kb, prev);
+            rec_read<DIM>(k[u][0], D, kb, prev);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const uint64_t j = 4 * g + q;
                 if (j >= B) break;
-                rec_coords<DIM>(k[u][1 + q], D, kb, cur);
+                rec_read<DIM>(k[u][1 + q], D, kb, cur);
 #pragma unroll
                 for (int d = 0; d < KD; ++d) {
                     if (!DIM && d >= D) break;
@@ -785,13 +821,13 @@ __global__ void __launch_bounds__(256) k_l2_choice(const KT* __restrict__ rec, E
         const uint64_t j0 = 4 * g;
         if (j0 >= B) continue;
         uint32_t prev[KD], cur[KD];
-        rec_coords<DIM>(k[u][0], D, kb, prev);
+        rec_read<DIM>(k[u][0], D, kb, prev);
         uint32_t ch[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const uint64_t j = j0 + q;
             if (j >= B) break;
-            rec_coords<DIM>(k[u][1 + q], D, kb, cur);
+            rec_read<DIM>(k[u][1 + q], D, kb, cur);
             ch[q] = (l2 && j > 0) ? l2_rule(cur, prev, D, fvb, fdb) : 0u;
             cnt += ch[q];
 #pragma unroll
@@ -853,7 +889,7 @@ __global__ void __launch_bounds__(kFlagThreads) k_l2_rows(const KT* __restrict__
     uint32_t carry[KD];
 #pragma unroll
     for (int d = 0; d < KD; ++d) carry[d] = 0;
-    if (base > 0 && base - 1 < B) rec_coords<DIM>(ldg_key(rec + base - 1), D, kb, carry);
+    if (base > 0 && base - 1 < B) rec_read<DIM>(ldg_key(rec + base - 1), D, kb, carry);
 #pragma unroll   // constant indices keep m[] in registers
     for (int k = 0; k < kFlagItems; ++k) {
         const uint64_t i = base + 32 * k + lane;
@@ -861,7 +897,7 @@ __global__ void __launch_bounds__(kFlagThreads) k_l2_rows(const KT* __restrict__
         uint32_t cur[KD], prev[KD];
 #pragma unroll
         for (int d = 0; d < KD; ++d) cur[d] = 0;
-        if (valid) rec_coords<DIM>(ldg_key(rec + i), D, kb, cur);
+        if (valid) rec_read<DIM>(ldg_key(rec + i), D, kb, cur);
 #pragma unroll
         for (int d = 0; d < KD; ++d) {
             if (!DIM && d >= D) break;
@@ -2043,13 +2079,17 @@ static void launch_quantize_rt(size_t ksz, uint32_t rel_esz, const void* pts, ui
 // sorted neighbours.
 template <typename KT, typename Hook>
 static void sort_and_link(void* key_idx, void* key_a, void* key_b, uint32_t* val_a, uint32_t* val_b, uint64_t n,
-                          int key_bits, uint32_t* counts, EncState* st, uint32_t* idrel, uint32_t* hist,
+                          int key_bits, uint32_t dims, uint32_t* counts, EncState* st, uint32_t* idrel, uint32_t* hist,
                           cudaStream_t stream, const Hook& marks) {
     KT* ka = static_cast<KT*>(key_a);
     KT* kb = static_cast<KT*>(key_b);
     const bool in_b = radix_sort_pairs<KT>(static_cast<const KT*>(key_idx), ka, val_a, kb, val_b, n, key_bits, counts,
                                            stream, marks, true);
-    k_level1<KT><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel, hist); count_launch();
+    if (dims == 3)
+        k_level1<KT, 3><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel, hist);
+    else
+        k_level1<KT, 0><<<grid_for(n), 256, 0, stream>>>(in_b ? kb : ka, in_b ? val_b : val_a, n, st, idrel, hist);
+    count_launch();
 }
 
 // Explicit records (keys of the points with idrel == 0, index order) and level 2: record
@@ -2060,19 +2100,28 @@ static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, ui
                        uint32_t kd_esz, uint8_t* choice2, void* keep, void* diff, uint32_t* scan32, StageTimer& T,
                        cudaStream_t stream) {
     KT* rec = static_cast<KT*>(rec_v);
-    device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT>{key_idx, rec}, n, scan32, &st->B, stream);
+    if constexpr (sizeof(KT) <= 8) {
+        if (d3)
+            device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, true>{key_idx, rec}, n, scan32, &st->B, stream);
+        else
+            device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, false>{key_idx, rec}, n, scan32, &st->B, stream);
+    } else {
+        device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, false>{key_idx, rec}, n, scan32, &st->B, stream);
+    }
     T.mark("explicit_records", stream);
     if (d3) {
         k_l2_stats<KT, 3><<<grid_for((n + 3) / 4, 256, 148u * 4u), 256, 0, stream>>>(rec, st); count_launch();
     } else {
         k_l2_stats<KT, 0><<<grid_for((n + 3) / 4, 256, 148u * 4u), 256, 0, stream>>>(rec, st); count_launch();
     }
+    T.mark("l2_stats", stream);
     const unsigned tiles = static_cast<unsigned>(flag_tiles(n));
     if (d3) {
         k_l2_choice<KT, 3><<<tiles, 256, 0, stream>>>(rec, st, l2, choice2, scan32); count_launch();
     } else {
         k_l2_choice<KT, 0><<<tiles, 256, 0, stream>>>(rec, st, l2, choice2, scan32); count_launch();
     }
+    T.mark("l2_choice", stream);
     // the flag scan of choice2 over tiles of n entries (entries j >= B are not records):
     // k_l2_choice wrote the tile counts
     scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(scan32, tiles, &st->ndiff,
@@ -2247,12 +2296,12 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
                    stream);
         };
         if (ksz == 16)
-            sort_and_link<u128>(key_idx, key_a, key_b, val_a, val_b, n, key_bits, counts, st, idrel, hist, stream, sort_marks);
+            sort_and_link<u128>(key_idx, key_a, key_b, val_a, val_b, n, key_bits, dims, counts, st, idrel, hist, stream, sort_marks);
         else if (ksz == 8)
-            sort_and_link<uint64_t>(key_idx, key_a, key_b, val_a, val_b, n, key_bits, counts, st, idrel, hist, stream,
+            sort_and_link<uint64_t>(key_idx, key_a, key_b, val_a, val_b, n, key_bits, dims, counts, st, idrel, hist, stream,
                                     sort_marks);
         else
-            sort_and_link<uint32_t>(key_idx, key_a, key_b, val_a, val_b, n, key_bits, counts, st, idrel, hist, stream,
+            sort_and_link<uint32_t>(key_idx, key_a, key_b, val_a, val_b, n, key_bits, dims, counts, st, idrel, hist, stream,
                                     sort_marks);
     }
     CHAIN_LAUNCH_CHECK("level 1");
@@ -2286,7 +2335,7 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
         run_level2<uint32_t>(reinterpret_cast<const uint32_t*>(key_idx), idrel, rec, n, st, l2, d3, kd_esz, choice2, keep,
                              diff, scan32, T, stream);
     CHAIN_LAUNCH_CHECK("level 2");
-    T.mark("level2", stream);
+    T.mark("l2_rows", stream);
     // The level-2 scan covers n >= B entries; its functors ignore entries j >= B (read
     // from the device), so no host round trip is needed for B.
 
