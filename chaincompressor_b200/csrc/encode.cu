@@ -781,7 +781,8 @@ __device__ __forceinline__ uint32_t l2_rule(const uint32_t* cur, const uint32_t*
 
 // choice2[j] for every record (1 = difference from the previous record), one CTA per
 // flag-scan tile of kFlagTile records; each CTA also writes its tile's count of
-// difference records, so the level-2 flag scan needs no counting pass.  Each thread
+// difference records and the last CTA scans them, so the level-2 flag scan needs no
+// launch before its ranked pass.  Each thread
 // takes four groups of four consecutive record keys, all loads first.
 template <typename KT, int DIM>
 __global__ void __launch_bounds__(256) k_l2_choice(const KT* __restrict__ rec, EncState* st, int l2,
@@ -850,11 +851,13 @@ __global__ void __launch_bounds__(256) k_l2_choice(const KT* __restrict__ rec, E
         for (int w = 0; w < 8; ++w) t += wsum[w];
         tile_counts[blockIdx.x] = t;
     }
+    // the last CTA turns the counts into the flag scan's tile prefixes (total: ndiff)
+    last_cta_scan_counts(tile_counts, &st->ndiff, &st->done_a);
 }
 // Writes record j < B as a kept row or as its ZigZag'd wrapped difference from the
 // previous record (lcps_cpp.cpp:1305-1454), ET bytes per value: the ranked pass of the
-// flag scan of choice2, with the tiles and ranks of flag_apply_kernel (tile_prefix from
-// scan_tilesums_kernel).  Each record's coordinates are decoded once (a difference
+// flag scan of choice2, with the tiles and ranks of flag_apply_kernel (tile_prefix left
+// by k_l2_choice).  Each record's coordinates are decoded once (a difference
 // record takes its predecessor's from the neighbouring lane, or from the previous
 // round's last lane) and the state's parameters are read once per thread.  DIM as for
 // k_l2_choice.
@@ -1553,13 +1556,58 @@ __device__ __forceinline__ void pack_fixed_tiles(const ET* __restrict__ data, ui
     }
 }
 
+// The same packing for a one-byte stream whose DIM dimensions all have the width W (1,
+// 2, 4 or 8, which divide 32): word t of dimension d holds records [t G, t G + G) (G = 32
+// / W) with the first in the top bits, stored byte-swapped as pack_fixed_tiles stores
+// it.  Thread t reads the group's G * DIM bytes with 4-byte loads and writes word t of
+// every dimension.
+template <int W, int DIM>
+__device__ __forceinline__ void pack_fixed_u8_equal(const uint8_t* __restrict__ data, uint64_t nrec,
+                                                    const FixedPack& fp) {
+    constexpr int G = 32 / W, NB = G * DIM, NW = NB / 4;
+    static_assert(NB % 4 == 0, "whole words per group");
+    const uint64_t nw = (nrec + G - 1) / G;
+    const bool aligned = (reinterpret_cast<uintptr_t>(data) & 3) == 0;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < nw; t += stride) {
+        const uint64_t r0 = t * G;
+        uint32_t acc[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) acc[d] = 0;
+        if (aligned && r0 + G <= nrec) {
+            const uint32_t* p = reinterpret_cast<const uint32_t*>(data + r0 * DIM);
+            uint32_t b[NW];
+#pragma unroll
+            for (int q = 0; q < NW; ++q) b[q] = __ldg(p + q);
+#pragma unroll
+            for (int k = 0; k < G; ++k)
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    const int j = k * DIM + d;
+                    const uint32_t v = ((b[j >> 2] >> (8 * (j & 3))) & 0xFFu) - fp.minv[d];
+                    acc[d] |= v << (32 - W * (k + 1));
+                }
+        } else {
+            for (int k = 0; k < G && r0 + k < nrec; ++k)
+#pragma unroll
+                for (int d = 0; d < DIM; ++d)
+                    acc[d] |= (static_cast<uint32_t>(data[(r0 + k) * DIM + d]) - fp.minv[d]) << (32 - W * (k + 1));
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) fp.words[d][t] = __byte_perm(acc[d], 0, 0x0123);
+    }
+}
+
 // Every fixed-coded component of a frame in one launch (blockIdx.y = component).
+// equal_w: the width all dimensions share when pack_fixed_u8_equal applies (1, 2, 4 or
+// 8; one-byte values, at most four dimensions), else 0.
 struct FixedJob {
     FixedPack fp;
     const void* data;
     uint64_t nrec;
     uint32_t dims;
     uint32_t esz;
+    uint32_t equal_w;
 };
 struct FixedJobs {
     FixedJob job[kCodeStreams];
@@ -1567,6 +1615,23 @@ struct FixedJobs {
 __global__ void __launch_bounds__(32 * kPackWarps, 3) k_pack_fixed(FixedJobs J) {
     __shared__ uint32_t stage[kPackWarps][33 * 32];
     const FixedJob& j = J.job[blockIdx.y];
+    if (j.equal_w) {
+        const uint8_t* d8 = static_cast<const uint8_t*>(j.data);
+#define CHAIN_PACK_EQ(W)                                                        \
+    switch (j.dims) {                                                         \
+        case 1: pack_fixed_u8_equal<W, 1>(d8, j.nrec, j.fp); return;          \
+        case 2: pack_fixed_u8_equal<W, 2>(d8, j.nrec, j.fp); return;          \
+        case 3: pack_fixed_u8_equal<W, 3>(d8, j.nrec, j.fp); return;          \
+        default: pack_fixed_u8_equal<W, 4>(d8, j.nrec, j.fp); return;         \
+    }
+        switch (j.equal_w) {
+            case 1: CHAIN_PACK_EQ(1)
+            case 2: CHAIN_PACK_EQ(2)
+            case 4: CHAIN_PACK_EQ(4)
+            default: CHAIN_PACK_EQ(8)
+        }
+#undef CHAIN_PACK_EQ
+    }
     uint32_t* sw = stage[threadIdx.x >> 5];
     if (j.esz == 1) pack_fixed_tiles(static_cast<const uint8_t*>(j.data), j.dims, j.nrec, j.fp, sw);
     else if (j.esz == 2) pack_fixed_tiles(static_cast<const uint16_t*>(j.data), j.dims, j.nrec, j.fp, sw);
@@ -2102,11 +2167,14 @@ static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, ui
     KT* rec = static_cast<KT*>(rec_v);
     if constexpr (sizeof(KT) <= 8) {
         if (d3)
-            device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, true>{key_idx, rec}, n, scan32, &st->B, stream);
+            device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, true>{key_idx, rec}, n, scan32, &st->B, stream,
+                         &st->done_a);
         else
-            device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, false>{key_idx, rec}, n, scan32, &st->B, stream);
+            device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, false>{key_idx, rec}, n, scan32, &st->B, stream,
+                         &st->done_a);
     } else {
-        device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, false>{key_idx, rec}, n, scan32, &st->B, stream);
+        device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, false>{key_idx, rec}, n, scan32, &st->B, stream,
+                         &st->done_a);
     }
     T.mark("explicit_records", stream);
     if (d3) {
@@ -2123,9 +2191,7 @@ static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, ui
     }
     T.mark("l2_choice", stream);
     // the flag scan of choice2 over tiles of n entries (entries j >= B are not records):
-    // k_l2_choice wrote the tile counts
-    scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(scan32, tiles, &st->ndiff,
-                                                                          SumOp<uint32_t>()); count_launch();
+    // k_l2_choice left the tile prefixes
 #define CHAIN_L2OUT(ET, DIM)                                                                                   \
     k_l2_rows<KT, ET, DIM><<<tiles, kFlagThreads, 0, stream>>>(rec, st, choice2, static_cast<ET*>(keep),       \
                                                                static_cast<ET*>(diff), scan32)
@@ -2498,6 +2564,13 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
             fj.nrec = c.records;
             fj.dims = c.dims;
             fj.esz = r.esz;
+            fj.equal_w = 0;
+            if (r.esz == 1 && c.dims <= 4) {
+                const uint32_t w0 = c.width[0];
+                bool eq = w0 == 1 || w0 == 2 || w0 == 4 || w0 == 8;
+                for (uint32_t d = 1; d < c.dims; ++d) eq = eq && c.width[d] == w0;
+                if (eq) fj.equal_w = w0;
+            }
             fixed_tiles = std::max<uint64_t>(fixed_tiles, (c.records + 1023) / 1024);
             ain.packed[s] = packed + packed_off[s];
             ain.packed_dim_stride[s] = packed_stride[s];

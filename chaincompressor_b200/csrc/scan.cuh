@@ -258,8 +258,58 @@ constexpr int kFlagThreads = 256;
 constexpr int kFlagItems = 16;
 constexpr int kFlagTile = kFlagThreads * kFlagItems;
 
+// In-place exclusive scan of `count` u32 tile counts by one CTA (blockDim a multiple of
+// 32, at most 1024), kPer consecutive counts per thread per round.  The counts are read
+// with ld.global.cg: the other CTAs of the same launch wrote them.  *total (may be null)
+// receives their sum.
+__device__ inline void block_scan_counts(uint32_t* counts, uint64_t count, uint32_t* total) {
+    constexpr int kPer = 8;
+    __shared__ uint32_t scratch[33];
+    uint32_t carry = 0;
+    const uint64_t per_round = static_cast<uint64_t>(blockDim.x) * kPer;
+    for (uint64_t base = 0; base < count; base += per_round) {
+        const uint64_t i0 = base + static_cast<uint64_t>(threadIdx.x) * kPer;
+        uint32_t v[kPer], sum = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            v[k] = i0 + k < count ? __ldcg(counts + i0 + k) : 0u;
+            sum += v[k];
+        }
+        uint32_t tot;
+        uint32_t ex = carry + block_exclusive_sum(sum, scratch, &tot);
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            if (i0 + k < count) counts[i0 + k] = ex;
+            ex += v[k];
+        }
+        carry += tot;
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+
+// The CTA of a launch that finishes last (done: a counter that is zero at launch, and
+// is zero again afterwards) turns the launch's tile counts into exclusive prefixes.
+// Every CTA calls it after writing its count; it returns true in the CTA that scanned.
+__device__ inline bool last_cta_scan_counts(uint32_t* counts, uint32_t* total, uint32_t* done) {
+    __shared__ bool s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    block_scan_counts(counts, gridDim.x, total);
+    if (threadIdx.x == 0) *done = 0;
+    return true;
+}
+
+// done (may be null): see last_cta_scan_counts; the tile counts then leave as exclusive
+// prefixes and *total receives their sum.
 template <typename Pred>
-__global__ void __launch_bounds__(kFlagThreads) flag_count_kernel(Pred pred, uint64_t n, uint32_t* tile_counts) {
+__global__ void __launch_bounds__(kFlagThreads) flag_count_kernel(Pred pred, uint64_t n, uint32_t* tile_counts,
+                                                                   uint32_t* total = nullptr, uint32_t* done = nullptr) {
     __shared__ uint32_t wsum[kFlagThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * kFlagItems;
@@ -276,6 +326,7 @@ __global__ void __launch_bounds__(kFlagThreads) flag_count_kernel(Pred pred, uin
         for (int w = 0; w < kFlagThreads / 32; ++w) t += wsum[w];
         tile_counts[blockIdx.x] = t;
     }
+    if (done) last_cta_scan_counts(tile_counts, total, done);
 }
 
 // kOutUnroll: rounds of out() calls unrolled together (more loads in flight against
@@ -310,16 +361,23 @@ __global__ void __launch_bounds__(kFlagThreads) flag_apply_kernel(Pred pred, Out
 inline uint64_t flag_tiles(uint64_t n) { return (n + kFlagTile - 1) / kFlagTile; }
 
 // `tile_buf` holds flag_tiles(n) u32 (scan_scratch_bytes(n) bytes suffice); *total
-// (may be null) receives the number of set flags.
+// (may be null) receives the number of set flags.  With `done` (a device counter that is
+// zero, see last_cta_scan_counts) the counting launch also scans the tile counts: two
+// launches instead of three.
 template <typename Pred, typename OutF, int kOutUnroll = 4>
-void device_flag_scan(Pred pred, OutF out, uint64_t n, uint32_t* tile_buf, uint32_t* total, cudaStream_t stream) {
+void device_flag_scan(Pred pred, OutF out, uint64_t n, uint32_t* tile_buf, uint32_t* total, cudaStream_t stream,
+                      uint32_t* done = nullptr) {
     const uint64_t tiles = flag_tiles(n);
     if (tiles == 0) {
         if (total) cudaMemsetAsync(total, 0, sizeof(uint32_t), stream);
         return;
     }
-    flag_count_kernel<Pred><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, n, tile_buf); count_launch();
-    scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(tile_buf, tiles, total, SumOp<uint32_t>()); count_launch();
+    flag_count_kernel<Pred><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, n, tile_buf, total, done);
+    count_launch();
+    if (!done) {
+        scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(tile_buf, tiles, total, SumOp<uint32_t>());
+        count_launch();
+    }
     flag_apply_kernel<Pred, OutF, kOutUnroll><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, out, n,
                                                                                                     tile_buf); count_launch();
 }
