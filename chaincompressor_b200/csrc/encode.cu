@@ -1892,19 +1892,32 @@ __device__ __forceinline__ void block_copy(uint8_t* dst, const uint8_t* src, uin
     for (uint32_t i = head + body + threadIdx.x; i < len; i += blockDim.x) dst[i] = src[i];
 }
 
-// One CTA per 4 KB segment; the piece of a segment is found by binary search, and for
-// a chunked piece the chunk by a second binary search over its segment prefix.
+// Each CTA copies a contiguous run of 4 KB segments: the pieces (at most max_pieces)
+// wait in shared memory, the run's first piece and, for a chunked piece, its first chunk
+// are found by binary search, and later segments advance both linearly.
+constexpr uint32_t kMaxPieces = 128;
 __global__ void __launch_bounds__(256) k_copy_pieces(const Piece* pieces, ChunkMaps maps, const EncState* st,
                                                       uint8_t* out) {
-    const uint32_t np = st->npieces;
+    __shared__ Piece sp[kMaxPieces];
+    const uint32_t np = min(st->npieces, kMaxPieces);
     const uint64_t nsegs = st->nsegs;
-    for (uint64_t g = blockIdx.x; g < nsegs; g += gridDim.x) {
-        uint32_t lo = 0, hi = np - 1;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (pieces[mid].seg_begin <= g) lo = mid; else hi = mid - 1;
+    for (uint32_t i = threadIdx.x; i < np; i += blockDim.x) sp[i] = pieces[i];
+    __syncthreads();
+    const uint64_t per = (nsegs + gridDim.x - 1) / gridDim.x;
+    const uint64_t g0 = static_cast<uint64_t>(blockIdx.x) * per, g1 = min(nsegs, g0 + per);
+    if (g0 >= g1) return;
+    uint32_t lo = 0, hi = np - 1;   // last piece with seg_begin <= g0
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (sp[mid].seg_begin <= g0) lo = mid; else hi = mid - 1;
+    }
+    uint32_t chunk = 0xffffffffu;   // current chunk of a chunked piece (searched on entry)
+    for (uint64_t g = g0; g < g1; ++g) {
+        while (lo + 1 < np && sp[lo + 1].seg_begin <= g) {
+            ++lo;
+            chunk = 0xffffffffu;
         }
-        const Piece pc = pieces[lo];
+        const Piece& pc = sp[lo];
         const uint8_t* src;
         uint8_t* dst;
         uint64_t len;
@@ -1916,11 +1929,17 @@ __global__ void __launch_bounds__(256) k_copy_pieces(const Piece* pieces, ChunkM
         } else {
             const ChunkMap& M = maps.m[pc.stream];
             const uint32_t ls = static_cast<uint32_t>(g - pc.seg_begin);
-            uint32_t a = 0, b = M.chunks - 1;   // last chunk with seg[k] <= ls
-            while (a < b) {
-                const uint32_t mid = (a + b + 1) >> 1;
-                if (M.seg[mid] <= ls) a = mid; else b = mid - 1;
+            if (chunk == 0xffffffffu) {   // last chunk with seg[k] <= ls
+                uint32_t a = 0, b = M.chunks - 1;
+                while (a < b) {
+                    const uint32_t mid = (a + b + 1) >> 1;
+                    if (M.seg[mid] <= ls) a = mid; else b = mid - 1;
+                }
+                chunk = a;
+            } else {
+                while (chunk + 1 < M.chunks && M.seg[chunk + 1] <= ls) ++chunk;
             }
+            const uint32_t a = chunk;
             const uint64_t clen = M.len[a];
             const uint64_t off = static_cast<uint64_t>(ls - M.seg[a]) * kCopySeg;
             src = M.slots + M.slot_cap * a + (M.slot_cap - clen) + off;
@@ -2495,7 +2514,7 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     uint64_t etab_total = 0;
     for (int s = 0; s < kCodeStreams; ++s)
         if (hs->ch[s].enc == kEncRaw || hs->ch[s].enc == kEncTagged) etab_total += hs->ch[s].sec_alphabet;
-    const uint64_t max_pieces = 128;
+    const uint64_t max_pieces = kMaxPieces;
     uint64_t bound = header_bytes(dims) + 40 + 8ull * hs->ndistinct;
     for (int s = 0; s < kCodeStreams; ++s) {
         const StreamChoice& c = hs->ch[s];
