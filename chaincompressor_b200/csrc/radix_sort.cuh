@@ -75,15 +75,17 @@ radix_hist_kernel(const KT* __restrict__ keys, uint64_t n, int shift, int bits, 
     if (threadIdx.x < bins) counts[static_cast<uint64_t>(threadIdx.x) * num_tiles + blockIdx.x] = hist[threadIdx.x];
 }
 
-// One CTA per digit: exclusive scan, in place, of the digit's row of tile counts
-// (counts[d * tiles .. d * tiles + tiles)); the row's total goes to row_total[d].
-__global__ void __launch_bounds__(kSortThreads)
+// One CTA of kRowscanThreads per digit: exclusive scan, in place, of the digit's row of
+// tile counts (counts[d * tiles .. d * tiles + tiles)); the row's total goes to
+// row_total[d].  A round covers 8192 tiles (about 25M four-byte keys).
+constexpr int kRowscanThreads = 1024;
+__global__ void __launch_bounds__(kRowscanThreads)
 radix_rowscan_kernel(uint32_t* __restrict__ counts, uint32_t num_tiles, uint32_t* __restrict__ row_total) {
     constexpr int kPer = 8;   // consecutive tiles per thread per round
     __shared__ uint32_t scratch[33];
     uint32_t* row = counts + static_cast<uint64_t>(blockIdx.x) * num_tiles;
     uint32_t carry = 0;
-    for (uint32_t base = 0; base < num_tiles; base += kSortThreads * kPer) {
+    for (uint32_t base = 0; base < num_tiles; base += kRowscanThreads * kPer) {
         const uint32_t t0 = base + threadIdx.x * kPer;
         uint32_t v[kPer];
         uint32_t sum = 0;
@@ -294,7 +296,7 @@ bool radix_sort_pairs(const KT* keys_in, KT* keys_a, uint32_t* vals_a, KT* keys_
         if (p > 0 || !first_counts_ready) {
             radix_hist_kernel<KT><<<tiles, kSortThreads, 0, stream>>>(kin, n, shift, plan.bits, counts, tiles); count_launch();
         }
-        radix_rowscan_kernel<<<1u << plan.bits, kSortThreads, 0, stream>>>(counts, tiles, row_total); count_launch();
+        radix_rowscan_kernel<<<1u << plan.bits, kRowscanThreads, 0, stream>>>(counts, tiles, row_total); count_launch();
         hook(false);
         launch_radix_scatter<KT>(plan.bits, tiles, stream, kin, vin, kout, vout, n, shift, counts, row_total);
         hook(true);
