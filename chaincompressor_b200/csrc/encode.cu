@@ -211,7 +211,7 @@ __device__ void qparams(EncState* st) {
         const double mx = from_ordered_bits(__ldcg(&st->maxbits[d]));
         const double qv = floor((mx - mn) / denom);
         if (!(qv >= 0.0 && qv < 0x1p63)) { set_error(&st->err, kErrQuantOverflow); return; }
-        if (qv >= 2147483648.0) { set_error(&st->err, kErrUnsupported); return; }
+        if (qv >= 4294967296.0) { set_error(&st->err, kErrUnsupported); return; }   // 32-bit q
         st->qmax[d] = static_cast<uint32_t>(qv);
         const uint32_t b = static_cast<uint32_t>(static_cast<uint64_t>(st->qmax[d]) / st->p);
         bmax = b > bmax ? b : bmax;
@@ -237,7 +237,7 @@ __device__ __forceinline__ bool within_error_bound(double restored, double origi
     return difference >= 0.0 ? remainder <= 0.0 : remainder >= 0.0;
 }
 
-// Block index b = q / p and rel = q - b*p for q < 2^31: a shift and a mask when p is a
+// Block index b = q / p and rel = q - b*p for q < 2^32: a shift and a mask when p is a
 // power of two, else a double-precision reciprocal estimate corrected to the exact
 // quotient (the estimate is off by at most one).
 struct BlockDiv {

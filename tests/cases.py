@@ -61,6 +61,11 @@ def case(name):
         # more than four dimensions: the statistics kernel that reads D at run time
         rng = np.random.default_rng(17)
         return rng.uniform(-5, 5, size=(20_000, 6)).astype(np.float32), 1e-2, 4, 2, {}
+    if name == "big_q":
+        # quantized values between 2^31 and 2^32 (about 3.3e9 steps per axis; p = 4 gives
+        # 30-bit block coordinates and 90-bit block keys)
+        rng = np.random.default_rng(18)
+        return rng.uniform(0, 1, size=(20_000, 3)), 1.5e-10, 4, 2, {}
     if name == "no_l1":
         pts = W.column(20_000, 5)
         return pts, W.eb_for(pts, 1e-3), 4, 2, {"l1": False}
@@ -106,4 +111,4 @@ def case(name):
 
 GPU_CASES = ["column", "column_qb11", "blobs200k", "blobs_clipped", "traj_f64_e4_p1", "traj_f64_e2",
              "uniform_p64_t25", "single_point", "one_block", "long_chain", "p1_big_threshold", "neg_threshold", "dims1", "dims2",
-             "dims4", "dims6", "no_l1", "no_l2", "no_bl", "big_values_tagged", "wide_jump", "negative_zero", "many_corrections", "wide_key"]
+             "dims4", "dims6", "big_q", "no_l1", "no_l2", "no_bl", "big_values_tagged", "wide_jump", "negative_zero", "many_corrections", "wide_key"]

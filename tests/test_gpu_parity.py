@@ -78,6 +78,10 @@ def test_errors(codec):
     with pytest.raises(N.ChainError) as e:
         codec.compress(_soa(bad), eb, p, t, layout=N.CHAIN_SOA)
     assert e.value.status == N.CHAIN_ERR_NONFINITE_INPUT
+    # quantized values of 2^32 and more are beyond this build (below 2^32 they are coded)
+    with pytest.raises(N.ChainError) as e:
+        codec.compress(_soa(pts), float(np.max(pts.max(0) - pts.min(0))) * 1e-11, p, t, layout=N.CHAIN_SOA)
+    assert e.value.status == N.CHAIN_ERR_UNSUPPORTED
     # the context stays usable after errors
     data = codec.compress(_soa(pts), eb, p, t, layout=N.CHAIN_SOA)
     assert codec.decompress(data).shape == pts.shape
