@@ -1288,14 +1288,36 @@ __global__ void __launch_bounds__(kStatsThreads, 4) k_stream_stats_lanes(StreamR
 // One CTA per (stream, kind): kind 0 = raw value table, kind 1 = tag table.
 __device__ void plan_stream(const StreamRefs& refs, EncState* st, uint32_t bytes_per_lane, uint32_t max_steps, int s);
 
+// The table bytes of stream s's chosen coding into out (and its length into the plan)
+// and its encoder symbol entries into et, by one CTA of kTableThreads; stage holds
+// 4 * kSerStageSyms bytes.
+__device__ void serialize_stream(EncState* st, const uint32_t* prob, const uint32_t* cum, const uint32_t* tag_prob,
+                                 const uint32_t* tag_cum, uint64_t hist_stride, int s, uint8_t* out, uint4* et,
+                                 uint32_t* stage) {
+    StreamChoice& c = st->ch[s];
+    const bool raw = c.enc == kEncRaw;
+    if (!raw && c.enc != kEncTagged) {
+        if (threadIdx.x == 0) c.table_len = 0;
+        return;
+    }
+    const uint32_t* pr = raw ? prob + hist_stride * s : tag_prob + 64 * s;
+    const uint32_t* cm = raw ? cum + hist_stride * s : tag_cum + 64 * s;
+    const uint32_t len = serialize_table_block(pr, c.sec_alphabet, out, stage);
+    if (threadIdx.x == 0) c.table_len = len;
+    for (uint32_t a = threadIdx.x; a < c.sec_alphabet; a += blockDim.x) et[a] = make_enc_symbol(pr[a], cm[a], c.sec_prec);
+}
+
 // The CTA that finishes last plans the launch's streams (plan_stream), so that the plan
 // needs no launch of its own; done is the launch's hand-off counter.  For IDR0 (s0 = 0)
-// each CTA first completes the statistics its table reads from the level-1 counts.
+// each CTA first completes the statistics its table reads from the level-1 counts.  With
+// ser_out (a launch of one stream), the last CTA also serialises that stream's table to
+// ser_out + s0 * ser_stride and writes its encoder entries to etab.
 __global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncState* st, uint32_t* hist,
                                                            uint64_t hist_stride, uint32_t* prob, uint32_t* cum,
                                                            uint32_t* tag_prob, uint32_t* tag_cum, int s0,
                                                            uint32_t bytes_per_lane, uint32_t max_steps,
-                                                           uint32_t* done) {
+                                                           uint32_t* done, uint8_t* ser_out, uint64_t ser_stride,
+                                                           uint4* etab) {
     extern __shared__ __align__(16) uint32_t tstage[];   // kTableStageBytes
     const int s = s0 + blockIdx.x, kind = blockIdx.y;
     const StreamRef r = refs.s[s];
@@ -1324,6 +1346,11 @@ __global__ void __launch_bounds__(kTableThreads) k_tables(StreamRefs refs, EncSt
     if (!s_last) return;
     __threadfence();
     if (threadIdx.x < gridDim.x) plan_stream(refs, st, bytes_per_lane, max_steps, s0 + threadIdx.x);
+    if (ser_out) {
+        __syncthreads();   // the plan of stream s0 is written
+        static_assert(4 * kSerStageSyms <= kTableStageBytes, "the serialisation stage fits the table stage");
+        serialize_stream(st, prob, cum, tag_prob, tag_cum, hist_stride, s0, ser_out + ser_stride * s0, etab, tstage);
+    }
     if (threadIdx.x == 0) *done = 0;
 }
 
@@ -1650,14 +1677,14 @@ __global__ void k_words_to_bytes(uint32_t* words, uint64_t nwords) {
         words[w] = __byte_perm(words[w], 0, 0x0123);
 }
 
-// Serialises every chosen table (blockIdx.y == 0, one CTA per stream) and writes the
-// streams' encoder symbol entries (make_enc_symbol) for their rANS sections (blockIdx.y
-// > 0: kEtabSlices CTAs per stream, each a slice of the alphabet).
+// Serialises every chosen table of streams s0.. (blockIdx.y == 0, one CTA per stream)
+// and writes the streams' encoder symbol entries (make_enc_symbol) for their rANS
+// sections (blockIdx.y > 0: kEtabSlices CTAs per stream, each a slice of the alphabet).
 __global__ void __launch_bounds__(1024) k_serialize_tables(EncState* st, const uint32_t* prob, const uint32_t* tag_prob,
                                                             uint64_t hist_stride, uint8_t* out, uint64_t out_stride,
-                                                            RansJobs J, StreamJobs sj) {
+                                                            int s0, RansJobs J, StreamJobs sj) {
     extern __shared__ __align__(16) uint32_t ser_stage[];   // kSerStageSyms u32
-    const int s = blockIdx.x;
+    const int s = s0 + blockIdx.x;
     if (blockIdx.y > 0) {
         if (sj.job[s] < 0) return;
         const RansJob& jb = J.job[sj.job[s]];
@@ -2292,6 +2319,10 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     need += Arena::need(hist_stride * kCodeStreams, 4) * 3;  // hist, prob, cum
     need += Arena::need(64 * kCodeStreams, 4) * 2;
     need += Arena::need(corr_cap, 4) * 2 + Arena::need(corr_cap, 8);  // correction gaps, ids, values
+    // serialised tables, and IDR0's encoder entries (written on the side stream before
+    // the coding buffers are sized)
+    const uint64_t table_stride = 4 * kRansMaxAlphabet + 64;
+    need += Arena::need(table_stride * kCodeStreams, 1) + Arena::need(kRansMaxAlphabet + 1, 16);
     need += 64 * 256;
     CHAIN_CUDA(ctx->frame.reserve(need));
     Arena& A = ctx->frame;
@@ -2325,7 +2356,9 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     uint32_t* corr_gaps = A.take<uint32_t>(corr_cap);
     uint32_t* corr_ids = A.take<uint32_t>(corr_cap);
     uint64_t* corr_dict = A.take<uint64_t>(corr_cap);
-    if (!tag_cum) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder frame arena too small");
+    uint8_t* tables = A.take<uint8_t>(table_stride * kCodeStreams);
+    uint4* etab0 = A.take<uint4>(kRansMaxAlphabet + 1);
+    if (!tag_cum || !etab0) return set_err(CHAIN_ERR_OUT_OF_MEMORY, "encoder frame arena too small");
 
     static_assert((kRansMaxAlphabet * kCodeStreams) % 4 == 0, "histograms zeroed in 16-byte words");
     k_init_state<<<148, 256, 0, stream>>>(st, dims, n, eb, static_cast<uint64_t>(p_eff), threshold, hist,
@@ -2404,7 +2437,8 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     CHAIN_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
     k_tables<<<dim3(1, 2), kTableThreads, kTableStageBytes, ctx->side>>>(idr, st, hist, hist_stride, prob, cum, tag_prob,
                                                                          tag_cum, 0, bytes_per_lane, max_steps,
-                                                                         &st->done_c); count_launch();
+                                                                         &st->done_c, tables, table_stride, etab0);
+    count_launch();
     CHAIN_CUDA(cudaEventRecord(ctx->join_ev, ctx->side));
     SideJoin join{ctx};
     CHAIN_LAUNCH_CHECK("IDR0 tables");
@@ -2438,7 +2472,8 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     join.ctx = nullptr;
     k_tables<<<dim3(kStreams - 1, 2), kTableThreads, kTableStageBytes, stream>>>(refs, st, hist, hist_stride, prob, cum,
                                                                                    tag_prob, tag_cum, 1, bytes_per_lane,
-                                                                                   max_steps, &st->done_b); count_launch();
+                                                                                   max_steps, &st->done_b, nullptr, 0,
+                                                                                   nullptr); count_launch();
     CHAIN_LAUNCH_CHECK("plan");
     T.mark("tables+plan", stream);
     CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
@@ -2476,7 +2511,8 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
         launch_stats(refs, st, hist, hist_stride, dims, nc, kCorrGaps, 2, stream);
         k_tables<<<dim3(2, 2), kTableThreads, kTableStageBytes, stream>>>(refs, st, hist, hist_stride, prob, cum,
                                                                          tag_prob, tag_cum, kCorrGaps, bytes_per_lane,
-                                                                         max_steps, &st->done_b); count_launch();
+                                                                         max_steps, &st->done_b, nullptr, 0, nullptr);
+        count_launch();
         CHAIN_LAUNCH_CHECK("corrections");
         CHAIN_CUDA(cudaMemcpyAsync(hs, st, sizeof(EncState), cudaMemcpyDeviceToHost, stream));
         CHAIN_CUDA(cudaStreamSynchronize(stream));
@@ -2510,9 +2546,8 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
             tags_total += c.records;
         }
     }
-    const uint64_t table_stride = 4 * kRansMaxAlphabet + 64;
-    uint64_t etab_total = 0;
-    for (int s = 0; s < kCodeStreams; ++s)
+    uint64_t etab_total = 0;   // IDR0's entries are in etab0
+    for (int s = 1; s < kCodeStreams; ++s)
         if (hs->ch[s].enc == kEncRaw || hs->ch[s].enc == kEncTagged) etab_total += hs->ch[s].sec_alphabet;
     const uint64_t max_pieces = kMaxPieces;
     uint64_t bound = header_bytes(dims) + 40 + 8ull * hs->ndistinct;
@@ -2526,7 +2561,7 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     }
     size_t need2 = Arena::need(slots_total, 1) + Arena::need(packed_total, 1) + Arena::need(tags_total + 1, 4) +
                    Arena::need(total_chunks + 1, 4) + Arena::need(total_chunks * 32 + 1, 4) * 2 +
-                   Arena::need(table_stride * kCodeStreams, 1) + Arena::need(max_pieces, sizeof(Piece)) +
+                   Arena::need(max_pieces, sizeof(Piece)) +
                    Arena::need(bound, 1) + Arena::need(etab_total + 1, 16) + Arena::need(total_chunks + 1, 8) +
                    Arena::need(total_chunks + kCodeStreams + 1, 4) + 11 * 256;
     CHAIN_CUDA(ctx->coded.reserve(need2));
@@ -2538,7 +2573,6 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     uint32_t* packed_states = C.take<uint32_t>(total_chunks * 32 + 1);
     uint32_t* tags = C.take<uint32_t>(tags_total + 1);
     uint32_t* chunk_len = C.take<uint32_t>(total_chunks + 1);
-    uint8_t* tables = C.take<uint8_t>(table_stride * kCodeStreams);
     Piece* pieces = C.take<Piece>(max_pieces);
     uint8_t* container = C.take<uint8_t>(bound);
     uint4* etab = C.take<uint4>(etab_total + 1);
@@ -2631,8 +2665,12 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
             jb.cum = c.enc == kEncRaw ? cum + hist_stride * s : tag_cum + 64 * s;
             jb.prec = c.sec_prec;
             jb.alphabet = c.sec_alphabet;
-            jb.etab = etab + etab_used;
-            etab_used += c.sec_alphabet;
+            if (s == 0) {
+                jb.etab = etab0;   // written with IDR0's table on the side stream
+            } else {
+                jb.etab = etab + etab_used;
+                etab_used += c.sec_alphabet;
+            }
             jb.chunks = c.sec_chunks;
             jb.lanes = c.sec_lanes;
             jb.S = c.sec_S;
@@ -2667,8 +2705,9 @@ static chain_status encode_frame_cap(chain_ctx* ctx, const void* points, chain_d
     T.mark("corrections+packing", stream);
     CHAIN_CUDA(cudaFuncSetAttribute(k_serialize_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(4 * kSerStageSyms)));
-    k_serialize_tables<<<dim3(kCodeStreams, 1 + kEtabSlices), 1024, 4 * kSerStageSyms, stream>>>(st, prob, tag_prob, hist_stride, tables,
-                                                                          table_stride, jobs, stream_jobs); count_launch();
+    // streams 1..: IDR0's table and entries came with its plan on the side stream
+    k_serialize_tables<<<dim3(kCodeStreams - 1, 1 + kEtabSlices), 1024, 4 * kSerStageSyms, stream>>>(
+        st, prob, tag_prob, hist_stride, tables, table_stride, 1, jobs, stream_jobs); count_launch();
     T.mark("serialize_tables", stream);
     if (jobs.total_blocks) {
         rans_plan_smem(jobs, false);
