@@ -934,8 +934,10 @@ __device__ __forceinline__ uint32_t rans_encode_step(uint32_t x, const uint4& e,
     rel -= __popc(b0) + 2 * __popc(b1);
     uint8_t* o = ow + rel + __popc(b0 & lt) + 2 * __popc(b1 & lt);
     if (nb > 0) o[nb - 1] = static_cast<uint8_t>(x);
-    if (nb > 1) o[nb - 2] = static_cast<uint8_t>(x >> 8);
-    if (nb > 2) o[0] = static_cast<uint8_t>(x >> 16);
+    if (b1) {   // some lane emits two or three bytes (rare: skipped warp-uniformly)
+        if (nb > 1) o[nb - 2] = static_cast<uint8_t>(x >> 8);
+        if (nb > 2) o[0] = static_cast<uint8_t>(x >> 16);
+    }
     if (act) {
         x >>= 8 * nb;
         const uint32_t q = __umulhi(x, e.z) >> (e.w >> 24);
