@@ -165,24 +165,6 @@ __host__ __device__ inline uint64_t spread3(uint64_t n) {
     n = (n | (n << 2)) & 0x1249249249249249ull;
     return n;
 }
-// 3-D Morton spreading of 10 bits in 32-bit arithmetic (bits i -> 3i).
-__host__ __device__ inline uint32_t spread3_32(uint32_t x) {
-    x &= 0x3FFu;
-    x = (x | (x << 16)) & 0x030000FFu;
-    x = (x | (x << 8)) & 0x0300F00Fu;
-    x = (x | (x << 4)) & 0x030C30C3u;
-    x = (x | (x << 2)) & 0x09249249u;
-    return x;
-}
-// The same for the 10 bits a 30-bit key holds per dimension, in 32-bit arithmetic.
-__host__ __device__ inline uint32_t compact3_32(uint32_t x) {
-    x &= 0x09249249u;
-    x = (x ^ (x >> 2)) & 0x030C30C3u;
-    x = (x ^ (x >> 4)) & 0x0300F00Fu;
-    x = (x ^ (x >> 8)) & 0xFF0000FFu;
-    x = (x ^ (x >> 16)) & 0x000003FFu;
-    return x;
-}
 __host__ __device__ inline uint32_t compact3(uint64_t n) {
     n &= 0x1249249249249249ull;
     n = (n ^ (n >> 2)) & 0x10C30C30C30C30C3ull;
@@ -258,14 +240,17 @@ __host__ __device__ inline void block_unkey128(u128 k, int dims, int kb, uint32_
 }
 
 // Key of block coordinates b and its inverse, for a key type of 32, 64 or 128 bits.
-// (A 32-bit key of three dimensions has kb <= 10: its interleave runs in 32-bit words.)
+// Three dimensions in a 4- or 8-byte key (kb <= 21) take the plain concatenation of
+// the coordinates, b0 | b1 << kb | b2 << 2 kb, instead of the interleave: the encoder
+// only needs equal keys <=> equal blocks (no order of blocks), and the fields come back
+// with shifts.
 template <typename KT>
 __host__ __device__ inline KT make_block_key(const uint32_t* b, int dims, int kb) {
     if constexpr (sizeof(KT) == 16) {
         return block_key128(b, dims, kb);
     } else {
-        if constexpr (sizeof(KT) == 4)
-            if (dims == 3) return spread3_32(b[0]) | (spread3_32(b[1]) << 1) | (spread3_32(b[2]) << 2);
+        if (dims == 3)
+            return static_cast<KT>(b[0]) | (static_cast<KT>(b[1]) << kb) | (static_cast<KT>(b[2]) << (2 * kb));
         return static_cast<KT>(block_key(b, dims, kb));
     }
 }
@@ -274,14 +259,13 @@ __host__ __device__ inline void block_coords(KT k, int dims, int kb, uint32_t* b
     if constexpr (sizeof(KT) == 16) {
         block_unkey128(k, dims, kb, b);
     } else {
-        if constexpr (sizeof(KT) == 4)
-            if (dims == 3) {
-                const uint32_t k32 = static_cast<uint32_t>(k);
-                b[0] = compact3_32(k32);
-                b[1] = compact3_32(k32 >> 1);
-                b[2] = compact3_32(k32 >> 2);
-                return;
-            }
+        if (dims == 3) {
+            const KT mask = (static_cast<KT>(1) << kb) - 1;
+            b[0] = static_cast<uint32_t>(k & mask);
+            b[1] = static_cast<uint32_t>((k >> kb) & mask);
+            b[2] = static_cast<uint32_t>(k >> (2 * kb));
+            return;
+        }
         block_unkey(static_cast<uint64_t>(k), dims, kb, b);
     }
 }

@@ -473,6 +473,7 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
     // contended shared-memory bins
     PackedCount8 vc, tc;
     const int D = DIM ? DIM : static_cast<int>(st->dims);
+    const int kb3 = st->kb;   // field width of a concatenated 3-D key
     const int64_t maxb_bits = st->maxb_bits;
     const int64_t thr = st->threshold;
     const int64_t c = static_cast<int64_t>(D) * maxb_bits;
@@ -521,9 +522,17 @@ k_level1(const KT* __restrict__ skey, const uint32_t* __restrict__ sidx, uint64_
                 uint32_t out = 0;
                 if (k + 1 < n && keys[u][j + 1] == keys[u][j]) {
                     const uint32_t dist = idxs[u][j + 1] - idxs[u][j];
-                    // bit j of block coordinate d sits at key bit j * D + d, so the widest
-                    // coordinate of the block has ceil(bitlen(key) / D) bits
-                    const int local_bits = (key_bitlen(keys[u][j]) + D - 1) / D;
+                    // bits of the block's widest coordinate: of the OR of the three fields
+                    // of a concatenated 3-D key, else ceil(bitlen(key) / D) of an
+                    // interleaved one (bit j of coordinate d sits at key bit j * D + d)
+                    int local_bits;
+                    if constexpr (DIM == 3 && sizeof(KT) <= 8) {
+                        const KT kk = keys[u][j];
+                        const KT m = (static_cast<KT>(1) << kb3) - 1;
+                        local_bits = bitlen64(static_cast<uint64_t>((kk & m) | ((kk >> kb3) & m) | (kk >> (2 * kb3))));
+                    } else {
+                        local_bits = (key_bitlen(keys[u][j]) + D - 1) / D;
+                    }
                     const int tag_bits = bitlen32(static_cast<uint32_t>(local_bits));
                     const int64_t a = static_cast<int64_t>(local_bits) * D + tag_bits;
                     const int64_t smaller = a < c ? a : c;
@@ -605,72 +614,25 @@ struct ExplicitIn {
     const uint32_t* idrel;
     __device__ uint32_t operator()(uint64_t i) const { return idrel[i] == 0 ? 1u : 0u; }
 };
-// An explicit record is kept in one key-sized word, which moves D times fewer bytes
-// than separate coordinates through the level-2 passes: for three dimensions with kb <=
-// 21 (kPack3) the block coordinates packed at a fixed field width (rec3_pack; the level-2
-// passes then unpack them with shifts), otherwise the point's block key (decoded where
-// it is used).
-template <typename KT, bool kPack3>
+// An explicit record is kept as its point's block key, which moves D times fewer bytes
+// than separate coordinates through the level-2 passes (rec_read takes the coordinates
+// back out: three shifts for three dimensions in a 4- or 8-byte key).
+template <typename KT>
 struct ExplicitOut {
     const KT* key;
     KT* rec;
-    __device__ void operator()(uint64_t i, uint32_t pos, uint32_t flag) const;
-};
-
-// Block coordinates of a record key (D dimensions of kb bits each).
-template <int DIM, typename KT>
-__device__ __forceinline__ void rec_coords(KT k, int D, int kb, uint32_t* b) {
-    if constexpr (DIM == 3 && sizeof(KT) == 4) {   // kb <= 10
-        const uint32_t k32 = static_cast<uint32_t>(k);
-        b[0] = compact3_32(k32);
-        b[1] = compact3_32(k32 >> 1);
-        b[2] = compact3_32(k32 >> 2);
-    } else if constexpr (DIM == 3 && sizeof(KT) <= 8) {   // kb <= 21: the 3-D Morton compaction
-        const uint64_t k64 = static_cast<uint64_t>(k);
-        b[0] = compact3(k64);
-        b[1] = compact3(k64 >> 1);
-        b[2] = compact3(k64 >> 2);
-    } else {
-        block_coords<KT>(k, D, kb, b);
+    __device__ void operator()(uint64_t i, uint32_t pos, uint32_t flag) const {
+        if (flag) rec[pos] = key[i];
     }
-}
+};
 
 // Level-2 work runs with DIM = 3 (three dimensions, kb <= 21) or DIM = 0 (any shape).
 __device__ __forceinline__ bool l2_dim3(const EncState* st) { return st->dims == 3 && st->kb <= 21; }
 
-// Three block coordinates of kb <= 21 bits packed into a key-sized word: fields of 10 bits
-// in a 32-bit word (3 kb <= 32 there, so kb <= 10), of 21 bits in a 64-bit one.
-// (16-byte keys have kb > 21 in three dimensions: their records stay keys.)
-template <typename KT>
-struct Rec3 {
-    static constexpr int kField = sizeof(KT) == 4 ? 10 : 21;
-    static constexpr KT kMask = (KT(1) << kField) - 1;
-};
-template <typename KT>
-__device__ __forceinline__ KT rec3_pack(KT key) {
-    uint32_t b[3];
-    rec_coords<3, KT>(key, 3, 0, b);
-    constexpr int F = Rec3<KT>::kField;
-    return static_cast<KT>(b[0]) | (static_cast<KT>(b[1]) << F) | (static_cast<KT>(b[2]) << (2 * F));
-}
-template <typename KT, bool kPack3>
-__device__ void ExplicitOut<KT, kPack3>::operator()(uint64_t i, uint32_t pos, uint32_t flag) const {
-    if (!flag) return;
-    if constexpr (kPack3) rec[pos] = rec3_pack<KT>(key[i]);
-    else rec[pos] = key[i];
-}
-
-// Block coordinates of an explicit record (as ExplicitOut stored it).
+// Block coordinates of an explicit record (a block key, make_block_key).
 template <int DIM, typename KT>
 __device__ __forceinline__ void rec_read(KT r, int D, int kb, uint32_t* b) {
-    if constexpr (DIM == 3 && sizeof(KT) <= 8) {
-        constexpr int F = Rec3<KT>::kField;
-        b[0] = static_cast<uint32_t>(r & Rec3<KT>::kMask);
-        b[1] = static_cast<uint32_t>((r >> F) & Rec3<KT>::kMask);
-        b[2] = static_cast<uint32_t>((r >> (2 * F)) & Rec3<KT>::kMask);
-    } else {
-        block_coords<KT>(r, D, kb, b);
-    }
+    block_coords<KT>(r, DIM ? DIM : D, kb, b);
 }
 
 // ------------------------------------------------------------------- level 2
@@ -2211,17 +2173,7 @@ static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, ui
                        uint32_t kd_esz, uint8_t* choice2, void* keep, void* diff, uint32_t* scan32, StageTimer& T,
                        cudaStream_t stream) {
     KT* rec = static_cast<KT*>(rec_v);
-    if constexpr (sizeof(KT) <= 8) {
-        if (d3)
-            device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, true>{key_idx, rec}, n, scan32, &st->B, stream,
-                         &st->done_a);
-        else
-            device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, false>{key_idx, rec}, n, scan32, &st->B, stream,
-                         &st->done_a);
-    } else {
-        device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT, false>{key_idx, rec}, n, scan32, &st->B, stream,
-                         &st->done_a);
-    }
+    device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT>{key_idx, rec}, n, scan32, &st->B, stream, &st->done_a);
     T.mark("explicit_records", stream);
     if (d3) {
         k_l2_stats<KT, 3><<<grid_for((n + 3) / 4, 256, 148u * 4u), 256, 0, stream>>>(rec, st); count_launch();
