@@ -23,7 +23,7 @@ namespace chain {
 
 struct DecState {
     uint32_t err;
-    uint32_t pad0;
+    uint32_t done;          // hand-off counter of last-CTA scans (zero between them)
     uint32_t zeros;         // idrel == 0 count
     uint32_t ndiff_seen;
     uint64_t tag_bits[kCodeStreams];
@@ -33,6 +33,7 @@ struct DecState {
 
 __device__ void dec_init(DecState* st) {
     st->err = 0;
+    st->done = 0;
     st->zeros = 0;
     st->ndiff_seen = 0;
     for (int s = 0; s < kCodeStreams; ++s) { st->tag_bits[s] = 0; st->maxtag[s] = 0; }
@@ -339,9 +340,11 @@ struct ResetAddOp {
 };
 
 // Difference records per flag-scan tile from CH20's 1-bit packing: one CTA per tile,
-// one 32-record word per thread.
+// one 32-record word per thread; the last CTA turns the counts into the tiles' exclusive
+// prefixes and writes their total (last_cta_scan_counts).
 __global__ void __launch_bounds__(kFlagTile / 32) k_choice_counts(const uint8_t* cbits, uint64_t len, uint64_t off,
-                                                                  uint64_t B, uint32_t* tile_counts) {
+                                                                  uint64_t B, uint32_t* tile_counts, uint32_t* total,
+                                                                  uint32_t* done) {
     __shared__ uint32_t wsum[kFlagTile / 32 / 32];
     const uint64_t j0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile + 32ull * threadIdx.x;
     uint32_t c = 0;
@@ -357,6 +360,7 @@ __global__ void __launch_bounds__(kFlagTile / 32) k_choice_counts(const uint8_t*
         for (int w = 0; w < kFlagTile / 32 / 32; ++w) t += wsum[w];
         tile_counts[blockIdx.x] = t;
     }
+    last_cta_scan_counts(tile_counts, total, done);
 }
 
 // Choice values are clamped to {0, 1} for the ranks (so every derived index stays in
@@ -1319,15 +1323,14 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     uint32_t* tile_diff = reinterpret_cast<uint32_t*>(scanbuf);
     L2Vec* tile_l2 = reinterpret_cast<L2Vec*>(reinterpret_cast<uint8_t*>(scanbuf) + ((4 * l2tiles + 15) & ~15ull));
     if (l2tiles) {
+        // difference records per tile, scanned by the counting launch's last CTA
         if (choice_packed)
             k_choice_counts<<<static_cast<unsigned>(l2tiles), kFlagTile / 32, 0, stream>>>(
-                dcont, len, plan.comp[3].packed_off[0], B, tile_diff);
+                dcont, len, plan.comp[3].packed_off[0], B, tile_diff, ndiff_dev, &st->done);
         else
             flag_count_kernel<ChoiceIn><<<static_cast<unsigned>(l2tiles), kFlagThreads, 0, stream>>>(
-                ChoiceIn{streams[3]}, B, tile_diff);
+                ChoiceIn{streams[3]}, B, tile_diff, ndiff_dev, &st->done);
         count_launch();
-        scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(tile_diff, l2tiles, ndiff_dev,
-                                                                                SumOp<uint32_t>()); count_launch();
         const ResetAddOp l2op{static_cast<uint32_t>(range), static_cast<uint32_t>(range >> 32)};
         L2Geo g;
         g.choice2 = streams[3];
@@ -1363,7 +1366,7 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
     uint32_t* zeros_dev = reinterpret_cast<uint32_t*>(misc + 2);
     uint32_t* chained = drank;  // the choice ranks are no longer needed
     device_flag_scan(ZeroIn{streams[0]}, ZeroRankOut{streams[0], parent, chained, st, N}, N,
-                     reinterpret_cast<uint32_t*>(scanbuf), zeros_dev, stream);
+                     reinterpret_cast<uint32_t*>(scanbuf), zeros_dev, stream, &st->done);
     T.mark("zero_ranks", stream);
     int rounds = 1;
     while ((1ull << rounds) < N) ++rounds;
