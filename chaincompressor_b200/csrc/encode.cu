@@ -725,8 +725,8 @@ __device__ void l2_params(EncState* st) {
 
 // The level-2 rule (lcps_cpp.cpp:1305-1454) for record j given its and its
 // predecessor's coordinates: 1 = code it as the difference from the previous record.
-__device__ __forceinline__ uint32_t l2_rule(const uint32_t* cur, const uint32_t* prev, int D, uint64_t fvb,
-                                           uint64_t fdb) {
+__device__ __forceinline__ uint32_t l2_rule(const uint32_t* cur, const uint32_t* prev, int D, uint32_t fvb,
+                                           uint32_t fdb) {
     uint32_t mv = 0, md = 0;
     for (int d = 0; d < D; ++d) {
         mv = cur[d] > mv ? cur[d] : mv;
@@ -734,12 +734,15 @@ __device__ __forceinline__ uint32_t l2_rule(const uint32_t* cur, const uint32_t*
         md = a > md ? a : md;
     }
     const int tvw = bitlen32(mv), tdw = bitlen32(md);
-    const uint64_t tvb = static_cast<uint64_t>(D) * tvw + bitlen32(static_cast<uint32_t>(tvw));
-    const uint64_t tdb = static_cast<uint64_t>(D) * tdw + bitlen32(static_cast<uint32_t>(tdw));
-    const uint64_t value_bits = tvb < fvb ? tvb : fvb;
-    const uint64_t diff_bits = tdb > fdb ? tdb : fdb;
+    // at most 16 x 32 + 6 bits: 32-bit arithmetic is exact
+    const uint32_t tvb = static_cast<uint32_t>(D) * tvw + bitlen32(static_cast<uint32_t>(tvw));
+    const uint32_t tdb = static_cast<uint32_t>(D) * tdw + bitlen32(static_cast<uint32_t>(tdw));
+    const uint32_t value_bits = tvb < fvb ? tvb : fvb;
+    const uint32_t diff_bits = tdb > fdb ? tdb : fdb;
     return value_bits >= diff_bits ? 1u : 0u;
 }
+
+__device__ __forceinline__ uint64_t tile0_of_block() { return static_cast<uint64_t>(blockIdx.x) * kFlagTile; }
 
 // choice2[j] for every record (1 = difference from the previous record), one CTA per
 // flag-scan tile of kFlagTile records; each CTA also writes its tile's count of
@@ -755,11 +758,16 @@ __global__ void __launch_bounds__(256) k_l2_choice(const KT* __restrict__ rec, E
     if (DIM == 0 && l2_dim3(st)) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) l2_params(st);   // read by the level-2 output and the layout
     const uint32_t B = st->B;
+    if (tile0_of_block() >= B) {   // the grid covers n >= B entries: an empty tile counts 0
+        if (threadIdx.x == 0) tile_counts[blockIdx.x] = 0;
+        last_cta_scan_counts(tile_counts, &st->ndiff, &st->done_a);
+        return;
+    }
     const int D = DIM ? DIM : static_cast<int>(st->dims);
     const int kb = st->kb;
     const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile;
-    const uint64_t fvb = static_cast<uint64_t>(D) * bitlen32(st->rec_max);
-    const uint64_t fdb = static_cast<uint64_t>(D) * bitlen32(st->rec_maxdiff);
+    const uint32_t fvb = static_cast<uint32_t>(D) * bitlen32(st->rec_max);
+    const uint32_t fdb = static_cast<uint32_t>(D) * bitlen32(st->rec_maxdiff);
     constexpr int KD = DIM ? DIM : kMaxDims;
     constexpr int kG = 4;
     uint32_t cnt = 0;
@@ -831,38 +839,51 @@ __global__ void __launch_bounds__(kFlagThreads) k_l2_rows(const KT* __restrict__
     if (DIM == 0 && l2_dim3(st)) return;
     __shared__ uint32_t wsum[kFlagThreads / 32];
     const uint32_t B = st->B;
+    // the grid covers n >= B entries: tiles wholly past the records have nothing to write
+    if (static_cast<uint64_t>(blockIdx.x) * kFlagTile >= B) return;
     const int D = DIM ? DIM : static_cast<int>(st->dims);
     const int kb = st->kb;
     const int64_t wmin = st->wrap_min_corr, wmax = st->wrap_max_corr, wrange = st->wrap_range;
     constexpr int KD = DIM ? DIM : kMaxDims;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * kFlagItems;
+    // all of the slice's loads first: choice bytes, and the keys when they are at most
+    // eight bytes (one round trip to memory per warp instead of one per item)
+    constexpr bool kPre = sizeof(KT) <= 8;
+    KT kk[kPre ? kFlagItems : 1];
     uint32_t m[kFlagItems];
-    uint32_t c = 0;
 #pragma unroll
     for (int k = 0; k < kFlagItems; ++k) {
         const uint64_t i = base + 32 * k + lane;
-        m[k] = __ballot_sync(0xffffffffu, i < B && choice2[i] != 0);
+        m[k] = i < B ? choice2[i] : 0u;
+        if (kPre) kk[k] = i < B ? ldg_key(rec + i) : KT(0);
+    }
+    KT kprev = base > 0 && base - 1 < B ? ldg_key(rec + base - 1) : KT(0);
+    const uint32_t tp = tile_prefix[blockIdx.x];
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < kFlagItems; ++k) {
+        m[k] = __ballot_sync(0xffffffffu, m[k] != 0);
         c += __popc(m[k]);
     }
     if (lane == 0) wsum[warp] = c;
     __syncthreads();
-    uint32_t run = tile_prefix[blockIdx.x];
+    uint32_t run = tp;
     for (int w = 0; w < warp; ++w) run += wsum[w];
     const uint32_t lt = lanemask_lt();
     // coordinates of the record before this warp's slice (lane 0 of the first round)
     uint32_t carry[KD];
 #pragma unroll
     for (int d = 0; d < KD; ++d) carry[d] = 0;
-    if (base > 0 && base - 1 < B) rec_read<DIM>(ldg_key(rec + base - 1), D, kb, carry);
-#pragma unroll   // constant indices keep m[] in registers
+    if (base > 0 && base - 1 < B) rec_read<DIM>(kprev, D, kb, carry);
+#pragma unroll   // constant indices keep m[] and kk[] in registers
     for (int k = 0; k < kFlagItems; ++k) {
         const uint64_t i = base + 32 * k + lane;
         const bool valid = i < B;
         uint32_t cur[KD], prev[KD];
 #pragma unroll
         for (int d = 0; d < KD; ++d) cur[d] = 0;
-        if (valid) rec_read<DIM>(ldg_key(rec + i), D, kb, cur);
+        if (valid) rec_read<DIM>(kPre ? kk[k] : ldg_key(rec + i), D, kb, cur);
 #pragma unroll
         for (int d = 0; d < KD; ++d) {
             if (!DIM && d >= D) break;
@@ -883,13 +904,21 @@ __global__ void __launch_bounds__(kFlagThreads) k_l2_rows(const KT* __restrict__
 #pragma unroll
                 for (int d = 0; d < KD; ++d) {
                     if (!DIM && d >= D) break;
-                    // prediction = previous record (already inside [wrap_min, wrap_max])
-                    int64_t corr = static_cast<int64_t>(prev[d]) - static_cast<int64_t>(cur[d]);
-                    if (corr < wmin) corr += wrange;
-                    else if (corr > wmax) corr -= wrange;
-                    const uint64_t zz = corr >= 0 ? static_cast<uint64_t>(corr) << 1
-                                                  : (static_cast<uint64_t>(-(corr + 1)) << 1) | 1u;
-                    diff[row + d] = static_cast<ET>(zz);
+                    // prediction = previous record (already inside [wrap_min, wrap_max]);
+                    // three dimensions of at most 21 bits wrap and ZigZag in 32 bits
+                    if (DIM == 3) {
+                        int32_t corr = static_cast<int32_t>(prev[d]) - static_cast<int32_t>(cur[d]);
+                        if (corr < static_cast<int32_t>(wmin)) corr += static_cast<int32_t>(wrange);
+                        else if (corr > static_cast<int32_t>(wmax)) corr -= static_cast<int32_t>(wrange);
+                        diff[row + d] = static_cast<ET>((static_cast<uint32_t>(corr) << 1) ^
+                                                        static_cast<uint32_t>(corr >> 31));
+                    } else {
+                        int64_t corr = static_cast<int64_t>(prev[d]) - static_cast<int64_t>(cur[d]);
+                        if (corr < wmin) corr += wrange;
+                        else if (corr > wmax) corr -= wrange;
+                        diff[row + d] = static_cast<ET>((static_cast<uint64_t>(corr) << 1) ^
+                                                        static_cast<uint64_t>(corr >> 63));
+                    }
                 }
             }
         }
