@@ -614,17 +614,10 @@ struct ExplicitIn {
     const uint32_t* idrel;
     __device__ uint32_t operator()(uint64_t i) const { return idrel[i] == 0 ? 1u : 0u; }
 };
-// An explicit record is kept as its point's block key, which moves D times fewer bytes
-// than separate coordinates through the level-2 passes (rec_read takes the coordinates
-// back out: three shifts for three dimensions in a 4- or 8-byte key).
-template <typename KT>
-struct ExplicitOut {
-    const KT* key;
-    KT* rec;
-    __device__ void operator()(uint64_t i, uint32_t pos, uint32_t flag) const {
-        if (flag) rec[pos] = key[i];
-    }
-};
+// An explicit record is kept as its point's block key (device_flag_gather copies the
+// keys), which moves D times fewer bytes than separate coordinates through the level-2
+// passes (rec_read takes the coordinates back out: three shifts for three dimensions in
+// a 4- or 8-byte key).
 
 // Level-2 work runs with DIM = 3 (three dimensions, kb <= 21) or DIM = 0 (any shape).
 __device__ __forceinline__ bool l2_dim3(const EncState* st) { return st->dims == 3 && st->kb <= 21; }
@@ -2202,7 +2195,7 @@ static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, ui
                        uint32_t kd_esz, uint8_t* choice2, void* keep, void* diff, uint32_t* scan32, StageTimer& T,
                        cudaStream_t stream) {
     KT* rec = static_cast<KT*>(rec_v);
-    device_flag_scan(ExplicitIn<KT>{idrel}, ExplicitOut<KT>{key_idx, rec}, n, scan32, &st->B, stream, &st->done_a);
+    device_flag_gather(ExplicitIn<KT>{idrel}, key_idx, rec, n, scan32, &st->B, &st->done_a, stream);
     T.mark("explicit_records", stream);
     if (d3) {
         k_l2_stats<KT, 3><<<grid_for((n + 3) / 4, 256, 148u * 4u), 256, 0, stream>>>(rec, st); count_launch();

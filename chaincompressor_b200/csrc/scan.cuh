@@ -358,6 +358,48 @@ __global__ void __launch_bounds__(kFlagThreads) flag_apply_kernel(Pred pred, Out
     }
 }
 
+// The ranked pass of a compaction, dst[rank] = src[i] for every flagged i: each thread
+// loads its items' flags and (for values of at most eight bytes) source values before
+// the ballots, so a warp waits on memory once per tile instead of once per round of
+// stores.  Values are read for unflagged items too (the sectors are mostly shared).
+template <typename Pred, typename T>
+__global__ void __launch_bounds__(kFlagThreads) flag_gather_kernel(Pred pred, const T* __restrict__ src,
+                                                                    T* __restrict__ dst, uint64_t n,
+                                                                    const uint32_t* tile_prefix) {
+    __shared__ uint32_t wsum[kFlagThreads / 32];
+    constexpr bool kPre = sizeof(T) <= 8;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * kFlagItems;
+    uint32_t m[kFlagItems];
+    T v[kPre ? kFlagItems : 1];
+#pragma unroll
+    for (int k = 0; k < kFlagItems; ++k) {
+        const uint64_t i = base + 32 * k + lane;
+        m[k] = i < n ? pred(i) : 0u;
+        if (kPre) v[k] = i < n ? src[i] : T(0);
+    }
+    const uint32_t tp = tile_prefix[blockIdx.x];
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < kFlagItems; ++k) {
+        m[k] = __ballot_sync(0xffffffffu, m[k] != 0);
+        c += __popc(m[k]);
+    }
+    if (lane == 0) wsum[warp] = c;
+    __syncthreads();
+    uint32_t run = tp;
+    for (int w = 0; w < warp; ++w) run += wsum[w];
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < kFlagItems; ++k) {
+        if ((m[k] >> lane) & 1u) {
+            const uint64_t i = base + 32 * k + lane;
+            dst[run + __popc(m[k] & lt)] = kPre ? v[k] : src[i];
+        }
+        run += __popc(m[k]);
+    }
+}
+
 inline uint64_t flag_tiles(uint64_t n) { return (n + kFlagTile - 1) / kFlagTile; }
 
 // `tile_buf` holds flag_tiles(n) u32 (scan_scratch_bytes(n) bytes suffice); *total
@@ -380,6 +422,22 @@ void device_flag_scan(Pred pred, OutF out, uint64_t n, uint32_t* tile_buf, uint3
     }
     flag_apply_kernel<Pred, OutF, kOutUnroll><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, out, n,
                                                                                                     tile_buf); count_launch();
+}
+
+// device_flag_scan for a compaction (dst[rank] = src[i] for flagged i): the counting
+// launch scans the tile counts (`done` as there), then flag_gather_kernel.
+template <typename Pred, typename T>
+void device_flag_gather(Pred pred, const T* src, T* dst, uint64_t n, uint32_t* tile_buf, uint32_t* total,
+                        uint32_t* done, cudaStream_t stream) {
+    const uint64_t tiles = flag_tiles(n);
+    if (tiles == 0) {
+        if (total) cudaMemsetAsync(total, 0, sizeof(uint32_t), stream);
+        return;
+    }
+    flag_count_kernel<Pred><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, n, tile_buf, total, done);
+    count_launch();
+    flag_gather_kernel<Pred, T><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, src, dst, n, tile_buf);
+    count_launch();
 }
 
 // The same scan when the per-tile counts are already in `tile_buf` (a producer kernel
