@@ -337,6 +337,27 @@ struct ResetAddOp {
         return o;
     }
     __device__ __forceinline__ static L2Vec identity() { return L2Vec{0, {0, 0, 0}}; }
+    __device__ __forceinline__ static ResetAddOp make(uint64_t range) {
+        return ResetAddOp{static_cast<uint32_t>(range), static_cast<uint32_t>(range >> 32)};
+    }
+};
+// The same operator for range <= 2^31: a sum of two reduced values fits 32 bits.
+struct ResetAddOp32 {
+    uint32_t r;
+    __device__ __forceinline__ L2Vec operator()(const L2Vec& a, const L2Vec& b) const {
+        if (b.restart) return b;
+        L2Vec o;
+        o.restart = a.restart;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const uint32_t s = a.v[k] + b.v[k];
+            o.v[k] = s >= r ? s - r : s;
+        }
+        return o;
+    }
+    __device__ __forceinline__ static ResetAddOp32 make(uint64_t range) {
+        return ResetAddOp32{static_cast<uint32_t>(range)};
+    }
 };
 
 // Difference records per flag-scan tile from CH20's 1-bit packing: one CTA per tile,
@@ -542,6 +563,8 @@ constexpr uint32_t kPad24Words = 192 + 192 / 24;   // slots for 192 words
 constexpr uint32_t kL2WarpWords = 4 * kPad24Words;
 static_assert(kL2WarpWords >= 3 * 32 * kL2Rounds, "staged rows fit");
 constexpr size_t kL2ApplySmem = static_cast<size_t>(kL2Warps) * kL2WarpWords * 4;
+// Op: ResetAddOp, or ResetAddOp32 when range <= 2^31.
+template <typename Op>
 __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec* tile_prefix, uint32_t* compact,
                                                              DecState* st) {
     constexpr int P = kL2Rounds;   // records per lane
@@ -550,7 +573,7 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t j0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * P +
                         static_cast<uint64_t>(lane) * P;
-    const ResetAddOp op{static_cast<uint32_t>(g.range), static_cast<uint32_t>(g.range >> 32)};
+    const Op op = Op::make(g.range);
     uint32_t c[P];
     if (g.cbits) {   // records j0 .. j0 + 7: one byte of the packing (j0 is a multiple of 8)
         static_assert(P == 8, "one packed byte per lane");
@@ -1349,14 +1372,25 @@ chain_status decode_frame(chain_ctx* ctx, const void* container, size_t len, cha
         g.maxc = r / 2 - ((r & 1) == 0 ? 1 : 0);
         g.minc = -(r / 2);
         // per device, cheap; set on every call, always to the same value
-        CHAIN_CUDA(cudaFuncSetAttribute(k_l2_apply, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(kL2ApplySmem)));
+        const bool narrow = range <= (1ull << 31);
+        if (narrow)
+            CHAIN_CUDA(cudaFuncSetAttribute(k_l2_apply<ResetAddOp32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(kL2ApplySmem)));
+        else
+            CHAIN_CUDA(cudaFuncSetAttribute(k_l2_apply<ResetAddOp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(kL2ApplySmem)));
         for (uint32_t d0 = 0; d0 < D; d0 += 3) {
             g.d0 = d0;
             k_l2_tail<<<static_cast<unsigned>(l2tiles), 32 * kL2Warps, 0, stream>>>(g, tile_l2); count_launch();
             scan_tilesums_kernel<L2Vec, ResetAddOp><<<1, 1024, 0, stream>>>(tile_l2, l2tiles, static_cast<L2Vec*>(nullptr),
                                                                            l2op); count_launch();
-            k_l2_apply<<<static_cast<unsigned>(l2tiles), 32 * kL2Warps, kL2ApplySmem, stream>>>(g, tile_l2, compact, st); count_launch();
+            if (narrow)
+                k_l2_apply<ResetAddOp32><<<static_cast<unsigned>(l2tiles), 32 * kL2Warps, kL2ApplySmem, stream>>>(
+                    g, tile_l2, compact, st);
+            else
+                k_l2_apply<ResetAddOp><<<static_cast<unsigned>(l2tiles), 32 * kL2Warps, kL2ApplySmem, stream>>>(
+                    g, tile_l2, compact, st);
+            count_launch();
         }
     } else {
         CHAIN_CUDA(cudaMemsetAsync(ndiff_dev, 0, sizeof(uint32_t), stream));
