@@ -2198,9 +2198,9 @@ static void run_level2(const KT* key_idx, const uint32_t* idrel, void* rec_v, ui
     device_flag_gather(ExplicitIn<KT>{idrel}, key_idx, rec, n, scan32, &st->B, &st->done_a, stream);
     T.mark("explicit_records", stream);
     if (d3) {
-        k_l2_stats<KT, 3><<<grid_for((n + 3) / 4, 256, 148u * 4u), 256, 0, stream>>>(rec, st); count_launch();
+        k_l2_stats<KT, 3><<<grid_for((n + 3) / 4, 256, 148u * 16u), 256, 0, stream>>>(rec, st); count_launch();
     } else {
-        k_l2_stats<KT, 0><<<grid_for((n + 3) / 4, 256, 148u * 4u), 256, 0, stream>>>(rec, st); count_launch();
+        k_l2_stats<KT, 0><<<grid_for((n + 3) / 4, 256, 148u * 16u), 256, 0, stream>>>(rec, st); count_launch();
     }
     T.mark("l2_stats", stream);
     const unsigned tiles = static_cast<unsigned>(flag_tiles(n));
