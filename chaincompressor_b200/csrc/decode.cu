@@ -430,6 +430,7 @@ struct L2Geo {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * kL2Rounds;
         uint32_t c = 0;
+        uint32_t off = tile_diff[blockIdx.x];   // in flight with the choice words
         // packed choices: lane k loads round k's word, then every lane takes them all
         const uint32_t mine = cbits && lane < kL2Rounds ? flags32(base + 32 * lane) : 0u;
 #pragma unroll
@@ -439,7 +440,6 @@ struct L2Geo {
         }
         if (lane == 0) s_cnt[warp] = c;
         __syncthreads();
-        uint32_t off = tile_diff[blockIdx.x];
         for (int w = 0; w < warp; ++w) off += s_cnt[w];
         return off;
     }
@@ -574,6 +574,9 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec
     const uint64_t j0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * P +
                         static_cast<uint64_t>(lane) * P;
     const Op op = Op::make(g.range);
+    // the tile's offsets, in flight with the choice loads instead of after the barriers
+    const uint32_t tdiff = g.tile_diff[blockIdx.x];
+    const L2Vec tpre = tile_prefix[blockIdx.x];
     uint32_t c[P];
     if (g.cbits) {   // records j0 .. j0 + 7: one byte of the packing (j0 is a multiple of 8)
         static_assert(P == 8, "one packed byte per lane");
@@ -606,7 +609,7 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec
     const uint32_t incl_cnt = warp_inclusive_sum(cnt);
     if (lane == 31) s_cnt[warp] = incl_cnt;
     __syncthreads();
-    uint64_t rank = g.tile_diff[blockIdx.x] + incl_cnt - cnt;   // diff records before j0
+    uint64_t rank = tdiff + incl_cnt - cnt;   // diff records before j0
     for (int w = 0; w < warp; ++w) rank += s_cnt[w];
     // every record's row first (one memory round trip for the lane), then the terms
     uint32_t raw[P][3];
@@ -679,7 +682,7 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec
     if (lane == 0) exc = ResetAddOp::identity();
     if (lane == 31) s_tot[warp] = inc;
     __syncthreads();
-    L2Vec carry = tile_prefix[blockIdx.x];
+    L2Vec carry = tpre;
     for (int w = 0; w < warp; ++w) carry = op(carry, s_tot[w]);
     carry = op(carry, exc);
     uint32_t o[3 * P];

@@ -157,6 +157,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(InF in, OutF o
     __shared__ T vals[Striped ? 2 * PADDED : PADDED];
     __shared__ T scratch[33];
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * TILE;
+    const T tp = tile_prefix[blockIdx.x];   // loaded with the tile, not after the scan's barriers
     scan_stage<T>(in, n, base, vals);
     __syncthreads();
     T local[I];
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(InF in, OutF o
         local[k] = base + j < n ? vals[scan_pad(j)] : Op::identity();
         agg = op(agg, local[k]);
     }
-    T ex = op(tile_prefix[blockIdx.x], block_exclusive_scan_op(agg, op, scratch, static_cast<T*>(nullptr)));
+    T ex = op(tp, block_exclusive_scan_op(agg, op, scratch, static_cast<T*>(nullptr)));
     if constexpr (Striped) {
         T* pre = vals + PADDED;
 #pragma unroll
@@ -337,6 +338,7 @@ __global__ void __launch_bounds__(kFlagThreads) flag_apply_kernel(Pred pred, Out
     __shared__ uint32_t wsum[kFlagThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kFlagTile + static_cast<uint64_t>(warp) * 32 * kFlagItems;
+    const uint32_t tp = tile_prefix[blockIdx.x];   // in flight with the flags
     uint32_t m[kFlagItems];
     uint32_t c = 0;
 #pragma unroll
@@ -347,7 +349,7 @@ __global__ void __launch_bounds__(kFlagThreads) flag_apply_kernel(Pred pred, Out
     }
     if (lane == 0) wsum[warp] = c;
     __syncthreads();
-    uint32_t run = tile_prefix[blockIdx.x];
+    uint32_t run = tp;
     for (int w = 0; w < warp; ++w) run += wsum[w];
     const uint32_t lt = lanemask_lt();
 #pragma unroll kOutUnroll
