@@ -727,6 +727,7 @@ __global__ void __launch_bounds__(32 * kL2Warps) k_l2_apply(L2Geo g, const L2Vec
 struct ZeroIn {
     const uint32_t* idrel;
     __device__ uint32_t operator()(uint64_t i) const { return idrel[i] == 0 ? 1u : 0u; }
+    __host__ __device__ const uint32_t* zero_words() const { return idrel; }
 };
 // Parent words: bit 31 set = resolved (the low bits are the chain's explicit point).
 constexpr uint32_t kResolved = 0x80000000u;

@@ -613,6 +613,7 @@ template <typename KT>
 struct ExplicitIn {
     const uint32_t* idrel;
     __device__ uint32_t operator()(uint64_t i) const { return idrel[i] == 0 ? 1u : 0u; }
+    __host__ __device__ const uint32_t* zero_words() const { return idrel; }
 };
 // An explicit record is kept as its point's block key (device_flag_gather copies the
 // keys), which moves D times fewer bytes than separate coordinates through the level-2

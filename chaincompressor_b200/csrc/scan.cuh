@@ -11,6 +11,9 @@
 // each thread scans a contiguous run, and out() is called from that run.
 #pragma once
 
+#include <type_traits>
+#include <utility>
+
 #include "chain_common.cuh"
 
 namespace chain {
@@ -330,6 +333,58 @@ __global__ void __launch_bounds__(kFlagThreads) flag_count_kernel(Pred pred, uin
     if (done) last_cta_scan_counts(tile_counts, total, done);
 }
 
+// flag_count_kernel for predicates that test a 4-byte word for zero (Pred::zero_words()
+// returns the words): 16-byte loads and per-thread counts, no ballots (the counts need no
+// element order within the tile).
+static __global__ void __launch_bounds__(kFlagThreads) flag_count_zero_words_kernel(const uint32_t* __restrict__ w, uint64_t n,
+                                                                             uint32_t* tile_counts, uint32_t* total,
+                                                                             uint32_t* done) {
+    static_assert(kFlagItems % 4 == 0, "whole 16-byte words per thread");
+    __shared__ uint32_t wsum[kFlagThreads / 32];
+    const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * kFlagTile;
+    uint32_t c = 0;
+    if ((reinterpret_cast<uintptr_t>(w) & 15) == 0 && tile0 + kFlagTile <= n) {
+        const uint4* v = reinterpret_cast<const uint4*>(w + tile0);
+#pragma unroll
+        for (int k = 0; k < kFlagItems / 4; ++k) {
+            const uint4 q = __ldg(v + k * kFlagThreads + threadIdx.x);
+            c += (q.x == 0u) + (q.y == 0u) + (q.z == 0u) + (q.w == 0u);
+        }
+    } else {
+        for (int k = 0; k < kFlagItems; ++k) {
+            const uint64_t i = tile0 + static_cast<uint64_t>(k) * kFlagThreads + threadIdx.x;
+            c += (i < n && w[i] == 0u) ? 1u : 0u;
+        }
+    }
+    c = warp_sum(c);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int k = 0; k < kFlagThreads / 32; ++k) t += wsum[k];
+        tile_counts[blockIdx.x] = t;
+    }
+    if (done) last_cta_scan_counts(tile_counts, total, done);
+}
+
+template <typename P, typename = void>
+struct HasZeroWords : std::false_type {};
+template <typename P>
+struct HasZeroWords<P, std::void_t<decltype(std::declval<const P&>().zero_words())>> : std::true_type {};
+
+// The counting launch of a flag scan (flag_count_kernel, or its zero-word form).
+template <typename Pred>
+void launch_flag_count(Pred pred, uint64_t n, uint64_t tiles, uint32_t* tile_buf, uint32_t* total, uint32_t* done,
+                       cudaStream_t stream) {
+    if constexpr (HasZeroWords<Pred>::value)
+        flag_count_zero_words_kernel<<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred.zero_words(), n,
+                                                                                                tile_buf, total, done);
+    else
+        flag_count_kernel<Pred><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, n, tile_buf, total,
+                                                                                          done);
+    count_launch();
+}
+
 // kOutUnroll: rounds of out() calls unrolled together (more loads in flight against
 // more registers; the best depth depends on out()).
 template <typename Pred, typename OutF, int kOutUnroll = 4>
@@ -416,8 +471,7 @@ void device_flag_scan(Pred pred, OutF out, uint64_t n, uint32_t* tile_buf, uint3
         if (total) cudaMemsetAsync(total, 0, sizeof(uint32_t), stream);
         return;
     }
-    flag_count_kernel<Pred><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, n, tile_buf, total, done);
-    count_launch();
+    launch_flag_count(pred, n, tiles, tile_buf, total, done, stream);
     if (!done) {
         scan_tilesums_kernel<uint32_t, SumOp<uint32_t>><<<1, 1024, 0, stream>>>(tile_buf, tiles, total, SumOp<uint32_t>());
         count_launch();
@@ -436,8 +490,7 @@ void device_flag_gather(Pred pred, const T* src, T* dst, uint64_t n, uint32_t* t
         if (total) cudaMemsetAsync(total, 0, sizeof(uint32_t), stream);
         return;
     }
-    flag_count_kernel<Pred><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, n, tile_buf, total, done);
-    count_launch();
+    launch_flag_count(pred, n, tiles, tile_buf, total, done, stream);
     flag_gather_kernel<Pred, T><<<static_cast<unsigned>(tiles), kFlagThreads, 0, stream>>>(pred, src, dst, n, tile_buf);
     count_launch();
 }
